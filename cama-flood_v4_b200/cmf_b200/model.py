@@ -1,0 +1,246 @@
+"""Host-side mirror of the reference driver interface for the GPU physics step.
+
+``HostModel`` plays CMF_DRV_INIT (src/cmf_drv_control_mod.F90:149-298) for a case written in the
+reference's file formats; ``PhysicsGPU`` is the GPU switch behind CMF_DRV_ADVANCE: each
+``advance()`` is one CMF_PHYSICS_ADVANCE (src/cmf_ctrl_physics_mod.F90:21-153) for every member.
+Errors surface as RuntimeError carrying the library's status and message; there is no CPU path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _abi
+from ._abi import check
+
+
+def _as_np(ptr, n, dtype):
+    if not ptr or n <= 0:
+        return np.zeros(0, dtype=dtype)
+    return np.ctypeslib.as_array(ptr, shape=(n,))
+
+
+class HostModel:
+    """Stand-alone host: reads input_cmf.nam, diminfo and the binary maps, runs the init chain."""
+
+    def __init__(self, casedir: str, nml: str = "input_cmf.nam"):
+        self.lib = _abi.load()
+        h = C.c_void_p()
+        check(self.lib.cmf_host_load(casedir.encode(), nml.encode(), C.byref(h)), "cmf_host_load")
+        self.h = h
+        self.dims = _abi.Dims()
+        self.params = _abi.Params()
+        self.maps = _abi.MapPtrs()
+        self.opts = _abi.Opts()
+        dt = C.c_double()
+        check(self.lib.cmf_host_describe(self.h, C.byref(self.dims), C.byref(self.params), C.byref(self.maps),
+                                         C.byref(self.opts), C.byref(dt)), "cmf_host_describe")
+        self.dt = dt.value
+        self._state = _abi.StatePtrs()
+        check(self.lib.cmf_host_state(self.h, C.byref(self._state)), "cmf_host_state")
+        nx, ny = C.c_int32(), C.c_int32()
+        self.i1seqx = np.zeros(self.dims.nseqmax, dtype=np.int32)
+        self.i1seqy = np.zeros(self.dims.nseqmax, dtype=np.int32)
+        check(self.lib.cmf_host_grid(self.h, C.byref(nx), C.byref(ny),
+                                     self.i1seqx.ctypes.data_as(_abi.i32p), self.i1seqy.ctypes.data_as(_abi.i32p)),
+              "cmf_host_grid")
+        self.nx, self.ny = nx.value, ny.value
+
+    @property
+    def nseq(self) -> int:
+        return self.dims.nseqall
+
+    def _len(self, name: str) -> int:
+        d = self.dims
+        N, L = d.nseqmax, d.nlfp
+        P, Lp = d.npthout, d.npthlev
+        table = {
+            "i1upst": N * d.upnmax, "fldstomax": N * L, "fldgrd": N * L, "fldhgt": N * L,
+            "pth_upst": P, "pth_down": P, "pth_dst": P, "pth_elv": P * Lp, "pth_wth": P * Lp, "pth_man": Lp,
+            "i1p_out": N * d.onmax, "i1p_inf": N * d.inmax,
+            "damseq": d.ndam, "damstat": d.ndam,
+        }
+        if name.startswith("dam_"):
+            return d.ndam
+        return table.get(name, N)
+
+    def map(self, name: str) -> np.ndarray:
+        """Copy of one static map array of the boundary (Fortran layout, 1-based index values)."""
+        ptr = getattr(self.maps, name)
+        dtype = np.int32 if dict(_abi.MAP_FIELDS)[name] is _abi.i32p else np.float64
+        return _as_np(ptr, self._len(name), dtype).copy()
+
+    def initial_state(self) -> dict:
+        d = self.dims
+        out = {}
+        for n in _abi.STATE_FIELDS:
+            ln = d.npthout * d.npthlev if n.startswith("pthflw") else d.nseqmax
+            out[n] = _as_np(getattr(self._state, n), ln, np.float64).copy()
+        return out
+
+    def conv_resol(self, runoff_map: np.ndarray) -> np.ndarray:
+        """CONV_RESOL: runoff map [mm/dt as DROFUNIT says] -> D2RUNOFF [m3/s]."""
+        a = np.ascontiguousarray(runoff_map, dtype=np.float64).ravel()
+        assert a.size == self.nx * self.ny
+        out = np.zeros(self.dims.nseqmax)
+        check(self.lib.cmf_host_conv_resol(self.h, a.ctypes.data_as(_abi.f64p), out.ctypes.data_as(_abi.f64p)),
+              "cmf_host_conv_resol")
+        return out
+
+    def runoff_from_cells(self, mm_per_day_cells: np.ndarray) -> np.ndarray:
+        """Per-sequence-cell runoff [mm/day] -> m3/s with CONV_RESOL's arithmetic."""
+        gr = self.map("grarea")
+        v = np.asarray(mm_per_day_cells, dtype=np.float64)
+        return np.maximum((v * gr) / 86400000.0, 0.0)
+
+    def grid_to_seq(self, grid: np.ndarray) -> np.ndarray:
+        g = np.asarray(grid).reshape(self.ny, self.nx)
+        return g[self.i1seqy - 1, self.i1seqx - 1]
+
+    def close(self) -> None:
+        if self.h:
+            self.lib.cmf_host_free(self.h)
+            self.h = None
+
+
+class PhysicsGPU:
+    """A GPU context running ``nmembers`` members of the host model's network."""
+
+    def __init__(self, host: HostModel, nmembers: int = 1, ldiag: bool = True, launch_mode: int = 0,
+                 device: int = 0, block_size: int = 0, opts_override: dict | None = None):
+        self.lib = _abi.load()
+        self.host = host
+        dims = _abi.Dims.from_buffer_copy(host.dims)
+        dims.nmembers = nmembers
+        opts = _abi.Opts.from_buffer_copy(host.opts)
+        opts.ldiag = int(ldiag)
+        opts.launch_mode = launch_mode
+        opts.device = device
+        opts.block_size = block_size
+        for k, v in (opts_override or {}).items():
+            setattr(opts, k, int(v))
+        self.dims, self.opts = dims, opts
+        self.M = nmembers
+        self.N = dims.nseqall
+        self.P = dims.npthout if opts.lpthout else 0
+        self.Lp = dims.npthlev if opts.lpthout else 0
+        h = C.c_void_p()
+        check(self.lib.cmf_gpu_create(C.byref(dims), C.byref(host.params), C.byref(host.maps), C.byref(opts),
+                                      C.byref(h)), "cmf_gpu_create")
+        self.h = h
+        st = host.initial_state()
+        self.set_state({k: np.tile(v, nmembers) for k, v in st.items()})
+
+    # ---- state ------------------------------------------------------------------------------
+    def _state_sizes(self, name: str) -> int:
+        if name.startswith("pthflw"):
+            return self.M * max(self.host.dims.npthout * self.host.dims.npthlev, 1)
+        return self.M * self.N
+
+    def set_state(self, state: dict) -> None:
+        sp = _abi.StatePtrs()
+        keep = []
+        for n in _abi.STATE_FIELDS:
+            if n in state and state[n] is not None:
+                a = np.ascontiguousarray(state[n], dtype=np.float64).ravel()
+                if a.size != self._state_sizes(n):
+                    raise ValueError(f"{n}: expected {self._state_sizes(n)} values, got {a.size}")
+                keep.append(a)
+                setattr(sp, n, a.ctypes.data_as(_abi.f64p))
+        check(self.lib.cmf_gpu_ctx_set_state(self.h, C.byref(sp)), "set_state")
+
+    def get_state(self) -> dict:
+        sp = _abi.StatePtrs()
+        out = {}
+        for n in _abi.STATE_FIELDS:
+            a = np.zeros(self._state_sizes(n))
+            out[n] = a
+            setattr(sp, n, a.ctypes.data_as(_abi.f64p))
+        check(self.lib.cmf_gpu_ctx_get_state(self.h, C.byref(sp)), "get_state")
+        return {k: v.reshape(self.M, -1) for k, v in out.items()}
+
+    def put_runoff(self, runoff: np.ndarray) -> None:
+        a = np.ascontiguousarray(runoff, dtype=np.float64).ravel()
+        if a.size != self.M * self.N:
+            raise ValueError("runoff must hold nmembers * NSEQALL values")
+        check(self.lib.cmf_gpu_ctx_put_runoff(self.h, a.ctypes.data_as(_abi.f64p), None), "put_runoff")
+
+    def advance(self, dt_def: float | None = None):
+        dt_def = self.host.dt if dt_def is None else dt_def
+        nt = np.zeros(self.M, dtype=np.int32)
+        dt = np.zeros(self.M)
+        b = (_abi.Budget * self.M)()
+        check(self.lib.cmf_gpu_ctx_physics_advance(self.h, dt_def, nt.ctypes.data_as(_abi.i32p),
+                                                   dt.ctypes.data_as(_abi.f64p), b), "physics_advance")
+        budgets = [{f: getattr(b[m], f) for f in _abi.BUDGET_FIELDS} for m in range(self.M)]
+        return nt, dt, budgets
+
+    def stage(self, dt_def: float | None = None) -> np.ndarray:
+        dt_def = self.host.dt if dt_def is None else dt_def
+        out = np.zeros(self.M)
+        check(self.lib.cmf_gpu_ctx_stage(self.h, dt_def, out.ctypes.data_as(_abi.f64p)), "stage")
+        return out
+
+    def substeps(self, dt_min_global: float, dt_def: float | None = None):
+        dt_def = self.host.dt if dt_def is None else dt_def
+        nt = np.zeros(self.M, dtype=np.int32)
+        dt = np.zeros(self.M)
+        b = (_abi.Budget * self.M)()
+        check(self.lib.cmf_gpu_ctx_substeps(self.h, dt_def, dt_min_global, nt.ctypes.data_as(_abi.i32p),
+                                            dt.ctypes.data_as(_abi.f64p), b), "substeps")
+        return nt, dt, [{f: getattr(b[m], f) for f in _abi.BUDGET_FIELDS} for m in range(self.M)]
+
+    def advance_device(self, ksteps: int, runoff_dev_ptr: int | None, stride: int, dt_def: float | None = None) -> None:
+        dt_def = self.host.dt if dt_def is None else dt_def
+        check(self.lib.cmf_gpu_ctx_advance_device(self.h, dt_def, ksteps, C.c_void_p(runoff_dev_ptr or 0), stride),
+              "advance_device")
+
+    def synchronize(self) -> None:
+        check(self.lib.cmf_gpu_ctx_synchronize(self.h), "synchronize")
+
+    def last_nt(self):
+        nt = np.zeros(self.M, dtype=np.int32)
+        dt = np.zeros(self.M)
+        check(self.lib.cmf_gpu_ctx_last_nt(self.h, nt.ctypes.data_as(_abi.i32p), dt.ctypes.data_as(_abi.f64p)), "last_nt")
+        return nt, dt
+
+    @property
+    def stream(self) -> int:
+        return int(self.lib.cmf_gpu_ctx_stream(self.h) or 0)
+
+    @property
+    def kernel_launches(self) -> int:
+        return int(self.lib.cmf_gpu_ctx_kernel_launches(self.h))
+
+    @property
+    def block_size(self) -> int:
+        return int(self.lib.cmf_gpu_ctx_block_size(self.h))
+
+    def get_diag(self) -> dict:
+        dp = _abi.DiagPtrs()
+        out = {}
+        MP = self.M * max(self.P, 1)
+        for n in _abi.DIAG_FIELDS:
+            if n == "pthflwsum" or n == "pthflwsum_aavg":
+                ln = MP
+            elif n == "pthflw_aavg":
+                ln = MP * max(self.Lp, 1)
+            else:
+                ln = self.M * self.N
+            a = np.zeros(ln)
+            out[n] = a
+            setattr(dp, n, a.ctypes.data_as(_abi.f64p))
+        check(self.lib.cmf_gpu_ctx_get_diag(self.h, C.byref(dp)), "get_diag")
+        return {k: v.reshape(self.M, -1) for k, v in out.items()}
+
+    def close(self) -> None:
+        if self.h:
+            self.lib.cmf_gpu_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,801 @@
+// cmf_engine.cu -- device context, graph construction, autotuner and the C ABI of cmf_gpu.h.
+//
+// A context owns the device copy of one river network (maps, CSR tables) and the state of
+// `nmembers` ensemble members.  One outer step is one CUDA graph launch:
+//   k_stage -> k_ntdt -> while (k < NTmax) { k_flux -> k_rate -> k_store -> k_ctl }
+// The loop is a conditional WHILE node whose condition the device sets (k_ntdt, k_ctl), so the
+// adaptive sub-step count never travels to the host.  launch_mode 1 replaces the conditional node
+// by a host loop (reads NTmax back), which tests use to cross-check the graph path.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/cmf_gpu.h"
+#include "cmf_kernels.cuh"
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int set_err(int code, const std::string &msg) {
+    g_last_error = msg;
+    return code;
+}
+
+#define CUDA_TRY(expr)                                                                          \
+    do {                                                                                        \
+        cudaError_t e_ = (expr);                                                                \
+        if (e_ != cudaSuccess)                                                                  \
+            return set_err(CMF_E_CUDA, std::string(#expr) + ": " + cudaGetErrorString(e_));     \
+    } while (0)
+
+constexpr int kImis = -9999;
+
+}  // namespace
+
+struct cmf_gpu_ctx {
+    cmf_dims dims{};
+    cmf_params params{};
+    cmf_opts opts{};
+    cmf::Net net{};
+    cmf::State st{};
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::vector<void *> allocs;
+    int block = 256;
+    int ncell_blocks = 0, npath_blocks = 0;
+    int nlev = 0, ndam_placed = 0;
+    size_t E = 0;
+    // graph
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    cudaGraphConditionalHandle cond{};
+    double dt_def_dev = -1.0;
+    int64_t launches = 0;
+    // host staging for the per-member control block
+    std::vector<cmf::MemberCtl> hctl;
+
+    template <class T>
+    int alloc(T **p, size_t n) {
+        void *q = nullptr;
+        if (n == 0) n = 1;
+        CUDA_TRY(cudaMalloc(&q, n * sizeof(T)));
+        CUDA_TRY(cudaMemsetAsync(q, 0, n * sizeof(T), stream));
+        allocs.push_back(q);
+        *p = static_cast<T *>(q);
+        return CMF_OK;
+    }
+    template <class P, class T>
+    int upload(P *p, const std::vector<T> &h) {
+        T *q = nullptr;
+        int rc = alloc(&q, h.size());
+        if (rc) return rc;
+        if (!h.empty()) CUDA_TRY(cudaMemcpyAsync(q, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, stream));
+        *p = q;
+        return CMF_OK;
+    }
+    template <class P, class T>
+    int upload_raw(P *p, const T *h, size_t n) {
+        T *q = nullptr;
+        int rc = alloc(&q, n);
+        if (rc) return rc;
+        if (h && n) CUDA_TRY(cudaMemcpyAsync(q, h, n * sizeof(T), cudaMemcpyHostToDevice, stream));
+        *p = q;
+        return CMF_OK;
+    }
+};
+
+namespace {
+
+int check_opts(const cmf_opts &o) {
+    if (o.lkine) return set_err(CMF_E_UNSUPPORTED, "LKINE (kinematic outflow) is not on the GPU path");
+    if (o.lslpmix) return set_err(CMF_E_UNSUPPORTED, "LSLPMIX is not on the GPU path");
+    if (o.lstg_es) return set_err(CMF_E_UNSUPPORTED, "LSTG_ES: the GPU path implements the default stage scheme");
+    if (o.lgdwdly) return set_err(CMF_E_UNSUPPORTED, "LGDWDLY (groundwater delay) is not on the GPU path");
+    if (o.lrosplit) return set_err(CMF_E_UNSUPPORTED, "LROSPLIT is not on the GPU path");
+    if (o.lwevap) return set_err(CMF_E_UNSUPPORTED, "LWEVAP is not on the GPU path");
+    if (o.lupsinf) return set_err(CMF_E_UNSUPPORTED, "LUPSINF is not on the GPU path");
+    if (o.lheatlink) return set_err(CMF_E_UNSUPPORTED, "LHEATLINK hooks run inside the sub-step loop on the host");
+    if (o.ltrace) return set_err(CMF_E_UNSUPPORTED, "LTRACE is not on the GPU path");
+    if (o.lslopemouth) return set_err(CMF_E_UNSUPPORTED, "LSLOPEMOUTH is not on the GPU path");
+    if (o.ldamyby) return set_err(CMF_E_UNSUPPORTED, "LDAMYBY is not on the GPU path");
+    if (!o.lspamat) return set_err(CMF_E_UNSUPPORTED, "the GPU path implements the LSPAMAT inflow gather");
+    return CMF_OK;
+}
+
+int build_net(cmf_gpu_ctx *c, const cmf_map_ptrs *mp) {
+    const cmf_dims &d = c->dims;
+    const int N = d.nseqall, R = d.nseqriv, L = d.nlfp;
+    cmf::Net &n = c->net;
+    n.N = N; n.R = R; n.L = L; n.M = d.nmembers;
+    n.P = c->opts.lpthout ? d.npthout : 0;
+    n.Lp = c->opts.lpthout ? d.npthlev : 0;
+    n.pgrv = c->params.pgrv; n.pmanfld = c->params.pmanfld; n.pdstmth = c->params.pdstmth;
+    n.pcadp = c->params.pcadp; n.pminslp = c->params.pminslp; n.dfrcinc = c->params.dfrcinc;
+    n.ladpstp = c->opts.ladpstp; n.lfldout = c->opts.lfldout; n.lpthout = c->opts.lpthout;
+    n.ldamout = c->opts.ldamout; n.llevee = c->opts.llevee; n.ldamh22 = c->opts.ldamh22; n.ldiag = c->opts.ldiag;
+    // ---- network
+    std::vector<int> next(N, -1);
+    for (int i = 0; i < R; i++) {
+        const int j = mp->i1next[i] - 1;
+        if (j <= i || j >= N) return set_err(CMF_E_ARG, "I1NEXT is not a topological order (I1NEXT(i) <= i)");
+        next[i] = j;
+    }
+    for (int i = R; i < N; i++)
+        if (mp->i1next[i] > 0) return set_err(CMF_E_ARG, "a river mouth has a downstream cell");
+    std::vector<int> up_ptr(N + 1, 0), up_idx;
+    up_idx.reserve(R);
+    for (int i = 0; i < N; i++) {
+        const int nu = mp->i1upn[i];
+        if (nu < 0 || nu > d.upnmax) return set_err(CMF_E_ARG, "I1UPN out of range");
+        for (int k = 0; k < nu; k++) {
+            const int j = mp->i1upst[(size_t)k * d.nseqmax + i] - 1;
+            if (j < 0 || j >= N || next[j] != i) return set_err(CMF_E_ARG, "I1UPST inconsistent with I1NEXT");
+            up_idx.push_back(j);
+        }
+        up_ptr[i + 1] = (int)up_idx.size();
+    }
+    c->E = up_idx.size();
+    int rc;
+    if ((rc = c->upload(&n.next, next)) || (rc = c->upload(&n.up_ptr, up_ptr)) || (rc = c->upload(&n.up_idx, up_idx)))
+        return rc;
+    std::vector<int> i2mask(mp->i2mask, mp->i2mask + N);
+    if ((rc = c->upload(&n.i2mask, i2mask))) return rc;
+    struct { const double *__restrict__ *dst; const double *src; size_t cnt; } arrs[] = {
+        {&n.rivelv, mp->rivelv, (size_t)N}, {&n.elevtn, mp->elevtn, (size_t)N}, {&n.nxtdst, mp->nxtdst, (size_t)N},
+        {&n.rivwth, mp->rivwth, (size_t)N}, {&n.rivhgt, mp->rivhgt, (size_t)N}, {&n.rivlen, mp->rivlen, (size_t)N},
+        {&n.rivman, mp->rivman, (size_t)N}, {&n.grarea, mp->grarea, (size_t)N}, {&n.rivstomax, mp->rivstomax, (size_t)N},
+        {&n.dwnelv, mp->dwnelv, (size_t)N}};
+    for (auto &a : arrs) {
+        if (!a.src) return set_err(CMF_E_ARG, "a required map pointer is NULL");
+        if ((rc = c->upload_raw(a.dst, a.src, a.cnt))) return rc;
+    }
+    // layer tables: (NSEQMAX,1,NLFP) -> [L][N]
+    auto layers = [&](const double *src, std::vector<double> &out) {
+        out.assign((size_t)L * N, 0.0);
+        for (int l = 0; l < L; l++) std::memcpy(&out[(size_t)l * N], src + (size_t)l * d.nseqmax, sizeof(double) * N);
+    };
+    std::vector<double> tmp;
+    if (!mp->fldstomax || !mp->fldgrd) return set_err(CMF_E_ARG, "FLDSTOMAX/FLDGRD missing");
+    layers(mp->fldstomax, tmp);
+    if ((rc = c->upload(&n.fldstomax, tmp))) return rc;
+    layers(mp->fldgrd, tmp);
+    if ((rc = c->upload(&n.fldgrd, tmp))) return rc;
+    if (c->opts.llevee) {
+        if (!mp->fldhgt) return set_err(CMF_E_ARG, "FLDHGT missing (levee scheme)");
+        layers(mp->fldhgt, tmp);
+        if ((rc = c->upload(&n.fldhgt, tmp))) return rc;
+    } else {
+        if ((rc = c->upload(&n.fldhgt, std::vector<double>(1, 0.0)))) return rc;
+    }
+    // ---- bifurcation paths
+    {
+        const int P = n.P, Lp = n.Lp;
+        std::vector<int> pu(std::max(P, 1), -1), pd(std::max(P, 1), -1), skip(std::max(P, 1), 3);
+        std::vector<double> dst(std::max(P, 1), 1.0), elv((size_t)std::max(P * Lp, 1), 0.0), wth(elv.size(), 1.0),
+            man(std::max(Lp, 1), 0.0);
+        std::vector<int> po_ptr(N + 1, 0), po_idx, pi_ptr(N + 1, 0), pi_idx;
+        if (P > 0) {
+            if (Lp > 64) return set_err(CMF_E_UNSUPPORTED, "NPTHLEV above 64");
+            for (int p = 0; p < P; p++) {
+                const int u = mp->pth_upst[p], v = mp->pth_down[p];
+                pu[p] = (u > 0 && u <= N) ? u - 1 : -1;
+                pd[p] = (v > 0 && v <= N) ? v - 1 : -1;
+                int s = 0;
+                if (pu[p] < 0 || pd[p] < 0) s = 3;
+                else {
+                    if (i2mask[pu[p]] > 0 || i2mask[pd[p]] > 0) s |= 1;
+                    if (i2mask[pu[p]] == 1 || i2mask[pd[p]] == 1) s |= 2;
+                }
+                skip[p] = s;
+                dst[p] = mp->pth_dst[p];
+                for (int l = 0; l < Lp; l++) {
+                    elv[(size_t)l * P + p] = mp->pth_elv[(size_t)l * P + p];
+                    wth[(size_t)l * P + p] = mp->pth_wth[(size_t)l * P + p];
+                }
+            }
+            for (int l = 0; l < Lp; l++) man[l] = mp->pth_man[l];
+            for (int i = 0; i < N; i++) {
+                for (int k = 0; k < mp->i1p_outn[i]; k++) po_idx.push_back(mp->i1p_out[(size_t)k * d.nseqmax + i] - 1);
+                po_ptr[i + 1] = (int)po_idx.size();
+                for (int k = 0; k < mp->i1p_infn[i]; k++) pi_idx.push_back(mp->i1p_inf[(size_t)k * d.nseqmax + i] - 1);
+                pi_ptr[i + 1] = (int)pi_idx.size();
+            }
+            for (int p : po_idx) if (p < 0 || p >= P) return set_err(CMF_E_ARG, "I1P_OUT out of range");
+            for (int p : pi_idx) if (p < 0 || p >= P) return set_err(CMF_E_ARG, "I1P_INF out of range");
+        }
+        if (po_idx.empty()) po_idx.push_back(0);
+        if (pi_idx.empty()) pi_idx.push_back(0);
+        if ((rc = c->upload(&n.pth_up, pu)) || (rc = c->upload(&n.pth_dn, pd)) || (rc = c->upload(&n.pth_skip, skip)) ||
+            (rc = c->upload(&n.pth_dst, dst)) || (rc = c->upload(&n.pth_elv, elv)) || (rc = c->upload(&n.pth_wth, wth)) ||
+            (rc = c->upload(&n.pth_man, man)) || (rc = c->upload(&n.pout_ptr, po_ptr)) || (rc = c->upload(&n.pout_idx, po_idx)) ||
+            (rc = c->upload(&n.pinf_ptr, pi_ptr)) || (rc = c->upload(&n.pinf_idx, pi_idx)))
+            return rc;
+    }
+    // ---- levee: compact the cells that do not carry the no-levee sentinels
+    {
+        std::vector<int> lev_id(N, -1);
+        std::vector<double> lh, lf, bh, ld, lb, lt, lfl;
+        if (c->opts.llevee) {
+            if (!mp->levhgt || !mp->levfrc || !mp->bashgt || !mp->levdst || !mp->levbassto || !mp->levtopsto || !mp->levfilsto)
+                return set_err(CMF_E_ARG, "levee parameter pointer missing");
+            for (int i = 0; i < N; i++) {
+                const bool sentinel = mp->bashgt[i] == 1.E18 && mp->levdst[i] == 1.E18 && mp->levbassto[i] == 1.E18 &&
+                                      mp->levtopsto[i] == 1.E18 && mp->levfilsto[i] == 1.E18 && mp->levfrc[i] == 1.0;
+                if (sentinel) continue;
+                lev_id[i] = (int)lh.size();
+                lh.push_back(mp->levhgt[i]); lf.push_back(mp->levfrc[i]); bh.push_back(mp->bashgt[i]);
+                ld.push_back(mp->levdst[i]); lb.push_back(mp->levbassto[i]); lt.push_back(mp->levtopsto[i]);
+                lfl.push_back(mp->levfilsto[i]);
+            }
+        }
+        c->nlev = (int)lh.size();
+        for (auto *v : {&lh, &lf, &bh, &ld, &lb, &lt, &lfl}) if (v->empty()) v->push_back(0.0);
+        if ((rc = c->upload(&n.lev_id, lev_id)) || (rc = c->upload(&n.levhgt, lh)) || (rc = c->upload(&n.levfrc, lf)) ||
+            (rc = c->upload(&n.bashgt, bh)) || (rc = c->upload(&n.levdst, ld)) || (rc = c->upload(&n.levbassto, lb)) ||
+            (rc = c->upload(&n.levtopsto, lt)) || (rc = c->upload(&n.levfilsto, lfl)))
+            return rc;
+    }
+    // ---- dams
+    {
+        std::vector<int> i1dam(N, 0), dam_id(N, -1), stat;
+        std::vector<double> qn, qf, qa, con, eme, nor, adj, rvu;
+        if (c->opts.ldamout) {
+            if (!mp->damseq || !mp->damstat || !mp->i1dam) return set_err(CMF_E_ARG, "dam table pointer missing");
+            for (int i = 0; i < N; i++) i1dam[i] = mp->i1dam[i];
+            for (int k = 0; k < d.ndam; k++) {
+                if (mp->damstat[k] == kImis) continue;
+                const int s = mp->damseq[k] - 1;
+                if (s < 0 || s >= N) return set_err(CMF_E_ARG, "DamSeq out of range");
+                if (dam_id[s] >= 0) return set_err(CMF_E_UNSUPPORTED, "two dams on one cell");
+                dam_id[s] = (int)stat.size();
+                stat.push_back(mp->damstat[k]);
+                qn.push_back(mp->dam_qn[k]); qf.push_back(mp->dam_qf[k]); qa.push_back(mp->dam_qa[k]);
+                con.push_back(mp->dam_convol[k]); eme.push_back(mp->dam_emevol[k]); nor.push_back(mp->dam_norvol[k]);
+                adj.push_back(mp->dam_adjvol[k]); rvu.push_back(mp->dam_r_volupa[k]);
+            }
+            for (int i = 0; i < N; i++)
+                if ((i1dam[i] == 1 || i1dam[i] == 11) && dam_id[i] < 0) return set_err(CMF_E_ARG, "I1DAM marks a dam cell without a dam");
+        }
+        c->ndam_placed = (int)stat.size();
+        if (stat.empty()) stat.push_back(0);
+        for (auto *v : {&qn, &qf, &qa, &con, &eme, &nor, &adj, &rvu}) if (v->empty()) v->push_back(0.0);
+        if ((rc = c->upload(&n.i1dam, i1dam)) || (rc = c->upload(&n.dam_id, dam_id)) || (rc = c->upload(&n.dam_stat, stat)) ||
+            (rc = c->upload(&n.qn, qn)) || (rc = c->upload(&n.qf, qf)) || (rc = c->upload(&n.qa, qa)) ||
+            (rc = c->upload(&n.convol, con)) || (rc = c->upload(&n.emevol, eme)) || (rc = c->upload(&n.norvol, nor)) ||
+            (rc = c->upload(&n.adjvol, adj)) || (rc = c->upload(&n.r_volupa, rvu)))
+            return rc;
+    }
+    return CMF_OK;
+}
+
+int alloc_state(cmf_gpu_ctx *c) {
+    cmf::State &s = c->st;
+    const size_t MN = (size_t)c->dims.nmembers * c->dims.nseqall;
+    const size_t MP = (size_t)c->dims.nmembers * std::max(c->net.P, 1);
+    const size_t MPL = (size_t)c->dims.nmembers * std::max(c->net.P * c->net.Lp, 1);
+    const bool dg = c->opts.ldiag;
+    double **cell[] = {&s.rivsto, &s.fldsto, &s.rivout_raw, &s.fldout_raw, &s.rivout_pre, &s.fldout_pre,
+                       &s.rivout_cur, &s.fldout_cur, &s.rivdph_pre, &s.fldsto_pre, &s.rivdph, &s.flddph,
+                       &s.fldfrc, &s.fldare, &s.sfcelv, &s.storge, &s.rivvel, &s.rivinf, &s.fldinf, &s.pthout,
+                       &s.outflw, &s.rate, &s.runoff};
+    int rc;
+    for (double **p : cell)
+        if ((rc = c->alloc(p, MN))) return rc;
+    const size_t opt_cells[] = {c->opts.llevee ? MN : 1, c->opts.ldamout ? MN : 1};
+    if ((rc = c->alloc(&s.levsto, opt_cells[0])) || (rc = c->alloc(&s.levdph, opt_cells[0]))) return rc;
+    if ((rc = c->alloc(&s.damsto, opt_cells[1])) || (rc = c->alloc(&s.daminf, opt_cells[1]))) return rc;
+    if ((rc = c->alloc(&s.pthflw_raw, MPL)) || (rc = c->alloc(&s.pthflw_pre, MPL)) || (rc = c->alloc(&s.pthsum_raw, MP)) ||
+        (rc = c->alloc(&s.pthsum, MP)))
+        return rc;
+    double **diag[] = {&s.a_rivout, &s.a_fldout, &s.a_outflw, &s.a_rivvel, &s.a_pthout, &s.a_runoff,
+                       &s.m_storge, &s.m_outflw, &s.m_rivdph};
+    for (double **p : diag)
+        if ((rc = c->alloc(p, dg ? MN : 1))) return rc;
+    if ((rc = c->alloc(&s.a_daminf, (dg && c->opts.ldamout) ? MN : 1))) return rc;
+    if ((rc = c->alloc(&s.a_pthflw, dg ? MPL : 1)) || (rc = c->alloc(&s.a_pthsum, dg ? MP : 1))) return rc;
+    if ((rc = c->alloc(&s.ctl, c->dims.nmembers)) || (rc = c->alloc(&s.loop, 1))) return rc;
+    // budget partials sized for the smallest block the autotuner may pick (64 threads)
+    const size_t nblk_max = (size_t)(c->dims.nseqall + 63) / 64;
+    if ((rc = c->alloc(&s.partials, (size_t)c->dims.nmembers * nblk_max * cmf::kBudgets))) return rc;
+    return CMF_OK;
+}
+
+void set_blocks(cmf_gpu_ctx *c, int block) {
+    c->block = block;
+    c->ncell_blocks = (c->dims.nseqall + block - 1) / block;
+    c->npath_blocks = c->net.P > 0 ? (c->net.P + block - 1) / block : 0;
+}
+
+// Enqueue one sub-step (phases A, B, C and the control kernel).
+void enqueue_substep(cmf_gpu_ctx *c, int use_cond) {
+    const dim3 gc(c->ncell_blocks, c->dims.nmembers);
+    const dim3 gcp(c->ncell_blocks + c->npath_blocks, c->dims.nmembers);
+    cmf::k_flux<<<gcp, c->block, 0, c->stream>>>(c->net, c->st, c->ncell_blocks);
+    cmf::k_rate<<<gc, c->block, 0, c->stream>>>(c->net, c->st);
+    cmf::k_store<<<gcp, c->block, 0, c->stream>>>(c->net, c->st, c->ncell_blocks);
+    cmf::k_ctl<<<1, 256, 0, c->stream>>>(c->net, c->st, c->ncell_blocks, c->cond, use_cond);
+}
+
+void enqueue_prologue(cmf_gpu_ctx *c, int use_cond) {
+    const dim3 gc(c->ncell_blocks, c->dims.nmembers);
+    cmf::k_stage<<<gc, c->block, 0, c->stream>>>(c->net, c->st);
+    cmf::k_ntdt<<<1, 256, 0, c->stream>>>(c->net, c->st, c->cond, use_cond);
+}
+
+int build_graph(cmf_gpu_ctx *c) {
+    if (c->exec) { cudaGraphExecDestroy(c->exec); c->exec = nullptr; }
+    if (c->graph) { cudaGraphDestroy(c->graph); c->graph = nullptr; }
+    CUDA_TRY(cudaGraphCreate(&c->graph, 0));
+    CUDA_TRY(cudaGraphConditionalHandleCreate(&c->cond, c->graph, 1u, cudaGraphCondAssignDefault));
+    CUDA_TRY(cudaStreamBeginCaptureToGraph(c->stream, c->graph, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    enqueue_prologue(c, 1);
+    cudaStreamCaptureStatus status;
+    const cudaGraphNode_t *deps = nullptr;
+    size_t ndeps = 0;
+    cudaGraph_t captured = nullptr;
+    CUDA_TRY(cudaStreamGetCaptureInfo(c->stream, &status, nullptr, &captured, &deps, &ndeps));
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = c->cond;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t cnode;
+    CUDA_TRY(cudaGraphAddNode(&cnode, captured, deps, ndeps, &cp));
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    CUDA_TRY(cudaStreamUpdateCaptureDependencies(c->stream, &cnode, 1, cudaStreamSetCaptureDependencies));
+    cudaGraph_t g2 = nullptr;
+    CUDA_TRY(cudaStreamEndCapture(c->stream, &g2));
+    CUDA_TRY(cudaStreamBeginCaptureToGraph(c->stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    enqueue_substep(c, 1);
+    cudaGraph_t g3 = nullptr;
+    CUDA_TRY(cudaStreamEndCapture(c->stream, &g3));
+    CUDA_TRY(cudaGraphInstantiate(&c->exec, c->graph, 0));
+    return CMF_OK;
+}
+
+int sync_dt_def(cmf_gpu_ctx *c, double dt_def) {
+    if (!(dt_def > 0.0)) return set_err(CMF_E_ARG, "DT must be positive");
+    if (dt_def == c->dt_def_dev) return CMF_OK;
+    for (auto &m : c->hctl) {
+        m.dt_def = dt_def;
+        unsigned long long b;
+        std::memcpy(&b, &dt_def, sizeof b);
+        m.dtmin_bits = b;
+    }
+    // only the first two fields and the atomicMin target change; copy the whole block (small)
+    CUDA_TRY(cudaMemcpyAsync(c->st.ctl, c->hctl.data(), c->hctl.size() * sizeof(cmf::MemberCtl), cudaMemcpyHostToDevice, c->stream));
+    c->dt_def_dev = dt_def;
+    return CMF_OK;
+}
+
+int launch_outer(cmf_gpu_ctx *c) {
+    if (c->opts.launch_mode == 0) {
+        CUDA_TRY(cudaGraphLaunch(c->exec, c->stream));
+        c->launches += 2;   // prologue; the loop body adds 4 per sub-step (counted on read-back)
+        return CMF_OK;
+    }
+    enqueue_prologue(c, 0);
+    CUDA_TRY(cudaGetLastError());
+    cmf::LoopCtl lc;
+    CUDA_TRY(cudaMemcpyAsync(&lc, c->st.loop, sizeof lc, cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    for (int k = 0; k < lc.ntmax; k++) enqueue_substep(c, 0);
+    CUDA_TRY(cudaGetLastError());
+    c->launches += 2 + 4LL * lc.ntmax;
+    return CMF_OK;
+}
+
+int read_ctl(cmf_gpu_ctx *c) {
+    CUDA_TRY(cudaMemcpyAsync(c->hctl.data(), c->st.ctl, c->hctl.size() * sizeof(cmf::MemberCtl), cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    return CMF_OK;
+}
+
+int autotune(cmf_gpu_ctx *c) {
+    // times one sub-step (phases A, B, C) of the zero state for each candidate block size
+    const int cands[] = {128, 256, 512};
+    std::vector<cmf::MemberCtl> probe(c->dims.nmembers);
+    for (auto &m : probe) { m = cmf::MemberCtl{}; m.dt_def = 3600.0; m.dt = 600.0; m.nt = 1; m.it = 0; }
+    CUDA_TRY(cudaMemcpyAsync(c->st.ctl, probe.data(), probe.size() * sizeof(cmf::MemberCtl), cudaMemcpyHostToDevice, c->stream));
+    cudaEvent_t e0, e1;
+    CUDA_TRY(cudaEventCreate(&e0));
+    CUDA_TRY(cudaEventCreate(&e1));
+    float best = 1e30f;
+    int best_b = 256;
+    for (int b : cands) {
+        set_blocks(c, b);
+        const dim3 gc(c->ncell_blocks, c->dims.nmembers), gcp(c->ncell_blocks + c->npath_blocks, c->dims.nmembers);
+        float tot = 0.f;
+        for (int rep = 0; rep < 4; rep++) {
+            CUDA_TRY(cudaEventRecord(e0, c->stream));
+            cmf::k_flux<<<gcp, b, 0, c->stream>>>(c->net, c->st, c->ncell_blocks);
+            cmf::k_rate<<<gc, b, 0, c->stream>>>(c->net, c->st);
+            cmf::k_store<<<gcp, b, 0, c->stream>>>(c->net, c->st, c->ncell_blocks);
+            CUDA_TRY(cudaEventRecord(e1, c->stream));
+            CUDA_TRY(cudaEventSynchronize(e1));
+            float ms = 0.f;
+            CUDA_TRY(cudaEventElapsedTime(&ms, e0, e1));
+            if (rep > 0) tot += ms;
+        }
+        c->launches += 12;
+        if (tot < best) { best = tot; best_b = b; }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    set_blocks(c, best_b);
+    return CMF_OK;
+}
+
+int zero_state(cmf_gpu_ctx *c) {
+    const size_t MN = (size_t)c->dims.nmembers * c->dims.nseqall;
+    cmf::State &s = c->st;
+    for (double *p : {s.rivsto, s.fldsto, s.rivout_raw, s.fldout_raw, s.rivout_pre, s.fldout_pre, s.rivout_cur, s.fldout_cur,
+                      s.rivdph_pre, s.fldsto_pre, s.rivdph, s.flddph, s.fldfrc, s.fldare, s.sfcelv, s.storge, s.rivvel,
+                      s.rivinf, s.fldinf, s.pthout, s.outflw, s.rate})
+        CUDA_TRY(cudaMemsetAsync(p, 0, MN * sizeof(double), c->stream));
+    if (c->opts.llevee) { CUDA_TRY(cudaMemsetAsync(s.levsto, 0, MN * 8, c->stream)); CUDA_TRY(cudaMemsetAsync(s.levdph, 0, MN * 8, c->stream)); }
+    if (c->opts.ldamout) { CUDA_TRY(cudaMemsetAsync(s.damsto, 0, MN * 8, c->stream)); CUDA_TRY(cudaMemsetAsync(s.daminf, 0, MN * 8, c->stream)); }
+    const size_t MPL = (size_t)c->dims.nmembers * std::max(c->net.P * c->net.Lp, 1);
+    const size_t MP = (size_t)c->dims.nmembers * std::max(c->net.P, 1);
+    CUDA_TRY(cudaMemsetAsync(s.pthflw_raw, 0, MPL * 8, c->stream));
+    CUDA_TRY(cudaMemsetAsync(s.pthflw_pre, 0, MPL * 8, c->stream));
+    CUDA_TRY(cudaMemsetAsync(s.pthsum_raw, 0, MP * 8, c->stream));
+    CUDA_TRY(cudaMemsetAsync(s.pthsum, 0, MP * 8, c->stream));
+    return CMF_OK;
+}
+
+template <class T>
+int h2d(cmf_gpu_ctx *c, T *dst, const T *src, size_t n) {
+    if (!src) return CMF_OK;
+    CUDA_TRY(cudaMemcpyAsync(dst, src, n * sizeof(T), cudaMemcpyHostToDevice, c->stream));
+    return CMF_OK;
+}
+template <class T>
+int d2h(cmf_gpu_ctx *c, T *dst, const T *src, size_t n) {
+    if (!dst) return CMF_OK;
+    CUDA_TRY(cudaMemcpyAsync(dst, src, n * sizeof(T), cudaMemcpyDeviceToHost, c->stream));
+    return CMF_OK;
+}
+
+// state arrays of the boundary are [M][NSEQMAX]; the device keeps [M][NSEQALL] (== NSEQMAX here)
+int finish_outer(cmf_gpu_ctx *c, int32_t *nt_out, double *dt_out, cmf_budget *b) {
+    int rc = read_ctl(c);
+    if (rc) return rc;
+    int err = 0;
+    int64_t sub = 0;
+    int ntmax = 0;
+    for (size_t m = 0; m < c->hctl.size(); m++) {
+        const cmf::MemberCtl &x = c->hctl[m];
+        if (x.err) err = x.err;
+        ntmax = std::max(ntmax, x.nt);
+        if (nt_out) nt_out[m] = x.nt;
+        if (dt_out) dt_out[m] = x.dt;
+        if (b) {
+            b[m].stopre = x.budget[0]; b[m].stonxt = x.budget[1]; b[m].stonew = x.budget[2];
+            b[m].rivinf = x.budget[3]; b[m].rivout = x.budget[4]; b[m].stopre2 = x.budget[5];
+            b[m].stonew2 = x.budget[6]; b[m].rivsto = x.budget[7]; b[m].fldsto = x.budget[8];
+            b[m].fldare = x.budget[9]; b[m].levsto = x.budget[10]; b[m].dam_miss = x.budget[11];
+        }
+    }
+    (void)sub;
+    if (c->opts.launch_mode == 0) c->launches += 4LL * ntmax;
+    if (err) {
+        for (auto &x : c->hctl) x.err = 0;
+        CUDA_TRY(cudaMemcpyAsync(c->st.ctl, c->hctl.data(), c->hctl.size() * sizeof(cmf::MemberCtl), cudaMemcpyHostToDevice, c->stream));
+        return set_err(CMF_E_NT_CAP, "adaptive sub-step count is not finite or above the cap (DT_MIN non-finite or tiny)");
+    }
+    return CMF_OK;
+}
+
+cmf_gpu_ctx *g_default = nullptr;
+
+}  // namespace
+
+extern "C" {
+
+int cmf_gpu_abi_version(void) { return CMF_GPU_ABI_VERSION; }
+const char *cmf_gpu_last_error(void) { return g_last_error.c_str(); }
+
+const char *cmf_gpu_strerror(int status) {
+    switch (status) {
+        case CMF_OK: return "ok";
+        case CMF_E_ARG: return "invalid argument or inconsistent dimensions";
+        case CMF_E_UNSUPPORTED: return "option combination not supported by the GPU path";
+        case CMF_E_STATE: return "GPU context not initialised";
+        case CMF_E_IO: return "cannot read a map, table or namelist";
+        case CMF_E_CUDA: return "CUDA runtime error";
+        case CMF_E_NT_CAP: return "adaptive sub-step count not finite or above the cap";
+        case CMF_E_NO_DEVICE: return "no usable CUDA device (sm_100a required)";
+        default: return "unknown status";
+    }
+}
+
+int cmf_gpu_create(const cmf_dims *dims, const cmf_params *params, const cmf_map_ptrs *maps, const cmf_opts *opts,
+                   cmf_gpu_ctx **out) {
+    if (!dims || !params || !maps || !opts || !out) return set_err(CMF_E_ARG, "null argument");
+    *out = nullptr;
+    if (dims->nseqall <= 0 || dims->nseqriv < 0 || dims->nseqriv > dims->nseqall || dims->nlfp <= 0 || dims->nmembers <= 0)
+        return set_err(CMF_E_ARG, "bad dimensions");
+    if (dims->nseqmax != dims->nseqall) return set_err(CMF_E_UNSUPPORTED, "NSEQMAX /= NSEQALL (MPI region padding)");
+    int rc = check_opts(*opts);
+    if (rc) return rc;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= opts->device) return set_err(CMF_E_NO_DEVICE, "no CUDA device");
+    cudaDeviceProp prop;
+    CUDA_TRY(cudaGetDeviceProperties(&prop, opts->device));
+    if (prop.major != 10) return set_err(CMF_E_NO_DEVICE, std::string("kernels are built for sm_100a; device is ") + prop.name);
+    CUDA_TRY(cudaSetDevice(opts->device));
+    auto *c = new cmf_gpu_ctx();
+    c->dims = *dims;
+    c->params = *params;
+    c->opts = *opts;
+    c->device = opts->device;
+    c->hctl.assign(dims->nmembers, cmf::MemberCtl{});
+    auto fail = [&](int code) {
+        cmf_gpu_destroy(c);
+        return code;
+    };
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess)
+        return fail(set_err(CMF_E_CUDA, "cudaStreamCreate failed"));
+    if ((rc = build_net(c, maps))) return fail(rc);
+    if ((rc = alloc_state(c))) return fail(rc);
+    if (opts->block_size > 0) {
+        if (opts->block_size % 32 || opts->block_size > 1024 || opts->block_size < 64)
+            return fail(set_err(CMF_E_ARG, "block_size must be a multiple of 32 in [64, 1024]"));
+        set_blocks(c, opts->block_size);
+    } else if ((rc = autotune(c))) {
+        return fail(rc);
+    }
+    if ((rc = zero_state(c))) return fail(rc);
+    c->dt_def_dev = -1.0;
+    if ((rc = sync_dt_def(c, 86400.0))) return fail(rc);
+    if (opts->launch_mode == 0 && (rc = build_graph(c))) return fail(rc);
+    if (cudaStreamSynchronize(c->stream) != cudaSuccess) return fail(set_err(CMF_E_CUDA, cudaGetErrorString(cudaGetLastError())));
+    *out = c;
+    return CMF_OK;
+}
+
+int cmf_gpu_destroy(cmf_gpu_ctx *c) {
+    if (!c) return CMF_OK;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    if (c->exec) cudaGraphExecDestroy(c->exec);
+    if (c->graph) cudaGraphDestroy(c->graph);
+    for (void *p : c->allocs) cudaFree(p);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return CMF_OK;
+}
+
+int cmf_gpu_ctx_set_state(cmf_gpu_ctx *c, const cmf_state_ptrs *p) {
+    if (!c || !p) return set_err(CMF_E_ARG, "null argument");
+    CUDA_TRY(cudaSetDevice(c->device));
+    const size_t MN = (size_t)c->dims.nmembers * c->dims.nseqall;
+    const size_t MPL = (size_t)c->dims.nmembers * c->net.P * c->net.Lp;
+    cmf::State &s = c->st;
+    int rc;
+    if ((rc = h2d(c, s.rivsto, p->rivsto, MN)) || (rc = h2d(c, s.fldsto, p->fldsto, MN)) ||
+        (rc = h2d(c, s.rivout_cur, p->rivout, MN)) || (rc = h2d(c, s.fldout_cur, p->fldout, MN)) ||
+        (rc = h2d(c, s.rivout_pre, p->rivout_pre, MN)) || (rc = h2d(c, s.fldout_pre, p->fldout_pre, MN)) ||
+        (rc = h2d(c, s.rivdph_pre, p->rivdph_pre, MN)) || (rc = h2d(c, s.fldsto_pre, p->fldsto_pre, MN)))
+        return rc;
+    if (c->opts.lpthout && MPL) {
+        if ((rc = h2d(c, s.pthflw_pre, p->pthflw_pre, MPL))) return rc;
+    }
+    if (c->opts.ldamout) {
+        if ((rc = h2d(c, s.damsto, p->damsto, MN)) || (rc = h2d(c, s.daminf, p->daminf, MN))) return rc;
+    }
+    if (c->opts.llevee) {
+        if ((rc = h2d(c, s.levsto, p->levsto, MN))) return rc;
+    }
+    // D2RIVOUT may differ from D2RIVOUT_PRE (restart): the first sub-step reads the host copy
+    cmf::LoopCtl lc{};
+    lc.split = 1;
+    CUDA_TRY(cudaMemcpyAsync(s.loop, &lc, sizeof lc, cudaMemcpyHostToDevice, c->stream));
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    return CMF_OK;
+}
+
+int cmf_gpu_ctx_get_state(cmf_gpu_ctx *c, const cmf_state_ptrs *p) {
+    if (!c || !p) return set_err(CMF_E_ARG, "null argument");
+    CUDA_TRY(cudaSetDevice(c->device));
+    const size_t MN = (size_t)c->dims.nmembers * c->dims.nseqall;
+    const size_t MPL = (size_t)c->dims.nmembers * c->net.P * c->net.Lp;
+    cmf::State &s = c->st;
+    cmf::LoopCtl lc{};
+    CUDA_TRY(cudaMemcpyAsync(&lc, s.loop, sizeof lc, cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    int rc;
+    if ((rc = d2h(c, p->rivsto, s.rivsto, MN)) || (rc = d2h(c, p->fldsto, s.fldsto, MN)) ||
+        (rc = d2h(c, p->rivout, lc.split ? s.rivout_cur : s.rivout_pre, MN)) ||
+        (rc = d2h(c, p->fldout, lc.split ? s.fldout_cur : s.fldout_pre, MN)) ||
+        (rc = d2h(c, p->rivout_pre, s.rivout_pre, MN)) || (rc = d2h(c, p->fldout_pre, s.fldout_pre, MN)) ||
+        (rc = d2h(c, p->rivdph_pre, s.rivdph_pre, MN)) || (rc = d2h(c, p->fldsto_pre, s.fldsto_pre, MN)))
+        return rc;
+    if (c->opts.lpthout && MPL) {
+        if ((rc = d2h(c, p->pthflw_pre, s.pthflw_pre, MPL)) || (rc = d2h(c, p->pthflw, s.pthflw_pre, MPL))) return rc;
+    }
+    if (c->opts.ldamout) {
+        if ((rc = d2h(c, p->damsto, s.damsto, MN)) || (rc = d2h(c, p->daminf, s.daminf, MN))) return rc;
+    }
+    if (c->opts.llevee) {
+        if ((rc = d2h(c, p->levsto, s.levsto, MN))) return rc;
+    }
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    return CMF_OK;
+}
+
+int cmf_gpu_ctx_put_runoff(cmf_gpu_ctx *c, const double *runoff, const double *rofsub) {
+    if (!c || !runoff) return set_err(CMF_E_ARG, "null argument");
+    (void)rofsub;   // D2ROFSUB only enters the physics through LROSPLIT/LGDWDLY, which are refused
+    CUDA_TRY(cudaSetDevice(c->device));
+    const size_t MN = (size_t)c->dims.nmembers * c->dims.nseqall;
+    CUDA_TRY(cudaMemcpyAsync(c->st.runoff, runoff, MN * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    return CMF_OK;
+}
+
+int cmf_gpu_ctx_physics_advance(cmf_gpu_ctx *c, double dt_def, int32_t *nt_out, double *dt_out, cmf_budget *b) {
+    if (!c) return set_err(CMF_E_STATE, "no context");
+    CUDA_TRY(cudaSetDevice(c->device));
+    int rc;
+    if ((rc = sync_dt_def(c, dt_def))) return rc;
+    if ((rc = launch_outer(c))) return rc;
+    CUDA_TRY(cudaGetLastError());
+    return finish_outer(c, nt_out, dt_out, b);
+}
+
+int cmf_gpu_ctx_advance_device(cmf_gpu_ctx *c, double dt_def, int32_t ksteps, const double *runoff_dev, int64_t stride) {
+    if (!c || ksteps < 0) return set_err(CMF_E_ARG, "bad argument");
+    CUDA_TRY(cudaSetDevice(c->device));
+    int rc;
+    if ((rc = sync_dt_def(c, dt_def))) return rc;
+    if (c->opts.launch_mode != 0) return set_err(CMF_E_UNSUPPORTED, "device pipeline needs launch_mode 0");
+    const size_t MN = (size_t)c->dims.nmembers * c->dims.nseqall;
+    for (int k = 0; k < ksteps; k++) {
+        if (runoff_dev)
+            CUDA_TRY(cudaMemcpyAsync(c->st.runoff, runoff_dev + (size_t)k * stride, MN * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+        CUDA_TRY(cudaGraphLaunch(c->exec, c->stream));
+        c->launches += 2;
+    }
+    return CMF_OK;
+}
+
+int cmf_gpu_ctx_synchronize(cmf_gpu_ctx *c) {
+    if (!c) return set_err(CMF_E_STATE, "no context");
+    CUDA_TRY(cudaSetDevice(c->device));
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    return CMF_OK;
+}
+
+int cmf_gpu_ctx_last_nt(cmf_gpu_ctx *c, int32_t *nt_out, double *dt_out) {
+    if (!c) return set_err(CMF_E_STATE, "no context");
+    CUDA_TRY(cudaSetDevice(c->device));
+    int rc = read_ctl(c);
+    if (rc) return rc;
+    for (size_t m = 0; m < c->hctl.size(); m++) {
+        if (nt_out) nt_out[m] = c->hctl[m].nt;
+        if (dt_out) dt_out[m] = c->hctl[m].dt;
+    }
+    return CMF_OK;
+}
+
+void *cmf_gpu_ctx_stream(cmf_gpu_ctx *c) { return c ? (void *)c->stream : nullptr; }
+int64_t cmf_gpu_ctx_kernel_launches(cmf_gpu_ctx *c) { return c ? c->launches : 0; }
+int32_t cmf_gpu_ctx_block_size(cmf_gpu_ctx *c) { return c ? c->block : 0; }
+
+int cmf_gpu_ctx_stage(cmf_gpu_ctx *c, double dt_def, double *dt_min_local) {
+    if (!c) return set_err(CMF_E_STATE, "no context");
+    CUDA_TRY(cudaSetDevice(c->device));
+    int rc;
+    if ((rc = sync_dt_def(c, dt_def))) return rc;
+    const dim3 gc(c->ncell_blocks, c->dims.nmembers);
+    cmf::k_stage<<<gc, c->block, 0, c->stream>>>(c->net, c->st);
+    CUDA_TRY(cudaGetLastError());
+    c->launches += 1;
+    if ((rc = read_ctl(c))) return rc;
+    if (dt_min_local) {
+        for (size_t m = 0; m < c->hctl.size(); m++) {
+            double v;
+            std::memcpy(&v, &c->hctl[m].dtmin_bits, sizeof v);
+            dt_min_local[m] = std::min(v, dt_def);
+        }
+    }
+    return CMF_OK;
+}
+
+int cmf_gpu_ctx_substeps(cmf_gpu_ctx *c, double dt_def, double dt_min_global, int32_t *nt_out, double *dt_out, cmf_budget *b) {
+    if (!c) return set_err(CMF_E_STATE, "no context");
+    CUDA_TRY(cudaSetDevice(c->device));
+    // install the reduced minimum as the atomicMin result, then run NT/DT and the sub-steps
+    for (auto &m : c->hctl) {
+        unsigned long long bits;
+        std::memcpy(&bits, &dt_min_global, sizeof bits);
+        m.dtmin_bits = bits;
+        m.dt_def = dt_def;
+    }
+    CUDA_TRY(cudaMemcpyAsync(c->st.ctl, c->hctl.data(), c->hctl.size() * sizeof(cmf::MemberCtl), cudaMemcpyHostToDevice, c->stream));
+    c->dt_def_dev = dt_def;
+    cmf::k_ntdt<<<1, 256, 0, c->stream>>>(c->net, c->st, c->cond, 0);
+    CUDA_TRY(cudaGetLastError());
+    cmf::LoopCtl lc;
+    CUDA_TRY(cudaMemcpyAsync(&lc, c->st.loop, sizeof lc, cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    for (int k = 0; k < lc.ntmax; k++) enqueue_substep(c, 0);
+    CUDA_TRY(cudaGetLastError());
+    c->launches += 1 + 4LL * lc.ntmax;
+    const int saved = c->opts.launch_mode;
+    c->opts.launch_mode = 1;
+    int rc = finish_outer(c, nt_out, dt_out, b);
+    c->opts.launch_mode = saved;
+    return rc;
+}
+
+int cmf_gpu_ctx_get_diag(cmf_gpu_ctx *c, const cmf_diag_ptrs *p) {
+    if (!c || !p) return set_err(CMF_E_ARG, "null argument");
+    CUDA_TRY(cudaSetDevice(c->device));
+    const size_t MN = (size_t)c->dims.nmembers * c->dims.nseqall;
+    const size_t MP = (size_t)c->dims.nmembers * c->net.P;
+    const size_t MPL = MP * c->net.Lp;
+    cmf::State &s = c->st;
+    int rc;
+    struct { double *dst; const double *src; size_t n; } t[] = {
+        {p->rivdph, s.rivdph, MN}, {p->flddph, s.flddph, MN}, {p->fldfrc, s.fldfrc, MN}, {p->fldare, s.fldare, MN},
+        {p->sfcelv, s.sfcelv, MN}, {p->storge, s.storge, MN}, {p->rivvel, s.rivvel, MN}, {p->rivinf, s.rivinf, MN},
+        {p->fldinf, s.fldinf, MN}, {p->pthout, s.pthout, MN}, {p->outflw, s.outflw, MN},
+        {p->pthflwsum, s.pthsum, MP}, {p->levdph, c->opts.llevee ? s.levdph : nullptr, MN}};
+    for (auto &x : t) {
+        if (!x.dst || !x.src || !x.n) continue;
+        if ((rc = d2h(c, x.dst, x.src, x.n))) return rc;
+    }
+    if (c->opts.ldiag) {
+        struct { double *dst; const double *src; size_t n; } a[] = {
+            {p->rivout_aavg, s.a_rivout, MN}, {p->fldout_aavg, s.a_fldout, MN}, {p->outflw_aavg, s.a_outflw, MN},
+            {p->rivvel_aavg, s.a_rivvel, MN}, {p->pthout_aavg, s.a_pthout, MN}, {p->runoff_aavg, s.a_runoff, MN},
+            {p->daminf_aavg, c->opts.ldamout ? s.a_daminf : nullptr, MN}, {p->storge_amax, s.m_storge, MN},
+            {p->outflw_amax, s.m_outflw, MN}, {p->rivdph_amax, s.m_rivdph, MN}, {p->pthflw_aavg, s.a_pthflw, MPL},
+            {p->pthflwsum_aavg, s.a_pthsum, MP}};
+        for (auto &x : a) {
+            if (!x.dst || !x.src || !x.n) continue;
+            if ((rc = d2h(c, x.dst, x.src, x.n))) return rc;
+        }
+    }
+    // GDWRTN/ROFSUB are zero without groundwater delay or LROSPLIT (both refused)
+    if (p->gdwrtn_aavg) std::memset(p->gdwrtn_aavg, 0, MN * sizeof(double));
+    if (p->rofsub_aavg) std::memset(p->rofsub_aavg, 0, MN * sizeof(double));
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    return CMF_OK;
+}
+
+// ---- default context (the Fortran shim) ----------------------------------------------------
+int cmf_gpu_init(const cmf_dims *dims, const cmf_params *params, const cmf_map_ptrs *maps, const cmf_opts *opts) {
+    if (g_default) { cmf_gpu_destroy(g_default); g_default = nullptr; }
+    return cmf_gpu_create(dims, params, maps, opts, &g_default);
+}
+int cmf_gpu_set_state(const cmf_state_ptrs *st) {
+    return g_default ? cmf_gpu_ctx_set_state(g_default, st) : set_err(CMF_E_STATE, "cmf_gpu_init not called");
+}
+int cmf_gpu_get_state(const cmf_state_ptrs *st) {
+    return g_default ? cmf_gpu_ctx_get_state(g_default, st) : set_err(CMF_E_STATE, "cmf_gpu_init not called");
+}
+int cmf_gpu_put_runoff(const double *runoff, const double *rofsub) {
+    return g_default ? cmf_gpu_ctx_put_runoff(g_default, runoff, rofsub) : set_err(CMF_E_STATE, "cmf_gpu_init not called");
+}
+int cmf_gpu_physics_advance(double dt_def, int32_t *nt_out, double *dt_out, cmf_budget *b) {
+    return g_default ? cmf_gpu_ctx_physics_advance(g_default, dt_def, nt_out, dt_out, b)
+                     : set_err(CMF_E_STATE, "cmf_gpu_init not called");
+}
+int cmf_gpu_get_diag(const cmf_diag_ptrs *dg) {
+    return g_default ? cmf_gpu_ctx_get_diag(g_default, dg) : set_err(CMF_E_STATE, "cmf_gpu_init not called");
+}
+void cmf_gpu_finalize(void) {
+    if (g_default) cmf_gpu_destroy(g_default);
+    g_default = nullptr;
+}
+
+}  // extern "C"

@@ -1,0 +1,871 @@
+// cmf_kernels.cuh -- sm_100a device code of the CaMa-Flood physics time step (FP64).
+//
+// One outer step (CMF_PHYSICS_ADVANCE, src/cmf_ctrl_physics_mod.F90:21-153) is
+//   k_stage   stage scheme at the start of the step + CFL minimum      (:54-59, :161-210)
+//   k_ntdt    NT/DT per member, loop bound of the device-side sub-step loop (:205-206)
+//   NT x { k_flux  outflow + dam + bifurcation flux         (CMF_CALC_OUTFLW, CMF_DAMOUT_CALC,
+//                                                            CMF_CALC_PTHOUT / CMF_LEVEE_OPT_PTHOUT)
+//          k_rate  storage-out gather and outflow limiter rate (LSPAMAT steps 1-2)
+//          k_store rescale + inflow gather + dam balance + CALC_VARS_PRE + CMF_CALC_STONXT +
+//                  stage scheme + sub-step diagnostics        (LSPAMAT steps 2-3, :101-135)
+//          k_ctl   deterministic budget reduction, sub-step counter, loop condition }
+// Three grid-wide dependencies per sub-step remain (outflow needs the downstream stage; the rate
+// needs the upstream outflows; the inflow needs the downstream and upstream rates), so each
+// phase is one kernel and the phases are ordered by the graph.
+//
+// Arithmetic follows the reference statement by statement, compiled with -fmad=false so no
+// multiply-add is fused: x**(-1) is 1/x, x**2 is x*x, x**0.5 is an IEEE square root and every other
+// non-integral power is pow().  Default-real literals of the reference are promoted float values
+// (F(...) below).  All gathers sum in the reference's loop order (ascending upstream sequence);
+// there are no atomics on state, so results are independent of block size and timing.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#define CMF_F(x) ((double)(float)(x))
+
+namespace cmf {
+
+constexpr int kBudgets = 12;       // stopre stonxt stonew rivinf rivout stopre2 stonew2 rivsto fldsto fldare levsto dammiss
+constexpr int kNtCap = 10000;      // bound of the device-side sub-step loop
+
+struct MemberCtl {
+    double dt_def;                 // DT at entry (DT_DEF)
+    double dt;                     // sub-step DT
+    double dt_min;                 // CFL minimum of this outer step
+    double nadd;                   // NADD_adp before the current sub-step
+    unsigned long long dtmin_bits; // atomicMin target (positive doubles order like their bit patterns)
+    int nt;                        // sub-steps of this outer step
+    int it;                        // index of the next sub-step
+    int err;
+    int pad;
+    double budget[kBudgets];       // last finished sub-step
+};
+
+struct LoopCtl {
+    int k;            // sub-step counter of the device-side loop
+    int ntmax;        // max NT over members
+    int err;
+    int split;        // 1 until the first sub-step after a host state upload: D2RIVOUT /= D2RIVOUT_PRE
+};
+
+// Static data shared by all members (device pointers).
+struct Net {
+    int N, R, L, P, Lp, M;
+    const int *__restrict__ next;       // [N] 0-based downstream (river cells)
+    const int *__restrict__ up_ptr;     // [N+1] upstream CSR, ascending sequence (I1UPST order)
+    const int *__restrict__ up_idx;
+    const int *__restrict__ i2mask;     // [N]
+    const double *__restrict__ rivelv, *__restrict__ elevtn, *__restrict__ nxtdst, *__restrict__ rivwth;
+    const double *__restrict__ rivhgt, *__restrict__ rivlen, *__restrict__ rivman, *__restrict__ grarea;
+    const double *__restrict__ rivstomax, *__restrict__ dwnelv;
+    const double *__restrict__ fldstomax, *__restrict__ fldgrd, *__restrict__ fldhgt;   // [L][N]
+    // bifurcation paths
+    const int *__restrict__ pth_up, *__restrict__ pth_dn;   // [P] 0-based, -1 outside domain
+    const int *__restrict__ pth_skip;                        // [P] bit0 plain/LSPAMAT skip, bit1 levee skip
+    const double *__restrict__ pth_dst, *__restrict__ pth_elv, *__restrict__ pth_wth, *__restrict__ pth_man;
+    const int *__restrict__ pout_ptr, *__restrict__ pout_idx, *__restrict__ pinf_ptr, *__restrict__ pinf_idx;
+    // levee (compact per levee cell)
+    const int *__restrict__ lev_id;     // [N] -1 when the cell carries the no-levee sentinels
+    const double *__restrict__ levhgt, *__restrict__ levfrc, *__restrict__ bashgt, *__restrict__ levdst;
+    const double *__restrict__ levbassto, *__restrict__ levtopsto, *__restrict__ levfilsto;
+    // dams
+    const int *__restrict__ i1dam;      // [N]
+    const int *__restrict__ dam_id;     // [N] compact dam of the cell or -1
+    const int *__restrict__ dam_stat;   // [D]
+    const double *__restrict__ qn, *__restrict__ qf, *__restrict__ qa, *__restrict__ convol;
+    const double *__restrict__ emevol, *__restrict__ norvol, *__restrict__ adjvol, *__restrict__ r_volupa;
+    double pgrv, pmanfld, pdstmth, pcadp, pminslp, dfrcinc;
+    int ladpstp, lfldout, lpthout, ldamout, llevee, ldamh22, ldiag;
+};
+
+// Per-member state, member-major [M][N] (paths [M][Lp][P] / [M][P]).
+struct State {
+    double *rivsto, *fldsto, *levsto, *damsto, *daminf;
+    double *rivout_raw, *fldout_raw;          // outflow before the LSPAMAT rescale (phase A -> C)
+    double *rivout_pre, *fldout_pre;          // D2RIVOUT_PRE / D2FLDOUT_PRE (== D2RIVOUT / D2FLDOUT after a step)
+    double *rivout_cur, *fldout_cur;          // host-set D2RIVOUT / D2FLDOUT while LoopCtl.split
+    double *rivdph_pre, *fldsto_pre;
+    double *rivdph, *flddph, *fldfrc, *fldare, *sfcelv, *storge, *levdph, *rivvel;
+    double *rivinf, *fldinf, *pthout, *outflw, *rate;
+    double *pthflw_raw, *pthflw_pre, *pthsum_raw, *pthsum;
+    double *runoff;
+    // sub-step diagnostics
+    double *a_rivout, *a_fldout, *a_outflw, *a_rivvel, *a_pthout, *a_runoff, *a_daminf;
+    double *m_storge, *m_outflw, *m_rivdph, *a_pthflw, *a_pthsum;
+    MemberCtl *ctl;
+    LoopCtl *loop;
+    double *partials;                         // [M][nblk][kBudgets]
+};
+
+__device__ __forceinline__ double dmax(double a, double b) { return (a > b) ? a : b; }
+__device__ __forceinline__ double dmin(double a, double b) { return (a < b) ? a : b; }
+
+// ------------------------------------------------------------------------------------------
+// stage schemes (one cell)
+// ------------------------------------------------------------------------------------------
+struct StageOut {
+    double rivsto, fldsto, levsto, rivdph, flddph, fldfrc, fldare, levdph;
+};
+
+// CMF_CALC_FLDSTG_DEF body, src/cmf_calc_fldstg_mod.F90:46-97
+__device__ __forceinline__ StageOut stage_def(const Net &n, int i, double rivsto, double fldsto) {
+    StageOut o;
+    const int N = n.N, L = n.L;
+    const double pstoall = rivsto + fldsto;
+    const double rsm = n.rivstomax[i];
+    o.levsto = 0.0;
+    o.levdph = 0.0;
+    if (pstoall > rsm) {
+        const double len = n.rivlen[i], wth = n.rivwth[i];
+        const double inc = (n.grarea[i] / len) * n.dfrcinc;
+        int I = 0;   // 0-based layer
+        double sfil = rsm, wfil = wth, dfil = 0.0;
+        while (I < L) {
+            const double smax = n.fldstomax[(size_t)I * N + i];
+            if (!(pstoall > smax)) break;
+            sfil = smax;
+            wfil = wfil + inc;
+            dfil = dfil + n.fldgrd[(size_t)I * N + i] * inc;
+            I++;
+        }
+        double wadd;
+        if (I >= L) {
+            wadd = 0.0;
+            o.flddph = dfil + ((pstoall - sfil) / wfil) / len;
+        } else {
+            const double gr = n.fldgrd[(size_t)I * N + i];
+            const double sadd = pstoall - sfil;
+            wadd = -wfil + sqrt(wfil * wfil + ((2.0 * sadd) / len) / gr);
+            o.flddph = dfil + gr * wadd;
+        }
+        double rs = rsm + (len * wth) * o.flddph;
+        rs = dmin(rs, pstoall);
+        o.rivsto = rs;
+        o.rivdph = (rs / len) / wth;
+        o.fldsto = dmax(pstoall - rs, 0.0);
+        double frc = ((-wth + wfil) + wadd) / (inc * (double)L);
+        frc = dmax(frc, 0.0);
+        frc = dmin(frc, 1.0);
+        o.fldfrc = frc;
+        o.fldare = n.grarea[i] * frc;
+    } else {
+        o.rivsto = pstoall;
+        o.rivdph = dmax((pstoall / n.rivlen[i]) / n.rivwth[i], 0.0);
+        o.fldsto = 0.0;
+        o.flddph = 0.0;
+        o.fldfrc = 0.0;
+        o.fldare = 0.0;
+    }
+    return o;
+}
+
+// CMF_LEVEE_FLDSTG body, src/cmf_ctrl_levee_mod.F90:301-461
+__device__ __forceinline__ StageOut stage_levee(const Net &n, int i, double rivsto, double fldsto, double levsto) {
+    StageOut o;
+    const int N = n.N, L = n.L;
+    const double pstoall = (rivsto + fldsto) + levsto;
+    const double rsm = n.rivstomax[i];
+    const double len = n.rivlen[i], wth = n.rivwth[i];
+    const double inc = (n.grarea[i] / len) * n.dfrcinc;
+    const int lv = n.lev_id[i];
+    const double lbas = lv >= 0 ? n.levbassto[lv] : 1.E18;
+    if (pstoall > rsm) {
+        if (pstoall < lbas) {                                                       // case 1
+            int I = 0;
+            double sfil = rsm, wfil = wth, dfil = 0.0, wadd;
+            while (I < L) {
+                const double smax = n.fldstomax[(size_t)I * N + i];
+                if (!(pstoall > smax)) break;
+                sfil = smax; wfil = wfil + inc; dfil = dfil + n.fldgrd[(size_t)I * N + i] * inc;
+                I++;
+            }
+            if (I < L) {
+                const double gr = n.fldgrd[(size_t)I * N + i];
+                wadd = -wfil + sqrt(wfil * wfil + ((2.0 * (pstoall - sfil)) / len) / gr);
+                o.flddph = dfil + gr * wadd;
+            } else {
+                wadd = 0.0;
+                o.flddph = dfil + ((pstoall - sfil) / wfil) / len;
+            }
+            o.rivsto = rsm + (len * wth) * o.flddph;
+            o.rivdph = (o.rivsto / len) / wth;
+            o.fldsto = dmax(pstoall - o.rivsto, 0.0);
+            double frc = ((-wth + wfil) + wadd) / (inc * (double)L);
+            frc = dmax(frc, 0.0);
+            frc = dmin(frc, 1.0);
+            o.fldfrc = frc;
+            o.fldare = n.grarea[i] * frc;
+            o.levsto = 0.0;
+            o.levdph = 0.0;
+        } else {
+            const double lhgt = n.levhgt[lv], lfrc = n.levfrc[lv], bhgt = n.bashgt[lv], ldst = n.levdst[lv];
+            const double ltop = n.levtopsto[lv], lfil = n.levfilsto[lv];
+            if (pstoall < ltop) {                                                   // case 2
+                const double sadd = pstoall - lbas;
+                const double wadd = ldst + wth;
+                o.flddph = bhgt + (sadd / wadd) / len;
+                o.rivsto = rsm + (len * wth) * o.flddph;
+                o.rivdph = (o.rivsto / len) / wth;
+                o.fldsto = dmax(pstoall - o.rivsto, 0.0);
+                o.fldfrc = lfrc;
+                o.fldare = n.grarea[i] * lfrc;
+                o.levsto = 0.0;
+                o.levdph = 0.0;
+            } else if (pstoall < lfil) {                                            // case 3
+                o.flddph = lhgt;
+                o.rivsto = rsm + (len * wth) * o.flddph;
+                o.rivdph = (o.rivsto / len) / wth;
+                o.fldsto = dmax(ltop - o.rivsto, 0.0);
+                o.levsto = dmax((pstoall - o.rivsto) - o.fldsto, 0.0);
+                const int ilev = (int)(lfrc * (double)L) + 1;   // 1-based layer with the levee
+                double sfil = ltop, wfil = 0.0, dfil = 0.0, sadd;
+                int I = ilev;                                   // 1-based
+                while (I <= L) {
+                    sadd = ((ldst + wth) * (lhgt - n.fldhgt[(size_t)(I - 1) * N + i])) * len;
+                    if (pstoall < n.fldstomax[(size_t)(I - 1) * N + i] + sadd) break;
+                    sfil = n.fldstomax[(size_t)(I - 1) * N + i] + sadd;
+                    wfil = inc * (double)I - ldst;
+                    dfil = n.fldhgt[(size_t)(I - 1) * N + i] - bhgt;
+                    I++;
+                }
+                if (I <= L) {
+                    const double gr = n.fldgrd[(size_t)(I - 1) * N + i];
+                    const double wadd = -wfil + sqrt(wfil * wfil + ((2.0 * (pstoall - sfil)) / len) / gr);
+                    const double dadd = wadd * gr;
+                    o.levdph = (bhgt + dfil) + dadd;
+                    double frc = (wfil + ldst) / (inc * (double)L);
+                    frc = dmax(frc, 0.0);
+                    frc = dmin(frc, 1.0);
+                    o.fldfrc = frc;
+                    o.fldare = n.grarea[i] * frc;
+                } else {
+                    const double dadd = ((pstoall - sfil) / wfil) / len;
+                    o.levdph = (bhgt + dfil) + dadd;
+                    o.fldfrc = 1.0;
+                    o.fldare = n.grarea[i] * 1.0;
+                }
+            } else {                                                                // case 4
+                int I = 0;
+                double sfil = rsm, wfil = wth, dfil = 0.0, wadd;
+                while (I < L) {
+                    const double smax = n.fldstomax[(size_t)I * N + i];
+                    if (!(pstoall > smax)) break;
+                    sfil = smax; wfil = wfil + inc; dfil = dfil + n.fldgrd[(size_t)I * N + i] * inc;
+                    I++;
+                }
+                if (I < L) {
+                    const double gr = n.fldgrd[(size_t)I * N + i];
+                    wadd = -wfil + sqrt(wfil * wfil + ((2.0 * (pstoall - sfil)) / len) / gr);
+                    o.flddph = dfil + gr * wadd;
+                } else {
+                    wadd = 0.0;
+                    o.flddph = dfil + ((pstoall - sfil) / wfil) / len;
+                }
+                o.fldfrc = ((-wth + wfil) + wadd) / (inc * (double)L);
+                o.fldare = n.grarea[i] * o.fldfrc;
+                o.rivsto = rsm + (len * wth) * o.flddph;
+                o.rivdph = (o.rivsto / len) / wth;
+                const double sadd = ((o.flddph - lhgt) * (ldst + wth)) * len;
+                o.fldsto = dmax((ltop + sadd) - o.rivsto, 0.0);
+                o.levsto = dmax((pstoall - o.rivsto) - o.fldsto, 0.0);
+                o.levdph = o.flddph;
+            }
+        }
+    } else {                                                                        // case 0
+        o.rivsto = pstoall;
+        o.rivdph = dmax((pstoall / len) / wth, 0.0);
+        o.fldsto = 0.0; o.flddph = 0.0; o.fldfrc = 0.0; o.fldare = 0.0; o.levsto = 0.0; o.levdph = 0.0;
+    }
+    return o;
+}
+
+__device__ __forceinline__ void store_stage(const Net &n, const State &s, size_t gi, int i, const StageOut &o) {
+    s.rivsto[gi] = o.rivsto;
+    s.fldsto[gi] = o.fldsto;
+    s.rivdph[gi] = o.rivdph;
+    s.flddph[gi] = o.flddph;
+    s.fldfrc[gi] = o.fldfrc;
+    s.fldare[gi] = o.fldare;
+    s.sfcelv[gi] = n.rivelv[i] + o.rivdph;
+    if (n.llevee) {
+        s.levsto[gi] = o.levsto;
+        s.levdph[gi] = o.levdph;
+        s.storge[gi] = (o.rivsto + o.fldsto) + o.levsto;
+    } else {
+        s.storge[gi] = o.rivsto + o.fldsto;
+    }
+}
+
+template <int NV>
+__device__ __forceinline__ void block_sum(double (&v)[NV], double *smem /* [32*NV] */) {
+    // fixed-shape tree: warp butterfly, then warp 0 over the warp partials -> deterministic
+#pragma unroll
+    for (int k = 0; k < NV; k++)
+        for (int o = 16; o > 0; o >>= 1) v[k] = v[k] + __shfl_down_sync(0xffffffffu, v[k], o);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+    if (lane == 0)
+#pragma unroll
+        for (int k = 0; k < NV; k++) smem[warp * NV + k] = v[k];
+    __syncthreads();
+    if (warp == 0) {
+#pragma unroll
+        for (int k = 0; k < NV; k++) {
+            double x = lane < nw ? smem[lane * NV + k] : 0.0;
+            for (int o = 16; o > 0; o >>= 1) x = x + __shfl_down_sync(0xffffffffu, x, o);
+            v[k] = x;
+        }
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// k_stage: stage scheme at the top of CMF_PHYSICS_ADVANCE + CALC_ADPSTP minimum
+// ------------------------------------------------------------------------------------------
+__global__ void k_stage(Net n, State s) {
+    const int m = blockIdx.y;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double key = 1.0e308;
+    if (i < n.N) {
+        const size_t gi = (size_t)m * n.N + i;
+        const StageOut o = n.llevee ? stage_levee(n, i, s.rivsto[gi], s.fldsto[gi], s.levsto[gi])
+                                    : stage_def(n, i, s.rivsto[gi], s.fldsto[gi]);
+        store_stage(n, s, gi, i, o);
+        if (n.ladpstp && n.i2mask[i] == 0) {
+            const double ddph = dmax(o.rivdph, 0.01);
+            const double ddst = (i < n.R) ? n.nxtdst[i] : n.pdstmth;
+            key = (n.pcadp * ddst) * pow(n.pgrv * ddph, -0.5);
+        }
+    }
+    if (n.ladpstp) {
+        for (int o = 16; o > 0; o >>= 1) key = dmin(key, __shfl_down_sync(0xffffffffu, key, o));
+        __shared__ double wmin[32];
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+        if (lane == 0) wmin[warp] = key;
+        __syncthreads();
+        if (warp == 0) {
+            double x = lane < nw ? wmin[lane] : 1.0e308;
+            for (int o = 16; o > 0; o >>= 1) x = dmin(x, __shfl_down_sync(0xffffffffu, x, o));
+            if (lane == 0 && x < 1.0e308) atomicMin(&s.ctl[m].dtmin_bits, (unsigned long long)__double_as_longlong(x));
+        }
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// k_ntdt: NT and DT per member (src/cmf_ctrl_physics_mod.F90:205-206) and the loop bound
+// ------------------------------------------------------------------------------------------
+__global__ void k_ntdt(Net n, State s, cudaGraphConditionalHandle h, int use_cond) {
+    __shared__ int smax[32];
+    int ntmax = 1;
+    for (int m = threadIdx.x; m < n.M; m += blockDim.x) {
+        MemberCtl &c = s.ctl[m];
+        const double dt_def = c.dt_def;
+        int nt = 1;
+        double dt = dt_def;
+        if (n.ladpstp) {
+            const double dt_min = dmin(dt_def, __longlong_as_double((long long)c.dtmin_bits));
+            c.dt_min = dt_min;
+            const double x = dt_def * (1.0 / dt_min) - CMF_F(0.01);
+            if (!(x >= 0.0) || x > (double)(kNtCap - 1)) {
+                c.err = 2;           // non-finite or oversized NT: refuse to loop
+                nt = 0;
+            } else {
+                nt = (int)x + 1;
+                dt = dt_def * (double)(1.0f / (float)nt);
+            }
+            c.dtmin_bits = (unsigned long long)__double_as_longlong(dt_def);
+        } else {
+            c.dt_min = dt_def;
+        }
+        c.nt = nt;
+        c.dt = dt;
+        c.it = 0;
+        c.nadd = 0.0;
+        ntmax = max(ntmax, nt);
+    }
+    for (int o = 16; o > 0; o >>= 1) ntmax = max(ntmax, __shfl_down_sync(0xffffffffu, ntmax, o));
+    if ((threadIdx.x & 31) == 0) smax[threadIdx.x >> 5] = ntmax;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int v = 1;
+        for (int w = 0; w < (int)((blockDim.x + 31) >> 5); w++) v = max(v, smax[w]);
+        v = min(v, kNtCap);
+        s.loop->k = 0;
+        s.loop->ntmax = v;
+        if (use_cond) cudaGraphSetConditional(h, 1u);
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// phase A: outflow + dam + bifurcation flux
+// ------------------------------------------------------------------------------------------
+// CMF_CALC_OUTFLW river/floodplain/mouth discharge and limiter, src/cmf_calc_outflw_mod.F90:44-182
+__device__ __forceinline__ void cell_outflow(const Net &n, const State &s, int m, int i, double DT) {
+    const size_t base = (size_t)m * n.N, gi = base + i;
+    const double gdt = n.pgrv * DT;
+    const double rivelv = n.rivelv[i];
+    const double rivdph = s.rivdph[gi], rivdph_pre = s.rivdph_pre[gi];
+    const double sfc = rivelv + rivdph;
+    const double sfc_pre = rivelv + rivdph_pre;
+    const double flddph_pre = dmax(rivdph_pre - n.rivhgt[i], 0.0);
+    const double wth = n.rivwth[i];
+    const double man = n.rivman[i];
+    const double rivout_old = s.loop->split ? s.rivout_cur[gi] : s.rivout_pre[gi];
+    double rout, fout = 0.0, rvel;
+    if (i < n.R) {
+        const int j = n.next[i];
+        const size_t gj = base + j;
+        const double rj = n.rivelv[j];
+        const double dwn = rj + s.rivdph[gj];
+        const double dwn_pre = rj + s.rivdph_pre[gj];
+        const double inv_dst = 1.0 / n.nxtdst[i];
+        // river
+        {
+            const double dsfc = dmax(sfc, dwn);
+            const double dslp = (sfc - dwn) * inv_dst;
+            const double dflw = dsfc - rivelv;
+            const double dare = dmax(wth * dflw, 1.E-10);
+            const double dflw_pr = dmax(sfc_pre, dwn_pre) - rivelv;
+            const double dflw_im = dmax(sqrt(dflw * dflw_pr), 1.E-6);
+            const double dout_pr = s.rivout_pre[gi] * (1.0 / wth);
+            const double dout = (wth * (dout_pr + (gdt * dflw_im) * dslp))
+                              * (1.0 / (1.0 + ((gdt * (man * man)) * fabs(dout_pr)) * pow(dflw_im, -7.0 / 3.0)));
+            const double dvel = rivout_old * (1.0 / dare);
+            const bool mask = (dflw_im > CMF_F(1.E-5) && dare > CMF_F(1.E-5));
+            rout = mask ? dout : 0.0;
+            rvel = mask ? dvel : 0.0;
+        }
+        if (n.lfldout) {
+            const double len = n.rivlen[i], elv = n.elevtn[i];
+            const double dsfc = dmax(sfc, dwn);
+            double dslp = (sfc - dwn) * inv_dst;
+            dslp = dmax(-0.005, dmin(0.005, dslp));
+            const double dflw = dmax(dsfc - elv, 0.0);
+            double dare = s.fldsto[gi] * (1.0 / len);
+            dare = dmax(dare - s.flddph[gi] * wth, 0.0);
+            const double dflw_pr = dmax(sfc_pre, dwn_pre) - elv;
+            const double dflw_im = dmax(sqrt(dmax(dflw * dflw_pr, 0.0)), 1.E-6);
+            double dare_pr = s.fldsto_pre[gi] * (1.0 / len);
+            dare_pr = dmax(dare_pr - flddph_pre * wth, 1.E-6);
+            const double dare_im = dmax(sqrt(dare * dare_pr), 1.E-6);
+            const double dout_pr = s.fldout_pre[gi];
+            const double dout = (dout_pr + (gdt * dare_im) * dslp)
+                * (1.0 / (1.0 + (((gdt * (n.pmanfld * n.pmanfld)) * fabs(dout_pr)) * pow(dflw_im, -4.0 / 3.0)) * (1.0 / dare_im)));
+            const bool mask = (dflw_im > 1.E-5 && dare > 1.E-5);
+            fout = mask ? dout : 0.0;
+            if (!(fout * rout > 0.0)) fout = 0.0;
+        }
+        // storage-change limiter (v423), :176-182
+        const double dlim = dmax((-rout - fout) * DT, CMF_F(1.E-10));
+        const double rate = dmin((0.05 * s.storge[gi]) / dlim, 1.0);
+        rout = rout * rate;
+        fout = fout * rate;
+    } else {
+        const double inv_dst = 1.0 / n.pdstmth;
+        const double dwn = n.dwnelv[i];
+        {
+            const double dslp = (sfc - dwn) * inv_dst;
+            const double dare = dmax(wth * rivdph, 1.E-10);
+            const double dflw_im = dmax(sqrt(rivdph * rivdph_pre), 1.E-6);
+            const double dout_pr = s.rivout_pre[gi] * (1.0 / wth);
+            const double dout = (wth * (dout_pr + (gdt * dflw_im) * dslp))
+                              * (1.0 / (1.0 + ((gdt * (man * man)) * fabs(dout_pr)) * pow(dflw_im, -7.0 / 3.0)));
+            const double dvel = rivout_old * (1.0 / dare);
+            const bool mask = (dflw_im > CMF_F(1.E-5) && dare > CMF_F(1.E-5));
+            rout = mask ? dout : 0.0;
+            rvel = mask ? dvel : 0.0;
+        }
+        if (n.lfldout) {
+            const double len = n.rivlen[i], elv = n.elevtn[i];
+            double dslp = (sfc - dwn) * inv_dst;
+            dslp = dmax(-0.005, dmin(0.005, dslp));
+            const double dflw = sfc - elv;
+            const double dare = dmax(s.fldsto[gi] * (1.0 / len) - s.flddph[gi] * wth, 0.0);
+            const double dflw_pr = sfc_pre - elv;
+            const double dflw_im = dmax(sqrt(dmax(dflw * dflw_pr, 0.0)), 1.E-6);
+            const double dare_pr = dmax(s.fldsto_pre[gi] * (1.0 / len) - flddph_pre * wth, 1.E-6);
+            const double dare_im = dmax(sqrt(dare * dare_pr), 1.E-6);
+            const double dout_pr = s.fldout_pre[gi];
+            const double dout = (dout_pr + (gdt * dare_im) * dslp)
+                * (1.0 / (1.0 + (((gdt * (n.pmanfld * n.pmanfld)) * fabs(dout_pr)) * pow(dflw_im, -4.0 / 3.0)) * (1.0 / dare_im)));
+            const bool mask = (dflw_im > CMF_F(1.E-5) && dare > CMF_F(1.E-5));
+            fout = mask ? dout : 0.0;
+            if (!(fout * rout > 0.0)) fout = 0.0;
+        }
+    }
+    // reservoir operation, CMF_DAMOUT_CALC (src/cmf_ctrl_damout_mod.F90:316-498)
+    if (n.ldamout) {
+        const int code = n.i1dam[i];
+        if (code > 0) {
+            rout = 0.0;
+            fout = 0.0;
+            double dinf = s.runoff[gi];
+            const int d = n.dam_id[i];
+            if (d >= 0) {
+                // UPDATE_INFLOW 1b: inflow from the dam's upstream cells, in ascending sequence
+                for (int k = n.up_ptr[i]; k < n.up_ptr[i + 1]; k++) {
+                    const int j = n.up_idx[k];
+                    const int cj = n.i1dam[j];
+                    if (cj == 10 || cj == 11) {
+                        const double fpre = n.lfldout ? s.fldout_pre[base + j] : 0.0;
+                        dinf = (dinf + s.rivout_pre[base + j]) + fpre;
+                    }
+                }
+            }
+            s.daminf[gi] = dinf;
+            if (code == 10 && i < n.R) {
+                // UPDATE_INFLOW 1c: kinematic outflow upstream of a dam
+                const int j = n.next[i];
+                const double p23 = CMF_F(2. / 3.);
+                double dslope = (n.elevtn[i] - n.elevtn[j]) * (1.0 / n.nxtdst[i]);
+                dslope = dmax(dslope, n.pminslp);
+                const double dph = rivdph;
+                const double dvel = ((1.0 / man) * sqrt(dslope)) * pow(dph, p23);
+                const double darea = wth * dph;
+                rvel = dvel;
+                rout = dmin(darea * dvel, s.rivsto[gi] / DT);
+                const double slope_f = dmin(0.005, dslope);
+                const double fdph = s.flddph[gi];
+                const double dvel_f = ((1.0 / n.pmanfld) * sqrt(slope_f)) * pow(fdph, p23);
+                double dare_f = s.fldsto[gi] * (1.0 / n.rivlen[i]);
+                dare_f = dmax(dare_f - fdph * wth, 0.0);
+                fout = dmin(dare_f * dvel_f, s.fldsto[gi] / DT);
+            }
+            if (d >= 0 && n.dam_stat[d] > 0) {
+                const double vol = s.damsto[gi];
+                const double qn = n.qn[d], qf = n.qf[d], qa = n.qa[d], con = n.convol[d], eme = n.emevol[d];
+                double q = 0.0;
+                if (n.ldamh22) {
+                    const double nor = n.norvol[d];
+                    if (vol <= nor) q = qn * (vol / con);
+                    else if (nor < vol && vol <= con) {
+                        if (qf <= dinf) q = qn * CMF_F(0.5) + ((vol - nor) / (con - nor)) * (qf - qn);
+                        else { const double r = (vol - nor) / (eme - nor); q = qn * CMF_F(0.5) + (r * r) * (qf - qn); }
+                    } else if (con < vol && vol < eme) {
+                        if (qf <= dinf)
+                            q = qf + ((dmax(CMF_F(1.) - n.r_volupa[d] / CMF_F(0.2), 0.0) * (vol - con)) / (eme - con)) * (dinf - qf);
+                        else { const double r = (vol - nor) / (eme - nor); q = qn * CMF_F(0.5) + (r * r) * (qf - qn); }
+                    } else q = dmax(dinf, qf);
+                } else {
+                    const double adj = n.adjvol[d];
+                    if (vol <= con) q = qn * sqrt(vol / con);
+                    else if (vol > con && vol <= adj) q = qn + pow((vol - con) / (adj - con), 3.0) * (qa - qn);
+                    else if (vol > adj && vol <= eme) {
+                        const double t = qa + pow((vol - adj) / (eme - adj), CMF_F(0.1)) * (qf - qa);
+                        if (dinf >= qf) q = dmax(qn + ((vol - con) / (eme - con)) * (dinf - qn), t);
+                        else q = t;
+                    } else if (vol > eme) q = (dinf >= qf) ? dinf : qf;
+                }
+                q = dmin(dmin(q, vol / DT), (s.rivsto[gi] + s.fldsto[gi]) / DT);
+                q = dmax(q, 0.0);
+                rout = q;
+                fout = 0.0;
+            }
+        }
+    }
+    s.rivout_raw[gi] = rout;
+    s.fldout_raw[gi] = fout;
+    s.rivvel[gi] = rvel;
+}
+
+// CMF_CALC_PTHOUT (src/cmf_calc_pthout_mod.F90:34-94) / CMF_LEVEE_OPT_PTHOUT (src/cmf_ctrl_levee_mod.F90:508-601)
+__device__ __forceinline__ double path_flux(double wth, double pre, double gdt, double dflw_im, double dslp, double man,
+                                           bool recip) {
+    const double dout_pr = recip ? pre * (1.0 / wth) : pre / wth;
+    return (wth * (dout_pr + (gdt * dflw_im) * dslp)) / (1.0 + ((gdt * (man * man)) * fabs(dout_pr)) * pow(dflw_im, -7.0 / 3.0));
+}
+
+__device__ __forceinline__ void path_outflow(const Net &n, const State &s, int m, int p, double DT) {
+    const int P = n.P, Lp = n.Lp;
+    const size_t pb = (size_t)m * Lp * P;
+    const size_t base = (size_t)m * n.N;
+    const double gdt = n.pgrv * DT;
+    const int skip = n.pth_skip[p];
+    double sum = 0.0;
+    double flw[8];
+    const bool skipped = n.llevee ? (skip & 2) : (skip & 1);
+    if (skipped) {
+        for (int l = 0; l < Lp; l++) s.pthflw_raw[pb + (size_t)l * P + p] = 0.0;
+        s.pthsum_raw[(size_t)m * P + p] = 0.0;
+        return;
+    }
+    const int u = n.pth_up[p], d = n.pth_dn[p];
+    const double su = n.rivelv[u] + s.rivdph[base + u], sd = n.rivelv[d] + s.rivdph[base + d];
+    const double spu = n.rivelv[u] + s.rivdph_pre[base + u], spd = n.rivelv[d] + s.rivdph_pre[base + d];
+    double dslp = (su - sd) / n.pth_dst[p];
+    dslp = dmax(-0.005, dmin(0.005, dslp));
+    if (!n.llevee) {
+        for (int l = 0; l < Lp; l++) {
+            const size_t o = (size_t)l * P + p;
+            const double elv = n.pth_elv[o];
+            const double dflw = dmax(dmax(su, sd) - elv, 0.0);
+            const double dflw_pr = dmax(dmax(spu, spd) - elv, 0.0);
+            double dflw_im = sqrt(dflw * dflw_pr);
+            dflw_im = dmax(dflw_im, sqrt(dflw * 0.01));
+            const double f = (dflw_im > 1.E-5) ? path_flux(n.pth_wth[o], s.pthflw_pre[pb + o], gdt, dflw_im, dslp, n.pth_man[l], false) : 0.0;
+            if (l < 8) flw[l] = f;
+            s.pthflw_raw[pb + o] = f;
+        }
+    } else {
+        // level 1: river channel, semi-implicit depth
+        {
+            const double elv = n.pth_elv[p];
+            const double dflw = dmax(dmax(su, sd) - elv, 0.0);
+            const double dflw_pr = dmax(dmax(spu, spd) - elv, 0.0);
+            double dflw_im = sqrt(dflw * dflw_pr);
+            if (dflw_im <= 0.0) dflw_im = dflw;
+            const double f = (dflw_im > 1.E-5) ? path_flux(n.pth_wth[p], s.pthflw_pre[pb + p], gdt, dflw_im, dslp, n.pth_man[0], false) : 0.0;
+            flw[0] = f;
+            s.pthflw_raw[pb + p] = f;
+        }
+        if (Lp > 1) {
+            const int lu = n.lev_id[u], ld = n.lev_id[d];
+            double slu = su, sld = sd;
+            if (lu >= 0 && n.levfrc[lu] < 1.0) slu = dmin(n.elevtn[u] + s.levdph[base + u], su);
+            if (ld >= 0 && n.levfrc[ld] < 1.0) sld = dmin(n.elevtn[d] + s.levdph[base + d], sd);
+            for (int l = 1; l < Lp; l++) {
+                const size_t o = (size_t)l * P + p;
+                const double dflw = dmax(dmax(slu, sld) - n.pth_elv[o], 0.0);
+                const double f = (dflw > 1.E-5) ? path_flux(n.pth_wth[o], s.pthflw_pre[pb + o], gdt, dflw, dslp, n.pth_man[l], true) : 0.0;
+                if (l < 8) flw[l] = f;
+                s.pthflw_raw[pb + o] = f;
+            }
+        }
+    }
+    for (int l = 0; l < Lp; l++) sum = sum + (l < 8 ? flw[l] : s.pthflw_raw[pb + (size_t)l * P + p]);
+    if (sum != 0.0) {
+        const double rate = dmin((0.05 * dmin(s.storge[base + u], s.storge[base + d])) / fabs(sum * DT), 1.0);
+        for (int l = 0; l < Lp; l++) {
+            const size_t o = pb + (size_t)l * P + p;
+            s.pthflw_raw[o] = (l < 8 ? flw[l] : s.pthflw_raw[o]) * rate;
+        }
+        sum = sum * rate;
+    }
+    s.pthsum_raw[(size_t)m * P + p] = sum;
+}
+
+__global__ void k_flux(Net n, State s, int ncell_blocks) {
+    const int m = blockIdx.y;
+    const MemberCtl &c = s.ctl[m];
+    if (c.it >= c.nt) return;
+    const double DT = c.dt;
+    if ((int)blockIdx.x < ncell_blocks) {
+        const int i = blockIdx.x * blockDim.x + threadIdx.x;
+        if (i < n.N) cell_outflow(n, s, m, i, DT);
+    } else {
+        const int p = (blockIdx.x - ncell_blocks) * blockDim.x + threadIdx.x;
+        if (p < n.P) path_outflow(n, s, m, p, DT);
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// phase B: P2STOOUT and D2RATE, src/cmf_calc_outflw_mod.F90:410-451
+// ------------------------------------------------------------------------------------------
+__global__ void k_rate(Net n, State s) {
+    const int m = blockIdx.y;
+    const MemberCtl &c = s.ctl[m];
+    if (c.it >= c.nt) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n.N) return;
+    const double DT = c.dt;
+    const size_t base = (size_t)m * n.N, gi = base + i;
+    double so = dmax(s.rivout_raw[gi], 0.0) + dmax(s.fldout_raw[gi], 0.0);
+    for (int k = n.up_ptr[i]; k < n.up_ptr[i + 1]; k++) {
+        const int j = n.up_idx[k];
+        so = (so + dmax(-s.rivout_raw[base + j], 0.0)) + dmax(-s.fldout_raw[base + j], 0.0);
+    }
+    so = so * DT;
+    if (n.lpthout) {
+        const double *sum = s.pthsum_raw + (size_t)m * n.P;
+        for (int k = n.pout_ptr[i]; k < n.pout_ptr[i + 1]; k++) so = so + dmax(sum[n.pout_idx[k]], 0.0) * DT;
+        for (int k = n.pinf_ptr[i]; k < n.pinf_ptr[i + 1]; k++) so = so + dmax(-sum[n.pinf_idx[k]], 0.0) * DT;
+    }
+    const double dout = dmax(so, 1.E-10);
+    const double dsto = s.rivsto[gi] + s.fldsto[gi];
+    s.rate[gi] = dmin(dsto / dout, 1.0);
+}
+
+// ------------------------------------------------------------------------------------------
+// phase C: rescale + inflow + dam balance + VARS_PRE + STONXT + stage + diagnostics
+// ------------------------------------------------------------------------------------------
+__device__ __forceinline__ double scaled_pathsum(const Net &n, const double *sum_raw, const double *rate_m, int p) {
+    const double v = sum_raw[p];
+    if (n.pth_skip[p] & 1) return v;
+    return v >= 0.0 ? v * rate_m[n.pth_up[p]] : v * rate_m[n.pth_dn[p]];
+}
+
+__global__ void k_store(Net n, State s, int ncell_blocks) {
+    const int m = blockIdx.y;
+    const MemberCtl &c = s.ctl[m];
+    const bool active = c.it < c.nt;
+    if (!active) return;   // uniform per block (blockIdx.y), no barrier is skipped divergently
+    const double DT = c.dt;
+    const bool first = (c.it == 0);
+    const bool last = (c.it == c.nt - 1);
+    const size_t base = (size_t)m * n.N;
+    if ((int)blockIdx.x >= ncell_blocks) {
+        // bifurcation paths: LSPAMAT path rescale (:494-517), CALC_VARS_PRE copy, diagnostics
+        const int p = (blockIdx.x - ncell_blocks) * blockDim.x + threadIdx.x;
+        if (p >= n.P) return;
+        const int P = n.P, Lp = n.Lp;
+        const size_t pb = (size_t)m * Lp * P;
+        const double *rate_m = s.rate + base;
+        const bool sk = n.pth_skip[p] & 1;
+        const int u = n.pth_up[p], d = n.pth_dn[p];
+        double asum = 0.0;
+        for (int l = 0; l < Lp; l++) {
+            const size_t o = pb + (size_t)l * P + p;
+            double f = s.pthflw_raw[o];
+            if (!sk) f = (f >= 0.0) ? f * rate_m[u] : f * rate_m[d];
+            s.pthflw_pre[o] = f;
+            if (n.ldiag) {
+                double a = first ? f * DT : s.a_pthflw[o] + f * DT;
+                if (last) { a = a / (c.nadd + DT); asum = asum + a; }
+                s.a_pthflw[o] = a;
+            }
+        }
+        s.pthsum[(size_t)m * P + p] = scaled_pathsum(n, s.pthsum_raw + (size_t)m * P, rate_m, p);
+        if (n.ldiag && last) s.a_pthsum[(size_t)m * P + p] = asum;
+        return;
+    }
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double b[kBudgets];
+#pragma unroll
+    for (int k = 0; k < kBudgets; k++) b[k] = 0.0;
+    if (i < n.N) {
+        const size_t gi = base + i;
+        const double *rate_m = s.rate + base;
+        const double rate_i = rate_m[i];
+        // own outflow after the LSPAMAT rescale (:456-473)
+        double rout = s.rivout_raw[gi], fout = s.fldout_raw[gi];
+        if (i < n.R) {
+            const double r = (rout > 0.0) ? rate_i : rate_m[n.next[i]];
+            rout = rout * r;
+            fout = fout * r;
+        } else {
+            rout = rout * rate_i;
+            fout = fout * rate_i;
+        }
+        // inflow from the upstream cells, rescaled on the fly (:481-489); next(j) == i
+        double rinf = 0.0, finf = 0.0;
+        for (int k = n.up_ptr[i]; k < n.up_ptr[i + 1]; k++) {
+            const int j = n.up_idx[k];
+            const double rj = s.rivout_raw[base + j], fj = s.fldout_raw[base + j];
+            const double r = (rj > 0.0) ? rate_m[j] : rate_i;
+            rinf = rinf + rj * r;
+            finf = finf + fj * r;
+        }
+        double pout = 0.0;
+        if (n.lpthout) {
+            const double *sum = s.pthsum_raw + (size_t)m * n.P;
+            for (int k = n.pout_ptr[i]; k < n.pout_ptr[i + 1]; k++) pout = pout + scaled_pathsum(n, sum, rate_m, n.pout_idx[k]);
+            for (int k = n.pinf_ptr[i]; k < n.pinf_ptr[i + 1]; k++) pout = pout - scaled_pathsum(n, sum, rate_m, n.pinf_idx[k]);
+        }
+        const double runoff = s.runoff[gi];
+        // CMF_DAMOUT_WATBAL, src/cmf_ctrl_damout_mod.F90:516-535
+        if (n.ldamout) {
+            const int d = n.dam_id[i];
+            if (d >= 0) {
+                const double inflow = (rinf + finf) + runoff;
+                const double outflw = rout + fout;
+                const double s0 = s.damsto[gi];
+                const double s1 = (s0 + inflow * DT) - outflw * DT;
+                s.damsto[gi] = s1;
+                b[11] = ((s0 - s1) + inflow * DT) - outflw * DT;
+            }
+        }
+        // CALC_VARS_PRE, src/cmf_ctrl_physics_mod.F90:254-277
+        const double rivsto0 = s.rivsto[gi], fldsto0 = s.fldsto[gi];
+        s.rivout_pre[gi] = rout;
+        s.fldout_pre[gi] = fout;
+        s.rivdph_pre[gi] = s.rivdph[gi];
+        s.fldsto_pre[gi] = fldsto0;
+        // CMF_CALC_STONXT, src/cmf_calc_stonxt_mod.F90:53-100
+        b[0] = rivsto0 + fldsto0;
+        b[3] = rinf * DT + finf * DT;
+        b[4] = (rout * DT + fout * DT) + pout * DT;
+        double rs = (rivsto0 + rinf * DT) - rout * DT;
+        double fs = fldsto0;
+        if (rs < 0.0) { fs = fs + rs; rs = 0.0; }
+        fs = ((fs + finf * DT) - fout * DT) - pout * DT;
+        if (fs < 0.0) { rs = dmax(rs + fs, 0.0); fs = 0.0; }
+        b[1] = rs + fs;
+        const double outflw = rout + fout;
+        const double frc = s.fldfrc[gi];
+        rs = rs + (runoff * (1.0 - frc)) * DT;       // D2GDWRTN is zero without groundwater delay
+        fs = fs + (runoff * frc) * DT;
+        double levsto = n.llevee ? s.levsto[gi] : 0.0;
+        b[2] = n.llevee ? (rs + fs) + levsto : rs + fs;
+        // stage scheme, :125
+        const StageOut o = n.llevee ? stage_levee(n, i, rs, fs, levsto) : stage_def(n, i, rs, fs);
+        store_stage(n, s, gi, i, o);
+        b[5] = n.llevee ? (rs + fs) + levsto : rs + fs;
+        b[6] = n.llevee ? (o.rivsto + o.fldsto) + o.levsto : o.rivsto + o.fldsto;
+        b[7] = o.rivsto;
+        b[8] = o.fldsto;
+        b[9] = o.fldare;
+        b[10] = o.levsto;
+        s.rivinf[gi] = rinf;
+        s.fldinf[gi] = finf;
+        s.pthout[gi] = pout;
+        s.outflw[gi] = outflw;
+        // CMF_DIAG_AVEMAX_ADPSTP / GETAVE_ADPSTP, src/cmf_calc_diag_mod.F90:104-221
+        if (n.ldiag) {
+            const double na = c.nadd + DT;
+            auto acc = [&](double *a, double v) {
+                double x = first ? v * DT : a[gi] + v * DT;
+                if (last) x = x / na;
+                a[gi] = x;
+            };
+            acc(s.a_rivout, rout);
+            acc(s.a_fldout, fout);
+            acc(s.a_rivvel, s.rivvel[gi]);
+            acc(s.a_outflw, outflw);
+            acc(s.a_pthout, pout);        // D2PTHINF is never written by the reference (always 0)
+            acc(s.a_runoff, runoff);
+            if (n.ldamout) acc(s.a_daminf, s.daminf[gi]);
+            const double stg = n.llevee ? (o.rivsto + o.fldsto) + o.levsto : o.rivsto + o.fldsto;
+            s.m_outflw[gi] = first ? dmax(0.0, fabs(outflw)) : dmax(s.m_outflw[gi], fabs(outflw));
+            s.m_rivdph[gi] = first ? dmax(0.0, o.rivdph) : dmax(s.m_rivdph[gi], o.rivdph);
+            s.m_storge[gi] = first ? dmax(0.0, stg) : dmax(s.m_storge[gi], stg);
+        }
+    }
+    // per-block budget partials (fixed-shape tree -> deterministic)
+    __shared__ double red[32 * kBudgets];
+    block_sum<kBudgets>(b, red);
+    if (threadIdx.x == 0) {
+        double *dst = s.partials + ((size_t)m * ncell_blocks + blockIdx.x) * kBudgets;
+#pragma unroll
+        for (int k = 0; k < kBudgets; k++) dst[k] = b[k];
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// k_ctl: budgets, sub-step counter and the loop condition
+// ------------------------------------------------------------------------------------------
+__global__ void k_ctl(Net n, State s, int ncell_blocks, cudaGraphConditionalHandle h, int use_cond) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int m = warp; m < n.M; m += nw) {
+        MemberCtl &c = s.ctl[m];
+        if (c.it >= c.nt) continue;
+        for (int k = 0; k < kBudgets; k++) {
+            double x = 0.0;
+            for (int bk = lane; bk < ncell_blocks; bk += 32) x = x + s.partials[((size_t)m * ncell_blocks + bk) * kBudgets + k];
+            for (int o = 16; o > 0; o >>= 1) x = x + __shfl_down_sync(0xffffffffu, x, o);
+            if (lane == 0) c.budget[k] = x;
+        }
+        __syncwarp();
+        if (lane == 0) {
+            c.nadd = c.nadd + c.dt;
+            c.it = c.it + 1;
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const int k = s.loop->k + 1;
+        s.loop->k = k;
+        s.loop->split = 0;
+        if (use_cond) cudaGraphSetConditional(h, (k < s.loop->ntmax && k < kNtCap) ? 1u : 0u);
+    }
+}
+
+}  // namespace cmf

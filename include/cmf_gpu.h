@@ -1,0 +1,230 @@
+/*
+ * cmf_gpu.h -- C ABI of the B200 CaMa-Flood physics time step.
+ *
+ * Drop-in boundary: the call `CALL CMF_PHYSICS_ADVANCE` at src/cmf_drv_advance_mod.F90:101
+ * is replaced by cmf_gpu_physics_advance() when the GPU switch is on.  Every pointer argument
+ * is a plain host pointer to the reference's own module arrays, passed with ISO_C_BINDING c_loc:
+ *   - (NSEQMAX,1) arrays are contiguous double[NSEQMAX] in sequence order;
+ *   - (NSEQMAX,1,NLFP) arrays are double[NLFP][NSEQMAX] (layer-major);
+ *   - (NPTHOUT,NPTHLEV) arrays are double[NPTHLEV][NPTHOUT];
+ *   - 2-D index tables I1UPST(NSEQMAX,UPNMAX), I1P_OUT(NSEQMAX,ONMAX), I1P_INF(NSEQMAX,INMAX)
+ *     are column-major int32 and hold 1-based indices, exactly as Fortran allocates them.
+ * Sequence and path indices stay 1-based at the boundary (I1NEXT keeps the negative river-mouth
+ * codes).  The library converts them once, in cmf_gpu_init, to its device layout.
+ *
+ * Ensembles: with nmembers > 1 every state, runoff and diagnostic array is member-major,
+ * [nmembers][NSEQMAX] (or [nmembers][NPTHLEV][NPTHOUT]); maps are shared by all members and
+ * each member runs its own adaptive time step.
+ *
+ * Status convention (no exceptions cross the ABI): 0 = ok; negative = configuration or
+ * unsupported option (the Fortran shim writes cmf_gpu_strerror() to LOGNAM and STOPs 9, as
+ * src/cmf_ctrl_nmlist_mod.F90:302 does); positive = device-side failure.
+ * Threading: call from the serial part of the host program; one CUDA stream per context;
+ * calls are synchronous from the caller's view except the *_async variants.
+ */
+#ifndef CMF_GPU_H
+#define CMF_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CMF_GPU_ABI_VERSION 1
+
+/* ---- status codes ------------------------------------------------------------------------ */
+#define CMF_OK                0
+#define CMF_E_ARG            -1  /* null pointer, bad size or inconsistent dimensions            */
+#define CMF_E_UNSUPPORTED    -2  /* option combination the GPU path does not implement           */
+#define CMF_E_STATE          -3  /* call out of order (no context, not initialised)              */
+#define CMF_E_IO             -4  /* host model core: a map, table or namelist could not be read  */
+#define CMF_E_CUDA            1  /* CUDA runtime error (message via cmf_gpu_last_error)          */
+#define CMF_E_NT_CAP          2  /* adaptive sub-step count above the cap (non-finite DT_MIN)     */
+#define CMF_E_NO_DEVICE       3  /* no CUDA device or the sm_100a kernels cannot run on it       */
+
+/* ---- dimensions (src/yos_cmf_map.F90, src/yos_cmf_input.F90) ----------------------------- */
+typedef struct cmf_dims {
+    int32_t nseqall;    /* NSEQALL: river cells followed by river mouths                        */
+    int32_t nseqriv;    /* NSEQRIV                                                               */
+    int32_t nseqmax;    /* NSEQMAX (== NSEQALL for the single-region build)                      */
+    int32_t nlfp;       /* NLFP floodplain layers                                                 */
+    int32_t upnmax;     /* second extent of I1UPST                                                */
+    int32_t npthout;    /* NPTHOUT (1 when LPTHOUT is off, as the reference allocates)           */
+    int32_t npthlev;    /* NPTHLEV                                                                */
+    int32_t onmax;      /* second extent of I1P_OUT                                               */
+    int32_t inmax;      /* second extent of I1P_INF                                               */
+    int32_t ndam;       /* NDAM (0 when LDAMOUT is off)                                          */
+    int32_t nmembers;   /* ensemble members sharing the network (1 = the reference's single run) */
+} cmf_dims;
+
+/* ---- physical parameters (NPARAM, src/cmf_ctrl_nmlist_mod.F90:227-241) ------------------- */
+typedef struct cmf_params {
+    double pgrv;        /* PGRV                                                                   */
+    double pmanfld;     /* PMANFLD                                                                */
+    double pdstmth;     /* PDSTMTH                                                                */
+    double pcadp;       /* PCADP                                                                  */
+    double pminslp;     /* PMINSLP                                                                */
+    double dfrcinc;     /* DFRCINC = NLFP**(-1)                                                   */
+} cmf_params;
+
+/* ---- options (NRUNVER logicals; 0/1) ----------------------------------------------------- */
+typedef struct cmf_opts {
+    int32_t ladpstp, lfldout, lpthout, ldamout, llevee, lspamat;
+    /* options the GPU path refuses (cmf_gpu_init returns CMF_E_UNSUPPORTED when any is set) */
+    int32_t lkine, lslpmix, lstg_es, lgdwdly, lrosplit, lwevap, lupsinf, lheatlink, ltrace, lslopemouth;
+    int32_t ldamh22;     /* Hanazaki-2022 dam rule instead of the default Yamazaki-Funato rule   */
+    int32_t ldamyby;     /* refused: year-by-year dam activation                                  */
+    int32_t ldiag;       /* accumulate the CMF_DIAG_*_ADPSTP averages/maxima on the device       */
+    int32_t launch_mode; /* 0: one CUDA graph per coupling step with a device-side sub-step loop;
+                            1: host-driven launches (reads NT back before the sub-steps)          */
+    int32_t device;      /* CUDA device ordinal                                                   */
+    int32_t block_size;  /* 0: autotune; else threads per block for the cell kernels             */
+} cmf_opts;
+
+/* ---- static maps: Fortran module arrays (read-only, host memory) ------------------------- */
+typedef struct cmf_map_ptrs {
+    const int32_t *i1next;      /* I1NEXT(NSEQMAX)            1-based, mouth codes negative       */
+    const int32_t *i1upst;      /* I1UPST(NSEQMAX,UPNMAX)     1-based, column-major               */
+    const int32_t *i1upn;       /* I1UPN(NSEQMAX)                                                  */
+    const int32_t *i2mask;      /* I2MASK(NSEQMAX,1)          0 normal, 1 dam-upstream, 2 dam      */
+    const double *rivelv, *elevtn, *nxtdst, *rivwth, *rivhgt, *rivlen, *rivman, *grarea;
+    const double *rivstomax;    /* D2RIVSTOMAX                                                     */
+    const double *dwnelv;       /* D2DWNELV (downstream boundary elevation at the mouths)          */
+    const double *fldstomax;    /* D2FLDSTOMAX(NSEQMAX,1,NLFP)                                     */
+    const double *fldgrd;       /* D2FLDGRD(NSEQMAX,1,NLFP)                                        */
+    const double *fldhgt;       /* D2FLDHGT(NSEQMAX,1,NLFP)   (levee scheme only)                 */
+    /* bifurcation (LPTHOUT) */
+    const int32_t *pth_upst, *pth_down;       /* PTH_UPST/PTH_DOWN(NPTHOUT) 1-based, <=0 outside  */
+    const double *pth_dst;                    /* PTH_DST(NPTHOUT)                                */
+    const double *pth_elv, *pth_wth;          /* PTH_ELV/PTH_WTH(NPTHOUT,NPTHLEV)                */
+    const double *pth_man;                    /* PTH_MAN(NPTHLEV)                                */
+    const int32_t *i1p_out, *i1p_outn, *i1p_inf, *i1p_infn;
+    /* levee (LLEVEE), src/cmf_ctrl_levee_mod.F90:31-44 */
+    const double *levhgt, *levfrc, *bashgt, *levdst, *levbassto, *levtopsto, *levfilsto;
+    /* dams (LDAMOUT), src/cmf_ctrl_damout_mod.F90:45-74 */
+    const int32_t *damseq;                    /* DamSeq(NDAM) 1-based or IMIS                    */
+    const int32_t *damstat;                   /* DamStat(NDAM)                                   */
+    const int32_t *i1dam;                     /* I1DAM(NSEQMAX)                                  */
+    const double *dam_qn, *dam_qf, *dam_qa, *dam_convol, *dam_fldvol, *dam_emevol;
+    const double *dam_norvol, *dam_adjvol, *dam_r_volupa;
+} cmf_map_ptrs;
+
+/* ---- prognostic state (src/yos_cmf_prog.F90); member-major when nmembers > 1 -------------- */
+typedef struct cmf_state_ptrs {
+    double *rivsto, *fldsto;                  /* P2RIVSTO, P2FLDSTO (FP64 storage)               */
+    double *rivout, *fldout;                  /* D2RIVOUT, D2FLDOUT                              */
+    double *rivout_pre, *fldout_pre;          /* D2RIVOUT_PRE, D2FLDOUT_PRE                      */
+    double *rivdph_pre, *fldsto_pre;          /* D2RIVDPH_PRE, D2FLDSTO_PRE                      */
+    double *pthflw, *pthflw_pre;              /* D1PTHFLW, D1PTHFLW_PRE (NPTHOUT,NPTHLEV)        */
+    double *damsto, *daminf;                  /* P2DAMSTO, P2DAMINF                              */
+    double *levsto;                           /* P2LEVSTO                                        */
+} cmf_state_ptrs;
+
+/* ---- diagnostics (src/yos_cmf_diag.F90); NULL entries are skipped ------------------------ */
+typedef struct cmf_diag_ptrs {
+    double *rivdph, *flddph, *fldfrc, *fldare, *sfcelv, *storge, *rivvel;
+    double *rivinf, *fldinf, *pthout, *outflw, *pthflwsum, *levdph;
+    /* adaptive-step averages and maxima after CMF_DIAG_GETAVE_ADPSTP (needs opts.ldiag) */
+    double *rivout_aavg, *fldout_aavg, *outflw_aavg, *rivvel_aavg, *pthout_aavg;
+    double *gdwrtn_aavg, *runoff_aavg, *rofsub_aavg, *daminf_aavg;
+    double *storge_amax, *outflw_amax, *rivdph_amax;
+    double *pthflw_aavg, *pthflwsum_aavg;
+} cmf_diag_ptrs;
+
+/* ---- water budget of the last sub-step (CALC_WATBAL, src/cmf_ctrl_physics_mod.F90:216-248) */
+typedef struct cmf_budget {
+    double stopre, stonxt, stonew, rivinf, rivout;       /* P0GLB* written by CMF_CALC_STONXT      */
+    double stopre2, stonew2, rivsto, fldsto, fldare;     /* P0GLB* written by the stage scheme     */
+    double levsto;                                       /* P0GLBLEVSTO (levee scheme)             */
+    double dam_miss;                                     /* DamMiss of CMF_DAMOUT_WATBAL           */
+} cmf_budget;
+
+typedef struct cmf_gpu_ctx cmf_gpu_ctx;
+
+/* ======================================================================================== */
+/* Context API (any number of contexts: regional domains, ensembles)                        */
+/* ======================================================================================== */
+
+/* Replaces the device-relevant part of CMF_DRV_INIT (src/cmf_drv_control_mod.F90:149-298):
+ * uploads the static maps, builds the upstream/path CSR tables and validates the options. */
+int cmf_gpu_create(const cmf_dims *dims, const cmf_params *params, const cmf_map_ptrs *maps,
+                   const cmf_opts *opts, cmf_gpu_ctx **out);
+int cmf_gpu_destroy(cmf_gpu_ctx *ctx);
+
+/* Host -> device copy of the prognostic state (after CMF_PROG_INIT / CMF_RESTART_INIT /
+ * CMF_DAMOUT_INIT, src/cmf_drv_control_mod.F90:237-252).  NULL members are left unchanged. */
+int cmf_gpu_ctx_set_state(cmf_gpu_ctx *ctx, const cmf_state_ptrs *st);
+/* Device -> host copy of the prognostic state (before output/restart,
+ * src/cmf_drv_advance_mod.F90:121-152).  NULL members are skipped. */
+int cmf_gpu_ctx_get_state(cmf_gpu_ctx *ctx, const cmf_state_ptrs *st);
+/* Runoff after CMF_FORCING_PUT (src/MAIN_cmf.F90:105): D2RUNOFF [m3/s]; rofsub may be NULL. */
+int cmf_gpu_ctx_put_runoff(cmf_gpu_ctx *ctx, const double *runoff, const double *rofsub);
+/* One outer step, CMF_PHYSICS_ADVANCE (src/cmf_ctrl_physics_mod.F90:21-153).  dt_def is DT.
+ * nt_out[nmembers], dt_out[nmembers] and budget_out[nmembers] may be NULL. */
+int cmf_gpu_ctx_physics_advance(cmf_gpu_ctx *ctx, double dt_def, int32_t *nt_out, double *dt_out,
+                                cmf_budget *budget_out);
+int cmf_gpu_ctx_get_diag(cmf_gpu_ctx *ctx, const cmf_diag_ptrs *dg);
+
+/* Device-resident pipeline (no host round trip): runoff already in device memory, ksteps outer
+ * steps enqueued on the context's stream; runoff_dev holds ksteps consecutive [nmembers][NSEQMAX]
+ * fields (or one field reused when runoff_stride is 0). */
+int cmf_gpu_ctx_advance_device(cmf_gpu_ctx *ctx, double dt_def, int32_t ksteps,
+                               const double *runoff_dev, int64_t runoff_stride);
+int cmf_gpu_ctx_synchronize(cmf_gpu_ctx *ctx);
+/* Per-member sub-step counts of the last outer step, read back from the device. */
+int cmf_gpu_ctx_last_nt(cmf_gpu_ctx *ctx, int32_t *nt_out, double *dt_out);
+/* CUDA stream (cudaStream_t) the context launches on, for event timing by the caller. */
+void *cmf_gpu_ctx_stream(cmf_gpu_ctx *ctx);
+/* Number of kernels this context launched so far (graph launches count their kernel nodes). */
+int64_t cmf_gpu_ctx_kernel_launches(cmf_gpu_ctx *ctx);
+/* Block size the autotuner chose for the cell kernels. */
+int32_t cmf_gpu_ctx_block_size(cmf_gpu_ctx *ctx);
+
+/* Split outer step for basin-region sharding across GPUs (one 8-byte MIN all-reduce of DT_MIN
+ * per outer step, src/cmf_ctrl_mpi_mod.F90:261-281): stage + local CFL minimum ... */
+int cmf_gpu_ctx_stage(cmf_gpu_ctx *ctx, double dt_def, double *dt_min_local);
+/* ... then the sub-steps with the globally reduced DT_MIN. */
+int cmf_gpu_ctx_substeps(cmf_gpu_ctx *ctx, double dt_def, double dt_min_global, int32_t *nt_out,
+                         double *dt_out, cmf_budget *budget_out);
+
+/* ======================================================================================== */
+/* Default-context API bound by the Fortran ISO_C_BINDING shim                              */
+/* ======================================================================================== */
+int cmf_gpu_init(const cmf_dims *dims, const cmf_params *params, const cmf_map_ptrs *maps,
+                 const cmf_opts *opts);
+int cmf_gpu_set_state(const cmf_state_ptrs *st);
+int cmf_gpu_get_state(const cmf_state_ptrs *st);
+int cmf_gpu_put_runoff(const double *runoff, const double *rofsub);
+int cmf_gpu_physics_advance(double dt_def, int32_t *nt_out, double *dt_out, cmf_budget *budget_out);
+int cmf_gpu_get_diag(const cmf_diag_ptrs *dg);
+void cmf_gpu_finalize(void);
+const char *cmf_gpu_strerror(int status);
+const char *cmf_gpu_last_error(void);
+int cmf_gpu_abi_version(void);
+
+/* ======================================================================================== */
+/* Host model core: the reference's CMF_DRV_INIT for a stand-alone (non-Fortran) host        */
+/* ======================================================================================== */
+typedef struct cmf_host_model cmf_host_model;
+
+/* Reads input_cmf.nam (NRUNVER/NDIMTIME/NPARAM/NMAP/NLEVEE/NDAMOUT), diminfo and the binary
+ * maps of casedir, then runs CMF_RIVMAP_INIT, CMF_TOPO_INIT, CMF_LEVEE_INIT, CMF_PROG_INIT,
+ * CMF_PHYSICS_FLDSTG (host copy) and CMF_DAMOUT_INIT in the reference's order. */
+int cmf_host_load(const char *casedir, const char *nmlfile, cmf_host_model **out);
+void cmf_host_free(cmf_host_model *hm);
+/* Fills the ABI structs with pointers into the host model (valid until cmf_host_free);
+ * opts gets the namelist logicals and the GPU defaults; *dt gets DT. */
+int cmf_host_describe(const cmf_host_model *hm, cmf_dims *dims, cmf_params *params,
+                      cmf_map_ptrs *maps, cmf_opts *opts, double *dt);
+/* Pointers to the host model's initialised prognostic arrays (single member). */
+int cmf_host_state(cmf_host_model *hm, cmf_state_ptrs *st);
+/* CONV_RESOL (src/cmf_ctrl_forcing_mod.F90:795-831): runoff map [mm/dt, NX*NY] -> m3/s. */
+int cmf_host_conv_resol(const cmf_host_model *hm, const double *map, double *runoff_out);
+/* Grid position of every sequence cell (I1SEQX/I1SEQY, 1-based) and the grid size. */
+int cmf_host_grid(const cmf_host_model *hm, int32_t *nx, int32_t *ny, int32_t *i1seqx, int32_t *i1seqy);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CMF_GPU_H */

@@ -1,0 +1,108 @@
+"""ctypes wrapper of the CPU oracle (cmf_oracle.c).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and bench.py's CPU-baseline
+and reference arms as the checker.  The product never imports this module.
+
+Parity is unpinned: the reference (Fortran 90) cannot be compiled on this machine and ships no
+golden vectors for the physics step; see the header of cmf_oracle.c.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIBS: dict = {}
+
+
+def build() -> None:
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+
+
+def _lib(omp: bool = False):
+    key = "omp" if omp else "serial"
+    if key in _LIBS:
+        return _LIBS[key]
+    path = os.path.join(_HERE, "_build", "libcmf_oracle_omp.so" if omp else "libcmf_oracle.so")
+    if not os.path.exists(path):
+        build()
+    lib = C.CDLL(path)
+    lib.orc_create.restype = C.c_void_p
+    lib.orc_create.argtypes = [C.c_char_p, C.c_char_p, C.c_char_p, C.c_int]
+    lib.orc_physics_advance.argtypes = [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_double)]
+    lib.orc_physics_advance.restype = C.c_int
+    lib.orc_put_runoff_vec.argtypes = [C.c_void_p, C.POINTER(C.c_double)]
+    lib.orc_put_runoff_map.argtypes = [C.c_void_p, C.POINTER(C.c_double)]
+    lib.orc_dims.argtypes = [C.c_void_p, C.POINTER(C.c_int)]
+    lib.orc_budget.argtypes = [C.c_void_p, C.POINTER(C.c_double)]
+    lib.orc_darray.restype = C.POINTER(C.c_double)
+    lib.orc_darray.argtypes = [C.c_void_p, C.c_char_p, C.POINTER(C.c_int)]
+    lib.orc_iarray.restype = C.POINTER(C.c_int)
+    lib.orc_iarray.argtypes = [C.c_void_p, C.c_char_p, C.POINTER(C.c_int)]
+    lib.orc_threads.restype = C.c_int
+    _LIBS[key] = lib
+    return lib
+
+
+class Oracle:
+    """One CaMa-Flood model instance initialised exactly like CMF_DRV_INIT."""
+
+    def __init__(self, casedir: str, nml: str = "input_cmf.nam", omp: bool = False):
+        self.lib = _lib(omp)
+        err = C.create_string_buffer(256)
+        self.h = self.lib.orc_create(casedir.encode(), nml.encode(), err, 256)
+        if not self.h:
+            raise RuntimeError("oracle init failed: " + err.value.decode())
+        d = (C.c_int * 11)()
+        self.lib.orc_dims(self.h, d)
+        (self.nx, self.ny, self.nlfp, self.nseqmax, self.nseqall, self.nseqriv,
+         self.npthout, self.npthlev, self.ndam, self.upnmax, _) = list(d)
+
+    def threads(self) -> int:
+        return int(self.lib.orc_threads())
+
+    def put_runoff(self, runoff_m3s: np.ndarray) -> None:
+        a = np.ascontiguousarray(runoff_m3s, dtype=np.float64)
+        assert a.shape == (self.nseqmax,)
+        self.lib.orc_put_runoff_vec(self.h, a.ctypes.data_as(C.POINTER(C.c_double)))
+
+    def put_runoff_map(self, runoff_map: np.ndarray) -> None:
+        a = np.ascontiguousarray(runoff_map, dtype=np.float64).ravel()
+        assert a.size == self.nx * self.ny
+        self.lib.orc_put_runoff_map(self.h, a.ctypes.data_as(C.POINTER(C.c_double)))
+
+    def advance(self):
+        nt = C.c_int(0)
+        dt = C.c_double(0.0)
+        rc = self.lib.orc_physics_advance(self.h, C.byref(nt), C.byref(dt))
+        if rc:
+            raise RuntimeError(f"oracle advance failed rc={rc}")
+        return nt.value, dt.value
+
+    def budget(self) -> dict:
+        b = (C.c_double * 15)()
+        self.lib.orc_budget(self.h, b)
+        k = ["stopre", "stonxt", "stonew", "rivinf", "rivout", "stopre2", "stonew2", "rivsto", "fldsto",
+             "fldare", "levsto", "dam_miss", "dt", "dt_min", "nadd"]
+        return dict(zip(k, list(b)))
+
+    def d(self, name: str) -> np.ndarray:
+        n = C.c_int(0)
+        p = self.lib.orc_darray(self.h, name.encode(), C.byref(n))
+        if n.value < 0:
+            raise KeyError(name)
+        if n.value == 0:
+            return np.zeros(0)
+        return np.ctypeslib.as_array(p, shape=(n.value,)).copy()
+
+    def i(self, name: str) -> np.ndarray:
+        n = C.c_int(0)
+        p = self.lib.orc_iarray(self.h, name.encode(), C.byref(n))
+        if n.value < 0:
+            raise KeyError(name)
+        if n.value == 0:
+            return np.zeros(0, dtype=np.int32)
+        return np.ctypeslib.as_array(p, shape=(n.value,)).copy()
