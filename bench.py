@@ -1,0 +1,397 @@
+"""Benchmark of the B200 CaMa-Flood physics time step (CMF_PHYSICS_ADVANCE) on the config-1 workload.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--members M]
+
+One step is one coupling step (one hour of the config-1 forcing): the stage scheme, the CFL
+reduction and NT local-inertial sub-steps over the 1440x720-grid network of ~300k cells with
+12k bifurcation channels x 5 levels, levees on 10% of cells and 2000 dams.  The case is generated
+from a fixed seed in the reference's file formats (synthetic data; no dataset is read).
+
+Metric: cell-substeps/s = sum over steps and members of NSEQALL * NT / time.
+  value     device-resident: runoff already in HBM, one CUDA graph per step, CUDA events on the
+            library's stream, L2 flushed (256 MiB write) before every timed step;
+  e2e       the public API with host buffers: put_runoff (pinned host -> device), advance, and a
+            device -> host read of the step's averaged discharge, timed on the host clock.
+--impl reference times the reference algorithm's CPU implementation (the oracle restatement with
+OpenMP on all host cores; the Fortran reference itself cannot be compiled on this machine).
+Under torchrun every rank runs its own member(s) of the ensemble (weak scaling, no collective on
+the data path); rank 0 prints one JSON line.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path[:0] = [os.path.join(ROOT, "cama-flood_v4_b200"), os.path.join(ROOT, "oracle")]
+
+METRIC = "cell-steps/s on 1 B200: plain GPU vs surrogate-assisted at <=1% NSE loss; HBM GB/s"
+UNIT = "cell-substeps/s"
+CASE_CACHE = os.environ.get("CMF_BENCH_CASES", "/tmp/cmf_bench_cases")
+SPINUP_STEPS = 24
+
+
+# ----------------------------------------------------------------------------------------- setup
+def case_dir(name: str = "cfg1") -> str:
+    from cmf_b200 import synth
+
+    d = os.path.join(CASE_CACHE, name)
+    if not os.path.exists(os.path.join(d, "input_cmf.nam")):
+        spec = synth.spec_config1(seed=1) if name == "cfg1" else synth.spec_config0(seed=0)
+        tmp = d + f".tmp{os.getpid()}"
+        synth.write_case(synth.make_case(spec), tmp)
+        try:
+            os.rename(tmp, d)
+        except OSError:
+            pass   # another rank won the race; the contents are identical (same seed)
+    return d
+
+
+def runoff_fields(grarea: np.ndarray, nsteps: int, seed: int) -> np.ndarray:
+    """Hourly AR(1) phi=0.9 Gaussian-copula Gamma(0.8, 2.5 mm/day) runoff -> m3/s (CONV_RESOL)."""
+    from cmf_b200 import synth
+
+    gen = synth.AR1GammaRunoff(grarea.size, seed)
+    out = np.empty((nsteps, grarea.size))
+    for k in range(nsteps):
+        out[k] = np.maximum((gen.next().astype(np.float64) * grarea) / 86400000.0, 0.0)
+    return out
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+class ClockSampler:
+    """nvidia-smi sampling (200 ms) during the timed region."""
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            p = [x.strip() for x in ln.split(",")]
+            if len(p) < 8:
+                continue
+            try:
+                sm.append(float(p[1]))
+                mx.append(float(p[2]))
+            except ValueError:
+                continue
+            for k, nm in enumerate(names):
+                if p[4 + k].lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(mx)), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peaks() -> dict:
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return {"hbm_gbs": d.get("hbm_gbs", 6650.0), "source": "measured"}
+    return {"hbm_gbs": 6650.0, "source": "fallback"}
+
+
+def profiled_traffic(kernel: str):
+    """Per-launch DRAM bytes of `kernel` from the committed ncu summary, scaled to the bench
+    workload (the summary states the captured case's cells and the scaling rule)."""
+    p = os.path.join(ROOT, "profiles", f"ncu_{kernel}.md")
+    if not os.path.exists(p):
+        return None
+    txt = open(p).read()
+    m = re.search(r"dram_bytes_per_cell:\s*([0-9.eE+-]+)", txt)
+    return float(m.group(1)) if m else None
+
+
+# ----------------------------------------------------------------------------- algorithmic bytes
+def phase_bytes(N: int, E: int, L_bar: float, P: int, Lp: int, nlev: int, ndam: int, ldiag: bool) -> dict:
+    """Compulsory HBM bytes per launch of each sub-step kernel (every array element the kernel must
+    read or write once; gathers of neighbour values are L2 reuse and not counted again).
+      k_flux : static 7x8 (RIVELV ELEVTN NXTDST RIVWTH RIVHGT RIVLEN RIVMAN) + I1NEXT 4 + state reads
+               8x8 (RIVDPH RIVDPH_PRE RIVOUT_PRE FLDOUT_PRE FLDSTO FLDDPH FLDSTO_PRE STORGE)
+               + writes 3x8 (RIVOUT FLDOUT RIVVEL)                                  = 148 B/cell
+               + per path: endpoints 8, DST 8, skip 4, ELV/WTH/FLW_PRE/FLW 32 x Lp, FLWSUM 8
+      k_rate : RIVOUT FLDOUT 16 + CSR 4 + 4/edge + RIVSTO FLDSTO 16 + RATE 8        = 48 B/cell
+               + path CSR 8 and FLWSUM 8 per path end
+      k_store: RIVOUT FLDOUT RATE 24 + CSR 8 + I1NEXT 4 + RIVSTO FLDSTO RIVDPH FLDFRC RUNOFF 40
+               + RIVSTOMAX RIVLEN RIVWTH GRAREA RIVELV 40 + layers 16 L_bar + writes 12x8 96
+               (_PRE x4, RIVSTO FLDSTO RIVDPH FLDDPH FLDFRC FLDARE SFCELV STORGE) + RIVINF FLDINF
+               PTHOUT OUTFLW 32 + diagnostics 9 accumulators r/w + RIVVEL read 152   = 244+16 L_bar (+152)
+               + levee: index 4/cell + 7 params + LEVSTO r/w + LEVDPH w per levee cell
+               + dams: 112 B per dam, paths: FLW r/w 16 x Lp + FLWSUM 16 per path"""
+    flux = N * 148 + P * (8 + 8 + 4 + 32 * Lp + 8) + ndam * 112
+    rate = N * 48 + (E - N) * 4 + P * 2 * (8 + 8)
+    store = N * (244 + 16 * L_bar + (152 if ldiag else 0)) + N * 4 + nlev * (7 * 8 + 16 + 8) + ndam * 112 + P * (16 * Lp + 16)
+    return {"k_flux": flux, "k_rate": rate, "k_store": store}
+
+
+def mean_layers(state: dict, fldstomax: np.ndarray, rivstomax: np.ndarray, N: int, L: int) -> float:
+    """Mean floodplain layers the stage scheme scans per cell (0 for in-bank cells)."""
+    tot = state["rivsto"][0] + state["fldsto"][0] + state.get("levsto", np.zeros((1, N)))[0]
+    fsm = fldstomax.reshape(L, N)
+    flooded = tot > rivstomax
+    scanned = np.sum(tot[None, :] > fsm, axis=0) + 1
+    scanned = np.minimum(scanned, L)
+    return float(np.mean(np.where(flooded, scanned, 0)))
+
+
+# ------------------------------------------------------------------------------------- CPU arms
+def cpu_run(cdir: str, nsteps: int, warmup: int, seed: int, omp: bool = True, budget_s: float = 25.0):
+    """Runs the oracle on the bench workload from the same initial state and forcing; returns
+    (cell-substeps, seconds, threads, steps actually timed)."""
+    from oracle import Oracle
+
+    o = Oracle(cdir, omp=omp)
+    gr = o.d("grarea")
+    fields = runoff_fields(gr, warmup + nsteps, seed)
+    for k in range(warmup):
+        o.put_runoff(fields[k])
+        o.advance()
+    sub = 0
+    done = 0
+    t0 = time.perf_counter()
+    for k in range(warmup, warmup + nsteps):
+        o.put_runoff(fields[k])
+        nt, _ = o.advance()
+        sub += nt
+        done += 1
+        if time.perf_counter() - t0 > budget_s:
+            break
+    el = time.perf_counter() - t0
+    return o.nseqall * sub, el, o.threads(), done
+
+
+def reference_arm(args) -> int:
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return 0
+    cdir = case_dir("cfg1")
+    os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count() or 1))
+    os.environ.setdefault("OMP_PROC_BIND", "close")
+    cells, secs, threads, done = cpu_run(cdir, args.steps, args.warmup, seed=1, omp=True, budget_s=120.0)
+    v = cells / secs
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": done,
+        "warmup": args.warmup, "ms_per_step": secs / max(done, 1) * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded config-1 case)",
+        "config": {"workload": "config1: 1440x720 grid, 299157 cells, 12k bifurcation x5, levees 10%, 2000 dams, hourly AR(1) forcing",
+                   "members": 1},
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": f"{done} consecutive coupling steps after {args.warmup} warm-up steps, OpenMP oracle"},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+# -------------------------------------------------------------------------------------- GPU arm
+def gpu_arm(args) -> int:
+    import torch
+
+    ws, rank, local = dist_env()
+    if ws > 1:
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+    torch.cuda.set_device(local)
+    from cmf_b200 import HostModel, PhysicsGPU
+
+    cdir = case_dir("cfg1")
+    if ws > 1:
+        dist.barrier()
+    h = HostModel(cdir)
+    M = args.members
+    g = PhysicsGPU(h, nmembers=M, device=local)
+    N = h.dims.nseqall
+    gr = h.map("grarea")
+    W, K = args.warmup, args.steps
+    total = SPINUP_STEPS + W + 2 * K
+    fields = np.stack([runoff_fields(gr, total, seed=1 + 1000 * rank + m) for m in range(M)], axis=1)  # [T][M][N]
+    dev = torch.device("cuda", local)
+    runoff_dev = torch.from_numpy(fields).to(dev)
+    runoff_host = torch.from_numpy(fields).pin_memory()
+    stride = M * N
+    stream = torch.cuda.ExternalStream(g.stream, device=dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.int32, device=dev)
+
+    # spin-up and warm-up (device pipeline)
+    g.advance_device(SPINUP_STEPS + W, runoff_dev.data_ptr(), stride)
+    g.synchronize()
+
+    # ---- timed region: device-resident
+    c0 = g.counters()
+    l0 = g.kernel_launches
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(K)]
+    if ws > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        base = SPINUP_STEPS + W
+        for k in range(K):
+            with torch.cuda.stream(stream):
+                flush.fill_(k)
+                evs[k][0].record(stream)
+            g.advance_device(1, runoff_dev.data_ptr() + (base + k) * stride * 8, stride)
+            with torch.cuda.stream(stream):
+                evs[k][1].record(stream)
+        torch.cuda.synchronize()
+        g.synchronize()
+    ms = sum(a.elapsed_time(b) for a, b in evs)
+    c1 = g.counters()
+    member_sub = c1["member_substeps"] - c0["member_substeps"]
+    loop_iters = c1["loop_iters"] - c0["loop_iters"]
+    launches = 2 * K + 4 * loop_iters
+    secs = ms / 1e3
+    if ws > 1:
+        t = torch.tensor([secs], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        secs = float(t.item())
+        tot = torch.tensor([float(member_sub)], device=dev, dtype=torch.float64)
+        dist.all_reduce(tot, op=dist.ReduceOp.SUM)
+        member_sub_all = tot.item()
+    else:
+        member_sub_all = member_sub
+    value = N * member_sub_all / secs
+
+    # ---- e2e through the public API with host buffers
+    dsum = {"outflw_aavg": np.zeros(M * N)}
+    e2e_sub = 0
+    if ws > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for k in range(K):
+        g.put_runoff(runoff_host[SPINUP_STEPS + W + K + k].numpy())
+        nt, _, _ = g.advance()
+        e2e_sub += int(nt.sum())
+        g.get_diag_fields(dsum)
+    e2e_secs = time.perf_counter() - t0
+    if ws > 1:
+        t = torch.tensor([e2e_secs], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_secs = float(t.item())
+        tot = torch.tensor([float(e2e_sub)], device=dev, dtype=torch.float64)
+        dist.all_reduce(tot, op=dist.ReduceOp.SUM)
+        e2e_sub = tot.item()
+    e2e_value = N * e2e_sub / e2e_secs
+
+    # ---- roofline of the dominant kernel, timed live on the library's stream
+    st = g.get_state()
+    Lbar = mean_layers(st, h.map("fldstomax"), h.map("rivstomax"), N, h.dims.nlfp)
+    phases = g.time_phases(reps=10)
+    E = int(h.map("i1upn").sum())
+    P = g.P
+    Lp = g.Lp
+    nlev = int(np.sum(h.map("levbassto") < 1e17)) if h.opts.llevee else 0
+    ndam = h.dims.ndam
+    pb = phase_bytes(N, E, Lbar, P, Lp, nlev, ndam, True)
+    per_sub_ms = {k: phases[k] for k in ("k_flux", "k_rate", "k_store")}
+    dominant = max(per_sub_ms, key=per_sub_ms.get)
+    peaks = measured_peaks()
+    achieved = pb[dominant] * M / (per_sub_ms[dominant] * 1e-3) / 1e9
+    dpc = profiled_traffic(dominant)
+    roof = {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+            "frac": achieved / peaks["hbm_gbs"], "traffic": (dpc * N * M if dpc else None),
+            "kernel": dominant, "peak_source": peaks["source"] + " (hbm_gbs, burst copy)",
+            "algorithmic_bytes_per_launch": pb[dominant] * M,
+            "kernel_ms": {k: round(v, 5) for k, v in phases.items()},
+            "L_bar": Lbar,
+            "step_achieved_gbs": sum(pb.values()) * M * (loop_iters / max(K, 1)) / (secs / K) / 1e9}
+
+    out = 0
+    if rank == 0:
+        cpu = None
+        if ws == 1 and not args.no_cpu:
+            os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count() or 1))
+            cells, csecs, threads, done = cpu_run(cdir, 200, 2, seed=1, omp=True, budget_s=20.0)
+            cpu = {"value": cells / csecs, "unit": UNIT, "cores": threads, "kind": "port",
+                   "sample": f"{done} consecutive config-1 coupling steps (after 2 warm-up) of the OpenMP oracle, "
+                             f"{csecs:.1f} s on {threads} host threads"}
+        clocks = clk.summary()
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": K, "warmup": W,
+            "ms_per_step": secs / K * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic (seeded config-1 case in the reference's map formats)",
+            "config": {"workload": "config1: 1440x720 grid, 299157 cells, 12k bifurcation x5, levees 10%, 2000 dams, hourly AR(1) forcing",
+                       "members_per_gpu": M, "parallelism": f"ensemble members sharded over {ws} GPU(s), no collective",
+                       "l2": "256 MiB buffer written before every timed step", "nt_mean": member_sub / max(K * M, 1),
+                       "block_size": g.block_size, "launch": "one CUDA graph per coupling step, device-side sub-step loop"},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": M * N * 8,
+                    "d2h_bytes_per_step": M * N * 8 + M * 160},
+            "gpu_launches": int(launches),
+            "roofline": roof,
+            "cpu_baseline": cpu,
+            "clocks": clocks,
+        }
+        print(json.dumps(line))
+    if ws > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    g.close()
+    return out
+
+
+def main() -> int:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--members", type=int, default=1)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return reference_arm(args)
+    return gpu_arm(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -81,7 +81,7 @@ EXPORTS = [
     "cmf_gpu_create", "cmf_gpu_destroy", "cmf_gpu_ctx_set_state", "cmf_gpu_ctx_get_state", "cmf_gpu_ctx_put_runoff",
     "cmf_gpu_ctx_physics_advance", "cmf_gpu_ctx_get_diag", "cmf_gpu_ctx_advance_device", "cmf_gpu_ctx_synchronize",
     "cmf_gpu_ctx_last_nt", "cmf_gpu_ctx_stream", "cmf_gpu_ctx_kernel_launches", "cmf_gpu_ctx_block_size",
-    "cmf_gpu_ctx_stage", "cmf_gpu_ctx_substeps",
+    "cmf_gpu_ctx_stage", "cmf_gpu_ctx_substeps", "cmf_gpu_ctx_counters", "cmf_gpu_ctx_time_phases",
     "cmf_gpu_init", "cmf_gpu_set_state", "cmf_gpu_get_state", "cmf_gpu_put_runoff", "cmf_gpu_physics_advance",
     "cmf_gpu_get_diag", "cmf_gpu_finalize", "cmf_gpu_strerror", "cmf_gpu_last_error", "cmf_gpu_abi_version",
     "cmf_host_load", "cmf_host_free", "cmf_host_describe", "cmf_host_state", "cmf_host_conv_resol", "cmf_host_grid",
@@ -123,6 +123,15 @@ def load(build_if_missing: bool = True):
     lib.cmf_gpu_ctx_block_size.argtypes = [vp]
     lib.cmf_gpu_ctx_stage.argtypes = [vp, C.c_double, f64p]
     lib.cmf_gpu_ctx_substeps.argtypes = [vp, C.c_double, C.c_double, i32p, f64p, C.POINTER(Budget)]
+    lib.cmf_gpu_ctx_counters.argtypes = [vp, C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
+    lib.cmf_gpu_ctx_time_phases.argtypes = [vp, C.c_double, C.c_int32, f64p]
+    lib.cmf_gpu_init.argtypes = [C.POINTER(Dims), C.POINTER(Params), C.POINTER(MapPtrs), C.POINTER(Opts)]
+    lib.cmf_gpu_set_state.argtypes = [C.POINTER(StatePtrs)]
+    lib.cmf_gpu_get_state.argtypes = [C.POINTER(StatePtrs)]
+    lib.cmf_gpu_put_runoff.argtypes = [f64p, f64p]
+    lib.cmf_gpu_physics_advance.argtypes = [C.c_double, i32p, f64p, C.POINTER(Budget)]
+    lib.cmf_gpu_get_diag.argtypes = [C.POINTER(DiagPtrs)]
+    lib.cmf_gpu_strerror.argtypes = [C.c_int]
     lib.cmf_gpu_strerror.restype = C.c_char_p
     lib.cmf_gpu_last_error.restype = C.c_char_p
     lib.cmf_host_load.argtypes = [C.c_char_p, C.c_char_p, C.POINTER(vp)]

@@ -205,6 +205,17 @@ class PhysicsGPU:
         check(self.lib.cmf_gpu_ctx_last_nt(self.h, nt.ctypes.data_as(_abi.i32p), dt.ctypes.data_as(_abi.f64p)), "last_nt")
         return nt, dt
 
+    def counters(self):
+        a, b, c = C.c_int64(), C.c_int64(), C.c_int64()
+        check(self.lib.cmf_gpu_ctx_counters(self.h, C.byref(a), C.byref(b), C.byref(c)), "counters")
+        return {"member_substeps": a.value, "loop_iters": b.value, "outer_steps": c.value}
+
+    def time_phases(self, reps: int = 10, dt_def: float | None = None) -> dict:
+        dt_def = self.host.dt if dt_def is None else dt_def
+        ms = np.zeros(6)
+        check(self.lib.cmf_gpu_ctx_time_phases(self.h, dt_def, reps, ms.ctypes.data_as(_abi.f64p)), "time_phases")
+        return dict(zip(["k_stage", "k_ntdt", "k_flux", "k_rate", "k_store", "k_ctl"], ms.tolist()))
+
     @property
     def stream(self) -> int:
         return int(self.lib.cmf_gpu_ctx_stream(self.h) or 0)
@@ -233,6 +244,16 @@ class PhysicsGPU:
             setattr(dp, n, a.ctypes.data_as(_abi.f64p))
         check(self.lib.cmf_gpu_ctx_get_diag(self.h, C.byref(dp)), "get_diag")
         return {k: v.reshape(self.M, -1) for k, v in out.items()}
+
+    def get_diag_fields(self, out: dict) -> dict:
+        """Copies only the named diagnostics into the caller's float64 arrays (others skipped)."""
+        dp = _abi.DiagPtrs()
+        for n, a in out.items():
+            if n not in _abi.DIAG_FIELDS or a.dtype != np.float64 or not a.flags.c_contiguous:
+                raise ValueError(n)
+            setattr(dp, n, a.ctypes.data_as(_abi.f64p))
+        check(self.lib.cmf_gpu_ctx_get_diag(self.h, C.byref(dp)), "get_diag")
+        return out
 
     def close(self) -> None:
         if self.h:

@@ -596,9 +596,61 @@ int cmf_gpu_ctx_set_state(cmf_gpu_ctx *c, const cmf_state_ptrs *p) {
     }
     // D2RIVOUT may differ from D2RIVOUT_PRE (restart): the first sub-step reads the host copy
     cmf::LoopCtl lc{};
+    CUDA_TRY(cudaMemcpyAsync(&lc, s.loop, sizeof lc, cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
     lc.split = 1;
     CUDA_TRY(cudaMemcpyAsync(s.loop, &lc, sizeof lc, cudaMemcpyHostToDevice, c->stream));
     CUDA_TRY(cudaStreamSynchronize(c->stream));
+    return CMF_OK;
+}
+
+int cmf_gpu_ctx_counters(cmf_gpu_ctx *c, int64_t *member_substeps, int64_t *loop_iters, int64_t *outer_steps) {
+    if (!c) return set_err(CMF_E_STATE, "no context");
+    CUDA_TRY(cudaSetDevice(c->device));
+    cmf::LoopCtl lc{};
+    CUDA_TRY(cudaMemcpyAsync(&lc, c->st.loop, sizeof lc, cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    if (member_substeps) *member_substeps = lc.member_substeps;
+    if (loop_iters) *loop_iters = lc.loop_iters;
+    if (outer_steps) *outer_steps = lc.outer_steps;
+    return CMF_OK;
+}
+
+int cmf_gpu_ctx_time_phases(cmf_gpu_ctx *c, double dt_def, int32_t reps, double *ms_out) {
+    // Runs `reps` one-sub-step outer steps kernel by kernel with CUDA events between the kernels
+    // on the context's stream; ms_out[0..5] = mean ms of k_stage, k_ntdt, k_flux, k_rate, k_store, k_ctl.
+    if (!c || reps <= 0 || !ms_out) return set_err(CMF_E_ARG, "bad argument");
+    CUDA_TRY(cudaSetDevice(c->device));
+    int rc;
+    if ((rc = sync_dt_def(c, dt_def))) return rc;
+    cudaEvent_t ev[7];
+    for (auto &e : ev) CUDA_TRY(cudaEventCreate(&e));
+    double acc[6] = {0, 0, 0, 0, 0, 0};
+    const dim3 gc(c->ncell_blocks, c->dims.nmembers), gcp(c->ncell_blocks + c->npath_blocks, c->dims.nmembers);
+    for (int r = 0; r < reps; r++) {
+        CUDA_TRY(cudaEventRecord(ev[0], c->stream));
+        cmf::k_stage<<<gc, c->block, 0, c->stream>>>(c->net, c->st);
+        CUDA_TRY(cudaEventRecord(ev[1], c->stream));
+        cmf::k_ntdt<<<1, 256, 0, c->stream>>>(c->net, c->st, c->cond, 0);
+        CUDA_TRY(cudaEventRecord(ev[2], c->stream));
+        cmf::k_flux<<<gcp, c->block, 0, c->stream>>>(c->net, c->st, c->ncell_blocks);
+        CUDA_TRY(cudaEventRecord(ev[3], c->stream));
+        cmf::k_rate<<<gc, c->block, 0, c->stream>>>(c->net, c->st);
+        CUDA_TRY(cudaEventRecord(ev[4], c->stream));
+        cmf::k_store<<<gcp, c->block, 0, c->stream>>>(c->net, c->st, c->ncell_blocks);
+        CUDA_TRY(cudaEventRecord(ev[5], c->stream));
+        cmf::k_ctl<<<1, 256, 0, c->stream>>>(c->net, c->st, c->ncell_blocks, c->cond, 0);
+        CUDA_TRY(cudaEventRecord(ev[6], c->stream));
+        CUDA_TRY(cudaEventSynchronize(ev[6]));
+        for (int k = 0; k < 6; k++) {
+            float ms = 0.f;
+            CUDA_TRY(cudaEventElapsedTime(&ms, ev[k], ev[k + 1]));
+            acc[k] += ms;
+        }
+        c->launches += 6;
+    }
+    for (auto &e : ev) cudaEventDestroy(e);
+    for (int k = 0; k < 6; k++) ms_out[k] = acc[k] / reps;
     return CMF_OK;
 }
 

@@ -47,6 +47,9 @@ struct LoopCtl {
     int ntmax;        // max NT over members
     int err;
     int split;        // 1 until the first sub-step after a host state upload: D2RIVOUT /= D2RIVOUT_PRE
+    long long member_substeps;   // sum over outer steps and members of NT (throughput accounting)
+    long long loop_iters;        // sum over outer steps of NTmax (kernel-launch accounting)
+    long long outer_steps;
 };
 
 // Static data shared by all members (device pointers).
@@ -356,6 +359,7 @@ __global__ void k_stage(Net n, State s) {
 __global__ void k_ntdt(Net n, State s, cudaGraphConditionalHandle h, int use_cond) {
     __shared__ int smax[32];
     int ntmax = 1;
+    long long ntsum = 0;
     for (int m = threadIdx.x; m < n.M; m += blockDim.x) {
         MemberCtl &c = s.ctl[m];
         const double dt_def = c.dt_def;
@@ -381,16 +385,25 @@ __global__ void k_ntdt(Net n, State s, cudaGraphConditionalHandle h, int use_con
         c.it = 0;
         c.nadd = 0.0;
         ntmax = max(ntmax, nt);
+        ntsum += nt;
     }
-    for (int o = 16; o > 0; o >>= 1) ntmax = max(ntmax, __shfl_down_sync(0xffffffffu, ntmax, o));
-    if ((threadIdx.x & 31) == 0) smax[threadIdx.x >> 5] = ntmax;
+    __shared__ long long ssum[32];
+    for (int o = 16; o > 0; o >>= 1) {
+        ntmax = max(ntmax, __shfl_down_sync(0xffffffffu, ntmax, o));
+        ntsum += __shfl_down_sync(0xffffffffu, ntsum, o);
+    }
+    if ((threadIdx.x & 31) == 0) { smax[threadIdx.x >> 5] = ntmax; ssum[threadIdx.x >> 5] = ntsum; }
     __syncthreads();
     if (threadIdx.x == 0) {
         int v = 1;
-        for (int w = 0; w < (int)((blockDim.x + 31) >> 5); w++) v = max(v, smax[w]);
+        long long tot = 0;
+        for (int w = 0; w < (int)((blockDim.x + 31) >> 5); w++) { v = max(v, smax[w]); tot += ssum[w]; }
         v = min(v, kNtCap);
         s.loop->k = 0;
         s.loop->ntmax = v;
+        s.loop->member_substeps += tot;
+        s.loop->loop_iters += v;
+        s.loop->outer_steps += 1;
         if (use_cond) cudaGraphSetConditional(h, 1u);
     }
 }

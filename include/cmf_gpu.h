@@ -180,6 +180,13 @@ void *cmf_gpu_ctx_stream(cmf_gpu_ctx *ctx);
 int64_t cmf_gpu_ctx_kernel_launches(cmf_gpu_ctx *ctx);
 /* Block size the autotuner chose for the cell kernels. */
 int32_t cmf_gpu_ctx_block_size(cmf_gpu_ctx *ctx);
+/* Device-side counters since creation: sum over outer steps and members of NT, sum over outer
+ * steps of max NT (sub-step loop iterations) and the number of outer steps. */
+int cmf_gpu_ctx_counters(cmf_gpu_ctx *ctx, int64_t *member_substeps, int64_t *loop_iters, int64_t *outer_steps);
+/* Measurement helper: runs `reps` single-sub-step outer steps kernel by kernel with CUDA events
+ * between kernels on the context's stream (advances the state).  ms_out[6] receives the mean
+ * duration of the stage/CFL, NT/DT, flux, rate, storage and control kernels. */
+int cmf_gpu_ctx_time_phases(cmf_gpu_ctx *ctx, double dt_def, int32_t reps, double *ms_out);
 
 /* Split outer step for basin-region sharding across GPUs (one 8-byte MIN all-reduce of DT_MIN
  * per outer step, src/cmf_ctrl_mpi_mod.F90:261-281): stage + local CFL minimum ... */
