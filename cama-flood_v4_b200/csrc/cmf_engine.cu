@@ -751,13 +751,16 @@ int cmf_gpu_ctx_stage(cmf_gpu_ctx *c, double dt_def, double *dt_min_local) {
     CUDA_TRY(cudaGetLastError());
     c->launches += 1;
     if ((rc = read_ctl(c))) return rc;
-    if (dt_min_local) {
-        for (size_t m = 0; m < c->hctl.size(); m++) {
-            double v;
-            std::memcpy(&v, &c->hctl[m].dtmin_bits, sizeof v);
-            dt_min_local[m] = std::min(v, dt_def);
-        }
+    unsigned long long def_bits;
+    std::memcpy(&def_bits, &dt_def, sizeof def_bits);
+    for (size_t m = 0; m < c->hctl.size(); m++) {
+        double v;
+        std::memcpy(&v, &c->hctl[m].dtmin_bits, sizeof v);
+        if (dt_min_local) dt_min_local[m] = std::min(v, dt_def);
+        c->hctl[m].dtmin_bits = def_bits;   // the next stage starts its minimum from DT again
     }
+    CUDA_TRY(cudaMemcpyAsync(c->st.ctl, c->hctl.data(), c->hctl.size() * sizeof(cmf::MemberCtl), cudaMemcpyHostToDevice, c->stream));
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
     return CMF_OK;
 }
 
