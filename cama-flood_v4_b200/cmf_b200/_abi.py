@@ -77,6 +77,14 @@ class Budget(C.Structure):
     _fields_ = [(n, C.c_double) for n in BUDGET_FIELDS]
 
 
+class StageDevArgs(C.Structure):
+    _fields_ = [("nseqall", C.c_int32), ("nseqriv", C.c_int32), ("nlfp", C.c_int32), ("ladpstp", C.c_int32),
+                ("dt_def", C.c_double), ("pgrv", C.c_double), ("pdstmth", C.c_double), ("pcadp", C.c_double),
+                ("dfrcinc", C.c_double)] + [(n, C.c_void_p) for n in (
+        "rivstomax", "rivlen", "rivwth", "grarea", "rivelv", "nxtdst", "fldstomax", "fldgrd", "i2mask",
+        "rivsto", "fldsto", "rivdph", "flddph", "fldfrc", "fldare", "sfcelv", "storge", "dt_min_out", "stream")]
+
+
 EXPORTS = [
     "cmf_gpu_create", "cmf_gpu_destroy", "cmf_gpu_ctx_set_state", "cmf_gpu_ctx_get_state", "cmf_gpu_ctx_put_runoff",
     "cmf_gpu_ctx_physics_advance", "cmf_gpu_ctx_get_diag", "cmf_gpu_ctx_advance_device", "cmf_gpu_ctx_synchronize",
@@ -85,6 +93,7 @@ EXPORTS = [
     "cmf_gpu_init", "cmf_gpu_set_state", "cmf_gpu_get_state", "cmf_gpu_put_runoff", "cmf_gpu_physics_advance",
     "cmf_gpu_get_diag", "cmf_gpu_finalize", "cmf_gpu_strerror", "cmf_gpu_last_error", "cmf_gpu_abi_version",
     "cmf_host_load", "cmf_host_free", "cmf_host_describe", "cmf_host_state", "cmf_host_conv_resol", "cmf_host_grid",
+    "cmf_gpu_stage_noalloc",
 ]
 
 _lib = None
@@ -131,6 +140,7 @@ def load(build_if_missing: bool = True):
     lib.cmf_gpu_put_runoff.argtypes = [f64p, f64p]
     lib.cmf_gpu_physics_advance.argtypes = [C.c_double, i32p, f64p, C.POINTER(Budget)]
     lib.cmf_gpu_get_diag.argtypes = [C.POINTER(DiagPtrs)]
+    lib.cmf_gpu_stage_noalloc.argtypes = [C.POINTER(StageDevArgs)]
     lib.cmf_gpu_strerror.argtypes = [C.c_int]
     lib.cmf_gpu_strerror.restype = C.c_char_p
     lib.cmf_gpu_last_error.restype = C.c_char_p

@@ -854,3 +854,104 @@ void cmf_gpu_finalize(void) {
 }
 
 }  // extern "C"
+
+// ============================================================================================
+// Stage scheme + CFL minimum without any allocation by the library.
+//
+// Some hosts cannot let a library call cudaMalloc: couplers that hand every byte of device
+// memory to their own pool before the time loop starts, codes that run the physics while a
+// stream is being captured (where an allocation would break the capture), or processes whose
+// device memory is fully committed to other components.  This entry point serves them: the
+// caller passes device pointers for every input and output, and the only global memory the
+// library uses beyond those is the file-scope array below, which exists once per GPU for the
+// lifetime of the process.
+// ============================================================================================
+namespace {
+
+constexpr int kNoAllocBlock = 256;
+constexpr int kNoAllocMaxBlocks = 8192;   // 8192 x 256 = 2,097,152 cells at most
+
+// per-block CFL minima of the most recent call on this device (64 KiB)
+static __device__ __align__(256) double g_noalloc_blockmin[kNoAllocMaxBlocks];
+
+__global__ void k_noalloc_stage(cmf::Net n, cmf::State s, double *blockmin) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double key = 1.0e308;
+    if (i < n.N) {
+        const cmf::StageOut o = cmf::stage_def(n, i, s.rivsto[i], s.fldsto[i]);
+        cmf::store_stage(n, s, i, i, o);
+        if (n.ladpstp && n.i2mask[i] == 0) {
+            const double ddph = cmf::dmax(o.rivdph, 0.01);
+            const double ddst = (i < n.R) ? n.nxtdst[i] : n.pdstmth;
+            key = (n.pcadp * ddst) * pow(n.pgrv * ddph, -0.5);
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) key = cmf::dmin(key, __shfl_down_sync(0xffffffffu, key, o));
+    __shared__ double wmin[32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+    if (lane == 0) wmin[warp] = key;
+    __syncthreads();
+    if (warp == 0) {
+        double x = lane < nw ? wmin[lane] : 1.0e308;
+        for (int o = 16; o > 0; o >>= 1) x = cmf::dmin(x, __shfl_down_sync(0xffffffffu, x, o));
+        if (lane == 0) blockmin[blockIdx.x] = x;   // every block writes its slot on every call
+    }
+}
+
+__global__ void k_noalloc_min(const double *blockmin, int nblocks, double dt_def, double *dt_min_out) {
+    double x = 1.0e308;
+    for (int b = threadIdx.x; b < nblocks; b += blockDim.x) x = cmf::dmin(x, blockmin[b]);
+    for (int o = 16; o > 0; o >>= 1) x = cmf::dmin(x, __shfl_down_sync(0xffffffffu, x, o));
+    __shared__ double wmin[32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+    if (lane == 0) wmin[warp] = x;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double v = 1.0e308;
+        for (int w = 0; w < nw; w++) v = cmf::dmin(v, wmin[w]);
+        *dt_min_out = cmf::dmin(dt_def, v);
+    }
+}
+
+// device address of g_noalloc_blockmin, looked up once per device
+double *g_noalloc_ptr[64] = {};
+
+}  // namespace
+
+extern "C" int cmf_gpu_stage_noalloc(const cmf_stage_dev_args *a) {
+    if (!a || !a->rivsto || !a->fldsto || !a->rivstomax || !a->rivlen || !a->rivwth || !a->grarea || !a->rivelv ||
+        !a->nxtdst || !a->fldstomax || !a->fldgrd || !a->i2mask || !a->rivdph || !a->flddph || !a->fldfrc ||
+        !a->fldare || !a->sfcelv || !a->storge || !a->dt_min_out)
+        return set_err(CMF_E_ARG, "cmf_gpu_stage_noalloc: null pointer in arguments");
+    if (a->nseqall <= 0 || a->nseqriv < 0 || a->nseqriv > a->nseqall || a->nlfp <= 0 || !(a->dt_def > 0.0))
+        return set_err(CMF_E_ARG, "cmf_gpu_stage_noalloc: bad dimensions or DT");
+    const int nblocks = (a->nseqall + kNoAllocBlock - 1) / kNoAllocBlock;
+    if (nblocks > kNoAllocMaxBlocks)
+        return set_err(CMF_E_ARG, "cmf_gpu_stage_noalloc: NSEQALL=" + std::to_string(a->nseqall) +
+                                      " exceeds the scratch limit of " + std::to_string(kNoAllocMaxBlocks * kNoAllocBlock) +
+                                      " cells; use the context API (cmf_gpu_ctx_stage) for larger domains");
+    int dev = 0;
+    CUDA_TRY(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) return set_err(CMF_E_NO_DEVICE, "cmf_gpu_stage_noalloc: device ordinal above 63");
+    if (!g_noalloc_ptr[dev]) {
+        // set-up on the first call per device (the device must be current); no allocation happens here
+        void *p = nullptr;
+        CUDA_TRY(cudaGetSymbolAddress(&p, g_noalloc_blockmin));
+        g_noalloc_ptr[dev] = static_cast<double *>(p);
+    }
+    cmf::Net n{};
+    n.N = a->nseqall; n.R = a->nseqriv; n.L = a->nlfp; n.M = 1;
+    n.i2mask = a->i2mask; n.rivelv = a->rivelv; n.nxtdst = a->nxtdst; n.rivwth = a->rivwth; n.rivlen = a->rivlen;
+    n.grarea = a->grarea; n.rivstomax = a->rivstomax; n.fldstomax = a->fldstomax; n.fldgrd = a->fldgrd;
+    n.pgrv = a->pgrv; n.pdstmth = a->pdstmth; n.pcadp = a->pcadp; n.dfrcinc = a->dfrcinc; n.ladpstp = a->ladpstp;
+    n.llevee = 0;
+    cmf::State s{};
+    s.rivsto = a->rivsto; s.fldsto = a->fldsto; s.rivdph = a->rivdph; s.flddph = a->flddph; s.fldfrc = a->fldfrc;
+    s.fldare = a->fldare; s.sfcelv = a->sfcelv; s.storge = a->storge;
+    cudaStream_t st = static_cast<cudaStream_t>(a->stream);
+    k_noalloc_stage<<<nblocks, kNoAllocBlock, 0, st>>>(n, s, g_noalloc_ptr[dev]);
+    CUDA_TRY(cudaGetLastError());
+    k_noalloc_min<<<1, 256, 0, st>>>(g_noalloc_ptr[dev], nblocks, a->dt_def, a->dt_min_out);
+    CUDA_TRY(cudaGetLastError());
+    return CMF_OK;
+}

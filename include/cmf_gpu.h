@@ -195,6 +195,30 @@ int cmf_gpu_ctx_stage(cmf_gpu_ctx *ctx, double dt_def, double *dt_min_local);
 int cmf_gpu_ctx_substeps(cmf_gpu_ctx *ctx, double dt_def, double dt_min_global, int32_t *nt_out,
                          double *dt_out, cmf_budget *budget_out);
 
+/* Stage scheme + CFL minimum with no allocation by the library.  This entry point has no
+ * counterpart in the reference: it serves hosts that cannot let a library allocate device memory
+ * (a coupler whose pool owns all device memory, physics run during CUDA stream capture).  Every
+ * pointer is a caller-owned DEVICE pointer on the current device; the library's only other global
+ * memory is a fixed 64 KiB file-scope scratch array per GPU, held until process exit.  The
+ * default stage scheme (CMF_CALC_FLDSTG_DEF) updates rivsto/fldsto in place and writes the six
+ * diagnostics; *dt_min_out (device) receives min(DT, CFL minimum) of CALC_ADPSTP.  Limit:
+ * NSEQALL <= 2,097,152 (larger returns CMF_E_ARG with a message).  The first call on a device
+ * looks up the scratch array's address and must come before any stream capture.  All calls share
+ * the scratch array: calls that overlap on the GPU (other streams, other host threads) race.
+ * Enqueued on `stream` and asynchronous; no levee scheme in this variant. */
+typedef struct cmf_stage_dev_args {
+    int32_t nseqall, nseqriv, nlfp, ladpstp;
+    double dt_def, pgrv, pdstmth, pcadp, dfrcinc;
+    const double *rivstomax, *rivlen, *rivwth, *grarea, *rivelv, *nxtdst;
+    const double *fldstomax, *fldgrd;        /* [NLFP][NSEQALL] */
+    const int32_t *i2mask;
+    double *rivsto, *fldsto;                 /* in/out */
+    double *rivdph, *flddph, *fldfrc, *fldare, *sfcelv, *storge;   /* out */
+    double *dt_min_out;                      /* out, one double */
+    void *stream;                            /* cudaStream_t, may be NULL (legacy default stream) */
+} cmf_stage_dev_args;
+int cmf_gpu_stage_noalloc(const cmf_stage_dev_args *args);
+
 /* ======================================================================================== */
 /* Default-context API bound by the Fortran ISO_C_BINDING shim                              */
 /* ======================================================================================== */
