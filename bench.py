@@ -247,7 +247,7 @@ def gpu_arm(args) -> int:
         dist.barrier()
     h = HostModel(cdir)
     M = args.members
-    g = PhysicsGPU(h, nmembers=M, device=local)
+    g = PhysicsGPU(h, nmembers=M, device=local, launch_mode=args.launch_mode)
     N = h.dims.nseqall
     gr = h.map("grarea")
     W, K = args.warmup, args.steps
@@ -361,7 +361,9 @@ def gpu_arm(args) -> int:
             "config": {"workload": "config1: 1440x720 grid, 299157 cells, 12k bifurcation x5, levees 10%, 2000 dams, hourly AR(1) forcing",
                        "members_per_gpu": M, "parallelism": f"ensemble members sharded over {ws} GPU(s), no collective",
                        "l2": "256 MiB buffer written before every timed step", "nt_mean": member_sub / max(K * M, 1),
-                       "block_size": g.block_size, "launch": "one CUDA graph per coupling step, device-side sub-step loop"},
+                       "block_size": g.block_size,
+                       "launch": ("one CUDA graph per coupling step, device-side sub-step loop" if args.launch_mode == 0
+                                  else "host-driven kernel launches")},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": M * N * 8,
                     "d2h_bytes_per_step": M * N * 8 + M * 160},
             "gpu_launches": int(launches),
@@ -385,6 +387,9 @@ def main() -> int:
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--members", type=int, default=1)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--launch-mode", type=int, default=0, choices=[0, 1],
+                    help="0: CUDA graph with a device-side sub-step loop; 1: the same kernels as plain "
+                         "launches from a host loop (what ncu can profile kernel by kernel)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -319,7 +319,7 @@ void enqueue_substep(cmf_gpu_ctx *c, int use_cond) {
     cmf::k_flux<<<gcp, c->block, 0, c->stream>>>(c->net, c->st, c->ncell_blocks);
     cmf::k_rate<<<gc, c->block, 0, c->stream>>>(c->net, c->st);
     cmf::k_store<<<gcp, c->block, 0, c->stream>>>(c->net, c->st, c->ncell_blocks);
-    cmf::k_ctl<<<1, 256, 0, c->stream>>>(c->net, c->st, c->ncell_blocks, c->cond, use_cond);
+    cmf::k_ctl<<<1, 32 * cmf::kBudgets, 0, c->stream>>>(c->net, c->st, c->ncell_blocks, c->cond, use_cond);
 }
 
 void enqueue_prologue(cmf_gpu_ctx *c, int use_cond) {
@@ -468,7 +468,6 @@ int finish_outer(cmf_gpu_ctx *c, int32_t *nt_out, double *dt_out, cmf_budget *b)
     int rc = read_ctl(c);
     if (rc) return rc;
     int err = 0;
-    int64_t sub = 0;
     int ntmax = 0;
     for (size_t m = 0; m < c->hctl.size(); m++) {
         const cmf::MemberCtl &x = c->hctl[m];
@@ -483,7 +482,6 @@ int finish_outer(cmf_gpu_ctx *c, int32_t *nt_out, double *dt_out, cmf_budget *b)
             b[m].fldare = x.budget[9]; b[m].levsto = x.budget[10]; b[m].dam_miss = x.budget[11];
         }
     }
-    (void)sub;
     if (c->opts.launch_mode == 0) c->launches += 4LL * ntmax;
     if (err) {
         for (auto &x : c->hctl) x.err = 0;
@@ -639,7 +637,7 @@ int cmf_gpu_ctx_time_phases(cmf_gpu_ctx *c, double dt_def, int32_t reps, double 
         CUDA_TRY(cudaEventRecord(ev[4], c->stream));
         cmf::k_store<<<gcp, c->block, 0, c->stream>>>(c->net, c->st, c->ncell_blocks);
         CUDA_TRY(cudaEventRecord(ev[5], c->stream));
-        cmf::k_ctl<<<1, 256, 0, c->stream>>>(c->net, c->st, c->ncell_blocks, c->cond, 0);
+        cmf::k_ctl<<<1, 32 * cmf::kBudgets, 0, c->stream>>>(c->net, c->st, c->ncell_blocks, c->cond, 0);
         CUDA_TRY(cudaEventRecord(ev[6], c->stream));
         CUDA_TRY(cudaEventSynchronize(ev[6]));
         for (int k = 0; k < 6; k++) {
@@ -707,13 +705,17 @@ int cmf_gpu_ctx_advance_device(cmf_gpu_ctx *c, double dt_def, int32_t ksteps, co
     CUDA_TRY(cudaSetDevice(c->device));
     int rc;
     if ((rc = sync_dt_def(c, dt_def))) return rc;
-    if (c->opts.launch_mode != 0) return set_err(CMF_E_UNSUPPORTED, "device pipeline needs launch_mode 0");
     const size_t MN = (size_t)c->dims.nmembers * c->dims.nseqall;
     for (int k = 0; k < ksteps; k++) {
         if (runoff_dev)
             CUDA_TRY(cudaMemcpyAsync(c->st.runoff, runoff_dev + (size_t)k * stride, MN * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
-        CUDA_TRY(cudaGraphLaunch(c->exec, c->stream));
-        c->launches += 2;
+        if (c->opts.launch_mode == 0) {
+            CUDA_TRY(cudaGraphLaunch(c->exec, c->stream));
+            c->launches += 2;
+        } else {
+            // host-driven: the same kernels as plain launches (reads NTmax back once per step)
+            if ((rc = launch_outer(c))) return rc;
+        }
     }
     return CMF_OK;
 }

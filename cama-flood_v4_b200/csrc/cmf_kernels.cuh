@@ -842,32 +842,47 @@ __global__ void k_store(Net n, State s, int ncell_blocks) {
             s.m_storge[gi] = first ? dmax(0.0, stg) : dmax(s.m_storge[gi], stg);
         }
     }
-    // per-block budget partials (fixed-shape tree -> deterministic)
-    __shared__ double red[32 * kBudgets];
-    block_sum<kBudgets>(b, red);
-    if (threadIdx.x == 0) {
-        double *dst = s.partials + ((size_t)m * ncell_blocks + blockIdx.x) * kBudgets;
+    // per-block budget partials of the last sub-step (the only one the caller observes);
+    // fixed-shape tree -> deterministic; layout [m][k][block] for a coalesced final reduction
+    if (last) {
+        __shared__ double red[32 * kBudgets];
+        block_sum<kBudgets>(b, red);
+        if (threadIdx.x == 0) {
+            double *dst = s.partials + (size_t)m * kBudgets * ncell_blocks + blockIdx.x;
 #pragma unroll
-        for (int k = 0; k < kBudgets; k++) dst[k] = b[k];
+            for (int k = 0; k < kBudgets; k++) dst[(size_t)k * ncell_blocks] = b[k];
+        }
     }
 }
 
 // ------------------------------------------------------------------------------------------
 // k_ctl: budgets, sub-step counter and the loop condition
 // ------------------------------------------------------------------------------------------
+// launched with kBudgets warps: warp k reduces budget k of every member that just finished its
+// last sub-step (lanes stride over the block partials in a fixed order, then a fixed warp tree)
 __global__ void k_ctl(Net n, State s, int ncell_blocks, cudaGraphConditionalHandle h, int use_cond) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    for (int m = warp; m < n.M; m += nw) {
-        MemberCtl &c = s.ctl[m];
-        if (c.it >= c.nt) continue;
-        for (int k = 0; k < kBudgets; k++) {
-            double x = 0.0;
-            for (int bk = lane; bk < ncell_blocks; bk += 32) x = x + s.partials[((size_t)m * ncell_blocks + bk) * kBudgets + k];
-            for (int o = 16; o > 0; o >>= 1) x = x + __shfl_down_sync(0xffffffffu, x, o);
-            if (lane == 0) c.budget[k] = x;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int m = 0; m < n.M; m++) {
+        const MemberCtl &c = s.ctl[m];
+        if (c.it != c.nt - 1 || warp >= kBudgets) continue;   // uniform per warp
+        const double *src = s.partials + ((size_t)m * kBudgets + warp) * ncell_blocks;
+        double x0 = 0.0, x1 = 0.0, x2 = 0.0, x3 = 0.0;
+        int bk = lane;
+        for (; bk + 96 < ncell_blocks; bk += 128) {
+            x0 = x0 + src[bk];
+            x1 = x1 + src[bk + 32];
+            x2 = x2 + src[bk + 64];
+            x3 = x3 + src[bk + 96];
         }
-        __syncwarp();
-        if (lane == 0) {
+        for (; bk < ncell_blocks; bk += 32) x0 = x0 + src[bk];
+        double x = (x0 + x1) + (x2 + x3);
+        for (int o = 16; o > 0; o >>= 1) x = x + __shfl_down_sync(0xffffffffu, x, o);
+        if (lane == 0) s.ctl[m].budget[warp] = x;
+    }
+    __syncthreads();
+    for (int m = threadIdx.x; m < n.M; m += blockDim.x) {
+        MemberCtl &c = s.ctl[m];
+        if (c.it < c.nt) {
             c.nadd = c.nadd + c.dt;
             c.it = c.it + 1;
         }
