@@ -1227,15 +1227,15 @@ static void diag_getave_adpstp(orc_model *m) {
 }
 
 /* ============================================================================ ADVANCE */
-/* CMF_PHYSICS_ADVANCE, src/cmf_ctrl_physics_mod.F90:21-153 */
-int orc_physics_advance(orc_model *m, int *nt_out, double *dt_out) {
+/* CMF_PHYSICS_ADVANCE, src/cmf_ctrl_physics_mod.F90:21-153, split where the reference places
+ * CMF_MPI_ADPSTP (:200-202): orc_stage returns this domain's DT_MIN, orc_substeps takes the
+ * (possibly all-reduced) DT_MIN and runs the NT sub-steps. */
+double orc_stage(orc_model *m) {
     int N = m->nseqall, R = m->nseqriv;
     double DT_DEF = m->dt;
     physics_fldstg(m);
-    int NT = 1;
-    double DT = DT_DEF;
+    double dt_min = DT_DEF;
     if (m->ladpstp) {                                  /* CALC_ADPSTP, :161-210 */
-        double dt_min = DT_DEF;
         for (int i = 0; i < R; i++) {
             if (m->i2mask[i] == 0) {
                 double ddph = dmax(m->rivdph[i], 0.01), ddst = m->nxtdst[i];
@@ -1248,6 +1248,15 @@ int orc_physics_advance(orc_model *m, int *nt_out, double *dt_out) {
                 dt_min = dmin(dt_min, (m->pcadp * ddst) * opow(m->pgrv * ddph, -0.5));
             }
         }
+    }
+    return dt_min;
+}
+
+int orc_substeps(orc_model *m, double dt_min, int *nt_out, double *dt_out) {
+    double DT_DEF = m->dt;
+    int NT = 1;
+    double DT = DT_DEF;
+    if (m->ladpstp) {
         NT = (int)(DT_DEF * (1.0 / dt_min) - F(0.01)) + 1;
         DT = DT_DEF * (double)(1.0f / (float)NT);
         m->last_dtmin = dt_min;
@@ -1275,6 +1284,11 @@ int orc_physics_advance(orc_model *m, int *nt_out, double *dt_out) {
     if (nt_out) *nt_out = NT;
     if (dt_out) *dt_out = DT;
     return 0;
+}
+
+int orc_physics_advance(orc_model *m, int *nt_out, double *dt_out) {
+    const double dt_min = orc_stage(m);
+    return orc_substeps(m, dt_min, nt_out, dt_out);
 }
 
 /* ============================================================================ public API */

@@ -43,6 +43,9 @@ def _lib(omp: bool = False):
     lib.orc_iarray.restype = C.POINTER(C.c_int)
     lib.orc_iarray.argtypes = [C.c_void_p, C.c_char_p, C.POINTER(C.c_int)]
     lib.orc_threads.restype = C.c_int
+    lib.orc_stage.restype = C.c_double
+    lib.orc_stage.argtypes = [C.c_void_p]
+    lib.orc_substeps.argtypes = [C.c_void_p, C.c_double, C.POINTER(C.c_int), C.POINTER(C.c_double)]
     _LIBS[key] = lib
     return lib
 
@@ -80,6 +83,16 @@ class Oracle:
         rc = self.lib.orc_physics_advance(self.h, C.byref(nt), C.byref(dt))
         if rc:
             raise RuntimeError(f"oracle advance failed rc={rc}")
+        return nt.value, dt.value
+
+    def stage(self) -> float:
+        """Stage scheme + this domain's CFL minimum (before CMF_MPI_ADPSTP)."""
+        return float(self.lib.orc_stage(self.h))
+
+    def substeps(self, dt_min: float):
+        nt = C.c_int(0)
+        dt = C.c_double(0.0)
+        self.lib.orc_substeps(self.h, dt_min, C.byref(nt), C.byref(dt))
         return nt.value, dt.value
 
     def budget(self) -> dict:

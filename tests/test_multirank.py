@@ -1,0 +1,163 @@
+"""Multi-rank paths on CPU (gloo, world size 2) and the split stage/sub-step API on one GPU.
+
+Basin regions (cmf_b200.regions) are closed under I1NEXT and bifurcation, so ranks exchange only
+the 8-byte MIN of DT_MIN per outer step (CMF_MPI_ADPSTP, src/cmf_ctrl_mpi_mod.F90:261-281); the
+regional run must equal the whole-domain run bit for bit."""
+from __future__ import annotations
+
+import datetime
+import os
+import socket
+
+import numpy as np
+import pytest
+
+NSTEPS = 10
+
+
+def _free_port():
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    p = s.getsockname()[1]
+    s.close()
+    return p
+
+
+def _grid_runoff(nx, ny, k):
+    rng = np.random.default_rng(1000 + k)
+    g = rng.gamma(0.8, 2.5, size=nx * ny).astype(np.float32).astype(np.float64)
+    return g * 6.0
+
+
+def _region_worker(rank, world, port, region_dirs, out_dir):
+    import torch
+    import torch.distributed as dist
+    import sys
+
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    sys.path[:0] = [os.path.join(root, "cama-flood_v4_b200"), os.path.join(root, "oracle")]
+    from oracle import Oracle
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    o = Oracle(region_dirs[rank])
+    nts = []
+    for k in range(NSTEPS):
+        o.put_runoff_map(_grid_runoff(o.nx, o.ny, k))
+        local = o.stage()
+        t = torch.tensor([local], dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MIN)
+        nt, dt = o.substeps(float(t.item()))
+        nts.append((nt, dt))
+    gx, gy = o.i("i1seqx"), o.i("i1seqy")
+    flat = (gy - 1) * o.nx + (gx - 1)
+    grids = {}
+    for f in ("rivsto", "fldsto", "rivout", "fldout", "levsto", "damsto"):
+        g = np.full(o.nx * o.ny, np.nan)
+        g[flat] = o.d(f)
+        grids[f] = g
+    np.savez(os.path.join(out_dir, f"rank{rank}.npz"), nts=np.array(nts), **grids)
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_regions_partition_and_balance(case_dirs, tmp_path):
+    from cmf_b200 import regions
+
+    dirs = regions.split_case(case_dirs["cfg1s"], 2, str(tmp_path))
+    reg = np.fromfile(os.path.join(dirs[0], "mpireg.bin"), dtype="<i4")
+    land = reg != regions.IMIS
+    counts = [int(np.sum(reg == r)) for r in (1, 2)]
+    assert sum(counts) == int(land.sum()) and min(counts) > 0.3 * max(counts)
+    # every bifurcation channel stays inside one region
+    with open(os.path.join(dirs[0], "diminfo.txt")) as f:
+        nx = int(f.readline().split()[0])
+    for ix, iy, jx, jy in regions.read_bif_pairs(case_dirs["cfg1s"]):
+        assert reg[(iy - 1) * nx + ix - 1] == reg[(jy - 1) * nx + jx - 1]
+
+
+def test_gloo_regions_equal_whole_domain(case_dirs, tmp_path):
+    import torch.multiprocessing as mp
+
+    from cmf_b200 import regions
+    from oracle import Oracle
+
+    dirs = regions.split_case(case_dirs["cfg1s"], 2, str(tmp_path))
+    mp.start_processes(_region_worker, args=(2, _free_port(), dirs, str(tmp_path)), nprocs=2, join=True,
+                       start_method="spawn")
+    whole = Oracle(case_dirs["cfg1s"])
+    ref_nt = []
+    for k in range(NSTEPS):
+        whole.put_runoff_map(_grid_runoff(whole.nx, whole.ny, k))
+        ref_nt.append(whole.advance())
+    gx, gy = whole.i("i1seqx"), whole.i("i1seqy")
+    flat = (gy - 1) * whole.nx + (gx - 1)
+    parts = [dict(np.load(os.path.join(str(tmp_path), f"rank{r}.npz"))) for r in (0, 1)]
+    for p in parts:
+        assert [tuple(x) for x in p["nts"]] == [(int(a), float(b)) for a, b in ref_nt]
+    for f in ("rivsto", "fldsto", "rivout", "fldout", "levsto", "damsto"):
+        merged = np.where(np.isnan(parts[0][f]), parts[1][f], parts[0][f])[flat]
+        assert np.array_equal(merged.view(np.int64), whole.d(f).view(np.int64)), f
+
+
+def _member_worker(rank, world, port, nmembers, out_dir):
+    import torch
+    import torch.distributed as dist
+    import sys
+
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    sys.path[:0] = [os.path.join(root, "cama-flood_v4_b200")]
+    from cmf_b200.regions import members_for_rank
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    mine = torch.zeros(nmembers, dtype=torch.int64)
+    for m in members_for_rank(nmembers, world, rank):
+        mine[m] += 1
+    dist.all_reduce(mine)
+    np.save(os.path.join(out_dir, f"members{rank}.npy"), mine.numpy())
+    dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("nmembers", [7, 64])
+def test_gloo_member_sharding_covers_every_member_once(tmp_path, nmembers):
+    import torch.multiprocessing as mp
+
+    mp.start_processes(_member_worker, args=(2, _free_port(), nmembers, str(tmp_path)), nprocs=2, join=True,
+                       start_method="spawn")
+    for r in (0, 1):
+        assert np.all(np.load(os.path.join(str(tmp_path), f"members{r}.npy")) == 1)
+
+
+@pytest.mark.gpu
+def test_gpu_regions_with_host_min_equal_whole_domain(case_dirs, tmp_path):
+    """Two regional GPU contexts, DT_MIN reduced on the host between cmf_gpu_ctx_stage and
+    cmf_gpu_ctx_substeps, reproduce the whole-domain GPU context bit for bit."""
+    from cmf_b200 import HostModel, PhysicsGPU, regions
+
+    dirs = regions.split_case(case_dirs["cfg1s"], 2, str(tmp_path))
+    hw = HostModel(case_dirs["cfg1s"])
+    gw = PhysicsGPU(hw)
+    hs = [HostModel(d) for d in dirs]
+    gs = [PhysicsGPU(h) for h in hs]
+    for k in range(NSTEPS):
+        grid = _grid_runoff(hw.nx, hw.ny, k)
+        gw.put_runoff(hw.conv_resol(grid))
+        ntw, dtw, _ = gw.advance()
+        local = []
+        for h, g in zip(hs, gs):
+            g.put_runoff(h.conv_resol(grid))
+            local.append(g.stage()[0])
+        dtmin = min(local)
+        for g in gs:
+            nt, dt, _ = g.substeps(dtmin)
+            assert nt[0] == ntw[0] and dt[0] == dtw[0]
+    flat_w = (hw.i1seqy - 1) * hw.nx + (hw.i1seqx - 1)
+    sw = gw.get_state()
+    for f in ("rivsto", "fldsto", "rivout", "fldout", "levsto", "damsto"):
+        g = np.full(hw.nx * hw.ny, np.nan)
+        for h, p in zip(hs, gs):
+            g[(h.i1seqy - 1) * h.nx + (h.i1seqx - 1)] = p.get_state()[f][0]
+        assert np.array_equal(g[flat_w].view(np.int64), sw[f][0].view(np.int64)), f
