@@ -18,7 +18,7 @@ LIBDIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIBDIR, "libcmf_b200.so")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 
-SOURCES = ["cmf_engine.cu", "cmf_host.cpp"]
+SOURCES = ["cmf_engine.cu", "cmf_emu.cu", "cmf_host.cpp"]
 HEADERS = ["cmf_kernels.cuh"]
 
 NVCC_FLAGS = [

@@ -1,0 +1,402 @@
+"""Learned per-cell emulator of the coupling step (no counterpart in the reference).
+
+E1  trajectories: the GPU solver advances ensemble members; before each coupling step the features
+    of every cell are taken from the state, after it the target is the cell's mean outflow over the
+    step (D2OUTFLW_aAVG of the physics).
+E2  graph messages: 8 hops of upstream sums (CSR gather along I1NEXT) of the last-step outflow and
+    of the runoff, normalised by the receiving cell's discharge scale.
+E3  MLP 64 (30 used) -> 128 -> 128 -> 128 -> 1 with ReLU, BF16 weights and activations, FP32
+    accumulation on the tensor cores, FP32 master weights and Adam -- kernels in csrc/cmf_emu.cu.
+E4  rollout: predicted outflows update storage through the same upstream gather (mass conserved
+    exactly), the stage scheme recomputes depths.  Every `resync_hours` the plain solver, started
+    from the same state, judges a rotating subset of members: their daily-mean discharge error at
+    the gauges is measured, they are re-synced to the plain state, and a member whose error is
+    above the tolerance is handed back to the plain solver for good.
+E5  daily-discharge Nash-Sutcliffe efficiency, 1 - sum((s-o)^2) / sum((o - mean(o))^2)
+    (the NS formula of etc/validation/src/discharge_validation.py:39-53).
+Torch only allocates device buffers and holds pointers; the arithmetic runs in the library's kernels.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+
+import numpy as np
+
+from . import _abi
+from ._abi import check
+
+IN, HID, OUT = 64, 128, 64      # padded widths (30 input features, 1 output)
+NFEAT, HOPS = 30, 8
+
+
+class EmuNet(C.Structure):
+    _fields_ = [("nseqall", C.c_int32), ("nseqriv", C.c_int32)] + [(n, C.c_void_p) for n in (
+        "next", "up_ptr", "up_idx", "rivelv", "elevtn", "nxtdst", "rivwth", "rivhgt", "rivlen", "rivstomax", "qref")]
+
+
+class EmuMember(C.Structure):
+    _fields_ = [(n, C.c_void_p) for n in ("rivsto", "fldsto", "levsto", "rivdph", "flddph", "fldfrc", "qprev", "runoff",
+                                          "rivout_pre", "fldout_pre")]
+
+
+def _emu_lib():
+    lib = _abi.load()
+    if not getattr(lib, "_emu_ready", False):
+        vp, i, f, d = C.c_void_p, C.c_int, C.c_float, C.c_double
+        lib.cmf_emu_gemm.argtypes = [i, i, i, vp, i, i, vp, i, i, vp, i, vp, i, vp, i, i, i, vp]
+        lib.cmf_emu_relu_bwd.argtypes = [i, vp, vp, vp, vp, vp]
+        lib.cmf_emu_colsum.argtypes = [i, i, vp, vp, vp]
+        lib.cmf_emu_mse_grad.argtypes = [i, i, i, vp, vp, vp, vp, vp, vp]
+        lib.cmf_emu_adam.argtypes = [i, vp, vp, vp, vp, vp, f, f, f, f, i, f, vp]
+        lib.cmf_emu_features.argtypes = [C.POINTER(EmuNet), C.POINTER(EmuMember), i, vp, i, i, i, vp, vp, vp, vp, vp]
+        lib.cmf_emu_rollout.argtypes = [C.POINTER(EmuNet), C.POINTER(EmuMember), i, vp, vp, i, i, d, vp, vp]
+        lib.cmf_emu_last_error.restype = C.c_char_p
+        lib.cmf_gpu_ctx_emu_views.argtypes = [vp, C.c_int32, C.POINTER(EmuNet), C.POINTER(EmuMember)]
+        lib.cmf_gpu_ctx_copy_member.argtypes = [vp, C.c_int32, vp, C.c_int32]
+        lib._emu_ready = True
+    return lib
+
+
+def echeck(rc, what):
+    if rc != 0:
+        lib = _emu_lib()
+        raise RuntimeError(f"{what}: status {rc}: {lib.cmf_emu_last_error().decode()} {lib.cmf_gpu_last_error().decode()}")
+
+
+def qref_from_host(host) -> np.ndarray:
+    """Discharge scale per cell: upstream area x 2 mm/day (m3/s), accumulated along I1NEXT."""
+    gr = host.map("grarea")
+    nxt = host.map("i1next")
+    up = gr.copy()
+    for i in range(host.dims.nseqriv):
+        up[nxt[i] - 1] += up[i]
+    return np.maximum(up * 2.0e-3 / 86400.0, 1e-3)
+
+
+def pad64(n: int) -> int:
+    return (n + 63) // 64 * 64
+
+
+def nse(sim: np.ndarray, obs: np.ndarray) -> np.ndarray:
+    """Nash-Sutcliffe efficiency along axis 0 (time) for every column."""
+    o = obs - obs.mean(axis=0, keepdims=True)
+    den = np.sum(o * o, axis=0)
+    num = np.sum((sim - obs) ** 2, axis=0)
+    return 1.0 - num / np.maximum(den, 1e-300)
+
+
+def _raw_f64(ptr: int, n: int, dev):
+    """float64 device tensor aliasing library memory (valid while the context lives)."""
+    import torch
+
+    class _CAI:
+        def __init__(self, p, size):
+            self.__cuda_array_interface__ = {"shape": (size,), "typestr": "<f8", "data": (p, False), "version": 3}
+
+    return torch.as_tensor(_CAI(ptr, n), device=dev)
+
+
+class MLP:
+    """Parameters and the forward/backward/Adam chain on the GPU."""
+
+    def __init__(self, device, seed: int = 0, lr: float = 1e-3):
+        import torch
+
+        self.torch = torch
+        self.dev = device
+        self.lib = _emu_lib()
+        g = torch.Generator().manual_seed(seed)
+        shapes = [(IN, HID), (HID, HID), (HID, HID), (HID, OUT)]
+        self.W, self.Wb, self.b, self.mW, self.vW, self.mb, self.vb, self.gW, self.gb = ([] for _ in range(9))
+        for li, (k, n) in enumerate(shapes):
+            w = torch.randn(k, n, generator=g) * math.sqrt(2.0 / (NFEAT if li == 0 else k))
+            if li == 0:
+                w[NFEAT:, :] = 0.0          # padded input columns
+            if li == 3:
+                w[:, 1:] = 0.0              # only output column 0 is real
+                w *= 0.1
+            w = w.to(device)
+            self.W.append(w)
+            self.Wb.append(w.to(torch.bfloat16))
+            self.b.append(torch.zeros(n, device=device))
+            for lst in (self.mW, self.vW, self.gW):
+                lst.append(torch.zeros_like(w))
+            for lst in (self.mb, self.vb, self.gb):
+                lst.append(torch.zeros(n, device=device))
+        self.step = 0
+        self.lr = lr
+        self.stream = None
+
+    def state_dict(self):
+        return {"W": [w.cpu().numpy() for w in self.W], "b": [b.cpu().numpy() for b in self.b]}
+
+    def load(self, sd):
+        for k in range(4):
+            self.W[k].copy_(self.torch.from_numpy(np.asarray(sd["W"][k], dtype=np.float32)))
+            self.Wb[k].copy_(self.W[k].to(self.torch.bfloat16))
+            self.b[k].copy_(self.torch.from_numpy(np.asarray(sd["b"][k], dtype=np.float32)))
+
+    def _gemm(self, M, N, K, A, lda, ta, B, ldb, tb, C=None, Cb=None, bias=None, relu=0, acc=0, ksplit=1):
+        p = lambda t: (t.data_ptr() if t is not None else None)  # noqa: E731
+        echeck(self.lib.cmf_emu_gemm(M, N, K, p(A), lda, ta, p(B), ldb, tb, p(C), N if C is not None else 0, p(Cb),
+                                     N if Cb is not None else 0, p(bias), relu, acc, ksplit, self.stream), "gemm")
+
+    def forward(self, X, keep: bool = True):
+        """X: [R, 64] bf16 (R % 64 == 0) -> (Y fp32 [R, 64], activations for the backward pass)."""
+        torch = self.torch
+        R = X.shape[0]
+        acts = [X]
+        a = X
+        for li in range(3):
+            out = torch.empty(R, HID, dtype=torch.bfloat16, device=self.dev)
+            self._gemm(R, HID, a.shape[1], a, a.shape[1], 0, self.Wb[li], HID, 0, Cb=out, bias=self.b[li], relu=1)
+            acts.append(out)
+            a = out
+        Y = torch.empty(R, OUT, dtype=torch.float32, device=self.dev)
+        self._gemm(R, OUT, HID, a, HID, 0, self.Wb[3], OUT, 0, C=Y, bias=self.b[3])
+        return Y, (acts if keep else None)
+
+    def backward(self, acts, dY, dYb):
+        """Parameter gradients into gW/gb from dY = dLoss/dY ([R, 64], fp32 and bf16)."""
+        torch = self.torch
+        R = dY.shape[0]
+        ks = max(1, R // 4096)
+        for g in self.gW:
+            g.zero_()
+        dZf, dZb = dY, dYb
+        for li in (3, 2, 1, 0):
+            a = acts[li]
+            K_in = a.shape[1]
+            n_out = self.W[li].shape[1]
+            self._gemm(K_in, n_out, R, a, K_in, 1, dZb, n_out, 0, C=self.gW[li], acc=1, ksplit=ks)      # a^T dZ
+            echeck(self.lib.cmf_emu_colsum(R, n_out, dZf.data_ptr(), self.gb[li].data_ptr(), self.stream), "colsum")
+            if li == 0:
+                break
+            dA = torch.empty(R, K_in, dtype=torch.float32, device=self.dev)
+            self._gemm(R, K_in, n_out, dZb, n_out, 0, self.Wb[li], n_out, 1, C=dA)                        # dZ W^T
+            nz = torch.empty(R, K_in, dtype=torch.bfloat16, device=self.dev)
+            nzf = torch.empty(R, K_in, dtype=torch.float32, device=self.dev)
+            echeck(self.lib.cmf_emu_relu_bwd(R * K_in, dA.data_ptr(), a.data_ptr(), nz.data_ptr(), nzf.data_ptr(),
+                                             self.stream), "relu_bwd")
+            dZf, dZb = nzf, nz
+
+    def adam(self, wd: float = 0.0):
+        self.step += 1
+        for k in range(4):
+            echeck(self.lib.cmf_emu_adam(self.W[k].numel(), self.W[k].data_ptr(), self.Wb[k].data_ptr(), self.gW[k].data_ptr(),
+                                         self.mW[k].data_ptr(), self.vW[k].data_ptr(), self.lr, 0.9, 0.999, 1e-8, self.step,
+                                         wd, self.stream), "adam")
+            echeck(self.lib.cmf_emu_adam(self.b[k].numel(), self.b[k].data_ptr(), None, self.gb[k].data_ptr(),
+                                         self.mb[k].data_ptr(), self.vb[k].data_ptr(), self.lr, 0.9, 0.999, 1e-8, self.step,
+                                         0.0, self.stream), "adam")
+
+    def loss_and_grad(self, X, t, valid: int):
+        torch = self.torch
+        Y, acts = self.forward(X)
+        R = X.shape[0]
+        dY = torch.empty(R, OUT, dtype=torch.float32, device=self.dev)
+        dYb = torch.empty(R, OUT, dtype=torch.bfloat16, device=self.dev)
+        parts = torch.empty((R + 255) // 256, dtype=torch.float32, device=self.dev)
+        echeck(self.lib.cmf_emu_mse_grad(R, valid, OUT, Y.data_ptr(), t.data_ptr(), dY.data_ptr(), dYb.data_ptr(),
+                                         parts.data_ptr(), self.stream), "mse_grad")
+        self.backward(acts, dY, dYb)
+        return parts.sum() / valid
+
+
+class Features:
+    """E1/E2 for every member of a PhysicsGPU context: X [M * Np, 64] bf16 (member m at rows m*Np)."""
+
+    def __init__(self, phys, qref: np.ndarray):
+        import torch
+
+        self.torch = torch
+        self.phys = phys
+        self.lib = _emu_lib()
+        self.dev = torch.device("cuda", phys.opts.device)
+        self.M, self.N = phys.M, phys.N
+        self.Np = pad64(self.N)
+        self.qref = torch.tensor(qref, dtype=torch.float64, device=self.dev)
+        self.net = EmuNet()
+        check(self.lib.cmf_gpu_ctx_emu_views(phys.h, 0, C.byref(self.net), None), "emu_views")
+        self.net.qref = self.qref.data_ptr()
+        self.mb = EmuMember()
+        check(self.lib.cmf_gpu_ctx_emu_views(phys.h, 0, None, C.byref(self.mb)), "emu_views")
+        self.scratch = [torch.empty(self.M * self.N, dtype=torch.float32, device=self.dev) for _ in range(4)]
+        self.X = torch.zeros(self.M * self.Np, IN, dtype=torch.bfloat16, device=self.dev)
+        self.qout = torch.empty(self.M * self.N, dtype=torch.float64, device=self.dev)
+
+    def build(self):
+        s = self.scratch
+        echeck(self.lib.cmf_emu_features(C.byref(self.net), C.byref(self.mb), self.M, self.X.data_ptr(), IN, self.Np, HOPS,
+                                         s[0].data_ptr(), s[1].data_ptr(), s[2].data_ptr(), s[3].data_ptr(), None), "features")
+        return self.X
+
+    def qprev(self):
+        """[M, N] view (copy) of the last-step mean outflow."""
+        return _raw_f64(self.mb.qprev, self.M * self.N, self.dev).clone().view(self.M, self.N)
+
+    def rollout(self, Y, active):
+        echeck(self.lib.cmf_emu_rollout(C.byref(self.net), C.byref(self.mb), self.M, active.data_ptr(), Y.data_ptr(), OUT,
+                                        self.Np, float(self.phys.host.dt), self.qout.data_ptr(), None), "rollout")
+
+
+def target_transform(torch, q, qref):
+    return torch.log1p(torch.clamp(q, min=0.0) / qref)
+
+
+def residual_target(torch, q_new, q_prev, qref):
+    """Training target: change of log1p(Q/qref) over the step (the rollout adds it back)."""
+    return target_transform(torch, q_new, qref) - target_transform(torch, q_prev, qref)
+
+
+def runoff_generators(N: int, members: int, seed: int):
+    from . import synth
+
+    return [synth.AR1GammaRunoff(N, seed + 7919 * m) for m in range(members)]
+
+
+def runoff_step(gens, gr, scale: float = 1.0) -> np.ndarray:
+    return np.stack([np.maximum((g.next().astype(np.float64) * scale * gr) / 86400000.0, 0.0) for g in gens])
+
+
+def generate_trajectories(host, members: int, hours: int, spinup: int, seed: int, cells_per_snapshot: int | None = None):
+    """E1: the plain GPU solver advances `members` members (different runoff seeds); returns feature
+    rows X [S, 64] (bf16) and targets t [S] (fp32)."""
+    import torch
+
+    from .model import PhysicsGPU
+
+    phys = PhysicsGPU(host, nmembers=members)
+    N = phys.N
+    gr = host.map("grarea")
+    gens = runoff_generators(N, members, seed)
+    for _ in range(spinup):
+        phys.put_runoff(runoff_step(gens, gr))
+        phys.advance()
+    fe = Features(phys, qref_from_host(host))
+    rng = np.random.default_rng(seed)
+    Xs, ts = [], []
+    for _ in range(hours):
+        phys.put_runoff(runoff_step(gens, gr))
+        X = fe.build().clone()                        # state at the start of the step + its runoff
+        q0 = fe.qprev()
+        phys.advance()
+        t = residual_target(torch, fe.qprev(), q0, fe.qref[None, :]).float()   # mean outflow over the step
+        for m in range(members):
+            idx = np.arange(N) if cells_per_snapshot is None else rng.choice(N, size=min(cells_per_snapshot, N), replace=False)
+            it = torch.as_tensor(idx, device=fe.dev)
+            Xs.append(X[m * fe.Np + it])
+            ts.append(t[m][it])
+    phys.close()
+    return torch.cat(Xs), torch.cat(ts)
+
+
+def train(mlp: MLP, X, t, iters: int, batch: int, seed: int = 0, lr_max: float | None = None):
+    """Adam with cosine-decayed learning rate on random mini-batches of the trajectory rows."""
+    import torch
+
+    g = torch.Generator(device=X.device).manual_seed(seed)
+    S = X.shape[0]
+    hist = []
+    lr0 = lr_max if lr_max is not None else mlp.lr
+    for it in range(iters):
+        mlp.lr = lr0 * (0.05 + 0.95 * 0.5 * (1.0 + math.cos(math.pi * it / max(iters, 1))))
+        idx = torch.randint(0, S, (batch,), device=X.device, generator=g)
+        loss = mlp.loss_and_grad(X[idx].contiguous(), t[idx].contiguous(), batch)
+        mlp.adam()
+        if it % 50 == 0 or it == iters - 1:
+            hist.append((it, float(loss)))
+    return hist
+
+
+class SurrogateEnsemble:
+    """E4: ensemble advanced by the emulator with plain-solver judging and hand-back."""
+
+    def __init__(self, host, mlp: MLP, members: int, judge_slots: int, gauges: np.ndarray, tol_rel: float = 0.05,
+                 resync_hours: int = 24):
+        import torch
+
+        from .model import PhysicsGPU
+
+        self.torch = torch
+        self.host = host
+        self.mlp = mlp
+        self.M = members
+        self.emu = PhysicsGPU(host, nmembers=members)
+        self.judge = PhysicsGPU(host, nmembers=judge_slots)
+        self.fe = Features(self.emu, qref_from_host(host))
+        self.lib = _emu_lib()
+        self.gauges = np.asarray(gauges)
+        self.tol = tol_rel
+        self.resync = resync_hours
+        self.slots = judge_slots
+        self.plain = set()
+        self.active = torch.ones(members, dtype=torch.int32, device=self.fe.dev)
+        self.stats = {"judged": 0, "fallback": 0, "emu_member_hours": 0, "plain_member_hours": 0, "errors": []}
+
+    def set_state_from(self, phys):
+        for m in range(self.M):
+            check(self.lib.cmf_gpu_ctx_copy_member(self.emu.h, m, phys.h, m), "copy_member")
+
+    def emu_step(self):
+        X = self.fe.build()
+        Y, _ = self.mlp.forward(X, keep=False)
+        self.fe.rollout(Y, self.active)
+
+    def run(self, runoff: np.ndarray):
+        """runoff [hours, M, N] -> hourly mean discharge at the gauges [hours, M, G]."""
+        H = runoff.shape[0]
+        G = self.gauges
+        out = np.zeros((H, self.M, len(G)))
+        slots = []
+        judged = []
+        buf_e, buf_j = [], []
+        day = 0
+        for h in range(H):
+            if h % self.resync == 0:
+                plain = sorted(self.plain)[: self.slots]
+                free = self.slots - len(plain)
+                cand = [m for m in range(self.M) if m not in self.plain]
+                judged = [cand[(day * free + k) % len(cand)] for k in range(min(free, len(cand)))] if cand else []
+                slots = plain + judged
+                for k, m in enumerate(slots):
+                    check(self.lib.cmf_gpu_ctx_copy_member(self.judge.h, k, self.emu.h, m), "copy_member")
+                buf_e, buf_j = [], []
+                day += 1
+            self.emu.put_runoff(runoff[h])
+            self.active.copy_(self.torch.tensor([0 if m in self.plain else 1 for m in range(self.M)], dtype=self.torch.int32))
+            self.emu_step()
+            self.emu.stage()
+            self.stats["emu_member_hours"] += self.M - len(self.plain)
+            jr = np.zeros((self.slots, runoff.shape[2]))
+            for k, m in enumerate(slots):
+                jr[k] = runoff[h, m]
+            self.judge.put_runoff(jr)
+            self.judge.advance()
+            self.stats["plain_member_hours"] += len(slots)
+            qe = self.fe.qprev().cpu().numpy()
+            qj = self.emu.get_diag_fields  # noqa: F841  (kept for readability of the flow)
+            qjudge = self.judge.get_diag_fields({"outflw_aavg": np.zeros(self.slots * self.emu.N)})["outflw_aavg"]
+            qjudge = qjudge.reshape(self.slots, -1)
+            out[h] = qe[:, G]
+            for k, m in enumerate(slots):
+                if m in self.plain:
+                    out[h, m] = qjudge[k, G]
+            buf_e.append(qe[:, G].copy())
+            buf_j.append(qjudge[:, G].copy())
+            if (h + 1) % self.resync == 0:
+                we = np.stack(buf_e).mean(0)
+                wj = np.stack(buf_j).mean(0)
+                for k, m in enumerate(slots):
+                    if m in self.plain:
+                        check(self.lib.cmf_gpu_ctx_copy_member(self.emu.h, m, self.judge.h, k), "copy_member")
+                        continue
+                    err = float(np.median(np.abs(we[m] - wj[k]) / np.maximum(np.abs(wj[k]), 1e-6)))
+                    self.stats["errors"].append(err)
+                    self.stats["judged"] += 1
+                    if err > self.tol:
+                        self.plain.add(m)
+                        self.stats["fallback"] += 1
+                    check(self.lib.cmf_gpu_ctx_copy_member(self.emu.h, m, self.judge.h, k), "copy_member")
+        return out

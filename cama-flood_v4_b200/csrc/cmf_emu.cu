@@ -1,0 +1,393 @@
+// cmf_emu.cu -- device kernels of the learned per-cell emulator (no counterpart in the reference).
+//
+// A 4-layer MLP (input 32 -> 128 -> 128 -> 128 -> 1, ReLU) maps local state plus 8-hop upstream
+// messages of every cell to its mean outflow over the next coupling step.  BF16 operands, FP32
+// accumulation on the tensor cores (mma.sync m16n8k16), FP32 master weights updated by Adam.
+// The rollout kernel turns predicted outflows into a mass-conserving storage update along the
+// same upstream CSR the physics uses; the stage scheme then recomputes depths.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+
+#include "../../include/cmf_gpu.h"
+
+namespace {
+
+thread_local std::string g_emu_err;
+
+int emu_err(int code, const std::string &m) {
+    g_emu_err = m;
+    return code;
+}
+
+#define EMU_TRY(expr)                                                                         \
+    do {                                                                                      \
+        cudaError_t e_ = (expr);                                                              \
+        if (e_ != cudaSuccess) return emu_err(CMF_E_CUDA, std::string(#expr) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+// ------------------------------------------------------------------------------------------
+// GEMM: C[M,N] (+)= op(A)[M,K] * op(B)[K,N], bf16 in, fp32 accumulate.
+// A is [M][K] (transA=0) or [K][M] (transA=1); B is [K][N] (transB=0) or [N][K] (transB=1); all
+// row-major with leading dimensions lda/ldb.  Tiles of 64x64 per CTA (4 warps of 32x32), K steps
+// of 32 staged in shared memory with both operands stored K-contiguous ([m][k], [n][k]), so the
+// m16n8k16 fragments are plain 32-bit shared loads:
+//   A frag  a0={A[g][2t..]}, a1={A[g+8][2t..]}, a2={A[g][2t+8..]}, a3={A[g+8][2t+8..]}
+//   B frag  b0={B[k=2t..][n=g]}, b1={B[k=2t+8..][n=g]}          (g = lane/4, t = lane%4)
+//   C frag  c0,c1 = C[g][2t..], c2,c3 = C[g+8][2t..]
+// Epilogue: +bias[n], optional ReLU, store fp32 and/or bf16, or atomic-add fp32 (split-K).
+// M, N must be multiples of 64 and K of 32 (callers pad); K may be split over gridDim.z.
+// ------------------------------------------------------------------------------------------
+constexpr int TM = 64, TN = 64, TK = 32, PAD = 8;
+
+__device__ __forceinline__ void mma_bf16(float (&c)[4], const uint32_t (&a)[4], const uint32_t (&b)[2]) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
+        : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
+__global__ void __launch_bounds__(128) k_gemm(int M, int N, int K, const __nv_bfloat16 *__restrict__ A, int lda, int transA,
+                                              const __nv_bfloat16 *__restrict__ B, int ldb, int transB,
+                                              float *C, int ldc, __nv_bfloat16 *Cb, int ldcb, const float *__restrict__ bias,
+                                              int relu, int accumulate, int k_per_split) {
+    __shared__ __align__(16) __nv_bfloat16 As[TM][TK + PAD];
+    __shared__ __align__(16) __nv_bfloat16 Bs[TN][TK + PAD];
+    const int m0 = blockIdx.y * TM, n0 = blockIdx.x * TN;
+    const int kbeg = blockIdx.z * k_per_split, kend = min(K, kbeg + k_per_split);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
+    const int g = lane >> 2, t = lane & 3;
+    float acc[2][4][4];
+#pragma unroll
+    for (int i = 0; i < 2; i++)
+#pragma unroll
+        for (int j = 0; j < 4; j++)
+#pragma unroll
+            for (int r = 0; r < 4; r++) acc[i][j][r] = 0.f;
+    for (int k0 = kbeg; k0 < kend; k0 += TK) {
+        // stage A tile as [m][k] and B tile as [n][k]
+        for (int e = tid; e < TM * TK; e += blockDim.x) {
+            const int mm = e / TK, kk = e % TK;
+            const int gm = m0 + mm, gk = k0 + kk;
+            As[mm][kk] = transA ? A[(size_t)gk * lda + gm] : A[(size_t)gm * lda + gk];
+            const int nn = mm;
+            const int gn = n0 + nn;
+            Bs[nn][kk] = transB ? B[(size_t)gn * ldb + gk] : B[(size_t)gk * ldb + gn];
+        }
+        __syncthreads();
+#pragma unroll
+        for (int ks = 0; ks < TK; ks += 16) {
+            uint32_t af[2][4], bfr[4][2];
+#pragma unroll
+            for (int i = 0; i < 2; i++) {
+                const int r = wm + i * 16 + g;
+                af[i][0] = *reinterpret_cast<const uint32_t *>(&As[r][ks + 2 * t]);
+                af[i][1] = *reinterpret_cast<const uint32_t *>(&As[r + 8][ks + 2 * t]);
+                af[i][2] = *reinterpret_cast<const uint32_t *>(&As[r][ks + 2 * t + 8]);
+                af[i][3] = *reinterpret_cast<const uint32_t *>(&As[r + 8][ks + 2 * t + 8]);
+            }
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                const int c = wn + j * 8 + g;
+                bfr[j][0] = *reinterpret_cast<const uint32_t *>(&Bs[c][ks + 2 * t]);
+                bfr[j][1] = *reinterpret_cast<const uint32_t *>(&Bs[c][ks + 2 * t + 8]);
+            }
+#pragma unroll
+            for (int i = 0; i < 2; i++)
+#pragma unroll
+                for (int j = 0; j < 4; j++) mma_bf16(acc[i][j], af[i], bfr[j]);
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int i = 0; i < 2; i++)
+#pragma unroll
+        for (int j = 0; j < 4; j++)
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+                const int row = m0 + wm + i * 16 + g + h * 8;
+                const int col = n0 + wn + j * 8 + 2 * t;
+                float v0 = acc[i][j][2 * h], v1 = acc[i][j][2 * h + 1];
+                if (accumulate) {
+                    atomicAdd(&C[(size_t)row * ldc + col], v0);
+                    atomicAdd(&C[(size_t)row * ldc + col + 1], v1);
+                    continue;
+                }
+                if (bias) { v0 += bias[col]; v1 += bias[col + 1]; }
+                if (relu) { v0 = fmaxf(v0, 0.f); v1 = fmaxf(v1, 0.f); }
+                if (C) { C[(size_t)row * ldc + col] = v0; C[(size_t)row * ldc + col + 1] = v1; }
+                if (Cb) {
+                    Cb[(size_t)row * ldcb + col] = __float2bfloat16_rn(v0);
+                    Cb[(size_t)row * ldcb + col + 1] = __float2bfloat16_rn(v1);
+                }
+            }
+}
+
+// dZ = dA * (act > 0) -> bf16, for ReLU layers (act stored in bf16 by the forward pass)
+__global__ void k_relu_bwd(int n, const float *__restrict__ dA, const __nv_bfloat16 *__restrict__ act, __nv_bfloat16 *dZ,
+                           float *dZf) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float v = __bfloat162float(act[i]) > 0.f ? dA[i] : 0.f;
+    dZ[i] = __float2bfloat16_rn(v);
+    if (dZf) dZf[i] = v;
+}
+
+// column sums of a [rows][cols] fp32 matrix into out[cols] (bias gradients), one block per column
+__global__ void k_colsum(int rows, int cols, const float *__restrict__ X, float *out) {
+    const int c = blockIdx.x;
+    float s = 0.f;
+    for (int r = threadIdx.x; r < rows; r += blockDim.x) s += X[(size_t)r * cols + c];
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    __shared__ float w[32];
+    if ((threadIdx.x & 31) == 0) w[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        float t = 0.f;
+        for (int k = 0; k < (int)(blockDim.x >> 5); k++) t += w[k];
+        out[c] = t;
+    }
+}
+
+// Adam on fp32 master weights, bf16 copy for the tensor cores
+__global__ void k_adam(int n, float *w, __nv_bfloat16 *wb, const float *__restrict__ grad, float *m, float *v, float lr,
+                       float b1, float b2, float eps, float bc1, float bc2, float wd) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float gr = grad[i] + wd * w[i];
+    const float mi = b1 * m[i] + (1.f - b1) * gr;
+    const float vi = b2 * v[i] + (1.f - b2) * gr * gr;
+    m[i] = mi;
+    v[i] = vi;
+    const float upd = lr * (mi / bc1) / (sqrtf(vi / bc2) + eps);
+    const float wn = w[i] - upd;
+    w[i] = wn;
+    if (wb) wb[i] = __float2bfloat16_rn(wn);
+}
+
+// mean-squared-error gradient on column 0 of Y [rows][ldy]: dY = 2 (Y - t) / rows (other columns 0),
+// bf16 copy for the tensor cores, per-block loss partials
+__global__ void k_mse_grad(int rows, int valid, int ldy, const float *__restrict__ Y, const float *__restrict__ t, float *dY,
+                           __nv_bfloat16 *dYb, float *loss_part) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    float l = 0.f;
+    if (r < rows) {
+        const float e = (r < valid) ? Y[(size_t)r * ldy] - t[r] : 0.f;
+        l = e * e;
+        for (int c = 0; c < ldy; c++) {
+            const float v = (c == 0) ? 2.f * e / (float)valid : 0.f;
+            dY[(size_t)r * ldy + c] = v;
+            dYb[(size_t)r * ldy + c] = __float2bfloat16_rn(v);
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) l += __shfl_down_sync(0xffffffffu, l, o);
+    __shared__ float w[32];
+    if ((threadIdx.x & 31) == 0) w[threadIdx.x >> 5] = l;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        float s = 0.f;
+        for (int k = 0; k < (int)(blockDim.x >> 5); k++) s += w[k];
+        loss_part[blockIdx.x] = s;
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// features: 14 local + 16 message channels + 2 zero pads = 32 per cell, written as bf16 rows
+// ------------------------------------------------------------------------------------------
+struct EmuNet {
+    int N, R;
+    const int *next, *up_ptr, *up_idx;
+    const double *rivelv, *elevtn, *nxtdst, *rivwth, *rivhgt, *rivlen, *rivstomax, *qref;
+};
+
+__device__ __forceinline__ float slog(float x) { return copysignf(log1pf(fabsf(x)), x); }
+
+// local features of cell i of one member; msg0 <- hourly mean outflow of the last step (hop 0)
+__global__ void k_emu_local(EmuNet n, const double *rivsto, const double *fldsto, const double *levsto,
+                            const double *rivdph, const double *flddph, const double *fldfrc, const double *qprev,
+                            const double *runoff, __nv_bfloat16 *X, int ldx, int rows_per_member, float *msg_a, float *msg_b) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n.N) return;
+    // member blockIdx.y: state arrays are member-major [M][N], X rows [M][rows_per_member]
+    const size_t mo = (size_t)blockIdx.y * n.N;
+    rivsto += mo; fldsto += mo; if (levsto) levsto += mo; rivdph += mo; flddph += mo; fldfrc += mo; qprev += mo;
+    runoff += mo; msg_a += mo; msg_b += mo;
+    X += (size_t)blockIdx.y * rows_per_member * ldx;
+    const double q = n.qref[i];
+    const double S = rivsto[i] + fldsto[i] + (levsto ? levsto[i] : 0.0);
+    float f[14];
+    f[0] = slog((float)(S / n.rivstomax[i]));
+    f[1] = (float)(rivdph[i] / n.rivhgt[i]);
+    f[2] = slog((float)flddph[i]);
+    f[3] = slog((float)(qprev[i] / q));
+    f[4] = slog((float)(runoff[i] / q));
+    f[5] = (float)fldfrc[i];
+    const bool mouth = i >= n.R;
+    const int j = mouth ? i : n.next[i];
+    const double sfc = n.rivelv[i] + rivdph[i], sfcn = mouth ? n.elevtn[i] : n.rivelv[j] + rivdph[j];
+    f[6] = slog((float)(1000.0 * (sfc - sfcn) / (mouth ? 10000.0 : n.nxtdst[i])));
+    f[7] = slog((float)(1000.0 * (n.elevtn[i] - (mouth ? n.elevtn[i] : n.elevtn[j])) / n.nxtdst[i]));
+    f[8] = logf((float)n.rivlen[i]) - 9.5f;
+    f[9] = logf((float)n.rivwth[i]) - 4.0f;
+    f[10] = logf((float)n.rivhgt[i]) - 1.0f;
+    f[11] = logf((float)q) - 3.0f;
+    f[12] = mouth ? 1.f : 0.f;
+    f[13] = slog((float)(S / (q * 3600.0)));
+    __nv_bfloat16 *row = X + (size_t)i * ldx;
+#pragma unroll
+    for (int k = 0; k < 14; k++) row[k] = __float2bfloat16_rn(f[k]);
+    row[30] = __float2bfloat16_rn(0.f);
+    row[31] = __float2bfloat16_rn(0.f);
+    msg_a[i] = (float)qprev[i];
+    msg_b[i] = (float)runoff[i];
+}
+
+// one hop of upstream message passing: out[i] = sum over upstream j of in[j]; features at column c
+__global__ void k_emu_hop(EmuNet n, const float *in_a, const float *in_b, float *out_a, float *out_b, __nv_bfloat16 *X,
+                          int ldx, int rows_per_member, int col) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n.N) return;
+    const size_t mo = (size_t)blockIdx.y * n.N;
+    in_a += mo; in_b += mo; out_a += mo; out_b += mo;
+    X += (size_t)blockIdx.y * rows_per_member * ldx;
+    float a = 0.f, b = 0.f;
+    for (int k = n.up_ptr[i]; k < n.up_ptr[i + 1]; k++) {
+        const int j = n.up_idx[k];
+        a += in_a[j];
+        b += in_b[j];
+    }
+    out_a[i] = a;
+    out_b[i] = b;
+    const float q = (float)n.qref[i];
+    X[(size_t)i * ldx + col] = __float2bfloat16_rn(slog(a / q));
+    X[(size_t)i * ldx + col + 1] = __float2bfloat16_rn(slog(b / q));
+}
+
+// Mass-conserving rollout of one coupling step from the predicted change of the transformed mean
+// outflow: Q_i = qref_i * expm1(max(log1p(Qprev_i/qref_i) + y_i, 0)), limited to the storage the cell holds plus its own runoff over
+// DT (so storage never goes negative whatever its upstream delivers); storage then changes by
+// (inflow + runoff - outflow) * DT with the inflow gathered over the upstream CSR.
+__global__ void k_emu_rollout(EmuNet n, const float *y, int ldy, int rows_per_member, const int *active, double dt,
+                              const double *runoff, const double *rivsto, const double *fldsto, const double *levsto,
+                              const double *qprev, double *qout) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n.N || !active[blockIdx.y]) return;
+    const size_t mo = (size_t)blockIdx.y * n.N;
+    y += (size_t)blockIdx.y * rows_per_member * ldy;
+    runoff += mo; rivsto += mo; fldsto += mo; if (levsto) levsto += mo; qout += mo;
+    const double S = rivsto[i] + fldsto[i] + (levsto ? levsto[i] : 0.0);
+    // the network predicts the change of log1p(Q/qref) over the step (residual on the last outflow)
+    const double base = log1p(fmax(qprev[mo + i], 0.0) / n.qref[i]);
+    const double yi = fmax(base + (double)y[(size_t)i * ldy], 0.0);
+    double q = n.qref[i] * expm1(yi);
+    q = fmin(q, S / dt + runoff[i]);
+    qout[i] = fmax(q, 0.0);
+}
+
+__global__ void k_emu_update(EmuNet n, const int *active, double dt, const double *runoff, const double *qout, double *rivsto,
+                             double *fldsto, double *levsto, double *rivout_pre, double *fldout_pre, double *qprev) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n.N || !active[blockIdx.y]) return;
+    const size_t mo = (size_t)blockIdx.y * n.N;
+    runoff += mo; qout += mo; rivsto += mo; fldsto += mo; if (levsto) levsto += mo; rivout_pre += mo; fldout_pre += mo;
+    qprev += mo;
+    double inflow = 0.0;
+    for (int k = n.up_ptr[i]; k < n.up_ptr[i + 1]; k++) inflow += qout[n.up_idx[k]];
+    const double S = rivsto[i] + fldsto[i] + (levsto ? levsto[i] : 0.0);
+    const double Snew = fmax(S + (inflow + runoff[i] - qout[i]) * dt, 0.0);
+    rivsto[i] = Snew;   // the stage scheme re-splits river / floodplain / protected storage
+    fldsto[i] = 0.0;
+    if (levsto) levsto[i] = 0.0;
+    rivout_pre[i] = qout[i];
+    fldout_pre[i] = 0.0;
+    qprev[i] = qout[i];
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *cmf_emu_last_error(void) { return g_emu_err.c_str(); }
+
+int cmf_emu_gemm(int M, int N, int K, const void *A, int lda, int transA, const void *B, int ldb, int transB, float *C,
+                 int ldc, void *Cb, int ldcb, const float *bias, int relu, int accumulate, int ksplit, void *stream) {
+    if (M % TM || N % TN || K % TK || M <= 0 || N <= 0 || K <= 0)
+        return emu_err(CMF_E_ARG, "cmf_emu_gemm: M,N must be multiples of 64 and K of 32");
+    if (ksplit < 1) ksplit = 1;
+    int kps = ((K / ksplit + TK - 1) / TK) * TK;
+    const int splits = (K + kps - 1) / kps;
+    if (splits > 1 && !accumulate) return emu_err(CMF_E_ARG, "cmf_emu_gemm: split-K needs accumulate=1");
+    dim3 grid(N / TN, M / TM, splits);
+    k_gemm<<<grid, 128, 0, (cudaStream_t)stream>>>(M, N, K, (const __nv_bfloat16 *)A, lda, transA, (const __nv_bfloat16 *)B,
+                                                  ldb, transB, C, ldc, (__nv_bfloat16 *)Cb, ldcb, bias, relu, accumulate, kps);
+    EMU_TRY(cudaGetLastError());
+    return CMF_OK;
+}
+
+int cmf_emu_relu_bwd(int n, const float *dA, const void *act, void *dZ, float *dZf, void *stream) {
+    k_relu_bwd<<<(n + 255) / 256, 256, 0, (cudaStream_t)stream>>>(n, dA, (const __nv_bfloat16 *)act, (__nv_bfloat16 *)dZ, dZf);
+    EMU_TRY(cudaGetLastError());
+    return CMF_OK;
+}
+
+int cmf_emu_mse_grad(int rows, int valid, int ldy, const float *Y, const float *t, float *dY, void *dYb, float *loss_part,
+                     void *stream) {
+    k_mse_grad<<<(rows + 255) / 256, 256, 0, (cudaStream_t)stream>>>(rows, valid, ldy, Y, t, dY, (__nv_bfloat16 *)dYb, loss_part);
+    EMU_TRY(cudaGetLastError());
+    return CMF_OK;
+}
+
+int cmf_emu_colsum(int rows, int cols, const float *X, float *out, void *stream) {
+    k_colsum<<<cols, 256, 0, (cudaStream_t)stream>>>(rows, cols, X, out);
+    EMU_TRY(cudaGetLastError());
+    return CMF_OK;
+}
+
+int cmf_emu_adam(int n, float *w, void *wb, const float *grad, float *m, float *v, float lr, float b1, float b2, float eps,
+                 int step, float wd, void *stream) {
+    const float bc1 = 1.f - powf(b1, (float)step), bc2 = 1.f - powf(b2, (float)step);
+    k_adam<<<(n + 255) / 256, 256, 0, (cudaStream_t)stream>>>(n, w, (__nv_bfloat16 *)wb, grad, m, v, lr, b1, b2, eps, bc1, bc2, wd);
+    EMU_TRY(cudaGetLastError());
+    return CMF_OK;
+}
+
+// Features of one member: X [N_pad][32] bf16; scratch a/b/c/d float [N] for the message ping-pong.
+int cmf_emu_features(const cmf_emu_net *net, const cmf_emu_member *mb, int nmembers, void *X, int ldx, int rows_per_member,
+                     int hops, float *sa, float *sb, float *sc, float *sd, void *stream) {
+    if (!net || !mb || !X || hops < 0 || 14 + 2 * hops > 32 || ldx < 32 || nmembers < 1 || rows_per_member < net->nseqall)
+        return emu_err(CMF_E_ARG, "cmf_emu_features: bad arguments (14 + 2*hops must fit 32 columns)");
+    EmuNet n{net->nseqall, net->nseqriv, net->next, net->up_ptr, net->up_idx, net->rivelv, net->elevtn, net->nxtdst,
+             net->rivwth, net->rivhgt, net->rivlen, net->rivstomax, net->qref};
+    cudaStream_t st = (cudaStream_t)stream;
+    const dim3 blocks((n.N + 255) / 256, nmembers);
+    k_emu_local<<<blocks, 256, 0, st>>>(n, mb->rivsto, mb->fldsto, mb->levsto, mb->rivdph, mb->flddph, mb->fldfrc, mb->qprev,
+                                        mb->runoff, (__nv_bfloat16 *)X, ldx, rows_per_member, sa, sb);
+    float *ia = sa, *ib = sb, *oa = sc, *ob = sd;
+    for (int h = 0; h < hops; h++) {
+        k_emu_hop<<<blocks, 256, 0, st>>>(n, ia, ib, oa, ob, (__nv_bfloat16 *)X, ldx, rows_per_member, 14 + 2 * h);
+        float *t = ia; ia = oa; oa = t;
+        t = ib; ib = ob; ob = t;
+    }
+    EMU_TRY(cudaGetLastError());
+    return CMF_OK;
+}
+
+int cmf_emu_rollout(const cmf_emu_net *net, const cmf_emu_member *mb, int nmembers, const int *active_dev, const float *y,
+                    int ldy, int rows_per_member, double dt, double *qout, void *stream) {
+    if (!net || !mb || !y || !qout || !active_dev || nmembers < 1) return emu_err(CMF_E_ARG, "cmf_emu_rollout: null argument");
+    EmuNet n{net->nseqall, net->nseqriv, net->next, net->up_ptr, net->up_idx, net->rivelv, net->elevtn, net->nxtdst,
+             net->rivwth, net->rivhgt, net->rivlen, net->rivstomax, net->qref};
+    cudaStream_t st = (cudaStream_t)stream;
+    const dim3 blocks((n.N + 255) / 256, nmembers);
+    k_emu_rollout<<<blocks, 256, 0, st>>>(n, y, ldy, rows_per_member, active_dev, dt, mb->runoff, mb->rivsto, mb->fldsto,
+                                          mb->levsto, mb->qprev, qout);
+    k_emu_update<<<blocks, 256, 0, st>>>(n, active_dev, dt, mb->runoff, qout, mb->rivsto, mb->fldsto, mb->levsto,
+                                         mb->rivout_pre, mb->fldout_pre, mb->qprev);
+    EMU_TRY(cudaGetLastError());
+    return CMF_OK;
+}
+
+}  // extern "C"

@@ -739,6 +739,60 @@ int cmf_gpu_ctx_last_nt(cmf_gpu_ctx *c, int32_t *nt_out, double *dt_out) {
     return CMF_OK;
 }
 
+int cmf_gpu_ctx_emu_views(cmf_gpu_ctx *c, int32_t m, cmf_emu_net *net, cmf_emu_member *mb) {
+    if (!c || m < 0 || m >= c->dims.nmembers) return set_err(CMF_E_ARG, "bad member");
+    if (!c->opts.ldiag) return set_err(CMF_E_UNSUPPORTED, "emulator views need ldiag (D2OUTFLW_aAVG)");
+    const size_t o = (size_t)m * c->dims.nseqall;
+    if (net) {
+        net->nseqall = c->net.N; net->nseqriv = c->net.R;
+        net->next = c->net.next; net->up_ptr = c->net.up_ptr; net->up_idx = c->net.up_idx;
+        net->rivelv = c->net.rivelv; net->elevtn = c->net.elevtn; net->nxtdst = c->net.nxtdst;
+        net->rivwth = c->net.rivwth; net->rivhgt = c->net.rivhgt; net->rivlen = c->net.rivlen;
+        net->rivstomax = c->net.rivstomax; net->qref = nullptr;
+    }
+    if (mb) {
+        const cmf::State &s = c->st;
+        mb->rivsto = s.rivsto + o; mb->fldsto = s.fldsto + o; mb->levsto = c->opts.llevee ? s.levsto + o : nullptr;
+        mb->rivdph = s.rivdph + o; mb->flddph = s.flddph + o; mb->fldfrc = s.fldfrc + o;
+        mb->qprev = s.a_outflw + o; mb->runoff = s.runoff + o;
+        mb->rivout_pre = s.rivout_pre + o; mb->fldout_pre = s.fldout_pre + o;
+    }
+    return CMF_OK;
+}
+
+int cmf_gpu_ctx_copy_member(cmf_gpu_ctx *d, int32_t dm, cmf_gpu_ctx *s, int32_t sm) {
+    if (!d || !s || dm < 0 || sm < 0 || dm >= d->dims.nmembers || sm >= s->dims.nmembers)
+        return set_err(CMF_E_ARG, "bad member");
+    if (d->dims.nseqall != s->dims.nseqall || d->opts.llevee != s->opts.llevee || d->opts.ldamout != s->opts.ldamout ||
+        d->net.P != s->net.P || d->net.Lp != s->net.Lp || d->opts.ldiag != s->opts.ldiag)
+        return set_err(CMF_E_ARG, "contexts differ in network or options");
+    CUDA_TRY(cudaSetDevice(d->device));
+    const size_t N = d->dims.nseqall, od = (size_t)dm * N, os = (size_t)sm * N;
+    const cmf::State &A = d->st, &B = s->st;
+    double *cells_d[] = {A.rivsto, A.fldsto, A.rivout_pre, A.fldout_pre, A.rivdph_pre, A.fldsto_pre, A.rivdph, A.flddph,
+                         A.fldfrc, A.fldare, A.sfcelv, A.storge, A.runoff, A.a_outflw};
+    double *cells_s[] = {B.rivsto, B.fldsto, B.rivout_pre, B.fldout_pre, B.rivdph_pre, B.fldsto_pre, B.rivdph, B.flddph,
+                         B.fldfrc, B.fldare, B.sfcelv, B.storge, B.runoff, B.a_outflw};
+    for (size_t k = 0; k < sizeof(cells_d) / sizeof(cells_d[0]); k++) {
+        if (!d->opts.ldiag && k == 13) continue;
+        CUDA_TRY(cudaMemcpyAsync(cells_d[k] + od, cells_s[k] + os, N * 8, cudaMemcpyDeviceToDevice, s->stream));
+    }
+    if (d->opts.llevee) {
+        CUDA_TRY(cudaMemcpyAsync(A.levsto + od, B.levsto + os, N * 8, cudaMemcpyDeviceToDevice, s->stream));
+        CUDA_TRY(cudaMemcpyAsync(A.levdph + od, B.levdph + os, N * 8, cudaMemcpyDeviceToDevice, s->stream));
+    }
+    if (d->opts.ldamout) {
+        CUDA_TRY(cudaMemcpyAsync(A.damsto + od, B.damsto + os, N * 8, cudaMemcpyDeviceToDevice, s->stream));
+        CUDA_TRY(cudaMemcpyAsync(A.daminf + od, B.daminf + os, N * 8, cudaMemcpyDeviceToDevice, s->stream));
+    }
+    if (d->net.P > 0) {
+        const size_t PL = (size_t)d->net.P * d->net.Lp;
+        CUDA_TRY(cudaMemcpyAsync(A.pthflw_pre + dm * PL, B.pthflw_pre + sm * PL, PL * 8, cudaMemcpyDeviceToDevice, s->stream));
+    }
+    CUDA_TRY(cudaStreamSynchronize(s->stream));
+    return CMF_OK;
+}
+
 void *cmf_gpu_ctx_stream(cmf_gpu_ctx *c) { return c ? (void *)c->stream : nullptr; }
 int64_t cmf_gpu_ctx_kernel_launches(cmf_gpu_ctx *c) { return c ? c->launches : 0; }
 int32_t cmf_gpu_ctx_block_size(cmf_gpu_ctx *c) { return c ? c->block : 0; }

@@ -220,6 +220,49 @@ typedef struct cmf_stage_dev_args {
 int cmf_gpu_stage_noalloc(const cmf_stage_dev_args *args);
 
 /* ======================================================================================== */
+/* Learned per-cell emulator (no counterpart in the reference): device building blocks       */
+/* ======================================================================================== */
+/* Device views of a context's network (next: 0-based downstream, -1 at mouths; upstream CSR in
+ * the reference's I1UPST order).  qref (per-cell discharge scale, m3/s) is set by the caller. */
+typedef struct cmf_emu_net {
+    int32_t nseqall, nseqriv;
+    const int32_t *next, *up_ptr, *up_idx;
+    const double *rivelv, *elevtn, *nxtdst, *rivwth, *rivhgt, *rivlen, *rivstomax, *qref;
+} cmf_emu_net;
+/* Device views of one member's state; qprev is the mean outflow of the last coupling step
+ * (D2OUTFLW_aAVG of the physics, or the emulator's own prediction). */
+typedef struct cmf_emu_member {
+    double *rivsto, *fldsto, *levsto, *rivdph, *flddph, *fldfrc, *qprev, *runoff, *rivout_pre, *fldout_pre;
+} cmf_emu_member;
+int cmf_gpu_ctx_emu_views(cmf_gpu_ctx *ctx, int32_t member, cmf_emu_net *net, cmf_emu_member *mb);
+/* Device-to-device copy of one member's prognostic state and last-step averages between two
+ * contexts of the same network (hand-over between the emulator and the judging plain solver). */
+int cmf_gpu_ctx_copy_member(cmf_gpu_ctx *dst, int32_t dst_member, cmf_gpu_ctx *src, int32_t src_member);
+/* BF16 tensor-core GEMM, fp32 accumulate: C[M,N] (+)= op(A)[M,K] op(B)[K,N]; epilogue bias+ReLU,
+ * fp32 and/or bf16 output, or atomic accumulation for split-K (ksplit > 1). M,N % 64, K % 32. */
+int cmf_emu_gemm(int M, int N, int K, const void *A, int lda, int transA, const void *B, int ldb, int transB,
+                 float *C, int ldc, void *Cb, int ldcb, const float *bias, int relu, int accumulate, int ksplit,
+                 void *stream);
+int cmf_emu_relu_bwd(int n, const float *dA, const void *act, void *dZ, float *dZf, void *stream);
+int cmf_emu_colsum(int rows, int cols, const float *X, float *out, void *stream);
+/* MSE gradient on column 0 of Y (rows padded, `valid` real rows): dY fp32 + bf16, loss partials
+ * per 256-row block in loss_part[(rows+255)/256]. */
+int cmf_emu_mse_grad(int rows, int valid, int ldy, const float *Y, const float *t, float *dY, void *dYb,
+                     float *loss_part, void *stream);
+int cmf_emu_adam(int n, float *w, void *wb, const float *grad, float *m, float *v, float lr, float b1, float b2,
+                 float eps, int step, float wd, void *stream);
+/* 14 local features + 2 channels x `hops` upstream messages -> X rows (bf16, ldx >= 32), for
+ * nmembers members whose state arrays start at the member-0 views in mb (member-major [M][N]);
+ * member m's rows start at m * rows_per_member.  Scratch sa..sd: float [M][N] each. */
+int cmf_emu_features(const cmf_emu_net *net, const cmf_emu_member *mb, int nmembers, void *X, int ldx,
+                     int rows_per_member, int hops, float *sa, float *sb, float *sc, float *sd, void *stream);
+/* Mass-conserving step from predicted transformed outflows y (column 0, stride ldy) for every
+ * member with active_dev[m] != 0 (device int array); qout: double [M][N] scratch. */
+int cmf_emu_rollout(const cmf_emu_net *net, const cmf_emu_member *mb, int nmembers, const int *active_dev,
+                    const float *y, int ldy, int rows_per_member, double dt, double *qout, void *stream);
+const char *cmf_emu_last_error(void);
+
+/* ======================================================================================== */
 /* Default-context API bound by the Fortran ISO_C_BINDING shim                              */
 /* ======================================================================================== */
 int cmf_gpu_init(const cmf_dims *dims, const cmf_params *params, const cmf_map_ptrs *maps,

@@ -1,0 +1,156 @@
+"""Learned emulator: CPU reference checks, tensor-core kernels vs the CPU reference, training on
+solver trajectories, and what the trained network gains over the method without it."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+
+def _rand_params(rng, scale=0.1):
+    W = [rng.standard_normal((64, 128)) * scale, rng.standard_normal((128, 128)) * scale,
+         rng.standard_normal((128, 128)) * scale, rng.standard_normal((128, 64)) * scale]
+    W[0][30:, :] = 0
+    W[3][:, 1:] = 0
+    b = [rng.standard_normal(128) * 0.05, rng.standard_normal(128) * 0.05, rng.standard_normal(128) * 0.05,
+         rng.standard_normal(64) * 0.05]
+    return W, b
+
+
+def test_reference_backward_matches_finite_differences():
+    from emu_ref import loss_and_grads
+
+    rng = np.random.default_rng(0)
+    W, b = _rand_params(rng, 0.3)
+    X = rng.standard_normal((16, 64))
+    X[:, 30:] = 0
+    t = rng.standard_normal(16)
+    _, gW, gb = loss_and_grads(X, t, W, b, bf16=False)
+    eps = 1e-6
+    for li, (r, c) in [(0, (3, 7)), (1, (10, 20)), (2, (5, 100)), (3, (17, 0))]:
+        Wp = [w.copy() for w in W]
+        Wm = [w.copy() for w in W]
+        Wp[li][r, c] += eps
+        Wm[li][r, c] -= eps
+        num = (loss_and_grads(X, t, Wp, b, False)[0] - loss_and_grads(X, t, Wm, b, False)[0]) / (2 * eps)
+        assert abs(num - gW[li][r, c]) < 1e-5 * max(1.0, abs(num)), (li, num, gW[li][r, c])
+    bp = [v.copy() for v in b]
+    bp[2][9] += eps
+    bm = [v.copy() for v in b]
+    bm[2][9] -= eps
+    num = (loss_and_grads(X, t, W, bp, False)[0] - loss_and_grads(X, t, W, bm, False)[0]) / (2 * eps)
+    assert abs(num - gb[2][9]) < 1e-5 * max(1.0, abs(num))
+
+
+def test_nse_known_answers():
+    from cmf_b200.emulator import nse
+
+    obs = np.array([[1.0, 2.0], [2.0, 4.0], [3.0, 9.0], [4.0, 1.0]])
+    assert np.allclose(nse(obs, obs), 1.0)
+    assert np.allclose(nse(np.repeat(obs.mean(0, keepdims=True), 4, 0), obs), 0.0)
+    sim = obs + np.array([[0.1, 0.0]] * 4)
+    assert np.isclose(nse(sim, obs)[0], 1.0 - 4 * 0.01 / 5.0)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("ta,tb,ks", [(0, 0, 1), (1, 0, 1), (0, 1, 1), (1, 0, 4)])
+def test_gemm_kernel_matches_numpy(ta, tb, ks):
+    import torch
+
+    from cmf_b200.emulator import _emu_lib, echeck
+    from emu_ref import to_bf16
+
+    lib = _emu_lib()
+    rng = np.random.default_rng(ta * 2 + tb + ks)
+    M, N, K = 128, 64, 256
+    A = to_bf16(rng.standard_normal((K, M) if ta else (M, K)))
+    B = to_bf16(rng.standard_normal((N, K) if tb else (K, N)))
+    dev = torch.device("cuda", 0)
+    tA = torch.tensor(A, device=dev).to(torch.bfloat16)
+    tB = torch.tensor(B, device=dev).to(torch.bfloat16)
+    C = torch.zeros(M, N, device=dev)
+    echeck(lib.cmf_emu_gemm(M, N, K, tA.data_ptr(), A.shape[1], ta, tB.data_ptr(), B.shape[1], tb, C.data_ptr(), N,
+                            None, 0, None, 0, 1 if ks > 1 else 0, ks, None), "gemm")
+    torch.cuda.synchronize()
+    ref = (A.T if ta else A).astype(np.float64) @ (B.T if tb else B).astype(np.float64)
+    assert np.allclose(C.cpu().numpy(), ref, rtol=1e-5, atol=1e-3)
+
+
+@pytest.mark.gpu
+def test_training_kernels_gradients_match_cpu_reference():
+    import torch
+
+    from cmf_b200.emulator import MLP
+    from emu_ref import loss_and_grads, to_bf16
+
+    dev = torch.device("cuda", 0)
+    rng = np.random.default_rng(3)
+    mlp = MLP(dev, seed=1)
+    W, b = _rand_params(rng, 0.15)
+    mlp.load({"W": W, "b": b})
+    R = 512
+    X = to_bf16(rng.standard_normal((R, 64)))
+    X[:, 30:] = 0
+    t = rng.standard_normal(R).astype(np.float32)
+    loss = mlp.loss_and_grad(torch.tensor(X, device=dev).to(torch.bfloat16), torch.tensor(t, device=dev), R)
+    torch.cuda.synchronize()
+    rloss, gW, gb = loss_and_grads(X, t, [w.astype(np.float32) for w in W], [v.astype(np.float32) for v in b], bf16=True)
+    assert abs(float(loss) - rloss) <= 1e-3 * abs(rloss)
+    for li in range(4):
+        g = mlp.gW[li].cpu().numpy()
+        err = np.linalg.norm(g - gW[li]) / max(np.linalg.norm(gW[li]), 1e-30)
+        assert err < 2e-2, (li, err)
+        e2 = np.linalg.norm(mlp.gb[li].cpu().numpy() - gb[li]) / max(np.linalg.norm(gb[li]), 1e-30)
+        assert e2 < 2e-2, (li, e2)
+
+
+@pytest.mark.gpu
+def test_trained_emulator_beats_untrained_and_persistence(case_dirs):
+    """E1-E5 on the config-1 laws: train on solver trajectories, then roll out 24 h from a plain
+    state and compare the gauge discharge with the plain solver: the trained network must be far
+    closer than the untrained one and than persistence (last-step outflow held for the day)."""
+    import torch
+
+    from cmf_b200 import HostModel, PhysicsGPU
+    from cmf_b200 import emulator as E
+
+    h = HostModel(case_dirs["cfg1s"])
+    dev = torch.device("cuda", 0)
+    X, t = E.generate_trajectories(h, members=6, hours=72, spinup=12, seed=10)
+    mlp = E.MLP(dev, seed=0, lr=2e-3)
+    hist = E.train(mlp, X, t, iters=3000, batch=4096, seed=0)
+    print("training loss", hist[0], hist[-1])
+    assert hist[-1][1] < 0.5 * hist[0][1]
+    # evaluation: 24 h rollout from a spun-up plain state with unseen forcing
+    M = 2
+    gr = h.map("grarea")
+    gens = E.runoff_generators(h.dims.nseqall, M, 999)
+    plain = PhysicsGPU(h, nmembers=M)
+    for _ in range(24):
+        plain.put_runoff(E.runoff_step(gens, gr))
+        plain.advance()
+    qref = E.qref_from_host(h)
+    gauges = np.argsort(-qref)[:20]
+    runs = {}
+    for name, net in (("trained", mlp), ("untrained", E.MLP(dev, seed=5))):
+        ens = E.SurrogateEnsemble(h, net, members=M, judge_slots=1, gauges=gauges, resync_hours=10 ** 6)
+        ens.set_state_from(plain)
+        runs[name] = ens
+    q0 = runs["trained"].fe.qprev().cpu().numpy()[:, gauges]
+    truth = []
+    est = {k: [] for k in runs}
+    for hh in range(24):
+        r = E.runoff_step(gens, gr)
+        plain.put_runoff(r)
+        plain.advance()
+        truth.append(plain.get_diag_fields({"outflw_aavg": np.zeros(M * h.dims.nseqall)})["outflw_aavg"].reshape(M, -1)[:, gauges])
+        for k, ens in runs.items():
+            ens.emu.put_runoff(r)
+            ens.emu_step()
+            ens.emu.stage()
+            est[k].append(ens.fe.qprev().cpu().numpy()[:, gauges])
+    truth = np.stack(truth)
+    err = {k: float(np.mean(np.abs(np.stack(v) - truth) / np.maximum(np.abs(truth), 1e-3))) for k, v in est.items()}
+    err["persistence"] = float(np.mean(np.abs(q0[None] - truth) / np.maximum(np.abs(truth), 1e-3)))
+    print("mean relative gauge-discharge error over 24 h:", err)
+    assert err["trained"] < 0.5 * err["untrained"]
+    assert err["trained"] < err["persistence"]
