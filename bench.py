@@ -344,6 +344,14 @@ def gpu_arm(args) -> int:
             "L_bar": Lbar,
             "step_achieved_gbs": sum(pb.values()) * M * (loop_iters / max(K, 1)) / (secs / K) / 1e9}
 
+    sur = None
+    if ws == 1 and not args.no_surrogate:
+        from cmf_b200 import surrogate
+
+        try:
+            sur = surrogate.measure(h, dev, members=args.sur_members, days=args.sur_days)
+        except Exception as e:       # reported, never silently replaced by another number
+            sur = {"error": f"{type(e).__name__}: {e}"}
     out = 0
     if rank == 0:
         cpu = None
@@ -370,6 +378,7 @@ def gpu_arm(args) -> int:
             "roofline": roof,
             "cpu_baseline": cpu,
             "clocks": clocks,
+            "surrogate": sur,
         }
         print(json.dumps(line))
     if ws > 1:
@@ -387,6 +396,10 @@ def main() -> int:
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--members", type=int, default=1)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-surrogate", action="store_true",
+                    help="skip the surrogate-assisted vs plain ensemble measurement")
+    ap.add_argument("--sur-members", type=int, default=16)
+    ap.add_argument("--sur-days", type=int, default=4)
     ap.add_argument("--launch-mode", type=int, default=0, choices=[0, 1],
                     help="0: CUDA graph with a device-side sub-step loop; 1: the same kernels as plain "
                          "launches from a host loop (what ncu can profile kernel by kernel)")

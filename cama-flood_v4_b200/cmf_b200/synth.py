@@ -430,24 +430,28 @@ class DailyGammaRunoff:
 
 class AR1GammaRunoff:
     """Hourly runoff from a seeded AR(1) (phi=0.9) Gaussian process through a Gaussian copula
-    with Gamma(k=0.8, theta=2.5 mm/day) marginals (float32 mm/day)."""
+    with Gamma(k=0.8, theta=2.5 mm/day) marginals (float32 mm/day).  The Gamma quantile of the
+    standard-normal value is read from a table built once (400,001 points on z in [-9, 9])."""
+
+    _tables: dict = {}
 
     def __init__(self, ncell: int, seed: int, phi: float = 0.9, shape: float = 0.8, theta: float = 2.5):
-        from scipy.special import gammaincinv, ndtr
+        key = (shape, theta)
+        if key not in AR1GammaRunoff._tables:
+            from scipy.special import gammaincinv, ndtr
 
-        self._gi = gammaincinv
-        self._ndtr = ndtr
+            z = np.linspace(-9.0, 9.0, 400001)
+            u = np.clip(ndtr(z), 1e-300, 1.0 - 1e-16)
+            AR1GammaRunoff._tables[key] = (z, gammaincinv(shape, u) * theta)
+        self._z, self._q = AR1GammaRunoff._tables[key]
         self.rng = np.random.default_rng(seed + 2000003)
         self.phi = phi
-        self.shape = shape
-        self.theta = theta
         self.z = self.rng.standard_normal(ncell)
 
     def next(self) -> np.ndarray:
         eps = self.rng.standard_normal(self.z.shape[0])
         self.z = self.phi * self.z + np.sqrt(1.0 - self.phi * self.phi) * eps
-        u = np.clip(self._ndtr(self.z), 1e-12, 1.0 - 1e-12)
-        return (self._gi(self.shape, u) * self.theta).astype(np.float32)
+        return np.interp(self.z, self._z, self._q).astype(np.float32)
 
 
 # ----------------------------------------------------------------------------------------

@@ -55,7 +55,7 @@ __global__ void __launch_bounds__(128) k_gemm(int M, int N, int K, const __nv_bf
                                               int relu, int accumulate, int k_per_split) {
     __shared__ __align__(16) __nv_bfloat16 As[TM][TK + PAD];
     __shared__ __align__(16) __nv_bfloat16 Bs[TN][TK + PAD];
-    const int m0 = blockIdx.y * TM, n0 = blockIdx.x * TN;
+    const int m0 = blockIdx.x * TM, n0 = blockIdx.y * TN;   // row tiles on x: up to 2^31-1 of them
     const int kbeg = blockIdx.z * k_per_split, kend = min(K, kbeg + k_per_split);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
@@ -320,7 +320,7 @@ int cmf_emu_gemm(int M, int N, int K, const void *A, int lda, int transA, const 
     int kps = ((K / ksplit + TK - 1) / TK) * TK;
     const int splits = (K + kps - 1) / kps;
     if (splits > 1 && !accumulate) return emu_err(CMF_E_ARG, "cmf_emu_gemm: split-K needs accumulate=1");
-    dim3 grid(N / TN, M / TM, splits);
+    dim3 grid(M / TM, N / TN, splits);
     k_gemm<<<grid, 128, 0, (cudaStream_t)stream>>>(M, N, K, (const __nv_bfloat16 *)A, lda, transA, (const __nv_bfloat16 *)B,
                                                   ldb, transB, C, ldc, (__nv_bfloat16 *)Cb, ldcb, bias, relu, accumulate, kps);
     EMU_TRY(cudaGetLastError());

@@ -777,6 +777,10 @@ int cmf_gpu_ctx_copy_member(cmf_gpu_ctx *d, int32_t dm, cmf_gpu_ctx *s, int32_t 
         if (!d->opts.ldiag && k == 13) continue;
         CUDA_TRY(cudaMemcpyAsync(cells_d[k] + od, cells_s[k] + os, N * 8, cudaMemcpyDeviceToDevice, s->stream));
     }
+    // D2RIVOUT/D2FLDOUT equal the _PRE arrays after a step; keep the destination consistent even
+    // if it still reads the host-set copies (first step after an upload)
+    CUDA_TRY(cudaMemcpyAsync(A.rivout_cur + od, B.rivout_pre + os, N * 8, cudaMemcpyDeviceToDevice, s->stream));
+    CUDA_TRY(cudaMemcpyAsync(A.fldout_cur + od, B.fldout_pre + os, N * 8, cudaMemcpyDeviceToDevice, s->stream));
     if (d->opts.llevee) {
         CUDA_TRY(cudaMemcpyAsync(A.levsto + od, B.levsto + os, N * 8, cudaMemcpyDeviceToDevice, s->stream));
         CUDA_TRY(cudaMemcpyAsync(A.levdph + od, B.levdph + os, N * 8, cudaMemcpyDeviceToDevice, s->stream));

@@ -154,3 +154,40 @@ def test_trained_emulator_beats_untrained_and_persistence(case_dirs):
     print("mean relative gauge-discharge error over 24 h:", err)
     assert err["trained"] < 0.5 * err["untrained"]
     assert err["trained"] < err["persistence"]
+
+
+@pytest.mark.gpu
+def test_surrogate_controller_judges_resyncs_and_hands_back(case_dirs):
+    """Controller mechanics: a rotating subset is judged every 24 h and re-synced to the plain state;
+    with a tolerance nobody can meet, every judged member is handed back to the plain solver and from
+    then on reports the plain solver's discharge."""
+    import torch
+
+    from cmf_b200 import HostModel, PhysicsGPU
+    from cmf_b200 import emulator as E
+
+    h = HostModel(case_dirs["cfg0"])
+    dev = torch.device("cuda", 0)
+    M = 4
+    gr = h.map("grarea")
+    gens = E.runoff_generators(h.dims.nseqall, M, 5)
+    plain = PhysicsGPU(h, nmembers=M)
+    for _ in range(6):
+        plain.put_runoff(E.runoff_step(gens, gr))
+        plain.advance()
+    runoff = np.stack([E.runoff_step(gens, gr) for _ in range(48)])
+    G = np.argsort(-E.qref_from_host(h))[:10]
+    ens = E.SurrogateEnsemble(h, E.MLP(dev, seed=3), members=M, judge_slots=2, gauges=G, tol_rel=-1.0)
+    ens.set_state_from(plain)
+    out = ens.run(runoff)
+    # day 1 judges members 0 and 1, both fail and are handed back; on day 2 they fill both judge slots
+    assert ens.stats["judged"] == 2 and ens.stats["fallback"] == 2 and sorted(ens.plain) == [0, 1]
+    # members handed back after day 1 report the plain solver: compare with the truth on day 2
+    truth = []
+    for hh in range(48):
+        plain.put_runoff(runoff[hh])
+        plain.advance()
+        truth.append(plain.get_diag_fields({"outflw_aavg": np.zeros(M * h.dims.nseqall)})["outflw_aavg"].reshape(M, -1)[:, G])
+    truth = np.stack(truth)
+    for m in sorted(ens.plain)[:2]:
+        assert np.allclose(out[24:, m], truth[24:, m], rtol=1e-9, atol=1e-9)
