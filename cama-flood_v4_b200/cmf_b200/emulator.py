@@ -126,7 +126,7 @@ class MLP:
                 lst.append(torch.zeros(n, device=device))
         self.step = 0
         self.lr = lr
-        self.stream = None
+        self.stream = torch.cuda.current_stream(device).cuda_stream
 
     def state_dict(self):
         return {"W": [w.cpu().numpy() for w in self.W], "b": [b.cpu().numpy() for b in self.b]}
@@ -226,19 +226,28 @@ class Features:
         self.X = torch.zeros(self.M * self.Np, IN, dtype=torch.bfloat16, device=self.dev)
         self.qout = torch.empty(self.M * self.N, dtype=torch.float64, device=self.dev)
 
+    # The library works on its own non-blocking stream, the emulator on torch's current stream:
+    # every boundary drains the side that wrote last, so neither reads the other's arrays mid-update.
     def build(self):
+        self.phys.synchronize()
         s = self.scratch
         echeck(self.lib.cmf_emu_features(C.byref(self.net), C.byref(self.mb), self.M, self.X.data_ptr(), IN, self.Np, HOPS,
-                                         s[0].data_ptr(), s[1].data_ptr(), s[2].data_ptr(), s[3].data_ptr(), None), "features")
+                                         s[0].data_ptr(), s[1].data_ptr(), s[2].data_ptr(), s[3].data_ptr(),
+                                         self.torch.cuda.current_stream(self.dev).cuda_stream), "features")
         return self.X
 
     def qprev(self):
-        """[M, N] view (copy) of the last-step mean outflow."""
-        return _raw_f64(self.mb.qprev, self.M * self.N, self.dev).clone().view(self.M, self.N)
+        """[M, N] copy of the last-step mean outflow."""
+        self.phys.synchronize()
+        out = _raw_f64(self.mb.qprev, self.M * self.N, self.dev).clone().view(self.M, self.N)
+        self.torch.cuda.current_stream(self.dev).synchronize()
+        return out
 
     def rollout(self, Y, active):
         echeck(self.lib.cmf_emu_rollout(C.byref(self.net), C.byref(self.mb), self.M, active.data_ptr(), Y.data_ptr(), OUT,
-                                        self.Np, float(self.phys.host.dt), self.qout.data_ptr(), None), "rollout")
+                                        self.Np, float(self.phys.host.dt), self.qout.data_ptr(),
+                                        self.torch.cuda.current_stream(self.dev).cuda_stream), "rollout")
+        self.torch.cuda.current_stream(self.dev).synchronize()
 
 
 def target_transform(torch, q, qref):
@@ -281,6 +290,7 @@ def generate_trajectories(host, members: int, hours: int, spinup: int, seed: int
         phys.put_runoff(runoff_step(gens, gr))
         X = fe.build().clone()                        # state at the start of the step + its runoff
         q0 = fe.qprev()
+        torch.cuda.current_stream(fe.dev).synchronize()
         phys.advance()
         t = residual_target(torch, fe.qprev(), q0, fe.qref[None, :]).float()   # mean outflow over the step
         for m in range(members):
