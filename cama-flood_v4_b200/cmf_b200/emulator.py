@@ -51,6 +51,9 @@ def _emu_lib():
         lib.cmf_emu_adam.argtypes = [i, vp, vp, vp, vp, vp, f, f, f, f, i, f, vp]
         lib.cmf_emu_features.argtypes = [C.POINTER(EmuNet), C.POINTER(EmuMember), i, vp, i, i, i, vp, vp, vp, vp, vp]
         lib.cmf_emu_rollout.argtypes = [C.POINTER(EmuNet), C.POINTER(EmuMember), i, vp, vp, i, i, d, vp, vp]
+        lib.cmf_emu_mlp_pack_bytes.restype = C.c_size_t
+        lib.cmf_emu_mlp_pack.argtypes = [vp, vp, vp, vp, i, vp, vp]
+        lib.cmf_emu_mlp_fused.argtypes = [vp, i, i, vp, vp, vp, vp, vp, vp, vp]
         lib.cmf_emu_last_error.restype = C.c_char_p
         lib.cmf_gpu_ctx_emu_views.argtypes = [vp, C.c_int32, C.POINTER(EmuNet), C.POINTER(EmuMember)]
         lib.cmf_gpu_ctx_copy_member.argtypes = [vp, C.c_int32, vp, C.c_int32]
@@ -136,6 +139,7 @@ class MLP:
             self.W[k].copy_(self.torch.from_numpy(np.asarray(sd["W"][k], dtype=np.float32)))
             self.Wb[k].copy_(self.W[k].to(self.torch.bfloat16))
             self.b[k].copy_(self.torch.from_numpy(np.asarray(sd["b"][k], dtype=np.float32)))
+        self._packed_step = None
 
     def _gemm(self, M, N, K, A, lda, ta, B, ldb, tb, C=None, Cb=None, bias=None, relu=0, acc=0, ksplit=1):
         p = lambda t: (t.data_ptr() if t is not None else None)  # noqa: E731
@@ -156,6 +160,23 @@ class MLP:
         Y = torch.empty(R, OUT, dtype=torch.float32, device=self.dev)
         self._gemm(R, OUT, HID, a, HID, 0, self.Wb[3], OUT, 0, C=Y, bias=self.b[3])
         return Y, (acts if keep else None)
+
+    def infer(self, X, y=None):
+        """Fused inference: X [R, 64] bf16 (R % 16 == 0) -> y [R] fp32, equal to forward()'s column 0."""
+        torch = self.torch
+        if getattr(self, "_packed_step", None) != self.step or getattr(self, "_pack", None) is None:
+            if getattr(self, "_pack", None) is None:
+                self._pack = torch.empty(self.lib.cmf_emu_mlp_pack_bytes(), dtype=torch.uint8, device=self.dev)
+            echeck(self.lib.cmf_emu_mlp_pack(self.Wb[0].data_ptr(), self.Wb[1].data_ptr(), self.Wb[2].data_ptr(),
+                                             self.Wb[3].data_ptr(), OUT, self._pack.data_ptr(), self.stream), "mlp_pack")
+            self._packed_step = self.step
+        R = X.shape[0]
+        if y is None:
+            y = torch.empty(R, dtype=torch.float32, device=self.dev)
+        echeck(self.lib.cmf_emu_mlp_fused(X.data_ptr(), X.shape[1], R, self._pack.data_ptr(), self.b[0].data_ptr(),
+                                          self.b[1].data_ptr(), self.b[2].data_ptr(), self.b[3].data_ptr(), y.data_ptr(),
+                                          self.stream), "mlp_fused")
+        return y
 
     def backward(self, acts, dY, dYb):
         """Parameter gradients into gW/gb from dY = dLoss/dY ([R, 64], fp32 and bf16)."""
@@ -222,13 +243,15 @@ class Features:
         self.net.qref = self.qref.data_ptr()
         self.mb = EmuMember()
         check(self.lib.cmf_gpu_ctx_emu_views(phys.h, 0, None, C.byref(self.mb)), "emu_views")
-        self.scratch = [torch.empty(self.M * self.N, dtype=torch.float32, device=self.dev) for _ in range(4)]
-        self.X = torch.zeros(self.M * self.Np, IN, dtype=torch.bfloat16, device=self.dev)
-        self.qout = torch.empty(self.M * self.N, dtype=torch.float64, device=self.dev)
+        self.scratch = self.X = self.qout = None     # allocated on first use (views-only users need none)
 
     # The library works on its own non-blocking stream, the emulator on torch's current stream:
     # every boundary drains the side that wrote last, so neither reads the other's arrays mid-update.
     def build(self):
+        torch = self.torch
+        if self.X is None:
+            self.scratch = [torch.empty(self.M * self.N, dtype=torch.float32, device=self.dev) for _ in range(4)]
+            self.X = torch.zeros(self.M * self.Np, IN, dtype=torch.bfloat16, device=self.dev)
         self.phys.synchronize()
         s = self.scratch
         echeck(self.lib.cmf_emu_features(C.byref(self.net), C.byref(self.mb), self.M, self.X.data_ptr(), IN, self.Np, HOPS,
@@ -243,8 +266,20 @@ class Features:
         self.torch.cuda.current_stream(self.dev).synchronize()
         return out
 
-    def rollout(self, Y, active):
-        echeck(self.lib.cmf_emu_rollout(C.byref(self.net), C.byref(self.mb), self.M, active.data_ptr(), Y.data_ptr(), OUT,
+    def at(self, cells):
+        """[M, len(cells)] last-step mean outflow at the given cells (device gather, host array)."""
+        self.phys.synchronize()
+        v = _raw_f64(self.mb.qprev, self.M * self.N, self.dev).view(self.M, self.N)
+        return v.index_select(1, cells).cpu().numpy()
+
+    def runoff_view(self):
+        """[M, N] device view of the context's runoff input (written by the caller before a step)."""
+        return _raw_f64(self.mb.runoff, self.M * self.N, self.dev).view(self.M, self.N)
+
+    def rollout(self, Y, active, ldy: int = OUT):
+        if self.qout is None:
+            self.qout = self.torch.empty(self.M * self.N, dtype=self.torch.float64, device=self.dev)
+        echeck(self.lib.cmf_emu_rollout(C.byref(self.net), C.byref(self.mb), self.M, active.data_ptr(), Y.data_ptr(), ldy,
                                         self.Np, float(self.phys.host.dt), self.qout.data_ptr(),
                                         self.torch.cuda.current_stream(self.dev).cuda_stream), "rollout")
         self.torch.cuda.current_stream(self.dev).synchronize()
@@ -320,6 +355,45 @@ def train(mlp: MLP, X, t, iters: int, batch: int, seed: int = 0, lr_max: float |
     return hist
 
 
+class DeviceForcing:
+    """Hourly runoff of an M-member ensemble held in HBM.  `distinct` AR(1)-gamma fields per hour
+    (the config-1 forcing law, generated once on the host) are uploaded; member m uses field
+    m % distinct times its own lognormal(0, 0.3) factor, so members differ in timing and volume."""
+
+    def __init__(self, host, members: int, hours: int, seed: int, device, distinct: int = 8):
+        import torch
+
+        N = host.dims.nseqall
+        gr = host.map("grarea")
+        K = min(distinct, members)
+        gens = runoff_generators(N, K, seed)
+        self.fields = torch.empty(hours, K, N, dtype=torch.float64, device=device)
+        for h in range(hours):
+            self.fields[h].copy_(torch.from_numpy(runoff_step(gens, gr)))
+        rng = np.random.default_rng(seed + 1)
+        self.factor = torch.tensor(np.exp(0.3 * rng.standard_normal(members) - 0.045), device=device)[:, None]
+        self.idx = torch.arange(members, device=device) % K
+        self.buf = torch.empty(members, N, dtype=torch.float64, device=device)
+        self.torch = torch
+
+    def hour(self, h: int):
+        """[M, N] runoff of hour h (device; valid until the next call)."""
+        self.torch.mul(self.fields[h].index_select(0, self.idx), self.factor, out=self.buf)
+        return self.buf
+
+
+class ArrayForcing:
+    """Forcing from a host array [hours, M, N], uploaded once."""
+
+    def __init__(self, runoff: np.ndarray, device):
+        import torch
+
+        self.t = torch.tensor(np.ascontiguousarray(runoff, dtype=np.float64), device=device)
+
+    def hour(self, h: int):
+        return self.t[h]
+
+
 class SurrogateEnsemble:
     """E4: ensemble advanced by the emulator with plain-solver judging and hand-back."""
 
@@ -336,6 +410,7 @@ class SurrogateEnsemble:
         self.emu = PhysicsGPU(host, nmembers=members)
         self.judge = PhysicsGPU(host, nmembers=judge_slots)
         self.fe = Features(self.emu, qref_from_host(host))
+        self.jfe = Features(self.judge, qref_from_host(host))
         self.lib = _emu_lib()
         self.gauges = np.asarray(gauges)
         self.tol = tol_rel
@@ -351,19 +426,23 @@ class SurrogateEnsemble:
 
     def emu_step(self):
         X = self.fe.build()
-        Y, _ = self.mlp.forward(X, keep=False)
-        self.fe.rollout(Y, self.active)
+        self._y = self.mlp.infer(X, getattr(self, "_y", None))
+        self.fe.rollout(self._y, self.active, ldy=1)
 
-    def run(self, runoff: np.ndarray):
-        """runoff [hours, M, N] -> hourly mean discharge at the gauges [hours, M, G]."""
-        H = runoff.shape[0]
-        G = self.gauges
-        out = np.zeros((H, self.M, len(G)))
+    def run(self, forcing, hours: int, h0: int = 0):
+        """Advances `hours` coupling steps with forcing.hour(h0 + h) (device [M, N]); returns the
+        hourly mean discharge at the gauges [hours, M, G] (the judged plain value for members
+        handed back to the plain solver)."""
+        torch = self.torch
+        G = torch.as_tensor(self.gauges, device=self.fe.dev)
+        out = np.zeros((hours, self.M, len(self.gauges)))
         slots = []
-        judged = []
         buf_e, buf_j = [], []
         day = 0
-        for h in range(H):
+        emu_runoff = self.fe.runoff_view()
+        jfe = self.jfe
+        cur_plain = None
+        for h in range(hours):
             if h % self.resync == 0:
                 plain = sorted(self.plain)[: self.slots]
                 free = self.slots - len(plain)
@@ -372,41 +451,40 @@ class SurrogateEnsemble:
                 slots = plain + judged
                 for k, m in enumerate(slots):
                     check(self.lib.cmf_gpu_ctx_copy_member(self.judge.h, k, self.emu.h, m), "copy_member")
+                slot_idx = torch.as_tensor(slots + [slots[0]] * (self.slots - len(slots)) if slots else [0] * self.slots,
+                                           device=self.fe.dev)
                 buf_e, buf_j = [], []
                 day += 1
-            self.emu.put_runoff(runoff[h])
-            self.active.copy_(self.torch.tensor([0 if m in self.plain else 1 for m in range(self.M)], dtype=self.torch.int32))
+            if cur_plain != self.plain:
+                self.active.copy_(torch.tensor([0 if m in self.plain else 1 for m in range(self.M)], dtype=torch.int32))
+                cur_plain = set(self.plain)
+            r = forcing.hour(h0 + h)
+            emu_runoff.copy_(r)
+            jr = r.index_select(0, slot_idx)
+            torch.cuda.current_stream(self.fe.dev).synchronize()
+            self.judge.advance_device(1, jr.data_ptr(), 0)
             self.emu_step()
             self.emu.stage()
             self.stats["emu_member_hours"] += self.M - len(self.plain)
-            jr = np.zeros((self.slots, runoff.shape[2]))
-            for k, m in enumerate(slots):
-                jr[k] = runoff[h, m]
-            self.judge.put_runoff(jr)
-            self.judge.advance()
             self.stats["plain_member_hours"] += len(slots)
-            qe = self.fe.qprev().cpu().numpy()
-            qj = self.emu.get_diag_fields  # noqa: F841  (kept for readability of the flow)
-            qjudge = self.judge.get_diag_fields({"outflw_aavg": np.zeros(self.slots * self.emu.N)})["outflw_aavg"]
-            qjudge = qjudge.reshape(self.slots, -1)
-            out[h] = qe[:, G]
+            qe = self.fe.at(G)
+            qjudge = jfe.at(G)
+            out[h] = qe
             for k, m in enumerate(slots):
                 if m in self.plain:
-                    out[h, m] = qjudge[k, G]
-            buf_e.append(qe[:, G].copy())
-            buf_j.append(qjudge[:, G].copy())
+                    out[h, m] = qjudge[k]
+            buf_e.append(qe)
+            buf_j.append(qjudge)
             if (h + 1) % self.resync == 0:
                 we = np.stack(buf_e).mean(0)
                 wj = np.stack(buf_j).mean(0)
                 for k, m in enumerate(slots):
-                    if m in self.plain:
-                        check(self.lib.cmf_gpu_ctx_copy_member(self.emu.h, m, self.judge.h, k), "copy_member")
-                        continue
-                    err = float(np.median(np.abs(we[m] - wj[k]) / np.maximum(np.abs(wj[k]), 1e-6)))
-                    self.stats["errors"].append(err)
-                    self.stats["judged"] += 1
-                    if err > self.tol:
-                        self.plain.add(m)
-                        self.stats["fallback"] += 1
+                    if m not in self.plain:
+                        err = float(np.median(np.abs(we[m] - wj[k]) / np.maximum(np.abs(wj[k]), 1e-6)))
+                        self.stats["errors"].append(err)
+                        self.stats["judged"] += 1
+                        if err > self.tol:
+                            self.plain.add(m)
+                            self.stats["fallback"] += 1
                     check(self.lib.cmf_gpu_ctx_copy_member(self.emu.h, m, self.judge.h, k), "copy_member")
         return out

@@ -126,6 +126,130 @@ __global__ void __launch_bounds__(128) k_gemm(int M, int N, int K, const __nv_bf
             }
 }
 
+// ------------------------------------------------------------------------------------------
+// Fused inference: y[r] = w3 . relu(W2' relu(W1' relu(W0' x_r + b0) + b1) + b2) + b3[0]
+//
+// One warp owns 16 rows through all four layers.  The m16n8k16 accumulator of two adjacent
+// n-tiles (columns 16k..16k+7 and 16k+8..16k+15) holds, lane by lane, exactly the A fragment of
+// the k-slab 16k..16k+15 of the next layer, so activations never leave registers: bias, ReLU and
+// the bf16 rounding happen on the accumulator and the packed pairs feed the next layer's MMAs.
+// The weights are packed once in fragment order (kMlpPack* below: [layer][kslab][ntile][lane] of
+// {b0b1, b2b3}) and copied into shared memory by every CTA of a persistent grid; a warp's B
+// fragment is one 8-byte shared load per lane.  The chain of MMAs, bias/ReLU/bf16 points and the
+// K order are those of the layer-by-layer forward (k_gemm), so y equals its column 0 bit for bit.
+// Input columns 32..63 of X are zero padding (the first layer reads k-slabs 0 and 1 only).
+// ------------------------------------------------------------------------------------------
+constexpr int kMlpKs0 = 2, kMlpKsH = 8, kMlpNt = 16;
+constexpr int kMlpOff1 = kMlpKs0 * kMlpNt * 32;                 // uint2 offsets of each layer
+constexpr int kMlpOff2 = kMlpOff1 + kMlpKsH * kMlpNt * 32;
+constexpr int kMlpOff3 = kMlpOff2 + kMlpKsH * kMlpNt * 32;
+constexpr int kMlpPackWords = kMlpOff3 + kMlpKsH * 32;          // last layer: one n-tile (column 0 real)
+constexpr int kMlpThreads = 256, kMlpRowsPerCta = 128;
+
+__device__ __forceinline__ uint32_t pack_bf16x2(float lo, float hi) {
+    const __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);   // .x = lo (lower address / lower 16 bits)
+    return *reinterpret_cast<const uint32_t *>(&v);
+}
+
+__device__ __forceinline__ uint32_t bf16_pair(const __nv_bfloat16 *W, int ldw, int k, int n) {
+    __nv_bfloat162 v;
+    v.x = W[(size_t)k * ldw + n];
+    v.y = W[(size_t)(k + 1) * ldw + n];
+    return *reinterpret_cast<const uint32_t *>(&v);
+}
+
+// W0..W2 bf16 [K][128] row-major, W3 bf16 [128][ldw3]; one thread per packed uint2
+__global__ void k_mlp_pack(const __nv_bfloat16 *__restrict__ W0, const __nv_bfloat16 *__restrict__ W1,
+                           const __nv_bfloat16 *__restrict__ W2, const __nv_bfloat16 *__restrict__ W3, int ldw3, uint2 *out) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= kMlpPackWords) return;
+    const __nv_bfloat16 *W;
+    int ldw, rel;
+    if (e < kMlpOff1) { W = W0; ldw = 128; rel = e; }
+    else if (e < kMlpOff2) { W = W1; ldw = 128; rel = e - kMlpOff1; }
+    else if (e < kMlpOff3) { W = W2; ldw = 128; rel = e - kMlpOff2; }
+    else { W = W3; ldw = ldw3; rel = e - kMlpOff3; }
+    const int nts = (e < kMlpOff3) ? kMlpNt : 1;
+    const int lane = rel & 31, nt = (rel >> 5) % nts, ks = (rel >> 5) / nts;
+    const int g = lane >> 2, t = lane & 3;
+    const int n = nt * 8 + g, k = ks * 16 + 2 * t;
+    out[e] = make_uint2(bf16_pair(W, ldw, k, n), bf16_pair(W, ldw, k + 8, n));
+}
+
+template <int KS>
+__device__ __forceinline__ void mlp_layer(float (&acc)[kMlpNt][4], const uint32_t (&a)[kMlpKsH][4], const uint2 *__restrict__ w,
+                                          int lane) {
+#pragma unroll
+    for (int nt = 0; nt < kMlpNt; nt++) acc[nt][0] = acc[nt][1] = acc[nt][2] = acc[nt][3] = 0.f;
+#pragma unroll
+    for (int ks = 0; ks < KS; ks++)
+#pragma unroll
+        for (int nt = 0; nt < kMlpNt; nt++) {
+            const uint2 b2 = w[(ks * kMlpNt + nt) * 32 + lane];
+            const uint32_t b[2] = {b2.x, b2.y};
+            mma_bf16(acc[nt], a[ks], b);
+        }
+}
+
+// bias + ReLU + bf16 on the accumulator, repacked as the next layer's A fragments
+__device__ __forceinline__ void mlp_chain(const float (&acc)[kMlpNt][4], const float *__restrict__ bias, uint32_t (&a)[kMlpKsH][4],
+                                          int t) {
+#pragma unroll
+    for (int nt = 0; nt < kMlpNt; nt++) {
+        const int col = nt * 8 + 2 * t;
+        const float b0 = bias[col], b1 = bias[col + 1];
+        const float v0 = fmaxf(acc[nt][0] + b0, 0.f), v1 = fmaxf(acc[nt][1] + b1, 0.f);
+        const float v2 = fmaxf(acc[nt][2] + b0, 0.f), v3 = fmaxf(acc[nt][3] + b1, 0.f);
+        a[nt >> 1][(nt & 1) * 2 + 0] = pack_bf16x2(v0, v1);   // row g
+        a[nt >> 1][(nt & 1) * 2 + 1] = pack_bf16x2(v2, v3);   // row g + 8
+    }
+}
+
+__global__ void __launch_bounds__(kMlpThreads, 2) k_mlp_fused(const __nv_bfloat16 *__restrict__ X, int ldx, int rows,
+                                                              const uint2 *__restrict__ wpack, const float *__restrict__ b0,
+                                                              const float *__restrict__ b1, const float *__restrict__ b2,
+                                                              const float *__restrict__ b3, float *__restrict__ y) {
+    extern __shared__ __align__(16) uint2 sw[];
+    __shared__ float sb[3 * 128 + 4];
+    for (int e = threadIdx.x; e < kMlpPackWords; e += blockDim.x) sw[e] = wpack[e];
+    for (int e = threadIdx.x; e < 128; e += blockDim.x) { sb[e] = b0[e]; sb[128 + e] = b1[e]; sb[256 + e] = b2[e]; }
+    if (threadIdx.x == 0) sb[384] = b3[0];
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+    const int ntiles = (rows + kMlpRowsPerCta - 1) / kMlpRowsPerCta;
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const int r0 = tile * kMlpRowsPerCta + warp * 16;
+        if (r0 >= rows) continue;                    // rows is a multiple of 16: groups are whole
+        uint32_t a[kMlpKsH][4];
+        const __nv_bfloat16 *x0 = X + (size_t)(r0 + g) * ldx, *x1 = X + (size_t)(r0 + g + 8) * ldx;
+#pragma unroll
+        for (int ks = 0; ks < kMlpKs0; ks++) {
+            a[ks][0] = *reinterpret_cast<const uint32_t *>(x0 + ks * 16 + 2 * t);
+            a[ks][1] = *reinterpret_cast<const uint32_t *>(x1 + ks * 16 + 2 * t);
+            a[ks][2] = *reinterpret_cast<const uint32_t *>(x0 + ks * 16 + 8 + 2 * t);
+            a[ks][3] = *reinterpret_cast<const uint32_t *>(x1 + ks * 16 + 8 + 2 * t);
+        }
+        float acc[kMlpNt][4];
+        mlp_layer<kMlpKs0>(acc, a, sw, lane);
+        mlp_chain(acc, sb, a, t);
+        mlp_layer<kMlpKsH>(acc, a, sw + kMlpOff1, lane);
+        mlp_chain(acc, sb + 128, a, t);
+        mlp_layer<kMlpKsH>(acc, a, sw + kMlpOff2, lane);
+        mlp_chain(acc, sb + 256, a, t);
+        float o[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+        for (int ks = 0; ks < kMlpKsH; ks++) {
+            const uint2 b2 = sw[kMlpOff3 + ks * 32 + lane];
+            const uint32_t b[2] = {b2.x, b2.y};
+            mma_bf16(o, a[ks], b);
+        }
+        if (t == 0) {
+            y[r0 + g] = o[0] + sb[384];
+            y[r0 + g + 8] = o[2] + sb[384];
+        }
+    }
+}
+
 // dZ = dA * (act > 0) -> bf16, for ReLU layers (act stored in bf16 by the forward pass)
 __global__ void k_relu_bwd(int n, const float *__restrict__ dA, const __nv_bfloat16 *__restrict__ act, __nv_bfloat16 *dZ,
                            float *dZf) {
@@ -350,6 +474,36 @@ int cmf_emu_adam(int n, float *w, void *wb, const float *grad, float *m, float *
                  int step, float wd, void *stream) {
     const float bc1 = 1.f - powf(b1, (float)step), bc2 = 1.f - powf(b2, (float)step);
     k_adam<<<(n + 255) / 256, 256, 0, (cudaStream_t)stream>>>(n, w, (__nv_bfloat16 *)wb, grad, m, v, lr, b1, b2, eps, bc1, bc2, wd);
+    EMU_TRY(cudaGetLastError());
+    return CMF_OK;
+}
+
+size_t cmf_emu_mlp_pack_bytes(void) { return (size_t)kMlpPackWords * sizeof(uint2); }
+
+int cmf_emu_mlp_pack(const void *W0, const void *W1, const void *W2, const void *W3, int ldw3, void *pack, void *stream) {
+    if (!W0 || !W1 || !W2 || !W3 || !pack || ldw3 < 8) return emu_err(CMF_E_ARG, "cmf_emu_mlp_pack: bad arguments");
+    k_mlp_pack<<<(kMlpPackWords + 255) / 256, 256, 0, (cudaStream_t)stream>>>(
+        (const __nv_bfloat16 *)W0, (const __nv_bfloat16 *)W1, (const __nv_bfloat16 *)W2, (const __nv_bfloat16 *)W3, ldw3,
+        (uint2 *)pack);
+    EMU_TRY(cudaGetLastError());
+    return CMF_OK;
+}
+
+int cmf_emu_mlp_fused(const void *X, int ldx, int rows, const void *pack, const float *b0, const float *b1, const float *b2,
+                      const float *b3, float *y, void *stream) {
+    if (!X || !pack || !b0 || !b1 || !b2 || !b3 || !y || ldx < 32 || (ldx & 1) || rows < 0 || rows % 16)
+        return emu_err(CMF_E_ARG, "cmf_emu_mlp_fused: bad arguments (ldx >= 32 and even, rows % 16 == 0)");
+    if (((uintptr_t)X & 3) || ((uintptr_t)pack & 7)) return emu_err(CMF_E_ARG, "cmf_emu_mlp_fused: misaligned X or pack");
+    if (rows == 0) return CMF_OK;
+    int dev = 0, sms = 0;
+    EMU_TRY(cudaGetDevice(&dev));
+    EMU_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const int smem = (int)cmf_emu_mlp_pack_bytes();
+    EMU_TRY(cudaFuncSetAttribute(k_mlp_fused, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    const int ntiles = (rows + kMlpRowsPerCta - 1) / kMlpRowsPerCta;
+    const int grid = ntiles < 2 * sms ? ntiles : 2 * sms;
+    k_mlp_fused<<<grid, kMlpThreads, smem, (cudaStream_t)stream>>>((const __nv_bfloat16 *)X, ldx, rows, (const uint2 *)pack,
+                                                                   b0, b1, b2, b3, y);
     EMU_TRY(cudaGetLastError());
     return CMF_OK;
 }

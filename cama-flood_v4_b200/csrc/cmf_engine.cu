@@ -767,6 +767,7 @@ int cmf_gpu_ctx_copy_member(cmf_gpu_ctx *d, int32_t dm, cmf_gpu_ctx *s, int32_t 
         d->net.P != s->net.P || d->net.Lp != s->net.Lp || d->opts.ldiag != s->opts.ldiag)
         return set_err(CMF_E_ARG, "contexts differ in network or options");
     CUDA_TRY(cudaSetDevice(d->device));
+    CUDA_TRY(cudaStreamSynchronize(d->stream));   // nothing of the destination's may still be in flight
     const size_t N = d->dims.nseqall, od = (size_t)dm * N, os = (size_t)sm * N;
     const cmf::State &A = d->st, &B = s->st;
     double *cells_d[] = {A.rivsto, A.fldsto, A.rivout_pre, A.fldout_pre, A.rivdph_pre, A.fldsto_pre, A.rivdph, A.flddph,

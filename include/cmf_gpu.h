@@ -260,6 +260,15 @@ int cmf_emu_features(const cmf_emu_net *net, const cmf_emu_member *mb, int nmemb
  * member with active_dev[m] != 0 (device int array); qout: double [M][N] scratch. */
 int cmf_emu_rollout(const cmf_emu_net *net, const cmf_emu_member *mb, int nmembers, const int *active_dev,
                     const float *y, int ldy, int rows_per_member, double dt, double *qout, void *stream);
+/* Fused inference of the 4-layer MLP.  cmf_emu_mlp_pack re-lays the bf16 weights (W0..W2 [K][128],
+ * W3 [128][ldw3], row-major) into tensor-core fragment order in `pack` (cmf_emu_mlp_pack_bytes()
+ * bytes, device memory); cmf_emu_mlp_fused then maps X rows (bf16, ldx >= 32 and even, columns
+ * 32.. zero padding, rows % 16 == 0) to y[rows] (fp32) in one kernel with the activations kept in
+ * registers.  y equals column 0 of the layer-by-layer forward built from cmf_emu_gemm bit for bit. */
+size_t cmf_emu_mlp_pack_bytes(void);
+int cmf_emu_mlp_pack(const void *W0, const void *W1, const void *W2, const void *W3, int ldw3, void *pack, void *stream);
+int cmf_emu_mlp_fused(const void *X, int ldx, int rows, const void *pack, const float *b0, const float *b1,
+                      const float *b2, const float *b3, float *y, void *stream);
 const char *cmf_emu_last_error(void);
 
 /* ======================================================================================== */

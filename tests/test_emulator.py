@@ -104,6 +104,36 @@ def test_training_kernels_gradients_match_cpu_reference():
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("R", [16, 1040, 70000])
+def test_fused_inference_equals_layerwise_forward(R):
+    """The fused 4-layer kernel (activations in registers) against the layer-by-layer GEMM chain:
+    identical bits; and against the CPU bf16 reference within fp32 accumulation-order tolerance."""
+    import torch
+
+    from cmf_b200.emulator import MLP
+    from emu_ref import forward, to_bf16
+
+    dev = torch.device("cuda", 0)
+    rng = np.random.default_rng(R)
+    mlp = MLP(dev, seed=2)
+    W, b = _rand_params(rng, 0.2)
+    mlp.load({"W": W, "b": b})
+    X = to_bf16(rng.standard_normal((R, 64)) * 2.0)
+    X[:, 30:] = 0
+    tX = torch.tensor(X, device=dev).to(torch.bfloat16)
+    y = mlp.infer(tX)
+    Rp = (R + 63) // 64 * 64
+    Xp = torch.zeros(Rp, 64, dtype=torch.bfloat16, device=dev)
+    Xp[:R] = tX
+    Y, _ = mlp.forward(Xp, keep=False)
+    torch.cuda.synchronize()
+    assert torch.equal(y, Y[:R, 0].contiguous())
+    ref, _ = forward(X[:2048], [w.astype(np.float32) for w in W], [v.astype(np.float32) for v in b], bf16=True)
+    got = y[:2048].cpu().numpy()
+    assert np.allclose(got, ref[:, 0], rtol=2e-2, atol=2e-2 * float(np.abs(ref[:, 0]).max()))
+
+
+@pytest.mark.gpu
 def test_trained_emulator_beats_untrained_and_persistence(case_dirs):
     """E1-E5 on the config-1 laws: train on solver trajectories, then roll out 24 h from a plain
     state and compare the gauge discharge with the plain solver: the trained network must be far
@@ -179,7 +209,7 @@ def test_surrogate_controller_judges_resyncs_and_hands_back(case_dirs):
     G = np.argsort(-E.qref_from_host(h))[:10]
     ens = E.SurrogateEnsemble(h, E.MLP(dev, seed=3), members=M, judge_slots=2, gauges=G, tol_rel=-1.0)
     ens.set_state_from(plain)
-    out = ens.run(runoff)
+    out = ens.run(E.ArrayForcing(runoff, dev), runoff.shape[0])
     # day 1 judges members 0 and 1, both fail and are handed back; on day 2 they fill both judge slots
     assert ens.stats["judged"] == 2 and ens.stats["fallback"] == 2 and sorted(ens.plain) == [0, 1]
     # members handed back after day 1 report the plain solver: compare with the truth on day 2
