@@ -134,6 +134,14 @@ def load(build_if_missing: bool = True):
     lib.cmf_gpu_ctx_substeps.argtypes = [vp, C.c_double, C.c_double, i32p, f64p, C.POINTER(Budget)]
     lib.cmf_gpu_ctx_counters.argtypes = [vp, C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
     lib.cmf_gpu_ctx_time_phases.argtypes = [vp, C.c_double, C.c_int32, f64p]
+    lib.cmf_gpu_batch_create.argtypes = [C.POINTER(vp), C.c_int32, C.POINTER(vp)]
+    lib.cmf_gpu_batch_launch.argtypes = [vp, C.c_double]
+    lib.cmf_gpu_batch_advance.argtypes = [vp, C.c_double, i32p, f64p, C.POINTER(Budget)]
+    lib.cmf_gpu_batch_synchronize.argtypes = [vp]
+    lib.cmf_gpu_batch_stream.argtypes = [vp]
+    lib.cmf_gpu_batch_stream.restype = vp
+    lib.cmf_gpu_batch_destroy.argtypes = [vp]
+    lib.cmf_gpu_batch_destroy.restype = None
     lib.cmf_gpu_init.argtypes = [C.POINTER(Dims), C.POINTER(Params), C.POINTER(MapPtrs), C.POINTER(Opts)]
     lib.cmf_gpu_set_state.argtypes = [C.POINTER(StatePtrs)]
     lib.cmf_gpu_get_state.argtypes = [C.POINTER(StatePtrs)]
@@ -150,6 +158,11 @@ def load(build_if_missing: bool = True):
     lib.cmf_host_state.argtypes = [vp, C.POINTER(StatePtrs)]
     lib.cmf_host_conv_resol.argtypes = [vp, f64p, f64p]
     lib.cmf_host_grid.argtypes = [vp, i32p, i32p, i32p, i32p]
+    lib.cmf_host_write_restart.argtypes = [vp, C.POINTER(StatePtrs), C.c_char_p, C.c_int32, C.c_int32]
+    lib.cmf_host_read_restart.argtypes = [vp, C.POINTER(StatePtrs), C.c_char_p, C.c_int32, C.c_int32]
+    lib.cmf_host_map_to_vec.argtypes = [vp, C.POINTER(C.c_float), f64p]
+    lib.cmf_gpu_ctx_calc_outpre.argtypes = [vp]
+    lib.cmf_gpu_ctx_update_boundary.argtypes = [vp, f64p, f64p]
     _lib = lib
     return lib
 

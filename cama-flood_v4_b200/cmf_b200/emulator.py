@@ -26,13 +26,14 @@ import numpy as np
 from . import _abi
 from ._abi import check
 
-IN, HID, OUT = 64, 128, 64      # padded widths (30 input features, 1 output)
-NFEAT, HOPS = 30, 8
+IN, HID, OUT = 64, 128, 64      # padded widths (32 input features, 1 output)
+NFEAT, HOPS = 32, 8
 
 
 class EmuNet(C.Structure):
     _fields_ = [("nseqall", C.c_int32), ("nseqriv", C.c_int32)] + [(n, C.c_void_p) for n in (
-        "next", "up_ptr", "up_idx", "rivelv", "elevtn", "nxtdst", "rivwth", "rivhgt", "rivlen", "rivstomax", "qref")]
+        "next", "up_ptr", "up_idx", "rivelv", "elevtn", "nxtdst", "rivwth", "rivhgt", "rivlen", "rivstomax", "qref",
+        "rivman")] + [("pmanfld", C.c_double)]
 
 
 class EmuMember(C.Structure):
@@ -49,8 +50,8 @@ def _emu_lib():
         lib.cmf_emu_colsum.argtypes = [i, i, vp, vp, vp]
         lib.cmf_emu_mse_grad.argtypes = [i, i, i, vp, vp, vp, vp, vp, vp]
         lib.cmf_emu_adam.argtypes = [i, vp, vp, vp, vp, vp, f, f, f, f, i, f, vp]
-        lib.cmf_emu_features.argtypes = [C.POINTER(EmuNet), C.POINTER(EmuMember), i, vp, i, i, i, vp, vp, vp, vp, vp]
-        lib.cmf_emu_rollout.argtypes = [C.POINTER(EmuNet), C.POINTER(EmuMember), i, vp, vp, i, i, d, vp, vp]
+        lib.cmf_emu_features.argtypes = [C.POINTER(EmuNet), C.POINTER(EmuMember), i, vp, i, i, i, vp, vp]
+        lib.cmf_emu_rollout.argtypes = [C.POINTER(EmuNet), C.POINTER(EmuMember), i, vp, vp, i, i, d, i, vp, vp]
         lib.cmf_emu_mlp_pack_bytes.restype = C.c_size_t
         lib.cmf_emu_mlp_pack.argtypes = [vp, vp, vp, vp, i, vp, vp]
         lib.cmf_emu_mlp_fused.argtypes = [vp, i, i, vp, vp, vp, vp, vp, vp, vp]
@@ -250,13 +251,12 @@ class Features:
     def build(self):
         torch = self.torch
         if self.X is None:
-            self.scratch = [torch.empty(self.M * self.N, dtype=torch.float32, device=self.dev) for _ in range(4)]
+            self.scratch = torch.empty(2 * (HOPS + 1) * self.M * self.N, dtype=torch.float32, device=self.dev)
             self.X = torch.zeros(self.M * self.Np, IN, dtype=torch.bfloat16, device=self.dev)
         self.phys.synchronize()
-        s = self.scratch
         echeck(self.lib.cmf_emu_features(C.byref(self.net), C.byref(self.mb), self.M, self.X.data_ptr(), IN, self.Np, HOPS,
-                                         s[0].data_ptr(), s[1].data_ptr(), s[2].data_ptr(), s[3].data_ptr(),
-                                         self.torch.cuda.current_stream(self.dev).cuda_stream), "features")
+                                         self.scratch.data_ptr(), self.torch.cuda.current_stream(self.dev).cuda_stream),
+               "features")
         return self.X
 
     def qprev(self):
@@ -276,11 +276,11 @@ class Features:
         """[M, N] device view of the context's runoff input (written by the caller before a step)."""
         return _raw_f64(self.mb.runoff, self.M * self.N, self.dev).view(self.M, self.N)
 
-    def rollout(self, Y, active, ldy: int = OUT):
+    def rollout(self, Y, active, ldy: int = OUT, residual: bool = True):
         if self.qout is None:
             self.qout = self.torch.empty(self.M * self.N, dtype=self.torch.float64, device=self.dev)
         echeck(self.lib.cmf_emu_rollout(C.byref(self.net), C.byref(self.mb), self.M, active.data_ptr(), Y.data_ptr(), ldy,
-                                        self.Np, float(self.phys.host.dt), self.qout.data_ptr(),
+                                        self.Np, float(self.phys.host.dt), int(residual), self.qout.data_ptr(),
                                         self.torch.cuda.current_stream(self.dev).cuda_stream), "rollout")
         self.torch.cuda.current_stream(self.dev).synchronize()
 
@@ -304,7 +304,8 @@ def runoff_step(gens, gr, scale: float = 1.0) -> np.ndarray:
     return np.stack([np.maximum((g.next().astype(np.float64) * scale * gr) / 86400000.0, 0.0) for g in gens])
 
 
-def generate_trajectories(host, members: int, hours: int, spinup: int, seed: int, cells_per_snapshot: int | None = None):
+def generate_trajectories(host, members: int, hours: int, spinup: int, seed: int, cells_per_snapshot: int | None = None,
+                          residual: bool = True):
     """E1: the plain GPU solver advances `members` members (different runoff seeds); returns feature
     rows X [S, 64] (bf16) and targets t [S] (fp32)."""
     import torch
@@ -327,7 +328,8 @@ def generate_trajectories(host, members: int, hours: int, spinup: int, seed: int
         q0 = fe.qprev()
         torch.cuda.current_stream(fe.dev).synchronize()
         phys.advance()
-        t = residual_target(torch, fe.qprev(), q0, fe.qref[None, :]).float()   # mean outflow over the step
+        q1 = fe.qprev()                                                          # mean outflow over the step
+        t = (residual_target(torch, q1, q0, fe.qref[None, :]) if residual else target_transform(torch, q1, fe.qref[None, :])).float()
         for m in range(members):
             idx = np.arange(N) if cells_per_snapshot is None else rng.choice(N, size=min(cells_per_snapshot, N), replace=False)
             it = torch.as_tensor(idx, device=fe.dev)
@@ -337,17 +339,83 @@ def generate_trajectories(host, members: int, hours: int, spinup: int, seed: int
     return torch.cat(Xs), torch.cat(ts)
 
 
-def train(mlp: MLP, X, t, iters: int, batch: int, seed: int = 0, lr_max: float | None = None):
-    """Adam with cosine-decayed learning rate on random mini-batches of the trajectory rows."""
+def dagger_trajectories(host, mlp: "MLP", members: int, hours: int, spinup: int, seed: int,
+                        cells_per_snapshot: int | None = None):
+    """Rows from the emulator's own rollout (states it actually visits), labelled by the plain
+    solver: every hour each member's emulated state is copied into a plain context, the plain
+    solver advances it one step and its mean outflow is the target; the emulator then advances
+    itself.  Corrects the drift a network trained on solver states only accumulates."""
+    import torch
+
+    from .model import PhysicsGPU
+
+    residual = getattr(mlp, "residual", True)
+    ens = SurrogateEnsemble(host, mlp, members=members, judge_slots=1, gauges=np.zeros(1, dtype=np.int64),
+                            resync_hours=10 ** 9)
+    teach = PhysicsGPU(host, nmembers=members)
+    tf = Features(teach, qref_from_host(host))
+    N = teach.N
+    fo = DeviceForcing(host, members, spinup + hours, seed, tf.dev)
+    st = torch.cuda.current_stream(tf.dev)
+    for h in range(spinup):
+        r = fo.hour(h)
+        st.synchronize()
+        teach.advance_device(1, r.data_ptr(), 0)
+    teach.synchronize()
+    ens.set_state_from(teach)
+    rng = np.random.default_rng(seed)
+    Xs, ts = [], []
+    fe = ens.fe
+    for h in range(hours):
+        for m in range(members):
+            check(ens.lib.cmf_gpu_ctx_copy_member(teach.h, m, ens.emu.h, m), "copy_member")
+        r = fo.hour(spinup + h)
+        fe.runoff_view().copy_(r)
+        X = fe.build().clone()
+        q0 = fe.qprev()
+        st.synchronize()
+        teach.advance_device(1, r.data_ptr(), 0)
+        q1 = tf.qprev()
+        t = (residual_target(torch, q1, q0, fe.qref[None, :]) if residual else target_transform(torch, q1, fe.qref[None, :])).float()
+        for m in range(members):
+            idx = np.arange(N) if cells_per_snapshot is None else rng.choice(N, size=min(cells_per_snapshot, N), replace=False)
+            it = torch.as_tensor(idx, device=fe.dev)
+            Xs.append(X[m * fe.Np + it])
+            ts.append(t[m][it])
+        ens.emu_step()
+        ens.emu.stage()
+    teach.close()
+    ens.emu.close()
+    ens.judge.close()
+    return torch.cat(Xs), torch.cat(ts)
+
+
+def discharge_weights(X):
+    """Row weights sqrt(qref): feature column 11 holds log(qref) - 3 (bf16)."""
+    import torch
+
+    return torch.exp(0.5 * (X[:, 11].float() + 3.0))
+
+
+def train(mlp: MLP, X, t, iters: int, batch: int, seed: int = 0, lr_max: float | None = None, weights=None):
+    """Adam with cosine-decayed learning rate on random mini-batches of the trajectory rows (drawn
+    uniformly, or with probability proportional to `weights`)."""
     import torch
 
     g = torch.Generator(device=X.device).manual_seed(seed)
     S = X.shape[0]
     hist = []
     lr0 = lr_max if lr_max is not None else mlp.lr
+    cdf = None
+    if weights is not None:                   # inverse-CDF draws (any number of rows)
+        cdf = torch.cumsum(weights.double(), 0)
     for it in range(iters):
         mlp.lr = lr0 * (0.05 + 0.95 * 0.5 * (1.0 + math.cos(math.pi * it / max(iters, 1))))
-        idx = torch.randint(0, S, (batch,), device=X.device, generator=g)
+        if weights is None:
+            idx = torch.randint(0, S, (batch,), device=X.device, generator=g)
+        else:
+            u = torch.rand(batch, device=X.device, dtype=torch.float64, generator=g) * cdf[-1]
+            idx = torch.clamp(torch.searchsorted(cdf, u), max=S - 1)
         loss = mlp.loss_and_grad(X[idx].contiguous(), t[idx].contiguous(), batch)
         mlp.adam()
         if it % 50 == 0 or it == iters - 1:
@@ -427,7 +495,7 @@ class SurrogateEnsemble:
     def emu_step(self):
         X = self.fe.build()
         self._y = self.mlp.infer(X, getattr(self, "_y", None))
-        self.fe.rollout(self._y, self.active, ldy=1)
+        self.fe.rollout(self._y, self.active, ldy=1, residual=getattr(self.mlp, "residual", True))
 
     def run(self, forcing, hours: int, h0: int = 0):
         """Advances `hours` coupling steps with forcing.hour(h0 + h) (device [M, N]); returns the

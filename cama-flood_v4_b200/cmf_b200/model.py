@@ -94,6 +94,45 @@ class HostModel:
         v = np.asarray(mm_per_day_cells, dtype=np.float64)
         return np.maximum((v * gr) / 86400000.0, 0.0)
 
+    def _state_struct(self, state: dict, keep: list):
+        sp = _abi.StatePtrs()
+        for n in _abi.STATE_FIELDS:
+            if n in state and state[n] is not None:
+                a = state[n]
+                if a.dtype != np.float64 or not a.flags.c_contiguous:
+                    raise ValueError(n)
+                keep.append(a)
+                setattr(sp, n, a.ctypes.data_as(_abi.f64p))
+        return sp
+
+    def write_restart(self, path: str, state: dict, dbl: bool = True, stoonly: bool = False) -> None:
+        """CMF_RESTART_WRITE's binary file (src/cmf_ctrl_restart_mod.F90:389-482) from one member's
+        state arrays (keys of STATE_FIELDS, sequence order)."""
+        keep: list = []
+        st = {k: np.ascontiguousarray(v, dtype=np.float64).ravel() for k, v in state.items()}
+        sp = self._state_struct(st, keep)
+        check(self.lib.cmf_host_write_restart(self.h, C.byref(sp), path.encode(), int(dbl), int(stoonly)),
+              "cmf_host_write_restart")
+
+    def read_restart(self, path: str, dbl: bool = True, stoonly: bool = False) -> dict:
+        """CMF_RESTART_INIT's binary read (src/cmf_ctrl_restart_mod.F90:91-204) -> one member's state."""
+        d = self.dims
+        st = {n: np.zeros(d.npthout * d.npthlev if n.startswith("pthflw") else d.nseqmax) for n in _abi.STATE_FIELDS}
+        keep: list = []
+        sp = self._state_struct(st, keep)
+        check(self.lib.cmf_host_read_restart(self.h, C.byref(sp), path.encode(), int(dbl), int(stoonly)),
+              "cmf_host_read_restart")
+        return st
+
+    def map_to_vec(self, map2d: np.ndarray) -> np.ndarray:
+        """mapR2vecD: float32 NX x NY map (e.g. a sea-level record) -> sequence-order float64."""
+        a = np.ascontiguousarray(map2d, dtype=np.float32).ravel()
+        assert a.size == self.nx * self.ny
+        out = np.zeros(self.dims.nseqmax)
+        check(self.lib.cmf_host_map_to_vec(self.h, a.ctypes.data_as(C.POINTER(C.c_float)), out.ctypes.data_as(_abi.f64p)),
+              "cmf_host_map_to_vec")
+        return out
+
     def grid_to_seq(self, grid: np.ndarray) -> np.ndarray:
         g = np.asarray(grid).reshape(self.ny, self.nx)
         return g[self.i1seqy - 1, self.i1seqx - 1]
@@ -159,6 +198,43 @@ class PhysicsGPU:
             setattr(sp, n, a.ctypes.data_as(_abi.f64p))
         check(self.lib.cmf_gpu_ctx_get_state(self.h, C.byref(sp)), "get_state")
         return {k: v.reshape(self.M, -1) for k, v in out.items()}
+
+    def write_restart(self, path: str, member: int = 0, dbl: bool = True, stoonly: bool = False) -> None:
+        """Device state of one member -> the reference's binary restart file (and .pth)."""
+        st = self.get_state()
+        self.host.write_restart(path, {k: v[member] for k, v in st.items()}, dbl=dbl, stoonly=stoonly)
+
+    def read_restart(self, path: str, dbl: bool = True, stoonly: bool = False, members=None) -> None:
+        """Restart file -> the device state of the given members (all by default).  A storage-only
+        restart then reconstructs the previous-step flows with calc_outpre(), as CMF_DRV_INIT does."""
+        one = self.host.read_restart(path, dbl=dbl, stoonly=stoonly)
+        members = range(self.M) if members is None else list(members)
+        st = self.get_state()
+        for k, v in one.items():
+            for m in members:
+                st[k][m] = v
+        self.set_state(st)
+        if stoonly:
+            self.calc_outpre()
+
+    def calc_outpre(self) -> None:
+        """Stage scheme + CMF_CALC_OUTPRE on the device (storage-only restart)."""
+        check(self.lib.cmf_gpu_ctx_calc_outpre(self.h), "calc_outpre")
+
+    def update_boundary(self, sealev: np.ndarray | None = None, meansl: np.ndarray | None = None) -> None:
+        """CMF_BOUNDARY_UPDATE: D2DWNELV = D2ELEVTN (+ meansl) (+ sealev), sequence-order arrays."""
+        keep = []
+        ptrs = []
+        for a in (sealev, meansl):
+            if a is None:
+                ptrs.append(None)
+            else:
+                v = np.ascontiguousarray(a, dtype=np.float64).ravel()
+                if v.size != self.N:
+                    raise ValueError("boundary arrays hold NSEQALL values")
+                keep.append(v)
+                ptrs.append(v.ctypes.data_as(_abi.f64p))
+        check(self.lib.cmf_gpu_ctx_update_boundary(self.h, ptrs[0], ptrs[1]), "update_boundary")
 
     def put_runoff(self, runoff: np.ndarray) -> None:
         a = np.ascontiguousarray(runoff, dtype=np.float64).ravel()
@@ -265,3 +341,55 @@ class PhysicsGPU:
             self.close()
         except Exception:
             pass
+
+
+class PhysicsBatch:
+    """Contexts of several domains (each with its own members) advanced by one graph launch per
+    coupling step; every domain and member keeps its own adaptive DT."""
+
+    def __init__(self, contexts: list):
+        self.lib = _abi.load()
+        self.ctx = list(contexts)
+        arr = (C.c_void_p * len(self.ctx))(*[c.h.value if isinstance(c.h, C.c_void_p) else c.h for c in self.ctx])
+        h = C.c_void_p()
+        check(self.lib.cmf_gpu_batch_create(arr, len(self.ctx), C.byref(h)), "cmf_gpu_batch_create")
+        self.h = h
+        self.members = sum(c.M for c in self.ctx)
+
+    def launch(self, dt_def: float | None = None) -> None:
+        dt_def = self.ctx[0].host.dt if dt_def is None else dt_def
+        check(self.lib.cmf_gpu_batch_launch(self.h, dt_def), "batch_launch")
+
+    def advance(self, dt_def: float | None = None):
+        """One coupling step of every domain; returns per-domain lists (nt, dt) like PhysicsGPU.advance."""
+        dt_def = self.ctx[0].host.dt if dt_def is None else dt_def
+        nt = np.zeros(self.members, dtype=np.int32)
+        dt = np.zeros(self.members)
+        b = (_abi.Budget * self.members)()
+        check(self.lib.cmf_gpu_batch_advance(self.h, dt_def, nt.ctypes.data_as(_abi.i32p), dt.ctypes.data_as(_abi.f64p), b),
+              "batch_advance")
+        out, off = [], 0
+        for c in self.ctx:
+            out.append((nt[off:off + c.M], dt[off:off + c.M],
+                        [{f: getattr(b[off + m], f) for f in _abi.BUDGET_FIELDS} for m in range(c.M)]))
+            off += c.M
+        return out
+
+    def synchronize(self) -> None:
+        check(self.lib.cmf_gpu_batch_synchronize(self.h), "batch_synchronize")
+
+    @property
+    def stream(self) -> int:
+        return self.lib.cmf_gpu_batch_stream(self.h)
+
+    def close(self) -> None:
+        if self.h:
+            self.lib.cmf_gpu_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+

@@ -319,40 +319,77 @@ __global__ void k_mse_grad(int rows, int valid, int ldy, const float *__restrict
 }
 
 // ------------------------------------------------------------------------------------------
-// features: 14 local + 16 message channels + 2 zero pads = 32 per cell, written as bf16 rows
+// features: 14 local + 16 message channels + 2 hydraulic estimates = 32 per cell (bf16 rows)
+//
+// The upstream messages are computed first as fp32 planes (one coalesced pass per hop), then one
+// assembly pass writes each cell's 32 features as four 16-byte stores; nothing writes X columns
+// one at a time (rows are 128 bytes apart, so column writes would touch every row's sector per hop).
 // ------------------------------------------------------------------------------------------
 struct EmuNet {
     int N, R;
     const int *next, *up_ptr, *up_idx;
-    const double *rivelv, *elevtn, *nxtdst, *rivwth, *rivhgt, *rivlen, *rivstomax, *qref;
+    const double *rivelv, *elevtn, *nxtdst, *rivwth, *rivhgt, *rivlen, *rivstomax, *qref, *rivman;
+    double pmanfld;
 };
 
 __device__ __forceinline__ float slog(float x) { return copysignf(log1pf(fabsf(x)), x); }
 
-// local features of cell i of one member; msg0 <- hourly mean outflow of the last step (hop 0)
-__global__ void k_emu_local(EmuNet n, const double *rivsto, const double *fldsto, const double *levsto,
-                            const double *rivdph, const double *flddph, const double *fldfrc, const double *qprev,
-                            const double *runoff, __nv_bfloat16 *X, int ldx, int rows_per_member, float *msg_a, float *msg_b) {
+// hop-0 inputs: last-step mean outflow and runoff of every member, as fp32 planes
+__global__ void k_emu_seed(EmuNet n, const double *__restrict__ qprev, const double *__restrict__ runoff, float *pa, float *pb) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n.N) return;
+    const size_t gi = (size_t)blockIdx.y * n.N + i;
+    pa[gi] = (float)qprev[gi];
+    pb[gi] = (float)runoff[gi];
+}
+
+// one hop of upstream message passing: out[i] = sum over upstream j of in[j], ascending upstream order
+__global__ void k_emu_hop(EmuNet n, const float *__restrict__ in_a, const float *__restrict__ in_b, float *out_a, float *out_b) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n.N) return;
+    const size_t mo = (size_t)blockIdx.y * n.N;
+    float a = 0.f, b = 0.f;
+    for (int k = n.up_ptr[i]; k < n.up_ptr[i + 1]; k++) {
+        const int j = n.up_idx[k];
+        a += in_a[mo + j];
+        b += in_b[mo + j];
+    }
+    out_a[mo + i] = a;
+    out_b[mo + i] = b;
+}
+
+// Manning discharge of a rectangular section of area A, hydraulic depth h and friction slope s
+__device__ __forceinline__ float manning_q(float area, float h, float s, float man) {
+    if (!(area > 0.f) || !(h > 0.f)) return 0.f;
+    return copysignf(area * cbrtf(h * h) * sqrtf(fabsf(s)) / man, s);
+}
+
+// features of cell i of member blockIdx.y; planes [2*(hops+1)][M*N] (0,1 = seeds; 2h+2, 2h+3 = hop h)
+__global__ void k_emu_assemble(EmuNet n, const double *__restrict__ rivsto, const double *__restrict__ fldsto,
+                               const double *__restrict__ levsto, const double *__restrict__ rivdph,
+                               const double *__restrict__ flddph, const double *__restrict__ fldfrc,
+                               const double *__restrict__ qprev, const double *__restrict__ runoff,
+                               const float *__restrict__ planes, size_t plane, int hops, __nv_bfloat16 *X, int ldx,
+                               int rows_per_member) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n.N) return;
     // member blockIdx.y: state arrays are member-major [M][N], X rows [M][rows_per_member]
-    const size_t mo = (size_t)blockIdx.y * n.N;
-    rivsto += mo; fldsto += mo; if (levsto) levsto += mo; rivdph += mo; flddph += mo; fldfrc += mo; qprev += mo;
-    runoff += mo; msg_a += mo; msg_b += mo;
-    X += (size_t)blockIdx.y * rows_per_member * ldx;
+    const size_t mo = (size_t)blockIdx.y * n.N, gi = mo + i;
     const double q = n.qref[i];
-    const double S = rivsto[i] + fldsto[i] + (levsto ? levsto[i] : 0.0);
-    float f[14];
+    const double S = rivsto[gi] + fldsto[gi] + (levsto ? levsto[gi] : 0.0);
+    float f[32];
     f[0] = slog((float)(S / n.rivstomax[i]));
-    f[1] = (float)(rivdph[i] / n.rivhgt[i]);
-    f[2] = slog((float)flddph[i]);
-    f[3] = slog((float)(qprev[i] / q));
-    f[4] = slog((float)(runoff[i] / q));
-    f[5] = (float)fldfrc[i];
+    f[1] = (float)(rivdph[gi] / n.rivhgt[i]);
+    f[2] = slog((float)flddph[gi]);
+    f[3] = slog((float)(qprev[gi] / q));
+    f[4] = slog((float)(runoff[gi] / q));
+    f[5] = (float)fldfrc[gi];
     const bool mouth = i >= n.R;
     const int j = mouth ? i : n.next[i];
-    const double sfc = n.rivelv[i] + rivdph[i], sfcn = mouth ? n.elevtn[i] : n.rivelv[j] + rivdph[j];
-    f[6] = slog((float)(1000.0 * (sfc - sfcn) / (mouth ? 10000.0 : n.nxtdst[i])));
+    const double dst = mouth ? 10000.0 : n.nxtdst[i];
+    const double sfc = n.rivelv[i] + rivdph[gi], sfcn = mouth ? n.elevtn[i] : n.rivelv[j] + rivdph[mo + j];
+    const float slope = (float)((sfc - sfcn) / dst);
+    f[6] = slog(1000.f * slope);
     f[7] = slog((float)(1000.0 * (n.elevtn[i] - (mouth ? n.elevtn[i] : n.elevtn[j])) / n.nxtdst[i]));
     f[8] = logf((float)n.rivlen[i]) - 9.5f;
     f[9] = logf((float)n.rivwth[i]) - 4.0f;
@@ -360,43 +397,43 @@ __global__ void k_emu_local(EmuNet n, const double *rivsto, const double *fldsto
     f[11] = logf((float)q) - 3.0f;
     f[12] = mouth ? 1.f : 0.f;
     f[13] = slog((float)(S / (q * 3600.0)));
-    __nv_bfloat16 *row = X + (size_t)i * ldx;
+    const float qf = (float)q;
 #pragma unroll
-    for (int k = 0; k < 14; k++) row[k] = __float2bfloat16_rn(f[k]);
-    row[30] = __float2bfloat16_rn(0.f);
-    row[31] = __float2bfloat16_rn(0.f);
-    msg_a[i] = (float)qprev[i];
-    msg_b[i] = (float)runoff[i];
-}
-
-// one hop of upstream message passing: out[i] = sum over upstream j of in[j]; features at column c
-__global__ void k_emu_hop(EmuNet n, const float *in_a, const float *in_b, float *out_a, float *out_b, __nv_bfloat16 *X,
-                          int ldx, int rows_per_member, int col) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n.N) return;
-    const size_t mo = (size_t)blockIdx.y * n.N;
-    in_a += mo; in_b += mo; out_a += mo; out_b += mo;
-    X += (size_t)blockIdx.y * rows_per_member * ldx;
-    float a = 0.f, b = 0.f;
-    for (int k = n.up_ptr[i]; k < n.up_ptr[i + 1]; k++) {
-        const int j = n.up_idx[k];
-        a += in_a[j];
-        b += in_b[j];
+    for (int h = 0; h < 8; h++) {
+        if (h < hops) {
+            f[14 + 2 * h] = slog(planes[(size_t)(2 + 2 * h) * plane + gi] / qf);
+            f[15 + 2 * h] = slog(planes[(size_t)(3 + 2 * h) * plane + gi] / qf);
+        } else {
+            f[14 + 2 * h] = f[15 + 2 * h] = 0.f;
+        }
     }
-    out_a[i] = a;
-    out_b[i] = b;
-    const float q = (float)n.qref[i];
-    X[(size_t)i * ldx + col] = __float2bfloat16_rn(slog(a / q));
-    X[(size_t)i * ldx + col + 1] = __float2bfloat16_rn(slog(b / q));
+    // hydraulic estimates: Manning discharge of the channel and of the floodplain at the current
+    // water-surface slope (the state the local-inertial scheme relaxes towards within an hour)
+    const float w = (float)n.rivwth[i], hr = (float)rivdph[gi], hf = (float)flddph[gi];
+    const float af = fmaxf((float)(fldsto[gi] / n.rivlen[i]) - hf * w, 0.f);
+    f[30] = slog(manning_q(w * hr, hr, slope, (float)n.rivman[i]) / qf);
+    f[31] = slog(manning_q(af, hf, fmaxf(-0.005f, fminf(0.005f, slope)), (float)n.pmanfld) / qf);
+    uint4 *row = reinterpret_cast<uint4 *>(X + ((size_t)blockIdx.y * rows_per_member + i) * ldx);
+#pragma unroll
+    for (int v = 0; v < 4; v++) {
+        uint4 u;
+        u.x = pack_bf16x2(f[8 * v + 0], f[8 * v + 1]);
+        u.y = pack_bf16x2(f[8 * v + 2], f[8 * v + 3]);
+        u.z = pack_bf16x2(f[8 * v + 4], f[8 * v + 5]);
+        u.w = pack_bf16x2(f[8 * v + 6], f[8 * v + 7]);
+        row[v] = u;
+    }
 }
 
-// Mass-conserving rollout of one coupling step from the predicted change of the transformed mean
-// outflow: Q_i = qref_i * expm1(max(log1p(Qprev_i/qref_i) + y_i, 0)), limited to the storage the cell holds plus its own runoff over
-// DT (so storage never goes negative whatever its upstream delivers); storage then changes by
-// (inflow + runoff - outflow) * DT with the inflow gathered over the upstream CSR.
+// Mass-conserving rollout of one coupling step from the predicted transformed mean outflow:
+// Q_i = qref_i * expm1(max(base_i + y_i, 0)) with base_i = log1p(Qprev_i/qref_i) when the network
+// predicts the change over the step (residual != 0) and 0 when it predicts the value itself, limited
+// to the storage the cell holds plus its own runoff over DT (so storage never goes negative whatever
+// its upstream delivers); storage then changes by (inflow + runoff - outflow) * DT with the inflow
+// gathered over the upstream CSR.
 __global__ void k_emu_rollout(EmuNet n, const float *y, int ldy, int rows_per_member, const int *active, double dt,
-                              const double *runoff, const double *rivsto, const double *fldsto, const double *levsto,
-                              const double *qprev, double *qout) {
+                              int residual, const double *runoff, const double *rivsto, const double *fldsto,
+                              const double *levsto, const double *qprev, double *qout) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n.N || !active[blockIdx.y]) return;
     const size_t mo = (size_t)blockIdx.y * n.N;
@@ -404,7 +441,7 @@ __global__ void k_emu_rollout(EmuNet n, const float *y, int ldy, int rows_per_me
     runoff += mo; rivsto += mo; fldsto += mo; if (levsto) levsto += mo; qout += mo;
     const double S = rivsto[i] + fldsto[i] + (levsto ? levsto[i] : 0.0);
     // the network predicts the change of log1p(Q/qref) over the step (residual on the last outflow)
-    const double base = log1p(fmax(qprev[mo + i], 0.0) / n.qref[i]);
+    const double base = residual ? log1p(fmax(qprev[mo + i], 0.0) / n.qref[i]) : 0.0;
     const double yi = fmax(base + (double)y[(size_t)i * ldy], 0.0);
     double q = n.qref[i] * expm1(yi);
     q = fmin(q, S / dt + runoff[i]);
@@ -508,35 +545,37 @@ int cmf_emu_mlp_fused(const void *X, int ldx, int rows, const void *pack, const 
     return CMF_OK;
 }
 
-// Features of one member: X [N_pad][32] bf16; scratch a/b/c/d float [N] for the message ping-pong.
+// Features of every member: X rows [M][rows_per_member][ldx] bf16 (columns 0..31 written);
+// planes: fp32 [2 * (hops + 1)][M * N] scratch for the message passes.
 int cmf_emu_features(const cmf_emu_net *net, const cmf_emu_member *mb, int nmembers, void *X, int ldx, int rows_per_member,
-                     int hops, float *sa, float *sb, float *sc, float *sd, void *stream) {
-    if (!net || !mb || !X || hops < 0 || 14 + 2 * hops > 32 || ldx < 32 || nmembers < 1 || rows_per_member < net->nseqall)
-        return emu_err(CMF_E_ARG, "cmf_emu_features: bad arguments (14 + 2*hops must fit 32 columns)");
+                     int hops, float *planes, void *stream) {
+    if (!net || !mb || !X || !planes || hops < 0 || hops > 8 || ldx < 32 || (ldx % 8) || nmembers < 1 ||
+        rows_per_member < net->nseqall || ((uintptr_t)X & 15) || !net->rivman)
+        return emu_err(CMF_E_ARG, "cmf_emu_features: bad arguments (hops <= 8, ldx % 8 == 0, X 16-byte aligned)");
     EmuNet n{net->nseqall, net->nseqriv, net->next, net->up_ptr, net->up_idx, net->rivelv, net->elevtn, net->nxtdst,
-             net->rivwth, net->rivhgt, net->rivlen, net->rivstomax, net->qref};
+             net->rivwth, net->rivhgt, net->rivlen, net->rivstomax, net->qref, net->rivman, net->pmanfld};
     cudaStream_t st = (cudaStream_t)stream;
     const dim3 blocks((n.N + 255) / 256, nmembers);
-    k_emu_local<<<blocks, 256, 0, st>>>(n, mb->rivsto, mb->fldsto, mb->levsto, mb->rivdph, mb->flddph, mb->fldfrc, mb->qprev,
-                                        mb->runoff, (__nv_bfloat16 *)X, ldx, rows_per_member, sa, sb);
-    float *ia = sa, *ib = sb, *oa = sc, *ob = sd;
-    for (int h = 0; h < hops; h++) {
-        k_emu_hop<<<blocks, 256, 0, st>>>(n, ia, ib, oa, ob, (__nv_bfloat16 *)X, ldx, rows_per_member, 14 + 2 * h);
-        float *t = ia; ia = oa; oa = t;
-        t = ib; ib = ob; ob = t;
-    }
+    const size_t plane = (size_t)nmembers * n.N;
+    k_emu_seed<<<blocks, 256, 0, st>>>(n, mb->qprev, mb->runoff, planes, planes + plane);
+    for (int h = 0; h < hops; h++)
+        k_emu_hop<<<blocks, 256, 0, st>>>(n, planes + (size_t)(2 * h) * plane, planes + (size_t)(2 * h + 1) * plane,
+                                          planes + (size_t)(2 * h + 2) * plane, planes + (size_t)(2 * h + 3) * plane);
+    k_emu_assemble<<<blocks, 256, 0, st>>>(n, mb->rivsto, mb->fldsto, mb->levsto, mb->rivdph, mb->flddph, mb->fldfrc,
+                                           mb->qprev, mb->runoff, planes, plane, hops, (__nv_bfloat16 *)X, ldx,
+                                           rows_per_member);
     EMU_TRY(cudaGetLastError());
     return CMF_OK;
 }
 
 int cmf_emu_rollout(const cmf_emu_net *net, const cmf_emu_member *mb, int nmembers, const int *active_dev, const float *y,
-                    int ldy, int rows_per_member, double dt, double *qout, void *stream) {
+                    int ldy, int rows_per_member, double dt, int residual, double *qout, void *stream) {
     if (!net || !mb || !y || !qout || !active_dev || nmembers < 1) return emu_err(CMF_E_ARG, "cmf_emu_rollout: null argument");
     EmuNet n{net->nseqall, net->nseqriv, net->next, net->up_ptr, net->up_idx, net->rivelv, net->elevtn, net->nxtdst,
-             net->rivwth, net->rivhgt, net->rivlen, net->rivstomax, net->qref};
+             net->rivwth, net->rivhgt, net->rivlen, net->rivstomax, net->qref, net->rivman, net->pmanfld};
     cudaStream_t st = (cudaStream_t)stream;
     const dim3 blocks((n.N + 255) / 256, nmembers);
-    k_emu_rollout<<<blocks, 256, 0, st>>>(n, y, ldy, rows_per_member, active_dev, dt, mb->runoff, mb->rivsto, mb->fldsto,
+    k_emu_rollout<<<blocks, 256, 0, st>>>(n, y, ldy, rows_per_member, active_dev, dt, residual, mb->runoff, mb->rivsto, mb->fldsto,
                                           mb->levsto, mb->qprev, qout);
     k_emu_update<<<blocks, 256, 0, st>>>(n, active_dev, dt, mb->runoff, qout, mb->rivsto, mb->fldsto, mb->levsto,
                                          mb->rivout_pre, mb->fldout_pre, mb->qprev);

@@ -59,6 +59,8 @@ struct cmf_gpu_ctx {
     int64_t launches = 0;
     // host staging for the per-member control block
     std::vector<cmf::MemberCtl> hctl;
+    // sea-level boundary inputs (allocated on first use)
+    double *bnd_sealev = nullptr, *bnd_meansl = nullptr;
 
     template <class T>
     int alloc(T **p, size_t n) {
@@ -88,6 +90,21 @@ struct cmf_gpu_ctx {
         *p = q;
         return CMF_OK;
     }
+};
+
+// Several contexts (regional domains of uneven size, each with its own members) advanced by ONE
+// graph launch per coupling step: every context's outer step is an independent branch of the
+// batch graph with its own WHILE node, so each domain loops over its own sub-step count while the
+// branches run concurrently on the device.
+struct cmf_gpu_batch {
+    std::vector<cmf_gpu_ctx *> ctx;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    std::vector<cudaEvent_t> ready;
+    cudaEvent_t done = nullptr;
+    int64_t launches = 0;
 };
 
 namespace {
@@ -313,28 +330,28 @@ void set_blocks(cmf_gpu_ctx *c, int block) {
 }
 
 // Enqueue one sub-step (phases A, B, C and the control kernel).
-void enqueue_substep(cmf_gpu_ctx *c, int use_cond) {
+void enqueue_substep(cmf_gpu_ctx *c, int use_cond, cudaGraphConditionalHandle cond) {
     const dim3 gc(c->ncell_blocks, c->dims.nmembers);
     const dim3 gcp(c->ncell_blocks + c->npath_blocks, c->dims.nmembers);
     cmf::k_flux<<<gcp, c->block, 0, c->stream>>>(c->net, c->st, c->ncell_blocks);
     cmf::k_rate<<<gc, c->block, 0, c->stream>>>(c->net, c->st);
     cmf::k_store<<<gcp, c->block, 0, c->stream>>>(c->net, c->st, c->ncell_blocks);
-    cmf::k_ctl<<<1, 32 * cmf::kBudgets, 0, c->stream>>>(c->net, c->st, c->ncell_blocks, c->cond, use_cond);
+    cmf::k_ctl<<<1, 32 * cmf::kBudgets, 0, c->stream>>>(c->net, c->st, c->ncell_blocks, cond, use_cond);
 }
+void enqueue_substep(cmf_gpu_ctx *c, int use_cond) { enqueue_substep(c, use_cond, c->cond); }
 
-void enqueue_prologue(cmf_gpu_ctx *c, int use_cond) {
+void enqueue_prologue(cmf_gpu_ctx *c, int use_cond, cudaGraphConditionalHandle cond) {
     const dim3 gc(c->ncell_blocks, c->dims.nmembers);
     cmf::k_stage<<<gc, c->block, 0, c->stream>>>(c->net, c->st);
-    cmf::k_ntdt<<<1, 256, 0, c->stream>>>(c->net, c->st, c->cond, use_cond);
+    cmf::k_ntdt<<<1, 256, 0, c->stream>>>(c->net, c->st, cond, use_cond);
 }
+void enqueue_prologue(cmf_gpu_ctx *c, int use_cond) { enqueue_prologue(c, use_cond, c->cond); }
 
-int build_graph(cmf_gpu_ctx *c) {
-    if (c->exec) { cudaGraphExecDestroy(c->exec); c->exec = nullptr; }
-    if (c->graph) { cudaGraphDestroy(c->graph); c->graph = nullptr; }
-    CUDA_TRY(cudaGraphCreate(&c->graph, 0));
-    CUDA_TRY(cudaGraphConditionalHandleCreate(&c->cond, c->graph, 1u, cudaGraphCondAssignDefault));
-    CUDA_TRY(cudaStreamBeginCaptureToGraph(c->stream, c->graph, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
-    enqueue_prologue(c, 1);
+// Captures one context's outer step (prologue, then a WHILE node around the sub-step body) into
+// `graph` as a branch with no dependencies, using the conditional handle `cond` of that graph.
+int capture_outer(cmf_gpu_ctx *c, cudaGraph_t graph, cudaGraphConditionalHandle cond) {
+    CUDA_TRY(cudaStreamBeginCaptureToGraph(c->stream, graph, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    enqueue_prologue(c, 1, cond);
     cudaStreamCaptureStatus status;
     const cudaGraphNode_t *deps = nullptr;
     size_t ndeps = 0;
@@ -342,7 +359,7 @@ int build_graph(cmf_gpu_ctx *c) {
     CUDA_TRY(cudaStreamGetCaptureInfo(c->stream, &status, nullptr, &captured, &deps, &ndeps));
     cudaGraphNodeParams cp = {};
     cp.type = cudaGraphNodeTypeConditional;
-    cp.conditional.handle = c->cond;
+    cp.conditional.handle = cond;
     cp.conditional.type = cudaGraphCondTypeWhile;
     cp.conditional.size = 1;
     cudaGraphNode_t cnode;
@@ -352,9 +369,19 @@ int build_graph(cmf_gpu_ctx *c) {
     cudaGraph_t g2 = nullptr;
     CUDA_TRY(cudaStreamEndCapture(c->stream, &g2));
     CUDA_TRY(cudaStreamBeginCaptureToGraph(c->stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
-    enqueue_substep(c, 1);
+    enqueue_substep(c, 1, cond);
     cudaGraph_t g3 = nullptr;
     CUDA_TRY(cudaStreamEndCapture(c->stream, &g3));
+    return CMF_OK;
+}
+
+int build_graph(cmf_gpu_ctx *c) {
+    if (c->exec) { cudaGraphExecDestroy(c->exec); c->exec = nullptr; }
+    if (c->graph) { cudaGraphDestroy(c->graph); c->graph = nullptr; }
+    CUDA_TRY(cudaGraphCreate(&c->graph, 0));
+    CUDA_TRY(cudaGraphConditionalHandleCreate(&c->cond, c->graph, 1u, cudaGraphCondAssignDefault));
+    int rc = capture_outer(c, c->graph, c->cond);
+    if (rc) return rc;
     CUDA_TRY(cudaGraphInstantiate(&c->exec, c->graph, 0));
     return CMF_OK;
 }
@@ -720,6 +747,96 @@ int cmf_gpu_ctx_advance_device(cmf_gpu_ctx *c, double dt_def, int32_t ksteps, co
     return CMF_OK;
 }
 
+void cmf_gpu_batch_destroy(cmf_gpu_batch *b) {
+    if (!b) return;
+    cudaSetDevice(b->device);
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    for (cudaEvent_t e : b->ready) if (e) cudaEventDestroy(e);
+    if (b->done) cudaEventDestroy(b->done);
+    if (b->stream) cudaStreamDestroy(b->stream);
+    delete b;
+}
+
+int cmf_gpu_batch_create(cmf_gpu_ctx *const *ctxs, int32_t n, cmf_gpu_batch **out) {
+    if (!ctxs || n < 1 || !out) return set_err(CMF_E_ARG, "cmf_gpu_batch_create: null argument or empty batch");
+    *out = nullptr;
+    for (int k = 0; k < n; k++) {
+        if (!ctxs[k]) return set_err(CMF_E_ARG, "cmf_gpu_batch_create: null context");
+        if (ctxs[k]->device != ctxs[0]->device) return set_err(CMF_E_ARG, "cmf_gpu_batch_create: contexts on different devices");
+        if (ctxs[k]->opts.launch_mode != 0) return set_err(CMF_E_ARG, "cmf_gpu_batch_create: contexts must use launch_mode 0");
+        for (int j = 0; j < k; j++)
+            if (ctxs[j] == ctxs[k]) return set_err(CMF_E_ARG, "cmf_gpu_batch_create: a context appears twice");
+    }
+    auto *b = new cmf_gpu_batch();
+    b->ctx.assign(ctxs, ctxs + n);
+    b->device = ctxs[0]->device;
+    auto fail = [&](int code) { cmf_gpu_batch_destroy(b); return code; };
+    if (cudaSetDevice(b->device) != cudaSuccess || cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&b->done, cudaEventDisableTiming) != cudaSuccess || cudaGraphCreate(&b->graph, 0) != cudaSuccess)
+        return fail(set_err(CMF_E_CUDA, "cmf_gpu_batch_create: stream/event/graph creation failed"));
+    b->ready.assign(n, nullptr);
+    for (int k = 0; k < n; k++) {
+        if (cudaEventCreateWithFlags(&b->ready[k], cudaEventDisableTiming) != cudaSuccess)
+            return fail(set_err(CMF_E_CUDA, "cmf_gpu_batch_create: event creation failed"));
+        cmf_gpu_ctx *c = ctxs[k];
+        if (cudaStreamSynchronize(c->stream) != cudaSuccess) return fail(set_err(CMF_E_CUDA, "context stream failed"));
+        cudaGraphConditionalHandle h;
+        if (cudaGraphConditionalHandleCreate(&h, b->graph, 1u, cudaGraphCondAssignDefault) != cudaSuccess)
+            return fail(set_err(CMF_E_CUDA, "cmf_gpu_batch_create: conditional handle"));
+        int rc = capture_outer(c, b->graph, h);
+        if (rc) return fail(rc);
+    }
+    if (cudaGraphInstantiate(&b->exec, b->graph, 0) != cudaSuccess)
+        return fail(set_err(CMF_E_CUDA, "cmf_gpu_batch_create: graph instantiation failed"));
+    *out = b;
+    return CMF_OK;
+}
+
+int cmf_gpu_batch_launch(cmf_gpu_batch *b, double dt_def) {
+    if (!b) return set_err(CMF_E_STATE, "no batch");
+    CUDA_TRY(cudaSetDevice(b->device));
+    int rc;
+    for (size_t k = 0; k < b->ctx.size(); k++) {
+        cmf_gpu_ctx *c = b->ctx[k];
+        if ((rc = sync_dt_def(c, dt_def))) return rc;
+        CUDA_TRY(cudaEventRecord(b->ready[k], c->stream));          // runoff, state uploads, DT
+        CUDA_TRY(cudaStreamWaitEvent(b->stream, b->ready[k], 0));
+    }
+    CUDA_TRY(cudaGraphLaunch(b->exec, b->stream));
+    CUDA_TRY(cudaEventRecord(b->done, b->stream));
+    for (cmf_gpu_ctx *c : b->ctx) {
+        CUDA_TRY(cudaStreamWaitEvent(c->stream, b->done, 0));      // later work of a context follows the step
+        c->launches += 2;
+    }
+    b->launches += 1;
+    return CMF_OK;
+}
+
+int cmf_gpu_batch_advance(cmf_gpu_batch *b, double dt_def, int32_t *nt_out, double *dt_out, cmf_budget *budget_out) {
+    int rc = cmf_gpu_batch_launch(b, dt_def);
+    if (rc) return rc;
+    size_t off = 0;
+    int first_err = CMF_OK;
+    for (cmf_gpu_ctx *c : b->ctx) {
+        rc = finish_outer(c, nt_out ? nt_out + off : nullptr, dt_out ? dt_out + off : nullptr,
+                          budget_out ? budget_out + off : nullptr);
+        if (rc && !first_err) first_err = rc;
+        off += (size_t)c->dims.nmembers;
+    }
+    return first_err;
+}
+
+int cmf_gpu_batch_synchronize(cmf_gpu_batch *b) {
+    if (!b) return set_err(CMF_E_STATE, "no batch");
+    CUDA_TRY(cudaSetDevice(b->device));
+    CUDA_TRY(cudaStreamSynchronize(b->stream));
+    return CMF_OK;
+}
+
+void *cmf_gpu_batch_stream(cmf_gpu_batch *b) { return b ? (void *)b->stream : nullptr; }
+
 int cmf_gpu_ctx_synchronize(cmf_gpu_ctx *c) {
     if (!c) return set_err(CMF_E_STATE, "no context");
     CUDA_TRY(cudaSetDevice(c->device));
@@ -748,7 +865,8 @@ int cmf_gpu_ctx_emu_views(cmf_gpu_ctx *c, int32_t m, cmf_emu_net *net, cmf_emu_m
         net->next = c->net.next; net->up_ptr = c->net.up_ptr; net->up_idx = c->net.up_idx;
         net->rivelv = c->net.rivelv; net->elevtn = c->net.elevtn; net->nxtdst = c->net.nxtdst;
         net->rivwth = c->net.rivwth; net->rivhgt = c->net.rivhgt; net->rivlen = c->net.rivlen;
-        net->rivstomax = c->net.rivstomax; net->qref = nullptr;
+        net->rivstomax = c->net.rivstomax; net->qref = nullptr; net->rivman = c->net.rivman;
+        net->pmanfld = c->net.pmanfld;
     }
     if (mb) {
         const cmf::State &s = c->st;
@@ -795,6 +913,43 @@ int cmf_gpu_ctx_copy_member(cmf_gpu_ctx *d, int32_t dm, cmf_gpu_ctx *s, int32_t 
         CUDA_TRY(cudaMemcpyAsync(A.pthflw_pre + dm * PL, B.pthflw_pre + sm * PL, PL * 8, cudaMemcpyDeviceToDevice, s->stream));
     }
     CUDA_TRY(cudaStreamSynchronize(s->stream));
+    return CMF_OK;
+}
+
+int cmf_gpu_ctx_calc_outpre(cmf_gpu_ctx *c) {
+    if (!c) return set_err(CMF_E_STATE, "no context");
+    // CMF_DRV_INIT (src/cmf_drv_control_mod.F90:273-277): stage scheme, then CMF_CALC_OUTPRE
+    const double dt = c->dt_def_dev > 0.0 ? c->dt_def_dev : 86400.0;
+    int rc = cmf_gpu_ctx_stage(c, dt, nullptr);
+    if (rc) return rc;
+    const dim3 g(c->ncell_blocks + c->npath_blocks, c->dims.nmembers);
+    cmf::k_outpre<<<g, c->block, 0, c->stream>>>(c->net, c->st, c->ncell_blocks);
+    CUDA_TRY(cudaGetLastError());
+    c->launches += 1;
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    return CMF_OK;
+}
+
+int cmf_gpu_ctx_update_boundary(cmf_gpu_ctx *c, const double *sealev, const double *meansl) {
+    if (!c) return set_err(CMF_E_STATE, "no context");
+    CUDA_TRY(cudaSetDevice(c->device));
+    const size_t N = c->dims.nseqall;
+    int rc;
+    if (sealev) {
+        if (!c->bnd_sealev && (rc = c->alloc(&c->bnd_sealev, N))) return rc;
+        CUDA_TRY(cudaMemcpyAsync(c->bnd_sealev, sealev, N * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    }
+    if (meansl) {
+        if (!c->bnd_meansl && (rc = c->alloc(&c->bnd_meansl, N))) return rc;
+        CUDA_TRY(cudaMemcpyAsync(c->bnd_meansl, meansl, N * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    }
+    // D2DWNELV is static data of the context (read by the graph's kernels through the same pointer)
+    cmf::k_boundary<<<(unsigned)((N + 255) / 256), 256, 0, c->stream>>>((int)N, c->net.elevtn, meansl ? c->bnd_meansl : nullptr,
+                                                                        sealev ? c->bnd_sealev : nullptr,
+                                                                        const_cast<double *>(c->net.dwnelv));
+    CUDA_TRY(cudaGetLastError());
+    c->launches += 1;
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
     return CMF_OK;
 }
 

@@ -608,6 +608,129 @@ int cmf_host_conv_resol(const cmf_host_model *hm, const double *map, double *out
     return CMF_OK;
 }
 
+// ---- binary restart (CMF_RESTART_WRITE / CMF_RESTART_INIT, src/cmf_ctrl_restart_mod.F90:91-482) ----
+// Record layout: one NX x NY map per variable (FP64 when LRESTDBL, else FP32), cells outside the
+// sequence filled with DMIS / RMIS = 1.E20, in the order rivsto, fldsto, [rivout_pre, fldout_pre,
+// rivdph_pre, fldsto_pre unless LSTOONLY], [damsto if LDAMOUT], [levsto if LLEVEE]; bifurcation
+// flows D1PTHFLW_PRE as one (NPTHOUT,NPTHLEV) record in <file>.pth.
+namespace {
+int rest_put(const cmf_host_model *hm, FILE *f, const double *vec, bool dbl) {
+    const size_t nxy = static_cast<size_t>(hm->nx) * hm->ny;
+    size_t w;
+    if (dbl) {
+        std::vector<double> map(nxy, 1.E20);
+        for (int i = 0; i < hm->nseqmax; i++) map[hm->g(hm->i1seqx[i], hm->i1seqy[i])] = vec[i];
+        w = std::fwrite(map.data(), sizeof(double), nxy, f);
+    } else {
+        std::vector<float> map(nxy, 1.E20f);
+        for (int i = 0; i < hm->nseqmax; i++) map[hm->g(hm->i1seqx[i], hm->i1seqy[i])] = static_cast<float>(vec[i]);
+        w = std::fwrite(map.data(), sizeof(float), nxy, f);
+    }
+    return w == nxy ? CMF_OK : CMF_E_IO;
+}
+int rest_get(const cmf_host_model *hm, FILE *f, double *vec, bool dbl) {
+    const size_t nxy = static_cast<size_t>(hm->nx) * hm->ny;
+    std::vector<double> map(nxy);
+    if (dbl) {
+        if (std::fread(map.data(), sizeof(double), nxy, f) != nxy) return CMF_E_IO;
+    } else {
+        std::vector<float> r(nxy);
+        if (std::fread(r.data(), sizeof(float), nxy, f) != nxy) return CMF_E_IO;
+        for (size_t k = 0; k < nxy; k++) map[k] = static_cast<double>(r[k]);
+    }
+    for (int i = 0; i < hm->nseqmax; i++) vec[i] = map[hm->g(hm->i1seqx[i], hm->i1seqy[i])];
+    return CMF_OK;
+}
+}  // namespace
+
+int cmf_host_write_restart(const cmf_host_model *hm, const cmf_state_ptrs *st, const char *file, int32_t lrestdbl,
+                           int32_t lstoonly) {
+    if (!hm || !st || !file || !st->rivsto || !st->fldsto) return CMF_E_ARG;
+    const auto &n = hm->nl;
+    if (!lstoonly && (!st->rivout_pre || !st->fldout_pre || !st->rivdph_pre || !st->fldsto_pre)) return CMF_E_ARG;
+    if ((n.ldamout && !st->damsto) || (n.llevee && !st->levsto) || (n.lpthout && !st->pthflw_pre)) return CMF_E_ARG;
+    FILE *f = std::fopen(file, "wb");
+    if (!f) return CMF_E_IO;
+    const bool dbl = lrestdbl != 0;
+    int rc = rest_put(hm, f, st->rivsto, dbl);
+    if (!rc) rc = rest_put(hm, f, st->fldsto, dbl);
+    if (!rc && !lstoonly) {
+        for (const double *v : {st->rivout_pre, st->fldout_pre, st->rivdph_pre, st->fldsto_pre})
+            if (!rc) rc = rest_put(hm, f, v, dbl);
+    }
+    if (!rc && n.ldamout) rc = rest_put(hm, f, st->damsto, dbl);
+    if (!rc && n.llevee) rc = rest_put(hm, f, st->levsto, dbl);
+    if (std::fclose(f) != 0 && !rc) rc = CMF_E_IO;
+    if (rc || !n.lpthout) return rc;
+    const std::string pth = std::string(file) + ".pth";
+    FILE *g = std::fopen(pth.c_str(), "wb");
+    if (!g) return CMF_E_IO;
+    const size_t np = static_cast<size_t>(hm->npthout) * hm->npthlev;
+    size_t w;
+    if (dbl) {
+        w = std::fwrite(st->pthflw_pre, sizeof(double), np, g);
+    } else {
+        std::vector<float> r(np);
+        for (size_t k = 0; k < np; k++) r[k] = static_cast<float>(st->pthflw_pre[k]);
+        w = std::fwrite(r.data(), sizeof(float), np, g);
+    }
+    if (std::fclose(g) != 0 || w != np) return CMF_E_IO;
+    return CMF_OK;
+}
+
+int cmf_host_read_restart(const cmf_host_model *hm, const cmf_state_ptrs *st, const char *file, int32_t lrestdbl,
+                          int32_t lstoonly) {
+    if (!hm || !st || !file || !st->rivsto || !st->fldsto || !st->rivout || !st->fldout || !st->rivout_pre ||
+        !st->fldout_pre || !st->rivdph_pre || !st->fldsto_pre)
+        return CMF_E_ARG;
+    const auto &n = hm->nl;
+    if ((n.ldamout && !st->damsto) || (n.llevee && !st->levsto) || (n.lpthout && (!st->pthflw_pre || !st->pthflw)))
+        return CMF_E_ARG;
+    const size_t N = static_cast<size_t>(hm->nseqmax), np = static_cast<size_t>(hm->npthout) * hm->npthlev;
+    for (double *v : {st->rivsto, st->fldsto, st->rivout, st->fldout, st->rivout_pre, st->fldout_pre, st->rivdph_pre,
+                      st->fldsto_pre})
+        std::fill(v, v + N, 0.0);
+    if (n.ldamout) std::fill(st->damsto, st->damsto + N, 0.0);
+    if (n.llevee) std::fill(st->levsto, st->levsto + N, 0.0);
+    if (n.lpthout) { std::fill(st->pthflw, st->pthflw + np, 0.0); std::fill(st->pthflw_pre, st->pthflw_pre + np, 0.0); }
+    FILE *f = std::fopen(file, "rb");
+    if (!f) return CMF_E_IO;
+    const bool dbl = lrestdbl != 0;
+    int rc = rest_get(hm, f, st->rivsto, dbl);
+    if (!rc) rc = rest_get(hm, f, st->fldsto, dbl);
+    if (!rc && !lstoonly) {
+        for (double *v : {st->rivout_pre, st->fldout_pre, st->rivdph_pre, st->fldsto_pre})
+            if (!rc) rc = rest_get(hm, f, v, dbl);
+    }
+    if (!rc && n.ldamout) rc = rest_get(hm, f, st->damsto, dbl);
+    if (!rc && n.llevee) rc = rest_get(hm, f, st->levsto, dbl);
+    std::fclose(f);
+    if (rc) return rc;
+    if (n.lpthout && !lstoonly) {
+        const std::string pth = std::string(file) + ".pth";
+        FILE *g = std::fopen(pth.c_str(), "rb");
+        if (!g) return CMF_E_IO;
+        size_t r;
+        if (dbl) {
+            r = std::fread(st->pthflw_pre, sizeof(double), np, g);
+        } else {
+            std::vector<float> v(np);
+            r = std::fread(v.data(), sizeof(float), np, g);
+            for (size_t k = 0; k < np; k++) st->pthflw_pre[k] = static_cast<double>(v[k]);
+        }
+        std::fclose(g);
+        if (r != np) return CMF_E_IO;
+    }
+    if (lstoonly) std::copy(st->fldsto, st->fldsto + N, st->fldsto_pre);   // :130-132
+    return CMF_OK;
+}
+
+int cmf_host_map_to_vec(const cmf_host_model *hm, const float *map, double *vec) {
+    if (!hm || !map || !vec) return CMF_E_ARG;
+    for (int i = 0; i < hm->nseqmax; i++) vec[i] = static_cast<double>(map[hm->g(hm->i1seqx[i], hm->i1seqy[i])]);
+    return CMF_OK;
+}
+
 int cmf_host_grid(const cmf_host_model *hm, int32_t *nx, int32_t *ny, int32_t *sx, int32_t *sy) {
     if (!hm) return CMF_E_ARG;
     if (nx) *nx = hm->nx;

@@ -896,4 +896,83 @@ __global__ void k_ctl(Net n, State s, int ncell_blocks, cudaGraphConditionalHand
     }
 }
 
+// ------------------------------------------------------------------------------------------
+// k_outpre: CMF_CALC_OUTPRE (src/cmf_opt_outflw_mod.F90:308-421) -- previous-step discharge by the
+// diffusive (Manning) wave, after a storage-only restart and the stage scheme.  Cells on blocks
+// [0, ncell_blocks), bifurcation paths on the blocks after them; the downstream surface elevation
+// is recomputed from the depth (the same sum the reference stores in D2SFCELV first).
+// ------------------------------------------------------------------------------------------
+__global__ void k_outpre(Net n, State s, int ncell_blocks) {
+    const int m = blockIdx.y;
+    const size_t base = (size_t)m * n.N;
+    const double p23 = CMF_F(2. / 3.);
+    if ((int)blockIdx.x < ncell_blocks) {
+        const int i = blockIdx.x * blockDim.x + threadIdx.x;
+        if (i >= n.N) return;
+        const size_t gi = base + i;
+        const double rivdph = s.rivdph[gi];
+        const double sfc = n.rivelv[i] + rivdph;
+        s.sfcelv[gi] = sfc;
+        s.rivdph_pre[gi] = rivdph;
+        double dslope, dsfcmax, dflw;
+        if (i < n.R) {
+            const int j = n.next[i];
+            const double sfcj = n.rivelv[j] + s.rivdph[base + j];
+            dsfcmax = dmax(sfc, sfcj);
+            dslope = (sfc - sfcj) * (1.0 / n.nxtdst[i]);
+            dflw = dsfcmax - n.rivelv[i];
+        } else {
+            dsfcmax = sfc;
+            dslope = (sfc - n.dwnelv[i]) * (1.0 / n.pdstmth);
+            dflw = rivdph;
+        }
+        const double dslope_f = dmax(-0.005, dmin(0.005, dslope));
+        const double darea = n.rivwth[i] * dflw;
+        double rout = 0.0;
+        if (darea > CMF_F(1.E-5)) {
+            rout = darea * (((1.0 / n.rivman[i]) * pow(dflw, p23)) * sqrt(fabs(dslope)));
+            if (dslope < 0.0) rout = -rout;
+        }
+        const double dflw_f = dmax(dsfcmax - n.elevtn[i], 0.0);
+        double dare_f = s.fldsto[gi] * (1.0 / n.rivlen[i]);
+        dare_f = dmax(dare_f - s.flddph[gi] * n.rivwth[i], 0.0);
+        double fout = 0.0;
+        if (dare_f > CMF_F(1.E-5)) {
+            fout = dare_f * (((1.0 / n.pmanfld) * pow(dflw_f, p23)) * sqrt(fabs(dslope_f)));
+            if (dslope_f < 0.0) fout = -fout;
+        }
+        s.rivout_pre[gi] = rout;
+        s.fldout_pre[gi] = n.lfldout ? fout : 0.0;
+    } else {
+        const int p = (blockIdx.x - ncell_blocks) * blockDim.x + threadIdx.x;
+        if (p >= n.P) return;
+        const int u = n.pth_up[p], d = n.pth_dn[p];
+        if (u < 0 || d < 0) return;                    // path leaves the domain
+        const size_t pb = (size_t)m * n.Lp * n.P;
+        const double su = n.rivelv[u] + s.rivdph[base + u], sd = n.rivelv[d] + s.rivdph[base + d];
+        const double dslope = (su - sd) * (1.0 / n.pth_dst[p]);
+        for (int l = 0; l < n.Lp; l++) {
+            const size_t o = (size_t)l * n.P + p;
+            const double dflw = dmax(dmax(su, sd) - n.pth_elv[o], 0.0);
+            double f = 0.0;
+            if (dflw > CMF_F(1.E-5)) {
+                f = (n.pth_wth[o] * dflw) * (((1.0 / n.pth_man[l]) * pow(dflw, p23)) * sqrt(fabs(dslope)));
+                if (dslope < 0.0) f = -f;
+            }
+            s.pthflw_pre[pb + o] = f;
+        }
+    }
+}
+
+// k_boundary: CMF_BOUNDARY_UPDATE (src/cmf_ctrl_boundary_mod.F90:267-304): downstream boundary
+// elevation D2DWNELV = D2ELEVTN (+ D2MEANSL) (+ D2SEALEV); only the mouths read it.
+__global__ void k_boundary(int N, const double *__restrict__ elevtn, const double *__restrict__ meansl,
+                           const double *__restrict__ sealev, double *dwnelv) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    double v = meansl ? elevtn[i] + meansl[i] : elevtn[i];
+    if (sealev) v = v + sealev[i];
+    dwnelv[i] = v;
+}
+
 }  // namespace cmf

@@ -188,6 +188,33 @@ int cmf_gpu_ctx_counters(cmf_gpu_ctx *ctx, int64_t *member_substeps, int64_t *lo
  * duration of the stage/CFL, NT/DT, flux, rate, storage and control kernels. */
 int cmf_gpu_ctx_time_phases(cmf_gpu_ctx *ctx, double dt_def, int32_t reps, double *ms_out);
 
+/* Storage-only restart (LSTOONLY): the stage scheme, then CMF_CALC_OUTPRE
+ * (src/cmf_opt_outflw_mod.F90:308-421) reconstructs D2RIVOUT_PRE, D2FLDOUT_PRE, D1PTHFLW_PRE and
+ * D2RIVDPH_PRE of every member from the storage by the diffusive (Manning) wave, as CMF_DRV_INIT
+ * does after a storage-only restart (src/cmf_drv_control_mod.F90:273-277).  Synchronous. */
+int cmf_gpu_ctx_calc_outpre(cmf_gpu_ctx *ctx);
+/* Downstream boundary of the mouths, CMF_BOUNDARY_UPDATE (src/cmf_ctrl_boundary_mod.F90:267-304):
+ * D2DWNELV = D2ELEVTN (+ meansl when non-NULL) (+ sealev when non-NULL); host arrays [NSEQALL]
+ * (sealev from CMF_BOUNDARY_GET_BIN's map via cmf_host_map_to_vec).  Synchronous. */
+int cmf_gpu_ctx_update_boundary(cmf_gpu_ctx *ctx, const double *sealev, const double *meansl);
+
+/* Batch of contexts on one device -- regional domains of uneven size, each with its own members --
+ * advanced by ONE graph launch per coupling step.  Each context's outer step (prologue + WHILE
+ * sub-step loop) is an independent branch of the batch graph, so every domain and member keeps its
+ * own adaptive DT (NT/DT per member as in CMF_PHYSICS_ADVANCE) and the branches run concurrently.
+ * Results equal those of advancing each context alone.  Contexts must use launch_mode 0 and stay
+ * alive while the batch exists.  cmf_gpu_batch_launch is asynchronous (ordered after each
+ * context's earlier work, and each context's later work waits for it); cmf_gpu_batch_advance also
+ * reads back NT/DT/budgets, concatenated over the contexts in batch order (sum of nmembers). */
+typedef struct cmf_gpu_batch cmf_gpu_batch;
+int cmf_gpu_batch_create(cmf_gpu_ctx *const *ctxs, int32_t nctx, cmf_gpu_batch **out);
+int cmf_gpu_batch_launch(cmf_gpu_batch *batch, double dt_def);
+int cmf_gpu_batch_advance(cmf_gpu_batch *batch, double dt_def, int32_t *nt_out, double *dt_out,
+                          cmf_budget *budget_out);
+int cmf_gpu_batch_synchronize(cmf_gpu_batch *batch);
+void *cmf_gpu_batch_stream(cmf_gpu_batch *batch);
+void cmf_gpu_batch_destroy(cmf_gpu_batch *batch);
+
 /* Split outer step for basin-region sharding across GPUs (one 8-byte MIN all-reduce of DT_MIN
  * per outer step, src/cmf_ctrl_mpi_mod.F90:261-281): stage + local CFL minimum ... */
 int cmf_gpu_ctx_stage(cmf_gpu_ctx *ctx, double dt_def, double *dt_min_local);
@@ -223,11 +250,13 @@ int cmf_gpu_stage_noalloc(const cmf_stage_dev_args *args);
 /* Learned per-cell emulator (no counterpart in the reference): device building blocks       */
 /* ======================================================================================== */
 /* Device views of a context's network (next: 0-based downstream, -1 at mouths; upstream CSR in
- * the reference's I1UPST order).  qref (per-cell discharge scale, m3/s) is set by the caller. */
+ * the reference's I1UPST order) and the floodplain Manning coefficient.  qref (per-cell discharge
+ * scale, m3/s) is set by the caller. */
 typedef struct cmf_emu_net {
     int32_t nseqall, nseqriv;
     const int32_t *next, *up_ptr, *up_idx;
-    const double *rivelv, *elevtn, *nxtdst, *rivwth, *rivhgt, *rivlen, *rivstomax, *qref;
+    const double *rivelv, *elevtn, *nxtdst, *rivwth, *rivhgt, *rivlen, *rivstomax, *qref, *rivman;
+    double pmanfld;
 } cmf_emu_net;
 /* Device views of one member's state; qprev is the mean outflow of the last coupling step
  * (D2OUTFLW_aAVG of the physics, or the emulator's own prediction). */
@@ -251,15 +280,17 @@ int cmf_emu_mse_grad(int rows, int valid, int ldy, const float *Y, const float *
                      float *loss_part, void *stream);
 int cmf_emu_adam(int n, float *w, void *wb, const float *grad, float *m, float *v, float lr, float b1, float b2,
                  float eps, int step, float wd, void *stream);
-/* 14 local features + 2 channels x `hops` upstream messages -> X rows (bf16, ldx >= 32), for
- * nmembers members whose state arrays start at the member-0 views in mb (member-major [M][N]);
- * member m's rows start at m * rows_per_member.  Scratch sa..sd: float [M][N] each. */
+/* 14 local features + 2 channels x `hops` (<= 8) upstream messages + 2 Manning estimates -> the
+ * first 32 columns of X rows (bf16, ldx % 8 == 0, X 16-byte aligned), for nmembers members whose
+ * state arrays start at the member-0 views in mb (member-major [M][N]); member m's rows start at
+ * m * rows_per_member.  planes: float scratch [2 * (hops + 1)][M * N]. */
 int cmf_emu_features(const cmf_emu_net *net, const cmf_emu_member *mb, int nmembers, void *X, int ldx,
-                     int rows_per_member, int hops, float *sa, float *sb, float *sc, float *sd, void *stream);
+                     int rows_per_member, int hops, float *planes, void *stream);
 /* Mass-conserving step from predicted transformed outflows y (column 0, stride ldy) for every
- * member with active_dev[m] != 0 (device int array); qout: double [M][N] scratch. */
+ * member with active_dev[m] != 0 (device int array); residual != 0: y is the change of
+ * log1p(Q/qref) over the step, else its value; qout: double [M][N] scratch. */
 int cmf_emu_rollout(const cmf_emu_net *net, const cmf_emu_member *mb, int nmembers, const int *active_dev,
-                    const float *y, int ldy, int rows_per_member, double dt, double *qout, void *stream);
+                    const float *y, int ldy, int rows_per_member, double dt, int residual, double *qout, void *stream);
 /* Fused inference of the 4-layer MLP.  cmf_emu_mlp_pack re-lays the bf16 weights (W0..W2 [K][128],
  * W3 [128][ldw3], row-major) into tensor-core fragment order in `pack` (cmf_emu_mlp_pack_bytes()
  * bytes, device memory); cmf_emu_mlp_fused then maps X rows (bf16, ldx >= 32 and even, columns
@@ -306,6 +337,20 @@ int cmf_host_state(cmf_host_model *hm, cmf_state_ptrs *st);
 int cmf_host_conv_resol(const cmf_host_model *hm, const double *map, double *runoff_out);
 /* Grid position of every sequence cell (I1SEQX/I1SEQY, 1-based) and the grid size. */
 int cmf_host_grid(const cmf_host_model *hm, int32_t *nx, int32_t *ny, int32_t *i1seqx, int32_t *i1seqy);
+/* mapR2vecD (src/cmf_utils_mod.F90:282-303): an NX x NY float map (e.g. a sea-level record of
+ * CMF_BOUNDARY_GET_BIN) to a double vector in sequence order. */
+int cmf_host_map_to_vec(const cmf_host_model *hm, const float *map, double *vec);
+/* Binary restart of one member's state in the reference's layout (CMF_RESTART_WRITE / WRTE_REST_BIN,
+ * src/cmf_ctrl_restart_mod.F90:389-482; CMF_RESTART_INIT / READ_REST_BIN, :91-204): NX x NY map
+ * records (FP64 when lrestdbl, else FP32; 1.E20 outside the sequence) rivsto, fldsto, [rivout_pre,
+ * fldout_pre, rivdph_pre, fldsto_pre unless lstoonly], [damsto], [levsto], and <file>.pth with
+ * D1PTHFLW_PRE.  The read zeroes every prognostic first and leaves rivout/fldout/pthflw at zero,
+ * as the reference's binary path does; with lstoonly it sets fldsto_pre = fldsto.  The caller
+ * names the file (the reference uses CRESTDIR//CVNREST//YYYYMMDDHH//'.bin'). */
+int cmf_host_write_restart(const cmf_host_model *hm, const cmf_state_ptrs *st, const char *file, int32_t lrestdbl,
+                           int32_t lstoonly);
+int cmf_host_read_restart(const cmf_host_model *hm, const cmf_state_ptrs *st, const char *file, int32_t lrestdbl,
+                          int32_t lstoonly);
 
 #ifdef __cplusplus
 }

@@ -1291,6 +1291,200 @@ int orc_physics_advance(orc_model *m, int *nt_out, double *dt_out) {
     return orc_substeps(m, dt_min, nt_out, dt_out);
 }
 
+/* ============================================================================ RESTART */
+/* Record I of a direct-access binary restart: one NX x NY map (FP64 when LRESTDBL, else FP32),
+ * cells outside the sequence hold DMIS / RMIS = 1.E20 (src/cmf_ctrl_nmlist_mod.F90:235-236).
+ * vecP2mapP / vecP2mapR, src/cmf_utils_mod.F90:111-154. */
+static int rest_write_map(const orc_model *m, FILE *f, const double *vec, int dbl) {
+    size_t nxy = (size_t)m->nx * m->ny;
+    if (dbl) {
+        double *map = dalloc(nxy);
+        for (size_t k = 0; k < nxy; k++) map[k] = 1.E20;
+        for (int i = 0; i < m->nseqmax; i++) map[(size_t)(m->i1seqy[i] - 1) * m->nx + (m->i1seqx[i] - 1)] = vec[i];
+        size_t w = fwrite(map, sizeof(double), nxy, f);
+        free(map);
+        return w == nxy ? 0 : -1;
+    }
+    float *map = (float *)calloc(nxy, sizeof(float));
+    for (size_t k = 0; k < nxy; k++) map[k] = 1.E20f;
+    for (int i = 0; i < m->nseqmax; i++) map[(size_t)(m->i1seqy[i] - 1) * m->nx + (m->i1seqx[i] - 1)] = (float)vec[i];
+    size_t w = fwrite(map, sizeof(float), nxy, f);
+    free(map);
+    return w == nxy ? 0 : -1;
+}
+
+/* mapP2vecP, src/cmf_utils_mod.F90:328-345 (a FP32 record is promoted once) */
+static int rest_read_map(const orc_model *m, FILE *f, double *vec, int dbl) {
+    size_t nxy = (size_t)m->nx * m->ny;
+    double *map = dalloc(nxy);
+    if (dbl) {
+        if (fread(map, sizeof(double), nxy, f) != nxy) { free(map); return -1; }
+    } else {
+        float *r = (float *)calloc(nxy, sizeof(float));
+        if (fread(r, sizeof(float), nxy, f) != nxy) { free(r); free(map); return -1; }
+        for (size_t k = 0; k < nxy; k++) map[k] = (double)r[k];
+        free(r);
+    }
+    for (int i = 0; i < m->nseqmax; i++) vec[i] = map[(size_t)(m->i1seqy[i] - 1) * m->nx + (m->i1seqx[i] - 1)];
+    free(map);
+    return 0;
+}
+
+/* WRTE_REST_BIN, src/cmf_ctrl_restart_mod.F90:389-482: records rivsto, fldsto, [rivout_pre,
+ * fldout_pre, rivdph_pre, fldsto_pre unless LSTOONLY], [damsto if LDAMOUT], [levsto if LLEVEE];
+ * bifurcation flows in <file>.pth as one (NPTHOUT,NPTHLEV) record.  The caller names the file
+ * (the reference builds CRESTDIR//CVNREST//YYYYMMDDHH//'.bin'). */
+int orc_write_restart(orc_model *m, const char *file, int dbl, int stoonly) {
+    FILE *f = fopen(file, "wb");
+    if (!f) return -1;
+    int rc = rest_write_map(m, f, m->rivsto, dbl) | rest_write_map(m, f, m->fldsto, dbl);
+    if (!stoonly)
+        rc |= rest_write_map(m, f, m->rivout_pre, dbl) | rest_write_map(m, f, m->fldout_pre, dbl) |
+              rest_write_map(m, f, m->rivdph_pre, dbl) | rest_write_map(m, f, m->fldsto_pre, dbl);
+    if (m->ldamout) rc |= rest_write_map(m, f, m->damsto, dbl);
+    if (m->llevee) rc |= rest_write_map(m, f, m->levsto, dbl);
+    fclose(f);
+    if (rc) return -1;
+    if (m->lpthout) {
+        char pth[1100];
+        snprintf(pth, sizeof pth, "%s.pth", file);
+        FILE *g = fopen(pth, "wb");
+        if (!g) return -1;
+        size_t n = (size_t)m->npthout * m->npthlev, w;
+        if (dbl) w = fwrite(m->pthflw_pre, sizeof(double), n, g);
+        else {
+            float *r = (float *)calloc(n ? n : 1, sizeof(float));
+            for (size_t k = 0; k < n; k++) r[k] = (float)m->pthflw_pre[k];
+            w = fwrite(r, sizeof(float), n, g);
+            free(r);
+        }
+        fclose(g);
+        if (w != n) return -1;
+    }
+    return 0;
+}
+
+/* CMF_RESTART_INIT + READ_REST_BIN, src/cmf_ctrl_restart_mod.F90:91-204: prognostics zeroed, the
+ * records read back; D2RIVOUT/D2FLDOUT/D1PTHFLW stay zero (the binary path does not set them);
+ * LSTOONLY: D2FLDSTO_PRE = P2FLDSTO (:130-132) and D1PTHFLW_PRE = 0. */
+int orc_read_restart(orc_model *m, const char *file, int dbl, int stoonly) {
+    int N = m->nseqmax;
+    size_t PL = (size_t)m->npthout * m->npthlev;
+    for (int i = 0; i < N; i++) {
+        m->rivsto[i] = m->fldsto[i] = m->rivout[i] = m->fldout[i] = 0.0;
+        m->rivout_pre[i] = m->fldout_pre[i] = m->rivdph_pre[i] = m->fldsto_pre[i] = 0.0;
+        if (m->ldamout) m->damsto[i] = 0.0;
+        if (m->llevee) m->levsto[i] = 0.0;
+    }
+    if (m->lpthout) for (size_t k = 0; k < PL; k++) m->pthflw[k] = m->pthflw_pre[k] = 0.0;
+    FILE *f = fopen(file, "rb");
+    if (!f) return -1;
+    int rc = rest_read_map(m, f, m->rivsto, dbl) | rest_read_map(m, f, m->fldsto, dbl);
+    if (!stoonly)
+        rc |= rest_read_map(m, f, m->rivout_pre, dbl) | rest_read_map(m, f, m->fldout_pre, dbl) |
+              rest_read_map(m, f, m->rivdph_pre, dbl) | rest_read_map(m, f, m->fldsto_pre, dbl);
+    if (m->ldamout) rc |= rest_read_map(m, f, m->damsto, dbl);
+    if (m->llevee) rc |= rest_read_map(m, f, m->levsto, dbl);
+    fclose(f);
+    if (rc) return -1;
+    if (m->lpthout && !stoonly) {
+        char pth[1100];
+        snprintf(pth, sizeof pth, "%s.pth", file);
+        FILE *g = fopen(pth, "rb");
+        if (!g) return -1;
+        size_t r;
+        if (dbl) r = fread(m->pthflw_pre, sizeof(double), PL, g);
+        else {
+            float *v = (float *)calloc(PL ? PL : 1, sizeof(float));
+            r = fread(v, sizeof(float), PL, g);
+            for (size_t k = 0; k < PL; k++) m->pthflw_pre[k] = (double)v[k];
+            free(v);
+        }
+        fclose(g);
+        if (r != PL) return -1;
+    }
+    if (stoonly) for (int i = 0; i < N; i++) m->fldsto_pre[i] = m->fldsto[i];
+    return 0;
+}
+
+/* CMF_BOUNDARY_UPDATE, src/cmf_ctrl_boundary_mod.F90:267-304: D2DWNELV = D2ELEVTN (+ D2MEANSL)
+ * (+ D2SEALEV); NULL leaves a term out. */
+void orc_update_boundary(orc_model *m, const double *sealev, const double *meansl) {
+    for (int i = 0; i < m->nseqmax; i++) {
+        double v = meansl ? m->elevtn[i] + meansl[i] : m->elevtn[i];
+        if (sealev) v = v + sealev[i];
+        m->dwnelv[i] = v;
+    }
+}
+
+/* CMF_PHYSICS_FLDSTG (stage scheme alone), src/cmf_ctrl_physics_mod.F90:288-305 */
+void orc_physics_fldstg(orc_model *m) { physics_fldstg(m); }
+
+/* CMF_CALC_OUTPRE, src/cmf_opt_outflw_mod.F90:308-421: previous-step discharge by the diffusive
+ * (Manning) wave for a storage-only restart; needs the stage scheme to have run. */
+void orc_calc_outpre(orc_model *m) {
+    int N = m->nseqall, R = m->nseqriv;
+    const double p23 = F(2. / 3.);
+    for (int i = 0; i < N; i++) {
+        m->sfcelv[i] = m->rivelv[i] + m->rivdph[i];
+        m->rivdph_pre[i] = m->rivdph[i];
+    }
+    for (int i = 0; i < R; i++) {
+        int j = m->i1next[i];
+        double dsfcmax = dmax(m->sfcelv[i], m->sfcelv[j]);
+        double dslope = (m->sfcelv[i] - m->sfcelv[j]) * (1.0 / m->nxtdst[i]);
+        double dslope_f = dmax(-0.005, dmin(0.005, dslope));
+        double dflw = dsfcmax - m->rivelv[i];
+        double darea = m->rivwth[i] * dflw;
+        if (darea > F(1.E-5)) {
+            m->rivout_pre[i] = darea * (((1.0 / m->rivman[i]) * opow(dflw, p23)) * sqrt(fabs(dslope)));
+            if (dslope < 0.0) m->rivout_pre[i] = -m->rivout_pre[i];
+        } else m->rivout_pre[i] = 0.0;
+        double dflw_f = dmax(dsfcmax - m->elevtn[i], 0.0);
+        double dare_f = m->fldsto[i] * (1.0 / m->rivlen[i]);
+        dare_f = dmax(dare_f - m->flddph[i] * m->rivwth[i], 0.0);
+        if (dare_f > F(1.E-5)) {
+            m->fldout_pre[i] = dare_f * (((1.0 / m->pmanfld) * opow(dflw_f, p23)) * sqrt(fabs(dslope_f)));
+            if (dslope_f < 0.0) m->fldout_pre[i] = -m->fldout_pre[i];
+        } else m->fldout_pre[i] = 0.0;
+    }
+    for (int i = R; i < N; i++) {
+        double dslope = (m->sfcelv[i] - m->dwnelv[i]) * (1.0 / m->pdstmth);
+        double dslope_f = dmax(-0.005, dmin(0.005, dslope));
+        double dflw = m->rivdph[i];
+        double darea = m->rivwth[i] * dflw;
+        if (darea > F(1.E-5)) {
+            m->rivout_pre[i] = darea * (((1.0 / m->rivman[i]) * opow(dflw, p23)) * sqrt(fabs(dslope)));
+            if (dslope < 0.0) m->rivout_pre[i] = -m->rivout_pre[i];
+        } else m->rivout_pre[i] = 0.0;
+        double dflw_f = dmax(m->sfcelv[i] - m->elevtn[i], 0.0);
+        double dare_f = m->fldsto[i] * (1.0 / m->rivlen[i]);
+        dare_f = dmax(dare_f - m->flddph[i] * m->rivwth[i], 0.0);
+        if (dare_f > F(1.E-5)) {
+            m->fldout_pre[i] = dare_f * (((1.0 / m->pmanfld) * opow(dflw_f, p23)) * sqrt(fabs(dslope_f)));
+            if (dslope_f < 0.0) m->fldout_pre[i] = -m->fldout_pre[i];
+        } else m->fldout_pre[i] = 0.0;
+    }
+    if (m->lpthout) {
+        int P = m->npthout, Lp = m->npthlev;
+        for (int p = 0; p < P; p++) {
+            int u = m->pth_upst[p] - 1, d = m->pth_down[p] - 1;
+            if (u < 0 || d < 0) continue;          /* path outside the domain (not in the reference's loop range) */
+            double dslope = (m->sfcelv[u] - m->sfcelv[d]) * (1.0 / m->pth_dst[p]);
+            for (int l = 0; l < Lp; l++) {
+                double dflw = dmax(m->sfcelv[u], m->sfcelv[d]) - m->pth_elv[(size_t)l * P + p];
+                dflw = dmax(dflw, 0.0);
+                double *o = &m->pthflw_pre[(size_t)l * P + p];
+                if (dflw > F(1.E-5)) {
+                    *o = (m->pth_wth[(size_t)l * P + p] * dflw) * (((1.0 / m->pth_man[l]) * opow(dflw, p23)) * sqrt(fabs(dslope)));
+                    if (dslope < 0.0) *o = -*o;
+                } else *o = 0.0;
+            }
+        }
+    }
+    if (!m->lfldout) for (int i = 0; i < m->nseqmax; i++) m->fldout_pre[i] = 0.0;
+}
+
 /* ============================================================================ public API */
 static void set_defaults(orc_model *m) {
     m->ladpstp = 1; m->lfplain = 1; m->lfldout = 1; m->lpthout = 0; m->ldamout = 0; m->llevee = 0;

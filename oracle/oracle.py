@@ -46,6 +46,11 @@ def _lib(omp: bool = False):
     lib.orc_stage.restype = C.c_double
     lib.orc_stage.argtypes = [C.c_void_p]
     lib.orc_substeps.argtypes = [C.c_void_p, C.c_double, C.POINTER(C.c_int), C.POINTER(C.c_double)]
+    lib.orc_write_restart.argtypes = [C.c_void_p, C.c_char_p, C.c_int, C.c_int]
+    lib.orc_read_restart.argtypes = [C.c_void_p, C.c_char_p, C.c_int, C.c_int]
+    lib.orc_physics_fldstg.argtypes = [C.c_void_p]
+    lib.orc_calc_outpre.argtypes = [C.c_void_p]
+    lib.orc_update_boundary.argtypes = [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double)]
     _LIBS[key] = lib
     return lib
 
@@ -94,6 +99,29 @@ class Oracle:
         dt = C.c_double(0.0)
         self.lib.orc_substeps(self.h, dt_min, C.byref(nt), C.byref(dt))
         return nt.value, dt.value
+
+    def write_restart(self, path: str, dbl: bool = True, stoonly: bool = False) -> None:
+        """WRTE_REST_BIN (src/cmf_ctrl_restart_mod.F90:389-482) to `path` (+ `path`.pth)."""
+        if self.lib.orc_write_restart(self.h, path.encode(), int(dbl), int(stoonly)) != 0:
+            raise OSError(f"oracle: cannot write restart {path}")
+
+    def read_restart(self, path: str, dbl: bool = True, stoonly: bool = False) -> None:
+        """CMF_RESTART_INIT / READ_REST_BIN (src/cmf_ctrl_restart_mod.F90:91-204)."""
+        if self.lib.orc_read_restart(self.h, path.encode(), int(dbl), int(stoonly)) != 0:
+            raise OSError(f"oracle: cannot read restart {path}")
+
+    def physics_fldstg(self) -> None:
+        self.lib.orc_physics_fldstg(self.h)
+
+    def calc_outpre(self) -> None:
+        """CMF_CALC_OUTPRE (src/cmf_opt_outflw_mod.F90:308-421)."""
+        self.lib.orc_calc_outpre(self.h)
+
+    def update_boundary(self, sealev=None, meansl=None) -> None:
+        """CMF_BOUNDARY_UPDATE (src/cmf_ctrl_boundary_mod.F90:267-304)."""
+        keep = [None if a is None else np.ascontiguousarray(a, dtype=np.float64) for a in (sealev, meansl)]
+        ptr = [None if a is None else a.ctypes.data_as(C.POINTER(C.c_double)) for a in keep]
+        self.lib.orc_update_boundary(self.h, ptr[0], ptr[1])
 
     def budget(self) -> dict:
         b = (C.c_double * 15)()
