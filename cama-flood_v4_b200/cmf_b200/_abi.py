@@ -162,6 +162,11 @@ def load(build_if_missing: bool = True):
     lib.cmf_host_read_restart.argtypes = [vp, C.POINTER(StatePtrs), C.c_char_p, C.c_int32, C.c_int32]
     lib.cmf_host_map_to_vec.argtypes = [vp, C.POINTER(C.c_float), f64p]
     lib.cmf_gpu_ctx_calc_outpre.argtypes = [vp]
+    lib.cmf_gpu_ctx_set_runoff_map.argtypes = [vp, C.c_int32, C.c_int32, C.c_int32, C.c_int32, i32p, i32p, f64p, C.c_double]
+    lib.cmf_gpu_ctx_put_runoff_grid.argtypes = [vp, vp, C.c_int32, C.c_int32, C.c_int32]
+    lib.cmf_host_read_inpmat.argtypes = [vp, C.c_char_p, C.c_int32, i32p, i32p, f64p]
+    lib.cmf_host_drofunit.argtypes = [vp]
+    lib.cmf_host_drofunit.restype = C.c_double
     lib.cmf_gpu_ctx_update_boundary.argtypes = [vp, f64p, f64p]
     _lib = lib
     return lib

@@ -46,6 +46,7 @@ class HostModel:
                                      self.i1seqx.ctypes.data_as(_abi.i32p), self.i1seqy.ctypes.data_as(_abi.i32p)),
               "cmf_host_grid")
         self.nx, self.ny = nx.value, ny.value
+        self.drofunit = float(self.lib.cmf_host_drofunit(self.h))
 
     @property
     def nseq(self) -> int:
@@ -123,6 +124,16 @@ class HostModel:
         check(self.lib.cmf_host_read_restart(self.h, C.byref(sp), path.encode(), int(dbl), int(stoonly)),
               "cmf_host_read_restart")
         return st
+
+    def read_inpmat(self, path: str, inpn: int):
+        """CMF_INPMAT_INIT_BIN: (inpx, inpy, inpa) in sequence order, [INPN][NSEQMAX] each."""
+        N = self.dims.nseqmax
+        ix = np.zeros(inpn * N, dtype=np.int32)
+        iy = np.zeros(inpn * N, dtype=np.int32)
+        ia = np.zeros(inpn * N)
+        check(self.lib.cmf_host_read_inpmat(self.h, path.encode(), inpn, ix.ctypes.data_as(_abi.i32p),
+                                            iy.ctypes.data_as(_abi.i32p), ia.ctypes.data_as(_abi.f64p)), "read_inpmat")
+        return ix.reshape(inpn, N), iy.reshape(inpn, N), ia.reshape(inpn, N)
 
     def map_to_vec(self, map2d: np.ndarray) -> np.ndarray:
         """mapR2vecD: float32 NX x NY map (e.g. a sea-level record) -> sequence-order float64."""
@@ -216,6 +227,47 @@ class PhysicsGPU:
         self.set_state(st)
         if stoonly:
             self.calc_outpre()
+
+    def set_runoff_map(self, inpmat=None) -> None:
+        """Device runoff interpolation: inpmat = (nxin, nyin, inpx, inpy, inpa) -> ROFF_INTERP; None ->
+        CONV_RESOL on the map grid."""
+        keep = []
+        if inpmat is None:
+            nxin, nyin, inpn = self.host.nx, self.host.ny, 1
+            ix, iy, ia = self.host.i1seqx, self.host.i1seqy, None
+            lint = 0
+        else:
+            nxin, nyin, ix, iy, ia = inpmat
+            ix = np.ascontiguousarray(ix, dtype=np.int32).ravel()
+            iy = np.ascontiguousarray(iy, dtype=np.int32).ravel()
+            ia = np.ascontiguousarray(ia, dtype=np.float64).ravel()
+            inpn = ix.size // self.N
+            lint = 1
+        keep += [ix, iy, ia]
+        self._rmap = (nxin, nyin)
+        check(self.lib.cmf_gpu_ctx_set_runoff_map(self.h, lint, nxin, nyin, inpn, ix.ctypes.data_as(_abi.i32p),
+                                                  iy.ctypes.data_as(_abi.i32p),
+                                                  None if ia is None else ia.ctypes.data_as(_abi.f64p),
+                                                  float(self.host.drofunit)), "set_runoff_map")
+
+    def put_runoff_grid(self, grid, clean: bool = False) -> None:
+        """Runoff fields [nmembers, NYIN, NXIN] (numpy fp32/fp64 on the host, or a CUDA tensor) ->
+        D2RUNOFF of every member through the device interpolation."""
+        if hasattr(grid, "data_ptr"):
+            import torch
+
+            is_float = grid.dtype == torch.float32
+            torch.cuda.current_stream(grid.device).synchronize()
+            check(self.lib.cmf_gpu_ctx_put_runoff_grid(self.h, C.c_void_p(grid.data_ptr()), int(is_float), 1, int(clean)),
+                  "put_runoff_grid")
+            return
+        a = np.ascontiguousarray(grid)
+        if a.dtype not in (np.float32, np.float64):
+            a = a.astype(np.float64)
+        if a.size != self.M * self._rmap[0] * self._rmap[1]:
+            raise ValueError("runoff grid must hold nmembers * NXIN * NYIN values")
+        check(self.lib.cmf_gpu_ctx_put_runoff_grid(self.h, a.ctypes.data_as(C.c_void_p), int(a.dtype == np.float32), 0,
+                                                   int(clean)), "put_runoff_grid")
 
     def calc_outpre(self) -> None:
         """Stage scheme + CMF_CALC_OUTPRE on the device (storage-only restart)."""

@@ -415,6 +415,52 @@ def _write_namelist(case: Case, outdir: str) -> None:
 DROFUNIT = 86400000.0  # mm/day -> m/s (src/cmf_ctrl_forcing_mod.F90, namelist NFORCE default for mm/day)
 
 
+def make_inpmat(nx: int, ny: int, i1seqx: np.ndarray, i1seqy: np.ndarray, grarea: np.ndarray, factor: int = 2,
+                inpn: int = 3, seed: int = 0):
+    """Synthetic input matrix for runoff on a grid `factor` times coarser than the map: each cell
+    draws from the coarse cell that contains it and from up to inpn - 1 neighbours, with areas that
+    sum to the cell area (mass conserving); unused entries have INPX = 0.  Returns
+    (nxin, nyin, inpx, inpy, inpa) in sequence order, [inpn][NSEQ]."""
+    rng = np.random.default_rng(seed)
+    n = i1seqx.size
+    nxin, nyin = (nx + factor - 1) // factor, (ny + factor - 1) // factor
+    inpx = np.zeros((inpn, n), dtype=np.int32)
+    inpy = np.zeros((inpn, n), dtype=np.int32)
+    inpa = np.zeros((inpn, n), dtype=np.float32)
+    cx, cy = (i1seqx - 1) // factor + 1, (i1seqy - 1) // factor + 1
+    w = rng.dirichlet(np.ones(inpn), size=n).T * (rng.random((inpn, n)) > 0.2)
+    w[0] = np.maximum(w[0], 0.2)
+    offs = [(0, 0), (1, 0), (0, 1), (-1, 0), (0, -1), (1, 1)]
+    xs, ys = [], []
+    for k in range(inpn):
+        dx, dy = offs[k % len(offs)]
+        x, y = cx + dx, cy + dy
+        w[k] = np.where((x >= 1) & (x <= nxin) & (y >= 1) & (y <= nyin), w[k], 0.0)
+        xs.append(x)
+        ys.append(y)
+    w = w / w.sum(axis=0, keepdims=True)
+    for k in range(inpn):
+        x, y = xs[k], ys[k]
+        ok = w[k] > 0
+        inpx[k] = np.where(ok, x, 0)
+        inpy[k] = np.where(ok, y, 0)
+        inpa[k] = np.where(ok, (w[k] * grarea).astype(np.float32), 0.0)
+    return nxin, nyin, inpx, inpy, inpa
+
+
+def write_inpmat(path: str, nx: int, ny: int, i1seqx: np.ndarray, i1seqy: np.ndarray, inpx, inpy, inpa) -> None:
+    """The input-matrix binary read by CMF_INPMAT_INIT_BIN (src/cmf_ctrl_forcing_mod.F90:418-458):
+    3*INPN direct-access records of NX x NY 4-byte values (INPX int32, INPY int32, INPA float32),
+    zero outside the sequence."""
+    inpn = inpx.shape[0]
+    with open(path, "wb") as f:
+        for arr, dt in ((inpx, np.int32), (inpy, np.int32), (inpa, np.float32)):
+            for k in range(inpn):
+                g = np.zeros((ny, nx), dtype=dt)
+                g[i1seqy - 1, i1seqx - 1] = arr[k]
+                f.write(g.tobytes())
+
+
 class DailyGammaRunoff:
     """i.i.d. Gamma(k=0.8, mean 2 mm/day) runoff per land cell per day (float32 mm/day)."""
 

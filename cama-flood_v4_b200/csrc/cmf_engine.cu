@@ -61,6 +61,11 @@ struct cmf_gpu_ctx {
     std::vector<cmf::MemberCtl> hctl;
     // sea-level boundary inputs (allocated on first use)
     double *bnd_sealev = nullptr, *bnd_meansl = nullptr;
+    // runoff interpolation (input matrix or nearest cell) and the staging of runoff fields
+    cmf::RunoffMap rmap{};
+    bool rmap_set = false;
+    void *rgrid = nullptr;
+    size_t rgrid_bytes = 0;
 
     template <class T>
     int alloc(T **p, size_t n) {
@@ -593,6 +598,7 @@ int cmf_gpu_destroy(cmf_gpu_ctx *c) {
     if (c->exec) cudaGraphExecDestroy(c->exec);
     if (c->graph) cudaGraphDestroy(c->graph);
     for (void *p : c->allocs) cudaFree(p);
+    if (c->rgrid) cudaFree(c->rgrid);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
     return CMF_OK;
@@ -950,6 +956,56 @@ int cmf_gpu_ctx_update_boundary(cmf_gpu_ctx *c, const double *sealev, const doub
     CUDA_TRY(cudaGetLastError());
     c->launches += 1;
     CUDA_TRY(cudaStreamSynchronize(c->stream));
+    return CMF_OK;
+}
+
+int cmf_gpu_ctx_set_runoff_map(cmf_gpu_ctx *c, int32_t linterp, int32_t nxin, int32_t nyin, int32_t inpn,
+                               const int32_t *inpx, const int32_t *inpy, const double *inpa, double drofunit) {
+    if (!c) return set_err(CMF_E_STATE, "no context");
+    if (nxin < 1 || nyin < 1 || !inpx || !inpy || !(drofunit > 0.0) || (linterp && (inpn < 1 || !inpa)) ||
+        (!linterp && inpn != 1))
+        return set_err(CMF_E_ARG, "cmf_gpu_ctx_set_runoff_map: bad arguments (CONV_RESOL takes inpn == 1, the cell grid)");
+    CUDA_TRY(cudaSetDevice(c->device));
+    const size_t N = c->dims.nseqall, n = (size_t)inpn * N;
+    for (size_t k = 0; k < n; k++) {
+        if (!linterp && (inpx[k] < 1 || inpx[k] > nxin || inpy[k] < 1 || inpy[k] > nyin))
+            return set_err(CMF_E_ARG, "cmf_gpu_ctx_set_runoff_map: a cell lies outside the runoff grid");
+    }
+    int rc;
+    const int32_t *dx, *dy;
+    const double *da = nullptr;
+    if ((rc = c->upload_raw(&dx, inpx, n)) || (rc = c->upload_raw(&dy, inpy, n))) return rc;
+    if (linterp && (rc = c->upload_raw(&da, inpa, n))) return rc;
+    c->rmap = cmf::RunoffMap{linterp ? 1 : 0, nxin, nyin, inpn, 0, dx, dy, da, drofunit};
+    c->rmap_set = true;
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    return CMF_OK;
+}
+
+int cmf_gpu_ctx_put_runoff_grid(cmf_gpu_ctx *c, const void *grid, int32_t is_float, int32_t on_device, int32_t clean) {
+    if (!c) return set_err(CMF_E_STATE, "no context");
+    if (!c->rmap_set) return set_err(CMF_E_STATE, "cmf_gpu_ctx_put_runoff_grid: no runoff map (cmf_gpu_ctx_set_runoff_map)");
+    if (!grid) return set_err(CMF_E_ARG, "null runoff field");
+    CUDA_TRY(cudaSetDevice(c->device));
+    const size_t bytes = (size_t)c->dims.nmembers * c->rmap.nxin * c->rmap.nyin * (is_float ? 4 : 8);
+    const void *src = grid;
+    if (!on_device) {
+        if (c->rgrid_bytes < bytes) {
+            if (c->rgrid) { cudaStreamSynchronize(c->stream); cudaFree(c->rgrid); c->rgrid = nullptr; c->rgrid_bytes = 0; }
+            CUDA_TRY(cudaMalloc(&c->rgrid, bytes));
+            c->rgrid_bytes = bytes;
+        }
+        CUDA_TRY(cudaMemcpyAsync(c->rgrid, grid, bytes, cudaMemcpyHostToDevice, c->stream));
+        src = c->rgrid;
+    }
+    cmf::RunoffMap r = c->rmap;
+    r.clean = clean ? 1 : 0;
+    const dim3 g((unsigned)((c->dims.nseqall + 255) / 256), c->dims.nmembers);
+    cmf::k_runoff_map<<<g, 256, 0, c->stream>>>(c->net, c->st, r, is_float ? nullptr : (const double *)src,
+                                                 is_float ? (const float *)src : nullptr);
+    CUDA_TRY(cudaGetLastError());
+    c->launches += 1;
+    if (!on_device) CUDA_TRY(cudaStreamSynchronize(c->stream));   // the host buffer may be reused on return
     return CMF_OK;
 }
 

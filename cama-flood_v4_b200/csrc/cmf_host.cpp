@@ -725,6 +725,34 @@ int cmf_host_read_restart(const cmf_host_model *hm, const cmf_state_ptrs *st, co
     return CMF_OK;
 }
 
+int cmf_host_read_inpmat(const cmf_host_model *hm, const char *file, int32_t inpn, int32_t *inpx, int32_t *inpy,
+                         double *inpa) {
+    if (!hm || !file || inpn < 1 || !inpx || !inpy || !inpa) return CMF_E_ARG;
+    FILE *f = std::fopen(file, "rb");
+    if (!f) return CMF_E_IO;
+    const size_t nxy = static_cast<size_t>(hm->nx) * hm->ny, N = static_cast<size_t>(hm->nseqmax);
+    std::vector<int32_t> ib(nxy);
+    std::vector<float> rb(nxy);
+    int rc = CMF_OK;
+    // records 1..INPN: INPX, INPN+1..2*INPN: INPY, 2*INPN+1..3*INPN: INPA (direct access, RECL = 4*NX*NY)
+    for (int part = 0; part < 3 && !rc; part++) {
+        for (int k = 0; k < inpn && !rc; k++) {
+            const size_t got = part < 2 ? std::fread(ib.data(), 4, nxy, f) : std::fread(rb.data(), 4, nxy, f);
+            if (got != nxy) { rc = CMF_E_IO; break; }
+            for (size_t i = 0; i < N; i++) {
+                const size_t gi = hm->g(hm->i1seqx[i], hm->i1seqy[i]);
+                if (part == 0) inpx[k * N + i] = ib[gi];                            // mapI2vecI
+                else if (part == 1) inpy[k * N + i] = ib[gi];
+                else inpa[k * N + i] = static_cast<double>(rb[gi]);              // mapR2vecD
+            }
+        }
+    }
+    std::fclose(f);
+    return rc;
+}
+
+double cmf_host_drofunit(const cmf_host_model *hm) { return hm ? hm->nl.drofunit : 0.0; }
+
 int cmf_host_map_to_vec(const cmf_host_model *hm, const float *map, double *vec) {
     if (!hm || !map || !vec) return CMF_E_ARG;
     for (int i = 0; i < hm->nseqmax; i++) vec[i] = static_cast<double>(map[hm->g(hm->i1seqx[i], hm->i1seqy[i])]);

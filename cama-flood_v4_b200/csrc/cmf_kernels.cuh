@@ -964,6 +964,52 @@ __global__ void k_outpre(Net n, State s, int ncell_blocks) {
     }
 }
 
+// ------------------------------------------------------------------------------------------
+// k_runoff_map: CMF_FORCING_PUT on the device (src/cmf_ctrl_forcing_mod.F90:716-831) for every
+// member: the runoff field PBUFF(NXIN,NYIN) of member m is grid[m][NYIN][NXIN] (fp64, or fp32
+// promoted exactly).  linterp: ROFF_INTERP over the input matrix (inpx/inpy/inpa [INPN][N]);
+// else CONV_RESOL at (inpx, inpy) = (I1SEQX, I1SEQY) with the cell area.  clean applies
+// CMF_FORCING_GET's NaN -> RMIS and max(., 0) (:486-494) to every value read.
+// ------------------------------------------------------------------------------------------
+struct RunoffMap {
+    int linterp, nxin, nyin, inpn, clean;
+    const int *__restrict__ inpx, *__restrict__ inpy;
+    const double *__restrict__ inpa;
+    double drofunit;
+};
+
+__global__ void k_runoff_map(Net n, State s, RunoffMap r, const double *__restrict__ gridd, const float *__restrict__ gridf) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n.N) return;
+    const int m = blockIdx.y;
+    const size_t g0 = (size_t)m * r.nxin * r.nyin;
+    const double rmis = CMF_F(1.E20);
+    auto val = [&](int ix, int iy) -> double {
+        const size_t k = g0 + (size_t)(iy - 1) * r.nxin + (ix - 1);
+        double v = gridd ? gridd[k] : (double)gridf[k];
+        if (r.clean) {
+            if (isnan(v)) v = rmis;
+            v = dmax(v, 0.0);
+        }
+        return v;
+    };
+    double out = 0.0;
+    if (r.linterp) {
+        for (int k = 0; k < r.inpn; k++) {
+            const int ix = r.inpx[(size_t)k * n.N + i], iy = r.inpy[(size_t)k * n.N + i];
+            if (ix > 0) {
+                if (ix > r.nxin || iy > r.nyin || iy < 1) continue;   // the reference logs and skips
+                const double v = val(ix, iy);
+                if (v != rmis) out = out + (v * r.inpa[(size_t)k * n.N + i]) / r.drofunit;
+            }
+        }
+    } else {
+        const double v = val(r.inpx[i], r.inpy[i]);
+        if (v != rmis) out = dmax((v * n.grarea[i]) / r.drofunit, 0.0);
+    }
+    s.runoff[(size_t)m * n.N + i] = out;
+}
+
 // k_boundary: CMF_BOUNDARY_UPDATE (src/cmf_ctrl_boundary_mod.F90:267-304): downstream boundary
 // elevation D2DWNELV = D2ELEVTN (+ D2MEANSL) (+ D2SEALEV); only the mouths read it.
 __global__ void k_boundary(int N, const double *__restrict__ elevtn, const double *__restrict__ meansl,

@@ -198,6 +198,21 @@ int cmf_gpu_ctx_calc_outpre(cmf_gpu_ctx *ctx);
  * (sealev from CMF_BOUNDARY_GET_BIN's map via cmf_host_map_to_vec).  Synchronous. */
 int cmf_gpu_ctx_update_boundary(cmf_gpu_ctx *ctx, const double *sealev, const double *meansl);
 
+/* Runoff interpolation on the device, CMF_FORCING_PUT (src/cmf_ctrl_forcing_mod.F90:716-831).
+ * cmf_gpu_ctx_set_runoff_map uploads the mapping once: linterp != 0 -> ROFF_INTERP with the input
+ * matrix INPX/INPY/INPA(NSEQMAX,INPN) (column-major, i.e. [INPN][NSEQALL]; read from CINPMAT by
+ * cmf_host_read_inpmat), runoff grid NXIN x NYIN; linterp == 0 -> CONV_RESOL with inpn == 1 and
+ * inpx/inpy = I1SEQX/I1SEQY (grid == map, area D2GRAREA).  cmf_gpu_ctx_put_runoff_grid then turns
+ * one runoff field per member, PBUFF(NXIN,NYIN) [mm/dt] laid out [nmembers][NYIN][NXIN] as fp64
+ * (is_float == 0) or fp32 (promoted exactly), into D2RUNOFF [m3/s] of every member.  on_device:
+ * grid is a device pointer (enqueued on the context's stream, asynchronous); else host memory
+ * (copied, synchronous).  clean != 0 first applies CMF_FORCING_GET's NaN -> RMIS and max(., 0)
+ * (:486-494). */
+int cmf_gpu_ctx_set_runoff_map(cmf_gpu_ctx *ctx, int32_t linterp, int32_t nxin, int32_t nyin, int32_t inpn,
+                               const int32_t *inpx, const int32_t *inpy, const double *inpa, double drofunit);
+int cmf_gpu_ctx_put_runoff_grid(cmf_gpu_ctx *ctx, const void *grid, int32_t is_float, int32_t on_device,
+                                int32_t clean);
+
 /* Batch of contexts on one device -- regional domains of uneven size, each with its own members --
  * advanced by ONE graph launch per coupling step.  Each context's outer step (prologue + WHILE
  * sub-step loop) is an independent branch of the batch graph, so every domain and member keeps its
@@ -337,6 +352,13 @@ int cmf_host_state(cmf_host_model *hm, cmf_state_ptrs *st);
 int cmf_host_conv_resol(const cmf_host_model *hm, const double *map, double *runoff_out);
 /* Grid position of every sequence cell (I1SEQX/I1SEQY, 1-based) and the grid size. */
 int cmf_host_grid(const cmf_host_model *hm, int32_t *nx, int32_t *ny, int32_t *i1seqx, int32_t *i1seqy);
+/* CMF_INPMAT_INIT_BIN (src/cmf_ctrl_forcing_mod.F90:418-458): reads the input-matrix file (3*INPN
+ * records of NX x NY 4-byte values: INPX int32 x INPN, INPY int32 x INPN, INPA float32 x INPN) into
+ * sequence order, [INPN][NSEQMAX] each (INPA promoted to double). */
+int cmf_host_read_inpmat(const cmf_host_model *hm, const char *file, int32_t inpn, int32_t *inpx, int32_t *inpy,
+                         double *inpa);
+/* DROFUNIT of the namelist NFORCE (runoff unit divisor, src/cmf_ctrl_forcing_mod.F90:59). */
+double cmf_host_drofunit(const cmf_host_model *hm);
 /* mapR2vecD (src/cmf_utils_mod.F90:282-303): an NX x NY float map (e.g. a sea-level record of
  * CMF_BOUNDARY_GET_BIN) to a double vector in sequence order. */
 int cmf_host_map_to_vec(const cmf_host_model *hm, const float *map, double *vec);

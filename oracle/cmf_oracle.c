@@ -1554,6 +1554,37 @@ int orc_put_runoff_map(orc_model *m, const double *map) {
     }
     return 0;
 }
+/* CMF_FORCING_GET's cleaning of a runoff field (src/cmf_ctrl_forcing_mod.F90:486-494): NaN -> RMIS,
+ * then max(., 0). */
+void orc_forcing_clean(double *grid, size_t n) {
+    for (size_t k = 0; k < n; k++) {
+        if (isnan(grid[k])) grid[k] = F(1.E20);
+        grid[k] = dmax(grid[k], 0.0);
+    }
+}
+
+/* ROFF_INTERP, src/cmf_ctrl_forcing_mod.F90:760-790: D2RUNOFF(ISEQ) = sum over the input-matrix
+ * entries with IXIN > 0 (inside NXIN x NYIN) of PBUFFIN(IXIN,IYIN) * INPA / DROFUNIT, skipping
+ * RMIS inputs.  inpx/inpy/inpa are [INPN][NSEQMAX] (INPX(NSEQMAX,INPN) column-major); grid is
+ * PBUFFIN(NXIN,NYIN). */
+int orc_roff_interp(orc_model *m, const double *grid, int nxin, int nyin, int inpn, const int *inpx, const int *inpy,
+                    const double *inpa) {
+    int N = m->nseqmax;
+    for (int i = 0; i < N; i++) {
+        double out = 0.0;
+        for (int k = 0; k < inpn; k++) {
+            int ix = inpx[(size_t)k * N + i], iy = inpy[(size_t)k * N + i];
+            if (ix > 0) {
+                if (ix > nxin || iy > nyin || iy < 1) continue;
+                double v = grid[(size_t)(iy - 1) * nxin + (ix - 1)];
+                if (v != F(1.E20)) out = out + (v * inpa[(size_t)k * N + i]) / m->drofunit;
+            }
+        }
+        m->runoff[i] = out;
+    }
+    return 0;
+}
+
 int orc_put_runoff_vec(orc_model *m, const double *vec) {
     memcpy(m->runoff, vec, sizeof(double) * (size_t)m->nseqmax);
     return 0;

@@ -50,6 +50,9 @@ def _lib(omp: bool = False):
     lib.orc_read_restart.argtypes = [C.c_void_p, C.c_char_p, C.c_int, C.c_int]
     lib.orc_physics_fldstg.argtypes = [C.c_void_p]
     lib.orc_calc_outpre.argtypes = [C.c_void_p]
+    lib.orc_forcing_clean.argtypes = [C.POINTER(C.c_double), C.c_size_t]
+    lib.orc_roff_interp.argtypes = [C.c_void_p, C.POINTER(C.c_double), C.c_int, C.c_int, C.c_int, C.POINTER(C.c_int),
+                                    C.POINTER(C.c_int), C.POINTER(C.c_double)]
     lib.orc_update_boundary.argtypes = [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double)]
     _LIBS[key] = lib
     return lib
@@ -116,6 +119,25 @@ class Oracle:
     def calc_outpre(self) -> None:
         """CMF_CALC_OUTPRE (src/cmf_opt_outflw_mod.F90:308-421)."""
         self.lib.orc_calc_outpre(self.h)
+
+    def put_runoff_grid(self, grid, inpmat=None, clean: bool = False) -> None:
+        """CMF_FORCING_PUT (src/cmf_ctrl_forcing_mod.F90:716-831) of one runoff field PBUFF(NXIN,NYIN)
+        given as [NYIN, NXIN]: ROFF_INTERP with inpmat = (nxin, nyin, inpx, inpy, inpa) ([INPN][N]
+        arrays), else CONV_RESOL.  clean applies CMF_FORCING_GET's NaN/negative cleaning first."""
+        g = np.array(grid, dtype=np.float64, order="C").ravel()
+        if clean:
+            self.lib.orc_forcing_clean(g.ctypes.data_as(C.POINTER(C.c_double)), g.size)
+        if inpmat is None:
+            self.put_runoff_map(g)
+            return
+        nxin, nyin, ix, iy, a = inpmat
+        ix = np.ascontiguousarray(ix, dtype=np.int32)
+        iy = np.ascontiguousarray(iy, dtype=np.int32)
+        a = np.ascontiguousarray(a, dtype=np.float64)
+        inpn = ix.size // self.nseqall
+        self.lib.orc_roff_interp(self.h, g.ctypes.data_as(C.POINTER(C.c_double)), nxin, nyin, inpn,
+                                 ix.ctypes.data_as(C.POINTER(C.c_int)), iy.ctypes.data_as(C.POINTER(C.c_int)),
+                                 a.ctypes.data_as(C.POINTER(C.c_double)))
 
     def update_boundary(self, sealev=None, meansl=None) -> None:
         """CMF_BOUNDARY_UPDATE (src/cmf_ctrl_boundary_mod.F90:267-304)."""
