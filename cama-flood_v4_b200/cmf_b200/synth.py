@@ -520,3 +520,17 @@ def spec_config1(seed: int = 1, scale: float = 1.0) -> CaseSpec:
                     npthout=max(4, int(round(12000 * scale * scale))), npthlev=5,
                     llevee=True, levee_frac=0.10, ldamout=True,
                     ndam=max(2, int(round(2000 * scale * scale))), dt=3600.0, ifrq_inp=1)
+
+
+def spec_config2(n_domains: int = 8, n_min: int = 50_000, n_max: int = 2_000_000, seed: int = 11) -> list:
+    """Regional domains of uneven size for the batched ensemble: `n_domains` networks with cell
+    counts log-spaced from n_min to n_max, each generated with the config-1 laws (bifurcation
+    channels, levees and dams in proportion to the cell count)."""
+    sizes = np.geomspace(n_min, n_max, n_domains)
+    specs = []
+    for d, n in enumerate(sizes):
+        sp = spec_config1(seed=seed + d, scale=float(np.sqrt(n / 300000.0)))
+        sp.name = f"cfg2_d{d}"
+        specs.append(sp)
+    return specs
+

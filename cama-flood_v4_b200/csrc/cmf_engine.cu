@@ -340,7 +340,7 @@ void enqueue_substep(cmf_gpu_ctx *c, int use_cond, cudaGraphConditionalHandle co
     const dim3 gcp(c->ncell_blocks + c->npath_blocks, c->dims.nmembers);
     cmf::k_flux<<<gcp, c->block, 0, c->stream>>>(c->net, c->st, c->ncell_blocks);
     cmf::k_rate<<<gc, c->block, 0, c->stream>>>(c->net, c->st);
-    cmf::k_store<<<gcp, c->block, 0, c->stream>>>(c->net, c->st, c->ncell_blocks);
+    cmf::k_store<<<gcp, c->block, cmf::store_smem(c->block), c->stream>>>(c->net, c->st, c->ncell_blocks);
     cmf::k_ctl<<<1, 32 * cmf::kBudgets, 0, c->stream>>>(c->net, c->st, c->ncell_blocks, cond, use_cond);
 }
 void enqueue_substep(cmf_gpu_ctx *c, int use_cond) { enqueue_substep(c, use_cond, c->cond); }
@@ -431,7 +431,7 @@ int read_ctl(cmf_gpu_ctx *c) {
 
 int autotune(cmf_gpu_ctx *c) {
     // times one sub-step (phases A, B, C) of the zero state for each candidate block size
-    const int cands[] = {128, 256, 512};
+    const int cands[] = {128, 256};   // the cell kernels are built for at most cmf::kCellThreads
     std::vector<cmf::MemberCtl> probe(c->dims.nmembers);
     for (auto &m : probe) { m = cmf::MemberCtl{}; m.dt_def = 3600.0; m.dt = 600.0; m.nt = 1; m.it = 0; }
     CUDA_TRY(cudaMemcpyAsync(c->st.ctl, probe.data(), probe.size() * sizeof(cmf::MemberCtl), cudaMemcpyHostToDevice, c->stream));
@@ -448,7 +448,7 @@ int autotune(cmf_gpu_ctx *c) {
             CUDA_TRY(cudaEventRecord(e0, c->stream));
             cmf::k_flux<<<gcp, b, 0, c->stream>>>(c->net, c->st, c->ncell_blocks);
             cmf::k_rate<<<gc, b, 0, c->stream>>>(c->net, c->st);
-            cmf::k_store<<<gcp, b, 0, c->stream>>>(c->net, c->st, c->ncell_blocks);
+            cmf::k_store<<<gcp, b, cmf::store_smem(b), c->stream>>>(c->net, c->st, c->ncell_blocks);
             CUDA_TRY(cudaEventRecord(e1, c->stream));
             CUDA_TRY(cudaEventSynchronize(e1));
             float ms = 0.f;
@@ -576,8 +576,8 @@ int cmf_gpu_create(const cmf_dims *dims, const cmf_params *params, const cmf_map
     if ((rc = build_net(c, maps))) return fail(rc);
     if ((rc = alloc_state(c))) return fail(rc);
     if (opts->block_size > 0) {
-        if (opts->block_size % 32 || opts->block_size > 1024 || opts->block_size < 64)
-            return fail(set_err(CMF_E_ARG, "block_size must be a multiple of 32 in [64, 1024]"));
+        if (opts->block_size % 32 || opts->block_size > cmf::kCellThreads || opts->block_size < 64)
+            return fail(set_err(CMF_E_ARG, "block_size must be a multiple of 32 in [64, 256]"));
         set_blocks(c, opts->block_size);
     } else if ((rc = autotune(c))) {
         return fail(rc);
@@ -668,7 +668,7 @@ int cmf_gpu_ctx_time_phases(cmf_gpu_ctx *c, double dt_def, int32_t reps, double 
         CUDA_TRY(cudaEventRecord(ev[3], c->stream));
         cmf::k_rate<<<gc, c->block, 0, c->stream>>>(c->net, c->st);
         CUDA_TRY(cudaEventRecord(ev[4], c->stream));
-        cmf::k_store<<<gcp, c->block, 0, c->stream>>>(c->net, c->st, c->ncell_blocks);
+        cmf::k_store<<<gcp, c->block, cmf::store_smem(c->block), c->stream>>>(c->net, c->st, c->ncell_blocks);
         CUDA_TRY(cudaEventRecord(ev[5], c->stream));
         cmf::k_ctl<<<1, 32 * cmf::kBudgets, 0, c->stream>>>(c->net, c->st, c->ncell_blocks, c->cond, 0);
         CUDA_TRY(cudaEventRecord(ev[6], c->stream));

@@ -26,7 +26,23 @@
 
 namespace cmf {
 
+// Occupancy of the latency-bound cell kernels: at most kCellThreads threads per block and the
+// minimum resident blocks per SM (caps registers at 65536 / (threads x blocks)); measured on
+// 16 config-1 members, more resident warps beat the few spills this costs.
+#ifndef CMF_FLUX_MINB
+#define CMF_FLUX_MINB 6
+#endif
+#ifndef CMF_STORE_MINB
+#define CMF_STORE_MINB 5
+#endif
+#ifndef CMF_STAGE_MINB
+#define CMF_STAGE_MINB 6
+#endif
+constexpr int kCellThreads = 256;
+
 constexpr int kBudgets = 12;       // stopre stonxt stonew rivinf rivout stopre2 stonew2 rivsto fldsto fldare levsto dammiss
+// dynamic shared memory of k_store: the last sub-step's budget terms, kBudgets per thread
+inline size_t store_smem(int block) { return (size_t)kBudgets * block * sizeof(double); }
 constexpr int kNtCap = 10000;      // bound of the device-side sub-step loop
 
 struct MemberCtl {
@@ -324,7 +340,7 @@ __device__ __forceinline__ void block_sum(double (&v)[NV], double *smem /* [32*N
 // ------------------------------------------------------------------------------------------
 // k_stage: stage scheme at the top of CMF_PHYSICS_ADVANCE + CALC_ADPSTP minimum
 // ------------------------------------------------------------------------------------------
-__global__ void k_stage(Net n, State s) {
+__global__ void __launch_bounds__(kCellThreads, CMF_STAGE_MINB) k_stage(Net n, State s) {
     const int m = blockIdx.y;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     double key = 1.0e308;
@@ -656,7 +672,7 @@ __device__ __forceinline__ void path_outflow(const Net &n, const State &s, int m
     s.pthsum_raw[(size_t)m * P + p] = sum;
 }
 
-__global__ void k_flux(Net n, State s, int ncell_blocks) {
+__global__ void __launch_bounds__(kCellThreads, CMF_FLUX_MINB) k_flux(Net n, State s, int ncell_blocks) {
     const int m = blockIdx.y;
     const MemberCtl &c = s.ctl[m];
     if (c.it >= c.nt) return;
@@ -706,7 +722,7 @@ __device__ __forceinline__ double scaled_pathsum(const Net &n, const double *sum
     return v >= 0.0 ? v * rate_m[n.pth_up[p]] : v * rate_m[n.pth_dn[p]];
 }
 
-__global__ void k_store(Net n, State s, int ncell_blocks) {
+__global__ void __launch_bounds__(kCellThreads, CMF_STORE_MINB) k_store(Net n, State s, int ncell_blocks) {
     const int m = blockIdx.y;
     const MemberCtl &c = s.ctl[m];
     const bool active = c.it < c.nt;
@@ -741,9 +757,15 @@ __global__ void k_store(Net n, State s, int ncell_blocks) {
         return;
     }
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    double b[kBudgets];
+    // budget terms of the last sub-step go to shared memory where they are computed (dynamic
+    // shared memory, kBudgets x blockDim doubles), so they hold no registers across the stage scheme
+    extern __shared__ double sbud[];
+    double *bt = sbud + threadIdx.x;
+    const int bstride = blockDim.x;
+    auto bput = [&](int k, double v) { if (last) bt[k * bstride] = v; };
+    if (last && i >= n.N)
 #pragma unroll
-    for (int k = 0; k < kBudgets; k++) b[k] = 0.0;
+        for (int k = 0; k < kBudgets; k++) bt[k * bstride] = 0.0;
     if (i < n.N) {
         const size_t gi = base + i;
         const double *rate_m = s.rate + base;
@@ -775,6 +797,7 @@ __global__ void k_store(Net n, State s, int ncell_blocks) {
         }
         const double runoff = s.runoff[gi];
         // CMF_DAMOUT_WATBAL, src/cmf_ctrl_damout_mod.F90:516-535
+        double dmiss = 0.0;
         if (n.ldamout) {
             const int d = n.dam_id[i];
             if (d >= 0) {
@@ -783,9 +806,10 @@ __global__ void k_store(Net n, State s, int ncell_blocks) {
                 const double s0 = s.damsto[gi];
                 const double s1 = (s0 + inflow * DT) - outflw * DT;
                 s.damsto[gi] = s1;
-                b[11] = ((s0 - s1) + inflow * DT) - outflw * DT;
+                dmiss = ((s0 - s1) + inflow * DT) - outflw * DT;
             }
         }
+        bput(11, dmiss);
         // CALC_VARS_PRE, src/cmf_ctrl_physics_mod.F90:254-277
         const double rivsto0 = s.rivsto[gi], fldsto0 = s.fldsto[gi];
         s.rivout_pre[gi] = rout;
@@ -793,30 +817,30 @@ __global__ void k_store(Net n, State s, int ncell_blocks) {
         s.rivdph_pre[gi] = s.rivdph[gi];
         s.fldsto_pre[gi] = fldsto0;
         // CMF_CALC_STONXT, src/cmf_calc_stonxt_mod.F90:53-100
-        b[0] = rivsto0 + fldsto0;
-        b[3] = rinf * DT + finf * DT;
-        b[4] = (rout * DT + fout * DT) + pout * DT;
+        bput(0, rivsto0 + fldsto0);
+        bput(3, rinf * DT + finf * DT);
+        bput(4, (rout * DT + fout * DT) + pout * DT);
         double rs = (rivsto0 + rinf * DT) - rout * DT;
         double fs = fldsto0;
         if (rs < 0.0) { fs = fs + rs; rs = 0.0; }
         fs = ((fs + finf * DT) - fout * DT) - pout * DT;
         if (fs < 0.0) { rs = dmax(rs + fs, 0.0); fs = 0.0; }
-        b[1] = rs + fs;
+        bput(1, rs + fs);
         const double outflw = rout + fout;
         const double frc = s.fldfrc[gi];
         rs = rs + (runoff * (1.0 - frc)) * DT;       // D2GDWRTN is zero without groundwater delay
         fs = fs + (runoff * frc) * DT;
         double levsto = n.llevee ? s.levsto[gi] : 0.0;
-        b[2] = n.llevee ? (rs + fs) + levsto : rs + fs;
+        bput(2, n.llevee ? (rs + fs) + levsto : rs + fs);
         // stage scheme, :125
         const StageOut o = n.llevee ? stage_levee(n, i, rs, fs, levsto) : stage_def(n, i, rs, fs);
         store_stage(n, s, gi, i, o);
-        b[5] = n.llevee ? (rs + fs) + levsto : rs + fs;
-        b[6] = n.llevee ? (o.rivsto + o.fldsto) + o.levsto : o.rivsto + o.fldsto;
-        b[7] = o.rivsto;
-        b[8] = o.fldsto;
-        b[9] = o.fldare;
-        b[10] = o.levsto;
+        bput(5, n.llevee ? (rs + fs) + levsto : rs + fs);
+        bput(6, n.llevee ? (o.rivsto + o.fldsto) + o.levsto : o.rivsto + o.fldsto);
+        bput(7, o.rivsto);
+        bput(8, o.fldsto);
+        bput(9, o.fldare);
+        bput(10, o.levsto);
         s.rivinf[gi] = rinf;
         s.fldinf[gi] = finf;
         s.pthout[gi] = pout;
@@ -846,6 +870,10 @@ __global__ void k_store(Net n, State s, int ncell_blocks) {
     // fixed-shape tree -> deterministic; layout [m][k][block] for a coalesced final reduction
     if (last) {
         __shared__ double red[32 * kBudgets];
+        __syncthreads();
+        double b[kBudgets];
+#pragma unroll
+        for (int k = 0; k < kBudgets; k++) b[k] = bt[k * bstride];
         block_sum<kBudgets>(b, red);
         if (threadIdx.x == 0) {
             double *dst = s.partials + (size_t)m * kBudgets * ncell_blocks + blockIdx.x;

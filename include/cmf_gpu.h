@@ -79,7 +79,7 @@ typedef struct cmf_opts {
     int32_t launch_mode; /* 0: one CUDA graph per coupling step with a device-side sub-step loop;
                             1: host-driven launches (reads NT back before the sub-steps)          */
     int32_t device;      /* CUDA device ordinal                                                   */
-    int32_t block_size;  /* 0: autotune; else threads per block for the cell kernels             */
+    int32_t block_size;  /* 0: autotune; else threads per block for the cell kernels (64..256)   */
 } cmf_opts;
 
 /* ---- static maps: Fortran module arrays (read-only, host memory) ------------------------- */
