@@ -151,22 +151,24 @@ def profiled_traffic(kernel: str):
 # ----------------------------------------------------------------------------- algorithmic bytes
 def phase_bytes(N: int, E: int, L_bar: float, P: int, Lp: int, nlev: int, ndam: int, ldiag: bool) -> dict:
     """Compulsory HBM bytes per launch of each sub-step kernel (every array element the kernel must
-    read or write once; gathers of neighbour values are L2 reuse and not counted again).
+    read or write once every sub-step; gathers of neighbour values are L2 reuse and not counted
+    again; outputs written on the last sub-step only -- D2RIVVEL, D2RIVINF, D2FLDINF, D2PTHOUT,
+    D2OUTFLW, D2FLDARE, D2SFCELV and the runoff average -- are not counted).
       k_flux : static 7x8 (RIVELV ELEVTN NXTDST RIVWTH RIVHGT RIVLEN RIVMAN) + I1NEXT 4 + state reads
                8x8 (RIVDPH RIVDPH_PRE RIVOUT_PRE FLDOUT_PRE FLDSTO FLDDPH FLDSTO_PRE STORGE)
-               + writes 3x8 (RIVOUT FLDOUT RIVVEL)                                  = 148 B/cell
+               + writes 2x8 (RIVOUT FLDOUT) + velocity average r/w 16 (diagnostics) = 140 (+16) B/cell
                + per path: endpoints 8, DST 8, skip 4, ELV/WTH/FLW_PRE/FLW 32 x Lp, FLWSUM 8
       k_rate : RIVOUT FLDOUT 16 + CSR 4 + 4/edge + RIVSTO FLDSTO 16 + RATE 8        = 48 B/cell
                + path CSR 8 and FLWSUM 8 per path end
       k_store: RIVOUT FLDOUT RATE 24 + CSR 8 + I1NEXT 4 + RIVSTO FLDSTO RIVDPH FLDFRC RUNOFF 40
-               + RIVSTOMAX RIVLEN RIVWTH GRAREA RIVELV 40 + layers 16 L_bar + writes 12x8 96
-               (_PRE x4, RIVSTO FLDSTO RIVDPH FLDDPH FLDFRC FLDARE SFCELV STORGE) + RIVINF FLDINF
-               PTHOUT OUTFLW 32 + diagnostics 9 accumulators r/w + RIVVEL read 152   = 244+16 L_bar (+152)
+               + RIVSTOMAX RIVLEN RIVWTH GRAREA 32 + layers 16 L_bar + writes 10x8 80 (_PRE x4,
+               RIVSTO FLDSTO RIVDPH FLDDPH FLDFRC STORGE) + diagnostics 7 accumulators r/w 112
+                                                                             = 188+16 L_bar (+112)
                + levee: index 4/cell + 7 params + LEVSTO r/w + LEVDPH w per levee cell
                + dams: 112 B per dam, paths: FLW r/w 16 x Lp + FLWSUM 16 per path"""
-    flux = N * 148 + P * (8 + 8 + 4 + 32 * Lp + 8) + ndam * 112
+    flux = N * (140 + (16 if ldiag else 0)) + P * (8 + 8 + 4 + 32 * Lp + 8) + ndam * 112
     rate = N * 48 + (E - N) * 4 + P * 2 * (8 + 8)
-    store = N * (244 + 16 * L_bar + (152 if ldiag else 0)) + N * 4 + nlev * (7 * 8 + 16 + 8) + ndam * 112 + P * (16 * Lp + 16)
+    store = N * (188 + 16 * L_bar + (112 if ldiag else 0)) + N * 4 + nlev * (7 * 8 + 16 + 8) + ndam * 112 + P * (16 * Lp + 16)
     return {"k_flux": flux, "k_rate": rate, "k_store": store}
 
 

@@ -648,40 +648,68 @@ int cmf_gpu_ctx_counters(cmf_gpu_ctx *c, int64_t *member_substeps, int64_t *loop
 }
 
 int cmf_gpu_ctx_time_phases(cmf_gpu_ctx *c, double dt_def, int32_t reps, double *ms_out) {
-    // Runs `reps` one-sub-step outer steps kernel by kernel with CUDA events between the kernels
-    // on the context's stream; ms_out[0..5] = mean ms of k_stage, k_ntdt, k_flux, k_rate, k_store, k_ctl.
+    // Runs `reps` outer steps kernel by kernel (the host-driven schedule) with CUDA events between
+    // the kernels on the context's stream, so every sub-step of the step is timed -- first, middle
+    // and last alike.  ms_out[0..5] = mean ms per launch of k_stage, k_ntdt (per outer step) and of
+    // k_flux, k_rate, k_store, k_ctl (per sub-step).  Advances the state like `reps` outer steps.
     if (!c || reps <= 0 || !ms_out) return set_err(CMF_E_ARG, "bad argument");
     CUDA_TRY(cudaSetDevice(c->device));
     int rc;
     if ((rc = sync_dt_def(c, dt_def))) return rc;
-    cudaEvent_t ev[7];
-    for (auto &e : ev) CUDA_TRY(cudaEventCreate(&e));
     double acc[6] = {0, 0, 0, 0, 0, 0};
+    long long nsub = 0;
+    std::vector<cudaEvent_t> ev;
+    auto need = [&](size_t n) -> int {
+        while (ev.size() < n) {
+            cudaEvent_t e;
+            CUDA_TRY(cudaEventCreate(&e));
+            ev.push_back(e);
+        }
+        return CMF_OK;
+    };
     const dim3 gc(c->ncell_blocks, c->dims.nmembers), gcp(c->ncell_blocks + c->npath_blocks, c->dims.nmembers);
-    for (int r = 0; r < reps; r++) {
+    for (int r = 0; r < reps && !rc; r++) {
+        if ((rc = need(3))) break;
         CUDA_TRY(cudaEventRecord(ev[0], c->stream));
         cmf::k_stage<<<gc, c->block, 0, c->stream>>>(c->net, c->st);
         CUDA_TRY(cudaEventRecord(ev[1], c->stream));
         cmf::k_ntdt<<<1, 256, 0, c->stream>>>(c->net, c->st, c->cond, 0);
         CUDA_TRY(cudaEventRecord(ev[2], c->stream));
-        cmf::k_flux<<<gcp, c->block, 0, c->stream>>>(c->net, c->st, c->ncell_blocks);
-        CUDA_TRY(cudaEventRecord(ev[3], c->stream));
-        cmf::k_rate<<<gc, c->block, 0, c->stream>>>(c->net, c->st);
-        CUDA_TRY(cudaEventRecord(ev[4], c->stream));
-        cmf::k_store<<<gcp, c->block, cmf::store_smem(c->block), c->stream>>>(c->net, c->st, c->ncell_blocks);
-        CUDA_TRY(cudaEventRecord(ev[5], c->stream));
-        cmf::k_ctl<<<1, 32 * cmf::kBudgets, 0, c->stream>>>(c->net, c->st, c->ncell_blocks, c->cond, 0);
-        CUDA_TRY(cudaEventRecord(ev[6], c->stream));
-        CUDA_TRY(cudaEventSynchronize(ev[6]));
-        for (int k = 0; k < 6; k++) {
-            float ms = 0.f;
-            CUDA_TRY(cudaEventElapsedTime(&ms, ev[k], ev[k + 1]));
-            acc[k] += ms;
+        cmf::LoopCtl lc;
+        CUDA_TRY(cudaMemcpyAsync(&lc, c->st.loop, sizeof lc, cudaMemcpyDeviceToHost, c->stream));
+        CUDA_TRY(cudaStreamSynchronize(c->stream));
+        float ms = 0.f;
+        CUDA_TRY(cudaEventElapsedTime(&ms, ev[0], ev[1]));
+        acc[0] += ms;
+        CUDA_TRY(cudaEventElapsedTime(&ms, ev[1], ev[2]));
+        acc[1] += ms;
+        const int nt = lc.ntmax;
+        if ((rc = need(4 * (size_t)nt + 1))) break;
+        CUDA_TRY(cudaEventRecord(ev[0], c->stream));
+        for (int k = 0; k < nt; k++) {
+            cmf::k_flux<<<gcp, c->block, 0, c->stream>>>(c->net, c->st, c->ncell_blocks);
+            CUDA_TRY(cudaEventRecord(ev[4 * k + 1], c->stream));
+            cmf::k_rate<<<gc, c->block, 0, c->stream>>>(c->net, c->st);
+            CUDA_TRY(cudaEventRecord(ev[4 * k + 2], c->stream));
+            cmf::k_store<<<gcp, c->block, cmf::store_smem(c->block), c->stream>>>(c->net, c->st, c->ncell_blocks);
+            CUDA_TRY(cudaEventRecord(ev[4 * k + 3], c->stream));
+            cmf::k_ctl<<<1, 32 * cmf::kBudgets, 0, c->stream>>>(c->net, c->st, c->ncell_blocks, c->cond, 0);
+            CUDA_TRY(cudaEventRecord(ev[4 * k + 4], c->stream));
         }
-        c->launches += 6;
+        CUDA_TRY(cudaGetLastError());
+        CUDA_TRY(cudaStreamSynchronize(c->stream));
+        for (int k = 0; k < 4 * nt; k++) {
+            CUDA_TRY(cudaEventElapsedTime(&ms, ev[k], ev[k + 1]));
+            acc[2 + (k & 3)] += ms;
+        }
+        nsub += nt;
+        c->launches += 2 + 4LL * nt;
     }
-    for (auto &e : ev) cudaEventDestroy(e);
-    for (int k = 0; k < 6; k++) ms_out[k] = acc[k] / reps;
+    for (cudaEvent_t e : ev) cudaEventDestroy(e);
+    if (rc) return rc;
+    ms_out[0] = acc[0] / reps;
+    ms_out[1] = acc[1] / reps;
+    for (int k = 2; k < 6; k++) ms_out[k] = nsub ? acc[k] / (double)nsub : 0.0;
     return CMF_OK;
 }
 

@@ -299,14 +299,19 @@ __device__ __forceinline__ StageOut stage_levee(const Net &n, int i, double rivs
     return o;
 }
 
-__device__ __forceinline__ void store_stage(const Net &n, const State &s, size_t gi, int i, const StageOut &o) {
+// diag_only: D2FLDARE and D2SFCELV are read by nothing inside the sub-step loop, so the sub-steps
+// write them on the last sub-step only (the values the caller observes are the same)
+__device__ __forceinline__ void store_stage(const Net &n, const State &s, size_t gi, int i, const StageOut &o,
+                                            bool diag_out = true) {
     s.rivsto[gi] = o.rivsto;
     s.fldsto[gi] = o.fldsto;
     s.rivdph[gi] = o.rivdph;
     s.flddph[gi] = o.flddph;
     s.fldfrc[gi] = o.fldfrc;
-    s.fldare[gi] = o.fldare;
-    s.sfcelv[gi] = n.rivelv[i] + o.rivdph;
+    if (diag_out) {
+        s.fldare[gi] = o.fldare;
+        s.sfcelv[gi] = n.rivelv[i] + o.rivdph;
+    }
     if (n.llevee) {
         s.levsto[gi] = o.levsto;
         s.levdph[gi] = o.levdph;
@@ -428,7 +433,7 @@ __global__ void k_ntdt(Net n, State s, cudaGraphConditionalHandle h, int use_con
 // phase A: outflow + dam + bifurcation flux
 // ------------------------------------------------------------------------------------------
 // CMF_CALC_OUTFLW river/floodplain/mouth discharge and limiter, src/cmf_calc_outflw_mod.F90:44-182
-__device__ __forceinline__ void cell_outflow(const Net &n, const State &s, int m, int i, double DT) {
+__device__ __forceinline__ void cell_outflow(const Net &n, const State &s, int m, int i, double DT, const MemberCtl &c) {
     const size_t base = (size_t)m * n.N, gi = base + i;
     const double gdt = n.pgrv * DT;
     const double rivelv = n.rivelv[i];
@@ -593,7 +598,15 @@ __device__ __forceinline__ void cell_outflow(const Net &n, const State &s, int m
     }
     s.rivout_raw[gi] = rout;
     s.fldout_raw[gi] = fout;
-    s.rivvel[gi] = rvel;
+    // D2RIVVEL is observed after the last sub-step; its sub-step average is accumulated here
+    // (CMF_DIAG_AVEMAX_ADPSTP, src/cmf_calc_diag_mod.F90:104-161) instead of in phase C
+    const bool first = (c.it == 0), last = (c.it == c.nt - 1);
+    if (last) s.rivvel[gi] = rvel;
+    if (n.ldiag) {
+        double a = first ? rvel * DT : s.a_rivvel[gi] + rvel * DT;
+        if (last) a = a / (c.nadd + DT);
+        s.a_rivvel[gi] = a;
+    }
 }
 
 // CMF_CALC_PTHOUT (src/cmf_calc_pthout_mod.F90:34-94) / CMF_LEVEE_OPT_PTHOUT (src/cmf_ctrl_levee_mod.F90:508-601)
@@ -679,7 +692,7 @@ __global__ void __launch_bounds__(kCellThreads, CMF_FLUX_MINB) k_flux(Net n, Sta
     const double DT = c.dt;
     if ((int)blockIdx.x < ncell_blocks) {
         const int i = blockIdx.x * blockDim.x + threadIdx.x;
-        if (i < n.N) cell_outflow(n, s, m, i, DT);
+        if (i < n.N) cell_outflow(n, s, m, i, DT, c);
     } else {
         const int p = (blockIdx.x - ncell_blocks) * blockDim.x + threadIdx.x;
         if (p < n.P) path_outflow(n, s, m, p, DT);
@@ -834,17 +847,19 @@ __global__ void __launch_bounds__(kCellThreads, CMF_STORE_MINB) k_store(Net n, S
         bput(2, n.llevee ? (rs + fs) + levsto : rs + fs);
         // stage scheme, :125
         const StageOut o = n.llevee ? stage_levee(n, i, rs, fs, levsto) : stage_def(n, i, rs, fs);
-        store_stage(n, s, gi, i, o);
+        store_stage(n, s, gi, i, o, last);
         bput(5, n.llevee ? (rs + fs) + levsto : rs + fs);
         bput(6, n.llevee ? (o.rivsto + o.fldsto) + o.levsto : o.rivsto + o.fldsto);
         bput(7, o.rivsto);
         bput(8, o.fldsto);
         bput(9, o.fldare);
         bput(10, o.levsto);
-        s.rivinf[gi] = rinf;
-        s.fldinf[gi] = finf;
-        s.pthout[gi] = pout;
-        s.outflw[gi] = outflw;
+        if (last) {   // diagnostics read by nothing inside the sub-step loop
+            s.rivinf[gi] = rinf;
+            s.fldinf[gi] = finf;
+            s.pthout[gi] = pout;
+            s.outflw[gi] = outflw;
+        }
         // CMF_DIAG_AVEMAX_ADPSTP / GETAVE_ADPSTP, src/cmf_calc_diag_mod.F90:104-221
         if (n.ldiag) {
             const double na = c.nadd + DT;
@@ -855,10 +870,16 @@ __global__ void __launch_bounds__(kCellThreads, CMF_STORE_MINB) k_store(Net n, S
             };
             acc(s.a_rivout, rout);
             acc(s.a_fldout, fout);
-            acc(s.a_rivvel, s.rivvel[gi]);
             acc(s.a_outflw, outflw);
             acc(s.a_pthout, pout);        // D2PTHINF is never written by the reference (always 0)
-            acc(s.a_runoff, runoff);
+            if (last) {
+                // runoff and DT are constant over the outer step: the same running sum of
+                // runoff*DT the accumulator would hold, rebuilt in registers on the last sub-step
+                const double rdt = runoff * DT;
+                double a = rdt;
+                for (int k = 1; k < c.nt; k++) a = a + rdt;
+                s.a_runoff[gi] = a / na;
+            }
             if (n.ldamout) acc(s.a_daminf, s.daminf[gi]);
             const double stg = n.llevee ? (o.rivsto + o.fldsto) + o.levsto : o.rivsto + o.fldsto;
             s.m_outflw[gi] = first ? dmax(0.0, fabs(outflw)) : dmax(s.m_outflw[gi], fabs(outflw));

@@ -183,9 +183,10 @@ int32_t cmf_gpu_ctx_block_size(cmf_gpu_ctx *ctx);
 /* Device-side counters since creation: sum over outer steps and members of NT, sum over outer
  * steps of max NT (sub-step loop iterations) and the number of outer steps. */
 int cmf_gpu_ctx_counters(cmf_gpu_ctx *ctx, int64_t *member_substeps, int64_t *loop_iters, int64_t *outer_steps);
-/* Measurement helper: runs `reps` single-sub-step outer steps kernel by kernel with CUDA events
- * between kernels on the context's stream (advances the state).  ms_out[6] receives the mean
- * duration of the stage/CFL, NT/DT, flux, rate, storage and control kernels. */
+/* Measurement helper: runs `reps` outer steps kernel by kernel with CUDA events between kernels
+ * on the context's stream (advances the state), timing every sub-step.  ms_out[6] receives the mean
+ * duration per launch of the stage/CFL and NT/DT kernels (once per outer step) and of the flux,
+ * rate, storage and control kernels (once per sub-step). */
 int cmf_gpu_ctx_time_phases(cmf_gpu_ctx *ctx, double dt_def, int32_t reps, double *ms_out);
 
 /* Storage-only restart (LSTOONLY): the stage scheme, then CMF_CALC_OUTPRE
