@@ -5,8 +5,9 @@ E1  trajectories: the GPU solver advances ensemble members; before each coupling
     step (D2OUTFLW_aAVG of the physics).
 E2  graph messages: 8 hops of upstream sums (CSR gather along I1NEXT) of the last-step outflow and
     of the runoff, normalised by the receiving cell's discharge scale.
-E3  MLP 64 (30 used) -> 128 -> 128 -> 128 -> 1 with ReLU, BF16 weights and activations, FP32
-    accumulation on the tensor cores, FP32 master weights and Adam -- kernels in csrc/cmf_emu.cu.
+E3  MLP 64 (32 used) -> 128 -> 128 -> 128 -> 1 with ReLU, BF16 weights and activations, FP32
+    accumulation on the tensor cores, FP32 master weights and Adam -- kernels in csrc/cmf_emu.cu
+    (training on mma.sync tiles; inference fused on tcgen05 with tensor-memory accumulators).
 E4  rollout: predicted outflows update storage through the same upstream gather (mass conserved
     exactly), the stage scheme recomputes depths.  Every `resync_hours` the plain solver, started
     from the same state, judges a rotating subset of members: their daily-mean discharge error at
@@ -55,6 +56,9 @@ def _emu_lib():
         lib.cmf_emu_mlp_pack_bytes.restype = C.c_size_t
         lib.cmf_emu_mlp_pack.argtypes = [vp, vp, vp, vp, i, vp, vp]
         lib.cmf_emu_mlp_fused.argtypes = [vp, i, i, vp, vp, vp, vp, vp, vp, vp]
+        lib.cmf_emu_mlp_tc_pack_bytes.restype = C.c_size_t
+        lib.cmf_emu_mlp_tc_pack.argtypes = [vp, vp, vp, vp, i, vp, vp]
+        lib.cmf_emu_mlp_tc.argtypes = [vp, i, i, vp, vp, vp, vp, vp, vp, vp]
         lib.cmf_emu_last_error.restype = C.c_char_p
         lib.cmf_gpu_ctx_emu_views.argtypes = [vp, C.c_int32, C.POINTER(EmuNet), C.POINTER(EmuMember)]
         lib.cmf_gpu_ctx_copy_member.argtypes = [vp, C.c_int32, vp, C.c_int32]
@@ -141,6 +145,7 @@ class MLP:
             self.Wb[k].copy_(self.W[k].to(self.torch.bfloat16))
             self.b[k].copy_(self.torch.from_numpy(np.asarray(sd["b"][k], dtype=np.float32)))
         self._packed_step = None
+        self._tc_step = None
 
     def _gemm(self, M, N, K, A, lda, ta, B, ldb, tb, C=None, Cb=None, bias=None, relu=0, acc=0, ksplit=1):
         p = lambda t: (t.data_ptr() if t is not None else None)  # noqa: E731
@@ -177,6 +182,24 @@ class MLP:
         echeck(self.lib.cmf_emu_mlp_fused(X.data_ptr(), X.shape[1], R, self._pack.data_ptr(), self.b[0].data_ptr(),
                                           self.b[1].data_ptr(), self.b[2].data_ptr(), self.b[3].data_ptr(), y.data_ptr(),
                                           self.stream), "mlp_fused")
+        return y
+
+    def infer_tc(self, X, y=None):
+        """Fused inference on the tcgen05 tensor cores: X [R, 64] bf16 -> y [R] fp32."""
+        torch = self.torch
+        if getattr(self, "_tc_step", None) != self.step or getattr(self, "_tc_pack", None) is None:
+            if getattr(self, "_tc_pack", None) is None:
+                self._tc_pack = torch.empty(self.lib.cmf_emu_mlp_tc_pack_bytes(), dtype=torch.uint8, device=self.dev)
+            echeck(self.lib.cmf_emu_mlp_tc_pack(self.Wb[0].data_ptr(), self.Wb[1].data_ptr(), self.Wb[2].data_ptr(),
+                                                self.Wb[3].data_ptr(), OUT, self._tc_pack.data_ptr(), self.stream),
+                   "mlp_tc_pack")
+            self._tc_step = self.step
+        R = X.shape[0]
+        if y is None:
+            y = torch.empty(R, dtype=torch.float32, device=self.dev)
+        echeck(self.lib.cmf_emu_mlp_tc(X.data_ptr(), X.shape[1], R, self._tc_pack.data_ptr(), self.b[0].data_ptr(),
+                                       self.b[1].data_ptr(), self.b[2].data_ptr(), self.b[3].data_ptr(), y.data_ptr(),
+                                       self.stream), "mlp_tc")
         return y
 
     def backward(self, acts, dY, dYb):
@@ -494,7 +517,7 @@ class SurrogateEnsemble:
 
     def emu_step(self):
         X = self.fe.build()
-        self._y = self.mlp.infer(X, getattr(self, "_y", None))
+        self._y = self.mlp.infer_tc(X, getattr(self, "_y", None))     # tcgen05 tensor cores
         self.fe.rollout(self._y, self.active, ldy=1, residual=getattr(self.mlp, "residual", True))
 
     def run(self, forcing, hours: int, h0: int = 0):

@@ -2,7 +2,9 @@
 //
 // A 4-layer MLP (input 32 -> 128 -> 128 -> 128 -> 1, ReLU) maps local state plus 8-hop upstream
 // messages of every cell to its mean outflow over the next coupling step.  BF16 operands, FP32
-// accumulation on the tensor cores (mma.sync m16n8k16), FP32 master weights updated by Adam.
+// accumulation on the tensor cores (mma.sync m16n8k16 tiles for training and a register-chained
+// fused inference; tcgen05 MMAs into tensor memory for the production inference), FP32 master
+// weights updated by Adam.
 // The rollout kernel turns predicted outflows into a mass-conserving storage update along the
 // same upstream CSR the physics uses; the stage scheme then recomputes depths.
 #include <cuda_bf16.h>
@@ -467,6 +469,238 @@ __global__ void k_emu_update(EmuNet n, const int *active, double dt, const doubl
     qprev[i] = qout[i];
 }
 
+
+// ------------------------------------------------------------------------------------------
+// Fused inference on the 5th-generation tensor cores (tcgen05, sm_100a).
+//
+// A CTA of 512 threads owns 128-row tiles of a persistent grid.  All four layers' weights sit in
+// shared memory as the MMA's B operands and the tile's activations as its A operand, both in the
+// K-major no-swizzle canonical layout: 16-byte rows of 8 bf16 grouped in 8-row core matrices,
+// byte offset (k/8)*(R*16) + (r/8)*128 + (r%8)*16 for an R-row operand (stride between the
+// 8-row groups 128 B, between the 8-wide k chunks R*16 B).  One thread issues the tcgen05.mma of
+// a layer (M=128, N=128 or 16, K=16 per instruction, fp32 accumulator in 128 TMEM columns) and a
+// tcgen05.commit onto an mbarrier; every thread waits on it (bounded), reads its row's accumulator
+// with tcgen05.ld (warp w reads TMEM lanes 32*(w%4).., columns 32*(w/4)..), adds the bias, applies
+// ReLU, rounds to bf16 and stores the next layer's A operand.  The last layer (N=16, column 0
+// real) adds b3 and writes y.  The rounding points equal the layer-by-layer chain (bf16 inputs,
+// fp32 accumulation, bf16 activations); the order of the fp32 additions inside an MMA is the
+// hardware's, so results agree with the mma.sync path to fp32 rounding, not bit for bit.
+// ------------------------------------------------------------------------------------------
+#ifndef CMF_TC_THREADS
+#define CMF_TC_THREADS 512
+#endif
+constexpr int kTcRows = 128, kTcThreads = CMF_TC_THREADS, kTcCols = 128;
+constexpr int kTcColsPerThread = kTcRows * kTcCols / kTcThreads;   // accumulator columns one thread reads
+constexpr int kTcW0 = 0;                              // byte offsets inside the packed image
+constexpr int kTcW1 = kTcW0 + 128 * 32 * 2;           // layer 0: N=128, K=32
+constexpr int kTcW2 = kTcW1 + 128 * 128 * 2;          // layers 1, 2: N=128, K=128
+constexpr int kTcW3 = kTcW2 + 128 * 128 * 2;          // layer 3: N=16, K=128
+constexpr int kTcWBytes = kTcW3 + 16 * 128 * 2;
+constexpr int kTcA = kTcWBytes;                       // activations: 128 rows x 128 k
+constexpr int kTcBias = kTcA + kTcRows * 128 * 2;     // b0 b1 b2 (3 x 128 floats), b3[0]
+constexpr int kTcMisc = kTcBias + (3 * 128 + 4) * 4;  // mbarrier (8 B), TMEM address (4 B)
+constexpr int kTcSmem = kTcMisc + 16;
+constexpr int kTcWaitLimit = 1 << 20;
+
+__device__ int g_mlp_tc_status;                       // 0 ok; 1: an MMA completion wait ran out
+
+__host__ __device__ constexpr uint64_t umma_smem_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+    // start address, leading- and stride-dimension byte offsets (16-byte units), version 1,
+    // base offset 0, no swizzle
+    return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+           ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+__host__ __device__ constexpr uint32_t umma_idesc_bf16_f32(int M, int N) {
+    // D fp32, A and B bf16, both K-major, N/8 and M/16
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+// byte offset of element (r, k) of an R-row K-major operand in the canonical layout
+__host__ __device__ constexpr uint32_t canon_off(int r, int k, int R) {
+    return (uint32_t)((k >> 3) * (R * 16) + (r >> 3) * 128 + (r & 7) * 16 + (k & 7) * 2);
+}
+
+// B operands of the four layers as one shared-memory image: element (n, k) = W[k][n]
+__global__ void k_mlp_tc_pack(const __nv_bfloat16 *__restrict__ W0, const __nv_bfloat16 *__restrict__ W1,
+                              const __nv_bfloat16 *__restrict__ W2, const __nv_bfloat16 *__restrict__ W3, int ldw3,
+                              __nv_bfloat16 *out) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    const int n0 = 128 * 32, n1 = 128 * 128, n3 = 16 * 128;
+    if (e >= n0 + 2 * n1 + n3) return;
+    int n, k, R, base;
+    const __nv_bfloat16 *W;
+    int ldw;
+    if (e < n0) { n = e / 32; k = e % 32; R = 128; base = kTcW0; W = W0; ldw = 128; }
+    else if (e < n0 + n1) { const int q = e - n0; n = q / 128; k = q % 128; R = 128; base = kTcW1; W = W1; ldw = 128; }
+    else if (e < n0 + 2 * n1) { const int q = e - n0 - n1; n = q / 128; k = q % 128; R = 128; base = kTcW2; W = W2; ldw = 128; }
+    else { const int q = e - n0 - 2 * n1; n = q / 128; k = q % 128; R = 16; base = kTcW3; W = W3; ldw = ldw3; }
+    out[(base + canon_off(n, k, R)) / 2] = W[(size_t)k * ldw + n];
+}
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc, uint32_t acc) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n"
+        :: "r"(tmem_d), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(acc));
+}
+
+__device__ __forceinline__ void umma_commit(uint32_t mbar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" :: "r"(mbar) : "memory");
+}
+
+// bounded wait on an mbarrier phase; false when the limit ran out
+__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity) {
+    for (int i = 0; i < kTcWaitLimit; i++) {
+        uint32_t ok;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}\n"
+            : "=r"(ok) : "r"(mbar), "r"(parity) : "memory");
+        if (ok) return true;
+    }
+    return false;
+}
+
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+          "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]),
+          "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]),
+          "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+        : "r"(taddr));
+}
+__device__ __forceinline__ void tmem_ld1(uint32_t taddr, uint32_t &v) {
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x1.b32 {%0}, [%1];" : "=r"(v) : "r"(taddr));
+}
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+// layer epilogue: bias + ReLU + bf16 of this thread's columns of row r into the A operand
+__device__ __forceinline__ void tc_epilogue_hidden(uint32_t tmem_row, int col0, const float *bias, unsigned char *sA, int r) {
+#pragma unroll
+    for (int h = 0; h < kTcColsPerThread / 32; h++) {
+        uint32_t v[32];
+        tmem_ld32(tmem_row + col0 + 32 * h, v);
+        tmem_wait_ld();
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            const int c = col0 + 32 * h + 8 * q;      // first of 8 columns = k chunk c/8 of the next layer
+            uint4 u;
+            uint32_t *w = reinterpret_cast<uint32_t *>(&u);
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                const float a = fmaxf(__uint_as_float(v[8 * q + 2 * j]) + bias[c + 2 * j], 0.f);
+                const float b = fmaxf(__uint_as_float(v[8 * q + 2 * j + 1]) + bias[c + 2 * j + 1], 0.f);
+                w[j] = pack_bf16x2(a, b);
+            }
+            *reinterpret_cast<uint4 *>(sA + canon_off(r, c, kTcRows)) = u;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kTcThreads, 1) k_mlp_tc(const __nv_bfloat16 *__restrict__ X, int ldx, int rows,
+                                                        const uint4 *__restrict__ wimg, const float *__restrict__ b0,
+                                                        const float *__restrict__ b1, const float *__restrict__ b2,
+                                                        const float *__restrict__ b3, float *__restrict__ y) {
+    extern __shared__ __align__(1024) unsigned char sm[];
+    unsigned char *sA = sm + kTcA;
+    float *sb = reinterpret_cast<float *>(sm + kTcBias);
+    uint64_t *mbar = reinterpret_cast<uint64_t *>(sm + kTcMisc);
+    uint32_t *tslot = reinterpret_cast<uint32_t *>(sm + kTcMisc + 8);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    // weights and biases into shared memory
+    for (int e = tid; e < kTcWBytes / 16; e += kTcThreads) reinterpret_cast<uint4 *>(sm)[e] = wimg[e];
+    for (int e = tid; e < 128; e += kTcThreads) { sb[e] = b0[e]; sb[128 + e] = b1[e]; sb[256 + e] = b2[e]; }
+    if (tid == 0) {
+        sb[384] = b3[0];
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_u32(mbar)) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {   // one warp allocates the accumulator columns and releases the allocation permit
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                     :: "r"(smem_u32(tslot)), "r"(kTcCols) : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    fence_async_smem();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tslot;
+    const uint32_t mb = smem_u32(mbar);
+    const uint32_t sw = smem_u32(sm), sa = smem_u32(sA);
+    const uint32_t id128 = umma_idesc_bf16_f32(128, 128), id16 = umma_idesc_bf16_f32(128, 16);
+    const int r = 32 * (warp & 3) + lane;                    // this thread's row (TMEM lane)
+    const uint32_t tmem_row = tmem + ((uint32_t)(32 * (warp & 3)) << 16);
+    const int col0 = kTcColsPerThread * (warp >> 2);         // this thread's accumulator columns
+    uint32_t phase = 0;
+    bool failed = false;
+    const int ntiles = (rows + kTcRows - 1) / kTcRows;
+    for (int tile = blockIdx.x; tile < ntiles && !failed; tile += gridDim.x) {
+        const int row0 = tile * kTcRows;
+        // X tile -> A operand (k 0..31): 128 rows x 4 chunks of 16 bytes
+        for (int q = tid; q < kTcRows * 4; q += kTcThreads) {
+            const int rr = q >> 2, kc = q & 3;
+            uint4 u = make_uint4(0u, 0u, 0u, 0u);
+            if (row0 + rr < rows) u = *reinterpret_cast<const uint4 *>(X + (size_t)(row0 + rr) * ldx + kc * 8);
+            *reinterpret_cast<uint4 *>(sA + canon_off(rr, kc * 8, kTcRows)) = u;
+        }
+        fence_async_smem();
+        tc_fence_before();
+        __syncthreads();
+#pragma unroll 1
+        for (int layer = 0; layer < 4; layer++) {
+            if (tid == 0) {
+                tc_fence_after();
+                const int ksteps = layer == 0 ? 2 : 8;
+                const uint32_t wb = sw + (layer == 0 ? kTcW0 : layer == 1 ? kTcW1 : layer == 2 ? kTcW2 : kTcW3);
+                const uint32_t blbo = layer == 3 ? 16 * 16 : 128 * 16;
+                for (int s = 0; s < ksteps; s++) {
+                    const uint64_t ad = umma_smem_desc(sa + 2 * s * (128 * 16), 128 * 16, 128);
+                    const uint64_t bd = umma_smem_desc(wb + 2 * s * blbo, blbo, 128);
+                    umma_bf16(tmem, ad, bd, layer == 3 ? id16 : id128, s > 0 ? 1u : 0u);
+                }
+                umma_commit(mb);
+            }
+            const bool ok = mbar_wait(mb, phase);
+            if (__syncthreads_or(ok ? 0 : 1)) { failed = true; break; }   // block-uniform exit
+            phase ^= 1u;
+            tc_fence_after();
+            if (layer < 3) {
+                tc_epilogue_hidden(tmem_row, col0, sb + 128 * layer, sA, r);
+                fence_async_smem();
+                tc_fence_before();
+                __syncthreads();
+            } else {
+                if (warp < 4) {
+                    uint32_t v;
+                    tmem_ld1(tmem_row, v);
+                    tmem_wait_ld();
+                    if (row0 + r < rows) y[row0 + r] = __uint_as_float(v) + sb[384];
+                }
+                tc_fence_before();
+                __syncthreads();
+            }
+        }
+    }
+    if (failed) {
+        if (tid == 0) atomicExch(&g_mlp_tc_status, 1);
+        mbar_wait(mb, phase);                                 // one more bounded wait for the MMA phase in flight
+        tc_fence_before();
+        __syncthreads();
+        tc_fence_after();
+    }
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(tmem), "r"(kTcCols) : "memory");
+}
+
 }  // namespace
 
 extern "C" {
@@ -543,6 +777,45 @@ int cmf_emu_mlp_fused(const void *X, int ldx, int rows, const void *pack, const 
                                                                    b0, b1, b2, b3, y);
     EMU_TRY(cudaGetLastError());
     return CMF_OK;
+}
+
+size_t cmf_emu_mlp_tc_pack_bytes(void) { return (size_t)kTcWBytes; }
+
+int cmf_emu_mlp_tc_pack(const void *W0, const void *W1, const void *W2, const void *W3, int ldw3, void *pack, void *stream) {
+    if (!W0 || !W1 || !W2 || !W3 || !pack || ldw3 < 16 || ((uintptr_t)pack & 15))
+        return emu_err(CMF_E_ARG, "cmf_emu_mlp_tc_pack: bad arguments (ldw3 >= 16, pack 16-byte aligned)");
+    const int n = 128 * 32 + 2 * 128 * 128 + 16 * 128;
+    k_mlp_tc_pack<<<(n + 255) / 256, 256, 0, (cudaStream_t)stream>>>(
+        (const __nv_bfloat16 *)W0, (const __nv_bfloat16 *)W1, (const __nv_bfloat16 *)W2, (const __nv_bfloat16 *)W3, ldw3,
+        (__nv_bfloat16 *)pack);
+    EMU_TRY(cudaGetLastError());
+    return CMF_OK;
+}
+
+int cmf_emu_mlp_tc(const void *X, int ldx, int rows, const void *pack, const float *b0, const float *b1, const float *b2,
+                   const float *b3, float *y, void *stream) {
+    if (!X || !pack || !b0 || !b1 || !b2 || !b3 || !y || ldx < 32 || (ldx % 8) || rows < 0)
+        return emu_err(CMF_E_ARG, "cmf_emu_mlp_tc: bad arguments (ldx >= 32 and a multiple of 8)");
+    if (((uintptr_t)X & 15) || ((uintptr_t)pack & 15)) return emu_err(CMF_E_ARG, "cmf_emu_mlp_tc: X and pack must be 16-byte aligned");
+    if (rows == 0) return CMF_OK;
+    int dev = 0, sms = 0, major = 0;
+    EMU_TRY(cudaGetDevice(&dev));
+    EMU_TRY(cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev));
+    if (major != 10) return emu_err(CMF_E_NO_DEVICE, "cmf_emu_mlp_tc: needs an sm_100 device");
+    EMU_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    EMU_TRY(cudaFuncSetAttribute(k_mlp_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem));
+    const int ntiles = (rows + kTcRows - 1) / kTcRows;
+    const int grid = ntiles < 2 * sms ? ntiles : 2 * sms;
+    k_mlp_tc<<<grid, kTcThreads, kTcSmem, (cudaStream_t)stream>>>((const __nv_bfloat16 *)X, ldx, rows, (const uint4 *)pack,
+                                                                  b0, b1, b2, b3, y);
+    EMU_TRY(cudaGetLastError());
+    return CMF_OK;
+}
+
+int cmf_emu_mlp_tc_status(void) {
+    int v = 0;
+    if (cudaMemcpyFromSymbol(&v, g_mlp_tc_status, sizeof v) != cudaSuccess) return emu_err(CMF_E_CUDA, "cmf_emu_mlp_tc_status: read failed");
+    return v ? CMF_E_CUDA : CMF_OK;
 }
 
 // Features of every member: X rows [M][rows_per_member][ldx] bf16 (columns 0..31 written);

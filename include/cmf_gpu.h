@@ -316,6 +316,19 @@ size_t cmf_emu_mlp_pack_bytes(void);
 int cmf_emu_mlp_pack(const void *W0, const void *W1, const void *W2, const void *W3, int ldw3, void *pack, void *stream);
 int cmf_emu_mlp_fused(const void *X, int ldx, int rows, const void *pack, const float *b0, const float *b1,
                       const float *b2, const float *b3, float *y, void *stream);
+/* The same fused inference on the 5th-generation tensor cores (tcgen05 MMA into tensor memory,
+ * sm_100a): cmf_emu_mlp_tc_pack lays the four layers' weights out as one shared-memory image
+ * (cmf_emu_mlp_tc_pack_bytes() bytes, 16-byte aligned device memory; W3 needs ldw3 >= 16 columns,
+ * column 0 is the output); cmf_emu_mlp_tc maps X rows (bf16, ldx >= 32 and a multiple of 8, X
+ * 16-byte aligned, columns 32.. ignored) to y[rows].  Rounding points as the layer-by-layer
+ * chain; fp32 accumulation order is the tensor core's.  cmf_emu_mlp_tc_status() reports (after
+ * the stream is synchronised) whether any launch gave up waiting for an MMA (CMF_E_CUDA). */
+size_t cmf_emu_mlp_tc_pack_bytes(void);
+int cmf_emu_mlp_tc_pack(const void *W0, const void *W1, const void *W2, const void *W3, int ldw3, void *pack,
+                        void *stream);
+int cmf_emu_mlp_tc(const void *X, int ldx, int rows, const void *pack, const float *b0, const float *b1,
+                   const float *b2, const float *b3, float *y, void *stream);
+int cmf_emu_mlp_tc_status(void);
 const char *cmf_emu_last_error(void);
 
 /* ======================================================================================== */

@@ -134,6 +134,38 @@ def test_fused_inference_equals_layerwise_forward(R):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("R", [16, 1040, 70000])
+def test_tcgen05_inference_matches_mma_sync_and_reference(R):
+    """The tcgen05 (tensor-memory) fused kernel against the mma.sync fused kernel and the CPU bf16
+    reference: same rounding points, so differences come only from the fp32 accumulation order
+    inside an MMA (and the bf16 roundings that such a difference may flip)."""
+    import torch
+
+    from cmf_b200.emulator import MLP, _emu_lib
+    from emu_ref import forward, to_bf16
+
+    dev = torch.device("cuda", 0)
+    rng = np.random.default_rng(R + 1)
+    mlp = MLP(dev, seed=2)
+    W, b = _rand_params(rng, 0.2)
+    mlp.load({"W": W, "b": b})
+    X = to_bf16(rng.standard_normal((R, 64)) * 2.0)
+    X[:, 30:] = 0
+    tX = torch.tensor(X, device=dev).to(torch.bfloat16)
+    y_tc = mlp.infer_tc(tX)
+    y_ms = mlp.infer(tX)
+    torch.cuda.synchronize()
+    assert _emu_lib().cmf_emu_mlp_tc_status() == 0
+    a, m = y_tc.cpu().numpy(), y_ms.cpu().numpy()
+    scale = float(np.abs(m).max())
+    assert np.all(np.isfinite(a))
+    assert np.abs(a - m).max() <= 2e-2 * scale, np.abs(a - m).max() / scale
+    assert np.median(np.abs(a - m)) <= 1e-3 * scale
+    ref, _ = forward(X[:2048], [w.astype(np.float32) for w in W], [v.astype(np.float32) for v in b], bf16=True)
+    assert np.allclose(a[:2048], ref[:, 0], rtol=2e-2, atol=2e-2 * float(np.abs(ref[:, 0]).max()))
+
+
+@pytest.mark.gpu
 def test_trained_emulator_beats_untrained_and_persistence(case_dirs):
     """E1-E5 on the config-1 laws: train on solver trajectories, then roll out 24 h from a plain
     state and compare the gauge discharge with the plain solver: the trained network must be far
