@@ -334,7 +334,6 @@ struct EmuNet {
     double pmanfld;
 };
 
-__device__ __forceinline__ float slog(float x) { return copysignf(log1pf(fabsf(x)), x); }
 
 // hop-0 inputs: last-step mean outflow and runoff of every member, as fp32 planes
 __global__ void k_emu_seed(EmuNet n, const double *__restrict__ qprev, const double *__restrict__ runoff, float *pa, float *pb) {
@@ -360,10 +359,20 @@ __global__ void k_emu_hop(EmuNet n, const float *__restrict__ in_a, const float 
     out_b[mo + i] = b;
 }
 
+// Features feed a bf16 network (8-bit mantissa), so they are computed in fp32 with fast
+// reciprocals and the hardware log/exp approximations: one reciprocal of the discharge scale per
+// cell instead of a division per feature.  Training and inference use this same kernel.
+// sign(x) log(1 + |x|); below 1e-3 the two-term series a - a^2/2 (relative error < a^2/3), where
+// the hardware logarithm of 1 + a would lose the small ratios (runoff over a large river's scale)
+__device__ __forceinline__ float fslog(float x) {
+    const float a = fabsf(x);
+    return copysignf(a < 1e-3f ? a * (1.f - 0.5f * a) : __logf(1.f + a), x);
+}
+
 // Manning discharge of a rectangular section of area A, hydraulic depth h and friction slope s
-__device__ __forceinline__ float manning_q(float area, float h, float s, float man) {
+__device__ __forceinline__ float manning_q(float area, float h, float s, float inv_man) {
     if (!(area > 0.f) || !(h > 0.f)) return 0.f;
-    return copysignf(area * cbrtf(h * h) * sqrtf(fabsf(s)) / man, s);
+    return copysignf(area * __expf(0.6666667f * __logf(h)) * sqrtf(fabsf(s)) * inv_man, s);
 }
 
 // features of cell i of member blockIdx.y; planes [2*(hops+1)][M*N] (0,1 = seeds; 2h+2, 2h+3 = hop h)
@@ -377,44 +386,46 @@ __global__ void k_emu_assemble(EmuNet n, const double *__restrict__ rivsto, cons
     if (i >= n.N) return;
     // member blockIdx.y: state arrays are member-major [M][N], X rows [M][rows_per_member]
     const size_t mo = (size_t)blockIdx.y * n.N, gi = mo + i;
-    const double q = n.qref[i];
-    const double S = rivsto[gi] + fldsto[gi] + (levsto ? levsto[gi] : 0.0);
+    const float qf = (float)n.qref[i];
+    const float iq = __frcp_rn(qf);
+    const double Sd = rivsto[gi] + fldsto[gi] + (levsto ? levsto[gi] : 0.0);
+    const float S = (float)Sd;
+    const float rdph = (float)rivdph[gi], fdph = (float)flddph[gi];
+    const float len = (float)n.rivlen[i], wth = (float)n.rivwth[i], hgt = (float)n.rivhgt[i];
     float f[32];
-    f[0] = slog((float)(S / n.rivstomax[i]));
-    f[1] = (float)(rivdph[gi] / n.rivhgt[i]);
-    f[2] = slog((float)flddph[gi]);
-    f[3] = slog((float)(qprev[gi] / q));
-    f[4] = slog((float)(runoff[gi] / q));
+    f[0] = fslog(S * __frcp_rn((float)n.rivstomax[i]));
+    f[1] = rdph * __frcp_rn(hgt);
+    f[2] = fslog(fdph);
+    f[3] = fslog((float)qprev[gi] * iq);
+    f[4] = fslog((float)runoff[gi] * iq);
     f[5] = (float)fldfrc[gi];
     const bool mouth = i >= n.R;
     const int j = mouth ? i : n.next[i];
-    const double dst = mouth ? 10000.0 : n.nxtdst[i];
+    const float inv_dst = __frcp_rn(mouth ? 10000.f : (float)n.nxtdst[i]);
     const double sfc = n.rivelv[i] + rivdph[gi], sfcn = mouth ? n.elevtn[i] : n.rivelv[j] + rivdph[mo + j];
-    const float slope = (float)((sfc - sfcn) / dst);
-    f[6] = slog(1000.f * slope);
-    f[7] = slog((float)(1000.0 * (n.elevtn[i] - (mouth ? n.elevtn[i] : n.elevtn[j])) / n.nxtdst[i]));
-    f[8] = logf((float)n.rivlen[i]) - 9.5f;
-    f[9] = logf((float)n.rivwth[i]) - 4.0f;
-    f[10] = logf((float)n.rivhgt[i]) - 1.0f;
-    f[11] = logf((float)q) - 3.0f;
+    const float slope = (float)(sfc - sfcn) * inv_dst;   // elevations subtracted in fp64
+    f[6] = fslog(1000.f * slope);
+    f[7] = fslog(1000.f * (float)(n.elevtn[i] - (mouth ? n.elevtn[i] : n.elevtn[j])) * __frcp_rn((float)n.nxtdst[i]));
+    f[8] = __logf(len) - 9.5f;
+    f[9] = __logf(wth) - 4.0f;
+    f[10] = __logf(hgt) - 1.0f;
+    f[11] = __logf(qf) - 3.0f;
     f[12] = mouth ? 1.f : 0.f;
-    f[13] = slog((float)(S / (q * 3600.0)));
-    const float qf = (float)q;
+    f[13] = fslog(S * iq * (1.f / 3600.f));
 #pragma unroll
     for (int h = 0; h < 8; h++) {
         if (h < hops) {
-            f[14 + 2 * h] = slog(planes[(size_t)(2 + 2 * h) * plane + gi] / qf);
-            f[15 + 2 * h] = slog(planes[(size_t)(3 + 2 * h) * plane + gi] / qf);
+            f[14 + 2 * h] = fslog(planes[(size_t)(2 + 2 * h) * plane + gi] * iq);
+            f[15 + 2 * h] = fslog(planes[(size_t)(3 + 2 * h) * plane + gi] * iq);
         } else {
             f[14 + 2 * h] = f[15 + 2 * h] = 0.f;
         }
     }
     // hydraulic estimates: Manning discharge of the channel and of the floodplain at the current
     // water-surface slope (the state the local-inertial scheme relaxes towards within an hour)
-    const float w = (float)n.rivwth[i], hr = (float)rivdph[gi], hf = (float)flddph[gi];
-    const float af = fmaxf((float)(fldsto[gi] / n.rivlen[i]) - hf * w, 0.f);
-    f[30] = slog(manning_q(w * hr, hr, slope, (float)n.rivman[i]) / qf);
-    f[31] = slog(manning_q(af, hf, fmaxf(-0.005f, fminf(0.005f, slope)), (float)n.pmanfld) / qf);
+    const float af = fmaxf((float)fldsto[gi] * __frcp_rn(len) - fdph * wth, 0.f);
+    f[30] = fslog(manning_q(wth * rdph, rdph, slope, __frcp_rn((float)n.rivman[i])) * iq);
+    f[31] = fslog(manning_q(af, fdph, fmaxf(-0.005f, fminf(0.005f, slope)), __frcp_rn((float)n.pmanfld)) * iq);
     uint4 *row = reinterpret_cast<uint4 *>(X + ((size_t)blockIdx.y * rows_per_member + i) * ldx);
 #pragma unroll
     for (int v = 0; v < 4; v++) {
