@@ -504,7 +504,7 @@ def main() -> int:
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-surrogate", action="store_true",
                     help="skip the surrogate-assisted vs plain ensemble measurement")
-    ap.add_argument("--sur-members", type=int, default=64)
+    ap.add_argument("--sur-members", type=int, default=256)
     ap.add_argument("--sur-days", type=int, default=2)
     ap.add_argument("--launch-mode", type=int, default=0, choices=[0, 1],
                     help="0: CUDA graph with a device-side sub-step loop; 1: the same kernels as plain "

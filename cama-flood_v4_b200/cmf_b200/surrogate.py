@@ -16,7 +16,7 @@ import numpy as np
 from . import emulator as E
 
 
-def measure(host, device, members: int = 64, days: int = 2, judge_slots: int = 2, train_members: int = 4,
+def measure(host, device, members: int = 256, days: int = 2, judge_slots: int = 2, train_members: int = 4,
             train_hours: int = 48, train_iters: int = 3000, cells_per_snapshot: int | None = 65536, seed: int = 100,
             gauges: int = 100, tol_rel: float = 0.05, spinup: int = 24) -> dict:
     import torch
