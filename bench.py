@@ -288,7 +288,7 @@ def gpu_arm(args) -> int:
     c1 = g.counters()
     member_sub = c1["member_substeps"] - c0["member_substeps"]
     loop_iters = c1["loop_iters"] - c0["loop_iters"]
-    launches = 2 * K + 4 * loop_iters
+    launches = 3 * K + 3 * loop_iters
     secs = ms / 1e3
     if ws > 1:
         t = torch.tensor([secs], device=dev, dtype=torch.float64)

@@ -342,7 +342,7 @@ class PhysicsGPU:
         dt_def = self.host.dt if dt_def is None else dt_def
         ms = np.zeros(6)
         check(self.lib.cmf_gpu_ctx_time_phases(self.h, dt_def, reps, ms.ctypes.data_as(_abi.f64p)), "time_phases")
-        return dict(zip(["k_stage", "k_ntdt", "k_flux", "k_rate", "k_store", "k_ctl"], ms.tolist()))
+        return dict(zip(["k_stage", "k_ntdt", "k_flux", "k_rate", "k_store", "k_budget"], ms.tolist()))
 
     @property
     def stream(self) -> int:

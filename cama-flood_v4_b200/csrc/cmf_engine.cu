@@ -2,8 +2,8 @@
 //
 // A context owns the device copy of one river network (maps, CSR tables) and the state of
 // `nmembers` ensemble members.  One outer step is one CUDA graph launch:
-//   k_stage -> k_ntdt -> while (k < NTmax) { k_flux -> k_rate -> k_store -> k_ctl }
-// The loop is a conditional WHILE node whose condition the device sets (k_ntdt, k_ctl), so the
+//   k_stage -> k_ntdt -> while (k < NTmax) { k_flux -> k_rate -> k_store } -> k_budget
+// The loop is a conditional WHILE node whose condition the device sets (k_ntdt, k_rate), so the
 // adaptive sub-step count never travels to the host.  launch_mode 1 replaces the conditional node
 // by a host loop (reads NTmax back), which tests use to cross-check the graph path.
 #include <cuda_runtime.h>
@@ -339,9 +339,8 @@ void enqueue_substep(cmf_gpu_ctx *c, int use_cond, cudaGraphConditionalHandle co
     const dim3 gc(c->ncell_blocks, c->dims.nmembers);
     const dim3 gcp(c->ncell_blocks + c->npath_blocks, c->dims.nmembers);
     cmf::k_flux<<<gcp, c->block, 0, c->stream>>>(c->net, c->st, c->ncell_blocks);
-    cmf::k_rate<<<gc, c->block, 0, c->stream>>>(c->net, c->st);
+    cmf::k_rate<<<gc, c->block, 0, c->stream>>>(c->net, c->st, 1, cond, use_cond);
     cmf::k_store<<<gcp, c->block, cmf::store_smem(c->block), c->stream>>>(c->net, c->st, c->ncell_blocks);
-    cmf::k_ctl<<<1, 32 * cmf::kBudgets, 0, c->stream>>>(c->net, c->st, c->ncell_blocks, cond, use_cond);
 }
 void enqueue_substep(cmf_gpu_ctx *c, int use_cond) { enqueue_substep(c, use_cond, c->cond); }
 
@@ -351,6 +350,12 @@ void enqueue_prologue(cmf_gpu_ctx *c, int use_cond, cudaGraphConditionalHandle c
     cmf::k_ntdt<<<1, 256, 0, c->stream>>>(c->net, c->st, cond, use_cond);
 }
 void enqueue_prologue(cmf_gpu_ctx *c, int use_cond) { enqueue_prologue(c, use_cond, c->cond); }
+
+// after the sub-step loop: the budgets of every member's last sub-step
+void enqueue_epilogue(cmf_gpu_ctx *c) {
+    cmf::k_budget<<<dim3(c->dims.nmembers, cmf::kBudgets), cmf::kBudgetThreads, 0, c->stream>>>(c->net, c->st,
+                                                                                           c->ncell_blocks);
+}
 
 // Captures one context's outer step (prologue, then a WHILE node around the sub-step body) into
 // `graph` as a branch with no dependencies, using the conditional handle `cond` of that graph.
@@ -371,6 +376,7 @@ int capture_outer(cmf_gpu_ctx *c, cudaGraph_t graph, cudaGraphConditionalHandle 
     CUDA_TRY(cudaGraphAddNode(&cnode, captured, deps, ndeps, &cp));
     cudaGraph_t body = cp.conditional.phGraph_out[0];
     CUDA_TRY(cudaStreamUpdateCaptureDependencies(c->stream, &cnode, 1, cudaStreamSetCaptureDependencies));
+    enqueue_epilogue(c);
     cudaGraph_t g2 = nullptr;
     CUDA_TRY(cudaStreamEndCapture(c->stream, &g2));
     CUDA_TRY(cudaStreamBeginCaptureToGraph(c->stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
@@ -409,7 +415,7 @@ int sync_dt_def(cmf_gpu_ctx *c, double dt_def) {
 int launch_outer(cmf_gpu_ctx *c) {
     if (c->opts.launch_mode == 0) {
         CUDA_TRY(cudaGraphLaunch(c->exec, c->stream));
-        c->launches += 2;   // prologue; the loop body adds 4 per sub-step (counted on read-back)
+        c->launches += 3;   // prologue and epilogue; the loop body adds 3 per sub-step (counted on read-back)
         return CMF_OK;
     }
     enqueue_prologue(c, 0);
@@ -418,8 +424,9 @@ int launch_outer(cmf_gpu_ctx *c) {
     CUDA_TRY(cudaMemcpyAsync(&lc, c->st.loop, sizeof lc, cudaMemcpyDeviceToHost, c->stream));
     CUDA_TRY(cudaStreamSynchronize(c->stream));
     for (int k = 0; k < lc.ntmax; k++) enqueue_substep(c, 0);
+    enqueue_epilogue(c);
     CUDA_TRY(cudaGetLastError());
-    c->launches += 2 + 4LL * lc.ntmax;
+    c->launches += 3 + 3LL * lc.ntmax;
     return CMF_OK;
 }
 
@@ -447,7 +454,7 @@ int autotune(cmf_gpu_ctx *c) {
         for (int rep = 0; rep < 4; rep++) {
             CUDA_TRY(cudaEventRecord(e0, c->stream));
             cmf::k_flux<<<gcp, b, 0, c->stream>>>(c->net, c->st, c->ncell_blocks);
-            cmf::k_rate<<<gc, b, 0, c->stream>>>(c->net, c->st);
+            cmf::k_rate<<<gc, b, 0, c->stream>>>(c->net, c->st, 0, c->cond, 0);
             cmf::k_store<<<gcp, b, cmf::store_smem(b), c->stream>>>(c->net, c->st, c->ncell_blocks);
             CUDA_TRY(cudaEventRecord(e1, c->stream));
             CUDA_TRY(cudaEventSynchronize(e1));
@@ -514,7 +521,7 @@ int finish_outer(cmf_gpu_ctx *c, int32_t *nt_out, double *dt_out, cmf_budget *b)
             b[m].fldare = x.budget[9]; b[m].levsto = x.budget[10]; b[m].dam_miss = x.budget[11];
         }
     }
-    if (c->opts.launch_mode == 0) c->launches += 4LL * ntmax;
+    if (c->opts.launch_mode == 0) c->launches += 3LL * ntmax;
     if (err) {
         for (auto &x : c->hctl) x.err = 0;
         CUDA_TRY(cudaMemcpyAsync(c->st.ctl, c->hctl.data(), c->hctl.size() * sizeof(cmf::MemberCtl), cudaMemcpyHostToDevice, c->stream));
@@ -650,8 +657,9 @@ int cmf_gpu_ctx_counters(cmf_gpu_ctx *c, int64_t *member_substeps, int64_t *loop
 int cmf_gpu_ctx_time_phases(cmf_gpu_ctx *c, double dt_def, int32_t reps, double *ms_out) {
     // Runs `reps` outer steps kernel by kernel (the host-driven schedule) with CUDA events between
     // the kernels on the context's stream, so every sub-step of the step is timed -- first, middle
-    // and last alike.  ms_out[0..5] = mean ms per launch of k_stage, k_ntdt (per outer step) and of
-    // k_flux, k_rate, k_store, k_ctl (per sub-step).  Advances the state like `reps` outer steps.
+    // and last alike.  ms_out[0..5] = mean ms per launch of k_stage, k_ntdt (per outer step), of
+    // k_flux, k_rate, k_store (per sub-step) and of k_budget (per outer step).  Advances the state
+    // like `reps` outer steps.
     if (!c || reps <= 0 || !ms_out) return set_err(CMF_E_ARG, "bad argument");
     CUDA_TRY(cudaSetDevice(c->device));
     int rc;
@@ -684,32 +692,35 @@ int cmf_gpu_ctx_time_phases(cmf_gpu_ctx *c, double dt_def, int32_t reps, double 
         CUDA_TRY(cudaEventElapsedTime(&ms, ev[1], ev[2]));
         acc[1] += ms;
         const int nt = lc.ntmax;
-        if ((rc = need(4 * (size_t)nt + 1))) break;
+        if ((rc = need(3 * (size_t)nt + 2))) break;
         CUDA_TRY(cudaEventRecord(ev[0], c->stream));
         for (int k = 0; k < nt; k++) {
             cmf::k_flux<<<gcp, c->block, 0, c->stream>>>(c->net, c->st, c->ncell_blocks);
-            CUDA_TRY(cudaEventRecord(ev[4 * k + 1], c->stream));
-            cmf::k_rate<<<gc, c->block, 0, c->stream>>>(c->net, c->st);
-            CUDA_TRY(cudaEventRecord(ev[4 * k + 2], c->stream));
+            CUDA_TRY(cudaEventRecord(ev[3 * k + 1], c->stream));
+            cmf::k_rate<<<gc, c->block, 0, c->stream>>>(c->net, c->st, 1, c->cond, 0);
+            CUDA_TRY(cudaEventRecord(ev[3 * k + 2], c->stream));
             cmf::k_store<<<gcp, c->block, cmf::store_smem(c->block), c->stream>>>(c->net, c->st, c->ncell_blocks);
-            CUDA_TRY(cudaEventRecord(ev[4 * k + 3], c->stream));
-            cmf::k_ctl<<<1, 32 * cmf::kBudgets, 0, c->stream>>>(c->net, c->st, c->ncell_blocks, c->cond, 0);
-            CUDA_TRY(cudaEventRecord(ev[4 * k + 4], c->stream));
+            CUDA_TRY(cudaEventRecord(ev[3 * k + 3], c->stream));
         }
+        enqueue_epilogue(c);
+        CUDA_TRY(cudaEventRecord(ev[3 * nt + 1], c->stream));
         CUDA_TRY(cudaGetLastError());
         CUDA_TRY(cudaStreamSynchronize(c->stream));
-        for (int k = 0; k < 4 * nt; k++) {
+        for (int k = 0; k < 3 * nt; k++) {
             CUDA_TRY(cudaEventElapsedTime(&ms, ev[k], ev[k + 1]));
-            acc[2 + (k & 3)] += ms;
+            acc[2 + k % 3] += ms;
         }
+        CUDA_TRY(cudaEventElapsedTime(&ms, ev[3 * nt], ev[3 * nt + 1]));
+        acc[5] += ms;
         nsub += nt;
-        c->launches += 2 + 4LL * nt;
+        c->launches += 3 + 3LL * nt;
     }
     for (cudaEvent_t e : ev) cudaEventDestroy(e);
     if (rc) return rc;
     ms_out[0] = acc[0] / reps;
     ms_out[1] = acc[1] / reps;
-    for (int k = 2; k < 6; k++) ms_out[k] = nsub ? acc[k] / (double)nsub : 0.0;
+    for (int k = 2; k < 5; k++) ms_out[k] = nsub ? acc[k] / (double)nsub : 0.0;
+    ms_out[5] = acc[5] / reps;
     return CMF_OK;
 }
 
@@ -772,7 +783,7 @@ int cmf_gpu_ctx_advance_device(cmf_gpu_ctx *c, double dt_def, int32_t ksteps, co
             CUDA_TRY(cudaMemcpyAsync(c->st.runoff, runoff_dev + (size_t)k * stride, MN * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
         if (c->opts.launch_mode == 0) {
             CUDA_TRY(cudaGraphLaunch(c->exec, c->stream));
-            c->launches += 2;
+            c->launches += 3;
         } else {
             // host-driven: the same kernels as plain launches (reads NTmax back once per step)
             if ((rc = launch_outer(c))) return rc;
@@ -842,7 +853,7 @@ int cmf_gpu_batch_launch(cmf_gpu_batch *b, double dt_def) {
     CUDA_TRY(cudaEventRecord(b->done, b->stream));
     for (cmf_gpu_ctx *c : b->ctx) {
         CUDA_TRY(cudaStreamWaitEvent(c->stream, b->done, 0));      // later work of a context follows the step
-        c->launches += 2;
+        c->launches += 3;
     }
     b->launches += 1;
     return CMF_OK;
@@ -1082,8 +1093,9 @@ int cmf_gpu_ctx_substeps(cmf_gpu_ctx *c, double dt_def, double dt_min_global, in
     CUDA_TRY(cudaMemcpyAsync(&lc, c->st.loop, sizeof lc, cudaMemcpyDeviceToHost, c->stream));
     CUDA_TRY(cudaStreamSynchronize(c->stream));
     for (int k = 0; k < lc.ntmax; k++) enqueue_substep(c, 0);
+    enqueue_epilogue(c);
     CUDA_TRY(cudaGetLastError());
-    c->launches += 1 + 4LL * lc.ntmax;
+    c->launches += 2 + 3LL * lc.ntmax;
     const int saved = c->opts.launch_mode;
     c->opts.launch_mode = 1;
     int rc = finish_outer(c, nt_out, dt_out, b);

@@ -5,10 +5,12 @@
 //   k_ntdt    NT/DT per member, loop bound of the device-side sub-step loop (:205-206)
 //   NT x { k_flux  outflow + dam + bifurcation flux         (CMF_CALC_OUTFLW, CMF_DAMOUT_CALC,
 //                                                            CMF_CALC_PTHOUT / CMF_LEVEE_OPT_PTHOUT)
-//          k_rate  storage-out gather and outflow limiter rate (LSPAMAT steps 1-2)
+//          k_rate  storage-out gather and outflow limiter rate (LSPAMAT steps 1-2); advances the
+//                  sub-step counter and the loop condition
 //          k_store rescale + inflow gather + dam balance + CALC_VARS_PRE + CMF_CALC_STONXT +
 //                  stage scheme + sub-step diagnostics        (LSPAMAT steps 2-3, :101-135)
-//          k_ctl   deterministic budget reduction, sub-step counter, loop condition }
+//        }
+//   k_budget  deterministic budget reduction of every member's last sub-step
 // Three grid-wide dependencies per sub-step remain (outflow needs the downstream stage; the rate
 // needs the upstream outflows; the inflow needs the downstream and upstream rates), so each
 // phase is one kernel and the phases are ordered by the graph.
@@ -59,7 +61,8 @@ struct MemberCtl {
 };
 
 struct LoopCtl {
-    int k;            // sub-step counter of the device-side loop
+    int k;            // sub-step counter of the device-side loop (advanced by k_rate)
+    int kcur;         // the sub-step the running k_flux/k_rate/k_store work on (set by k_flux)
     int ntmax;        // max NT over members
     int err;
     int split;        // 1 until the first sub-step after a host state upload: D2RIVOUT /= D2RIVOUT_PRE
@@ -433,7 +436,16 @@ __global__ void k_ntdt(Net n, State s, cudaGraphConditionalHandle h, int use_con
 // phase A: outflow + dam + bifurcation flux
 // ------------------------------------------------------------------------------------------
 // CMF_CALC_OUTFLW river/floodplain/mouth discharge and limiter, src/cmf_calc_outflw_mod.F90:44-182
-__device__ __forceinline__ void cell_outflow(const Net &n, const State &s, int m, int i, double DT, const MemberCtl &c) {
+// NADD_adp before sub-step k: the running sum of DT over the sub-steps already done (the same
+// additions CMF_DIAG_AVEMAX_ADPSTP performs, so the averages divide by the same value)
+__device__ __forceinline__ double nadd_before(int k, double dt) {
+    double a = 0.0;
+    for (int j = 0; j < k; j++) a = a + dt;
+    return a;
+}
+
+__device__ __forceinline__ void cell_outflow(const Net &n, const State &s, int m, int i, double DT, const MemberCtl &c,
+                                             int k) {
     const size_t base = (size_t)m * n.N, gi = base + i;
     const double gdt = n.pgrv * DT;
     const double rivelv = n.rivelv[i];
@@ -600,11 +612,11 @@ __device__ __forceinline__ void cell_outflow(const Net &n, const State &s, int m
     s.fldout_raw[gi] = fout;
     // D2RIVVEL is observed after the last sub-step; its sub-step average is accumulated here
     // (CMF_DIAG_AVEMAX_ADPSTP, src/cmf_calc_diag_mod.F90:104-161) instead of in phase C
-    const bool first = (c.it == 0), last = (c.it == c.nt - 1);
+    const bool first = (k == 0), last = (k == c.nt - 1);
     if (last) s.rivvel[gi] = rvel;
     if (n.ldiag) {
         double a = first ? rvel * DT : s.a_rivvel[gi] + rvel * DT;
-        if (last) a = a / (c.nadd + DT);
+        if (last) a = a / (nadd_before(k, DT) + DT);
         s.a_rivvel[gi] = a;
     }
 }
@@ -688,11 +700,13 @@ __device__ __forceinline__ void path_outflow(const Net &n, const State &s, int m
 __global__ void __launch_bounds__(kCellThreads, CMF_FLUX_MINB) k_flux(Net n, State s, int ncell_blocks) {
     const int m = blockIdx.y;
     const MemberCtl &c = s.ctl[m];
-    if (c.it >= c.nt) return;
+    const int k = s.loop->k;
+    if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) s.loop->kcur = k;   // for k_rate and k_store
+    if (k >= c.nt) return;
     const double DT = c.dt;
     if ((int)blockIdx.x < ncell_blocks) {
         const int i = blockIdx.x * blockDim.x + threadIdx.x;
-        if (i < n.N) cell_outflow(n, s, m, i, DT, c);
+        if (i < n.N) cell_outflow(n, s, m, i, DT, c, k);
     } else {
         const int p = (blockIdx.x - ncell_blocks) * blockDim.x + threadIdx.x;
         if (p < n.P) path_outflow(n, s, m, p, DT);
@@ -702,10 +716,19 @@ __global__ void __launch_bounds__(kCellThreads, CMF_FLUX_MINB) k_flux(Net n, Sta
 // ------------------------------------------------------------------------------------------
 // phase B: P2STOOUT and D2RATE, src/cmf_calc_outflw_mod.F90:410-451
 // ------------------------------------------------------------------------------------------
-__global__ void k_rate(Net n, State s) {
+// advance != 0: block (0,0) also moves the loop counter to the next sub-step and sets the WHILE
+// condition (every k_flux block has read the counter; k_rate and k_store read `kcur`)
+__global__ void k_rate(Net n, State s, int advance, cudaGraphConditionalHandle h, int use_cond) {
     const int m = blockIdx.y;
     const MemberCtl &c = s.ctl[m];
-    if (c.it >= c.nt) return;
+    const int k = s.loop->kcur;
+    if (advance && blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) {
+        const int kn = k + 1;
+        s.loop->k = kn;
+        s.loop->split = 0;
+        if (use_cond) cudaGraphSetConditional(h, (kn < s.loop->ntmax && kn < kNtCap) ? 1u : 0u);
+    }
+    if (k >= c.nt) return;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n.N) return;
     const double DT = c.dt;
@@ -738,11 +761,13 @@ __device__ __forceinline__ double scaled_pathsum(const Net &n, const double *sum
 __global__ void __launch_bounds__(kCellThreads, CMF_STORE_MINB) k_store(Net n, State s, int ncell_blocks) {
     const int m = blockIdx.y;
     const MemberCtl &c = s.ctl[m];
-    const bool active = c.it < c.nt;
+    const int kk = s.loop->kcur;
+    const bool active = kk < c.nt;
     if (!active) return;   // uniform per block (blockIdx.y), no barrier is skipped divergently
     const double DT = c.dt;
-    const bool first = (c.it == 0);
-    const bool last = (c.it == c.nt - 1);
+    const bool first = (kk == 0);
+    const bool last = (kk == c.nt - 1);
+    const double nadd = last ? nadd_before(kk, DT) : 0.0;   // only the averages of the last sub-step need it
     const size_t base = (size_t)m * n.N;
     if ((int)blockIdx.x >= ncell_blocks) {
         // bifurcation paths: LSPAMAT path rescale (:494-517), CALC_VARS_PRE copy, diagnostics
@@ -761,7 +786,7 @@ __global__ void __launch_bounds__(kCellThreads, CMF_STORE_MINB) k_store(Net n, S
             s.pthflw_pre[o] = f;
             if (n.ldiag) {
                 double a = first ? f * DT : s.a_pthflw[o] + f * DT;
-                if (last) { a = a / (c.nadd + DT); asum = asum + a; }
+                if (last) { a = a / (nadd + DT); asum = asum + a; }
                 s.a_pthflw[o] = a;
             }
         }
@@ -862,7 +887,7 @@ __global__ void __launch_bounds__(kCellThreads, CMF_STORE_MINB) k_store(Net n, S
         }
         // CMF_DIAG_AVEMAX_ADPSTP / GETAVE_ADPSTP, src/cmf_calc_diag_mod.F90:104-221
         if (n.ldiag) {
-            const double na = c.nadd + DT;
+            const double na = nadd + DT;
             auto acc = [&](double *a, double v) {
                 double x = first ? v * DT : a[gi] + v * DT;
                 if (last) x = x / na;
@@ -905,43 +930,27 @@ __global__ void __launch_bounds__(kCellThreads, CMF_STORE_MINB) k_store(Net n, S
 }
 
 // ------------------------------------------------------------------------------------------
-// k_ctl: budgets, sub-step counter and the loop condition
+// k_budget: after the sub-step loop, the budgets of every member's last sub-step
 // ------------------------------------------------------------------------------------------
-// launched with kBudgets warps: warp k reduces budget k of every member that just finished its
-// last sub-step (lanes stride over the block partials in a fixed order, then a fixed warp tree)
-__global__ void k_ctl(Net n, State s, int ncell_blocks, cudaGraphConditionalHandle h, int use_cond) {
+// grid (members, kBudgets), kBudgetThreads threads: block (m, k) reduces budget k of member m over
+// the block partials its last sub-step wrote -- thread t sums partials t, t+T, ... in order, then a
+// fixed warp tree and a fixed tree over the warps: the same sums whatever the timing
+constexpr int kBudgetThreads = 256;
+__global__ void __launch_bounds__(kBudgetThreads) k_budget(Net n, State s, int ncell_blocks) {
+    const int m = blockIdx.x, k = blockIdx.y;
+    if (s.ctl[m].nt < 1) return;                        // refused step (NT cap): no sub-step ran
+    const double *src = s.partials + ((size_t)m * kBudgets + k) * ncell_blocks;
+    double x = 0.0;
+    for (int b = threadIdx.x; b < ncell_blocks; b += kBudgetThreads) x = x + src[b];
+    for (int o = 16; o > 0; o >>= 1) x = x + __shfl_down_sync(0xffffffffu, x, o);
+    __shared__ double w[kBudgetThreads / 32];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (int m = 0; m < n.M; m++) {
-        const MemberCtl &c = s.ctl[m];
-        if (c.it != c.nt - 1 || warp >= kBudgets) continue;   // uniform per warp
-        const double *src = s.partials + ((size_t)m * kBudgets + warp) * ncell_blocks;
-        double x0 = 0.0, x1 = 0.0, x2 = 0.0, x3 = 0.0;
-        int bk = lane;
-        for (; bk + 96 < ncell_blocks; bk += 128) {
-            x0 = x0 + src[bk];
-            x1 = x1 + src[bk + 32];
-            x2 = x2 + src[bk + 64];
-            x3 = x3 + src[bk + 96];
-        }
-        for (; bk < ncell_blocks; bk += 32) x0 = x0 + src[bk];
-        double x = (x0 + x1) + (x2 + x3);
-        for (int o = 16; o > 0; o >>= 1) x = x + __shfl_down_sync(0xffffffffu, x, o);
-        if (lane == 0) s.ctl[m].budget[warp] = x;
-    }
-    __syncthreads();
-    for (int m = threadIdx.x; m < n.M; m += blockDim.x) {
-        MemberCtl &c = s.ctl[m];
-        if (c.it < c.nt) {
-            c.nadd = c.nadd + c.dt;
-            c.it = c.it + 1;
-        }
-    }
+    if (lane == 0) w[warp] = x;
     __syncthreads();
     if (threadIdx.x == 0) {
-        const int k = s.loop->k + 1;
-        s.loop->k = k;
-        s.loop->split = 0;
-        if (use_cond) cudaGraphSetConditional(h, (k < s.loop->ntmax && k < kNtCap) ? 1u : 0u);
+        double t = 0.0;
+        for (int j = 0; j < kBudgetThreads / 32; j++) t = t + w[j];
+        s.ctl[m].budget[k] = t;
     }
 }
 

@@ -185,8 +185,8 @@ int32_t cmf_gpu_ctx_block_size(cmf_gpu_ctx *ctx);
 int cmf_gpu_ctx_counters(cmf_gpu_ctx *ctx, int64_t *member_substeps, int64_t *loop_iters, int64_t *outer_steps);
 /* Measurement helper: runs `reps` outer steps kernel by kernel with CUDA events between kernels
  * on the context's stream (advances the state), timing every sub-step.  ms_out[6] receives the mean
- * duration per launch of the stage/CFL and NT/DT kernels (once per outer step) and of the flux,
- * rate, storage and control kernels (once per sub-step). */
+ * duration per launch of the stage/CFL and NT/DT kernels (once per outer step), of the flux, rate
+ * and storage kernels (once per sub-step) and of the budget kernel (once per outer step). */
 int cmf_gpu_ctx_time_phases(cmf_gpu_ctx *ctx, double dt_def, int32_t reps, double *ms_out);
 
 /* Storage-only restart (LSTOONLY): the stage scheme, then CMF_CALC_OUTPRE
