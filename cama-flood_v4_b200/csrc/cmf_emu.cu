@@ -492,7 +492,8 @@ __global__ void k_emu_update(EmuNet n, const int *active, double dt, const doubl
 // a layer (M=128, N=128 or 16, K=16 per instruction, fp32 accumulator in 128 TMEM columns) and a
 // tcgen05.commit onto an mbarrier; every thread waits on it (bounded), reads its row's accumulator
 // with tcgen05.ld (warp w reads TMEM lanes 32*(w%4).., columns 32*(w/4)..), adds the bias, applies
-// ReLU, rounds to bf16 and stores the next layer's A operand.  The last layer (N=16, column 0
+// ReLU and the bf16 rounding in one cvt and stores the next layer's A operand.  The next tile's X
+// rows are fetched into registers while the current tile's layers run.  The last layer (N=16, column 0
 // real) adds b3 and writes y.  The rounding points equal the layer-by-layer chain (bf16 inputs,
 // fp32 accumulation, bf16 activations); the order of the fp32 additions inside an MMA is the
 // hardware's, so results agree with the mma.sync path to fp32 rounding, not bit for bit.
@@ -594,7 +595,15 @@ __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence:
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 
-// layer epilogue: bias + ReLU + bf16 of this thread's columns of row r into the A operand
+// ReLU and round-to-nearest bf16 of two fp32 values in one instruction (ReLU commutes with the
+// rounding, so this equals rounding max(x, 0)); lo goes to the lower half
+__device__ __forceinline__ uint32_t relu_bf16x2(float lo, float hi) {
+    uint32_t d;
+    asm("cvt.rn.relu.bf16x2.f32 %0, %1, %2;" : "=r"(d) : "f"(hi), "f"(lo));
+    return d;
+}
+
+// layer epilogue: bias + ReLU + bf16 of this thread's columns of row r into the next layer's A operand
 __device__ __forceinline__ void tc_epilogue_hidden(uint32_t tmem_row, int col0, const float *bias, unsigned char *sA, int r) {
 #pragma unroll
     for (int h = 0; h < kTcColsPerThread / 32; h++) {
@@ -607,17 +616,15 @@ __device__ __forceinline__ void tc_epilogue_hidden(uint32_t tmem_row, int col0, 
             uint4 u;
             uint32_t *w = reinterpret_cast<uint32_t *>(&u);
 #pragma unroll
-            for (int j = 0; j < 4; j++) {
-                const float a = fmaxf(__uint_as_float(v[8 * q + 2 * j]) + bias[c + 2 * j], 0.f);
-                const float b = fmaxf(__uint_as_float(v[8 * q + 2 * j + 1]) + bias[c + 2 * j + 1], 0.f);
-                w[j] = pack_bf16x2(a, b);
-            }
+            for (int j = 0; j < 4; j++)
+                w[j] = relu_bf16x2(__uint_as_float(v[8 * q + 2 * j]) + bias[c + 2 * j],
+                                   __uint_as_float(v[8 * q + 2 * j + 1]) + bias[c + 2 * j + 1]);
             *reinterpret_cast<uint4 *>(sA + canon_off(r, c, kTcRows)) = u;
         }
     }
 }
 
-__global__ void __launch_bounds__(kTcThreads, 1) k_mlp_tc(const __nv_bfloat16 *__restrict__ X, int ldx, int rows,
+__global__ void __launch_bounds__(kTcThreads, 2) k_mlp_tc(const __nv_bfloat16 *__restrict__ X, int ldx, int rows,
                                                         const uint4 *__restrict__ wimg, const float *__restrict__ b0,
                                                         const float *__restrict__ b1, const float *__restrict__ b2,
                                                         const float *__restrict__ b3, float *__restrict__ y) {
@@ -654,14 +661,22 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_mlp_tc(const __nv_bfloat16 *_
     uint32_t phase = 0;
     bool failed = false;
     const int ntiles = (rows + kTcRows - 1) / kTcRows;
+    uint4 xnext = make_uint4(0u, 0u, 0u, 0u);                // this thread's X chunk of the first tile
+    {
+        const int row = blockIdx.x * kTcRows + (tid >> 2);
+        if (row < rows) xnext = *reinterpret_cast<const uint4 *>(X + (size_t)row * ldx + (tid & 3) * 8);
+    }
     for (int tile = blockIdx.x; tile < ntiles && !failed; tile += gridDim.x) {
         const int row0 = tile * kTcRows;
-        // X tile -> A operand (k 0..31): 128 rows x 4 chunks of 16 bytes
-        for (int q = tid; q < kTcRows * 4; q += kTcThreads) {
-            const int rr = q >> 2, kc = q & 3;
-            uint4 u = make_uint4(0u, 0u, 0u, 0u);
-            if (row0 + rr < rows) u = *reinterpret_cast<const uint4 *>(X + (size_t)(row0 + rr) * ldx + kc * 8);
-            *reinterpret_cast<uint4 *>(sA + canon_off(rr, kc * 8, kTcRows)) = u;
+        // X tile -> A operand (k 0..31): 128 rows x 4 chunks of 16 bytes, one chunk per thread,
+        // fetched during the previous tile (xnext); then fetch the next tile's chunk
+        static_assert(kTcRows * 4 == kTcThreads, "one X chunk per thread");
+        {
+            const int rr = tid >> 2, kc = tid & 3;
+            *reinterpret_cast<uint4 *>(sA + canon_off(rr, kc * 8, kTcRows)) = xnext;
+            const int nrow = row0 + gridDim.x * kTcRows + rr;
+            xnext = make_uint4(0u, 0u, 0u, 0u);
+            if (nrow < rows) xnext = *reinterpret_cast<const uint4 *>(X + (size_t)nrow * ldx + kc * 8);
         }
         fence_async_smem();
         tc_fence_before();
