@@ -467,9 +467,19 @@ class DeviceForcing:
         self.buf = torch.empty(members, N, dtype=torch.float64, device=device)
         self.torch = torch
 
+    def fill(self, h: int, out) -> None:
+        """Runoff of hour h into `out` ([M, N] device tensor, e.g. a context's runoff view) in one
+        pass: members m = j*K + k take field k, so the product broadcasts over j."""
+        M, N = out.shape
+        K = self.fields.shape[1]
+        if M % K == 0:
+            self.torch.mul(self.fields[h].unsqueeze(0), self.factor.view(M // K, K, 1), out=out.view(M // K, K, N))
+        else:
+            self.torch.mul(self.fields[h].index_select(0, self.idx), self.factor, out=out)
+
     def hour(self, h: int):
         """[M, N] runoff of hour h (device; valid until the next call)."""
-        self.torch.mul(self.fields[h].index_select(0, self.idx), self.factor, out=self.buf)
+        self.fill(h, self.buf)
         return self.buf
 
 
@@ -483,6 +493,9 @@ class ArrayForcing:
 
     def hour(self, h: int):
         return self.t[h]
+
+    def fill(self, h: int, out) -> None:
+        out.copy_(self.t[h])
 
 
 class SurrogateEnsemble:
@@ -521,7 +534,7 @@ class SurrogateEnsemble:
         self.fe.rollout(self._y, self.active, ldy=1, residual=getattr(self.mlp, "residual", True))
 
     def run(self, forcing, hours: int, h0: int = 0):
-        """Advances `hours` coupling steps with forcing.hour(h0 + h) (device [M, N]); returns the
+        """Advances `hours` coupling steps with the runoff forcing.fill(h0 + h, ...) writes; returns the
         hourly mean discharge at the gauges [hours, M, G] (the judged plain value for members
         handed back to the plain solver)."""
         torch = self.torch
@@ -549,9 +562,8 @@ class SurrogateEnsemble:
             if cur_plain != self.plain:
                 self.active.copy_(torch.tensor([0 if m in self.plain else 1 for m in range(self.M)], dtype=torch.int32))
                 cur_plain = set(self.plain)
-            r = forcing.hour(h0 + h)
-            emu_runoff.copy_(r)
-            jr = r.index_select(0, slot_idx)
+            forcing.fill(h0 + h, emu_runoff)                   # straight into the emulator's runoff input
+            jr = emu_runoff.index_select(0, slot_idx)
             torch.cuda.current_stream(self.fe.dev).synchronize()
             self.judge.advance_device(1, jr.data_ptr(), 0)
             self.emu_step()
