@@ -591,3 +591,41 @@ class SurrogateEnsemble:
                             self.stats["fallback"] += 1
                     check(self.lib.cmf_gpu_ctx_copy_member(self.emu.h, m, self.judge.h, k), "copy_member")
         return out
+
+
+def time_inference(rows: int, reps: int = 5, device: int = 0) -> dict:
+    """CUDA-event timing of the fused inference kernels on `rows` random feature rows (seeded
+    weights): the tcgen05 kernel and the mma.sync kernel, ms per call and TFLOP/s."""
+    import torch
+
+    dev = torch.device("cuda", device)
+    mlp = MLP(dev, seed=2)
+    g = torch.Generator(device=dev).manual_seed(1)
+    X = (torch.randn(rows, IN, device=dev, generator=g) * 2).to(torch.bfloat16)
+    X[:, NFEAT:] = 0
+    out = {"rows": rows}
+    flops = 2.0 * rows * (32 * HID + HID * HID * 2 + HID * 8)
+    for name, fn in (("tcgen05", mlp.infer_tc), ("mma_sync", mlp.infer)):
+        y = fn(X)
+        torch.cuda.synchronize()
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+        ev[0].record()
+        for _ in range(reps):
+            fn(X, y)
+        ev[1].record()
+        torch.cuda.synchronize()
+        ms = ev[0].elapsed_time(ev[1]) / reps
+        out[name] = {"ms": ms, "tflops": flops / (ms * 1e-3) / 1e12}
+    out["tcgen05_status"] = _emu_lib().cmf_emu_mlp_tc_status()
+    return out
+
+
+if __name__ == "__main__":
+    import argparse
+    import json
+
+    ap = argparse.ArgumentParser(description="time the fused emulator inference kernels")
+    ap.add_argument("--time-mlp", type=int, default=2 * 1024 * 1024, metavar="ROWS")
+    ap.add_argument("--reps", type=int, default=5)
+    a = ap.parse_args()
+    print(json.dumps(time_inference(a.time_mlp, a.reps)))
