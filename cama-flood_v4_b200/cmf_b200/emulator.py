@@ -420,9 +420,12 @@ def discharge_weights(X):
     return torch.exp(0.5 * (X[:, 11].float() + 3.0))
 
 
-def train(mlp: MLP, X, t, iters: int, batch: int, seed: int = 0, lr_max: float | None = None, weights=None):
+def train(mlp: MLP, X, t, iters: int, batch: int, seed: int = 0, lr_max: float | None = None, weights=None,
+          noise: float = 0.0):
     """Adam with cosine-decayed learning rate on random mini-batches of the trajectory rows (drawn
-    uniformly, or with probability proportional to `weights`)."""
+    uniformly, or with probability proportional to `weights`); `noise` > 0 adds Gaussian noise of
+    that standard deviation to the used feature columns of every batch (robustness to the
+    emulator's own drift during rollouts)."""
     import torch
 
     g = torch.Generator(device=X.device).manual_seed(seed)
@@ -439,7 +442,11 @@ def train(mlp: MLP, X, t, iters: int, batch: int, seed: int = 0, lr_max: float |
         else:
             u = torch.rand(batch, device=X.device, dtype=torch.float64, generator=g) * cdf[-1]
             idx = torch.clamp(torch.searchsorted(cdf, u), max=S - 1)
-        loss = mlp.loss_and_grad(X[idx].contiguous(), t[idx].contiguous(), batch)
+        xb = X[idx].contiguous()
+        if noise > 0.0:
+            xb[:, :NFEAT] = (xb[:, :NFEAT].float() + noise * torch.randn(batch, NFEAT, device=X.device, generator=g)
+                             ).to(torch.bfloat16)
+        loss = mlp.loss_and_grad(xb, t[idx].contiguous(), batch)
         mlp.adam()
         if it % 50 == 0 or it == iters - 1:
             hist.append((it, float(loss)))

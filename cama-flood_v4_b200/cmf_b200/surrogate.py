@@ -17,7 +17,7 @@ from . import emulator as E
 
 
 def measure(host, device, members: int = 256, days: int = 2, judge_slots: int = 2, train_members: int = 8,
-            train_hours: int = 96, train_iters: int = 6000, train_batch: int = 16384,
+            train_hours: int = 96, train_iters: int = 6000, train_batch: int = 16384, train_noise: float = 0.02,
             cells_per_snapshot: int | None = 65536, seed: int = 100, gauges: int = 100, tol_rel: float = 0.05,
             spinup: int = 24) -> dict:
     import torch
@@ -31,7 +31,8 @@ def measure(host, device, members: int = 256, days: int = 2, judge_slots: int = 
                                    cells_per_snapshot=cells_per_snapshot, residual=False)
     mlp = E.MLP(device, seed=0, lr=2e-3)
     mlp.residual = False
-    hist = E.train(mlp, X, t, iters=train_iters, batch=train_batch, seed=0, weights=E.discharge_weights(X))
+    hist = E.train(mlp, X, t, iters=train_iters, batch=train_batch, seed=0, weights=E.discharge_weights(X),
+                   noise=train_noise)
     torch.cuda.synchronize()
     train_s = time.perf_counter() - t0
     del X, t
@@ -116,7 +117,7 @@ def measure(host, device, members: int = 256, days: int = 2, judge_slots: int = 
         "judge_errors": [round(e, 4) for e in ens_stats["errors"]],
         "train_loss_first_last": [hist[0][1], hist[-1][1]], "train_seconds": train_s,
         "training": f"{train_members} members x {train_hours} h of solver trajectories, {train_iters} Adam steps "
-                    f"of {train_batch} rows",
+                    f"of {train_batch} rows, feature noise {train_noise}",
         "features_ms": feat_ms, "mlp_fused_ms": mlp_ms, "mlp_rows": rows, "mlp_kernel": "tcgen05 (tensor memory)",
         "mlp_tflops": flops / (mlp_ms * 1e-3) / 1e12 if mlp_ms > 0 else None,
         "mlp_mma_sync_ms": mlp_ms_mma_sync,
