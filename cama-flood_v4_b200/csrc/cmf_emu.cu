@@ -369,6 +369,39 @@ __device__ __forceinline__ float fslog(float x) {
     return copysignf(a < 1e-3f ? a * (1.f - 0.5f * a) : __logf(1.f + a), x);
 }
 
+// two hops in one pass: out1[i] = sum over upstream j of in[j]; out2[i] = sum over upstream j of
+// (sum over upstream k of j of in[k]) -- the same fp32 sums, in the same ascending order, as two
+// single-hop passes.  The first pair reads the fp64 last-step outflow and runoff directly (the
+// single-hop chain converts them to fp32 planes first: the same values).
+template <bool FromState>
+__global__ void k_emu_hop2(EmuNet n, const float *__restrict__ in_a, const float *__restrict__ in_b,
+                           const double *__restrict__ qa, const double *__restrict__ qb, float *o1a, float *o1b,
+                           float *o2a, float *o2b) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n.N) return;
+    const size_t mo = (size_t)blockIdx.y * n.N;
+    auto va = [&](int j) { return FromState ? (float)qa[mo + j] : in_a[mo + j]; };
+    auto vb = [&](int j) { return FromState ? (float)qb[mo + j] : in_b[mo + j]; };
+    float a1 = 0.f, b1 = 0.f, a2 = 0.f, b2 = 0.f;
+    for (int k = n.up_ptr[i]; k < n.up_ptr[i + 1]; k++) {
+        const int j = n.up_idx[k];
+        a1 += va(j);
+        b1 += vb(j);
+        float sa = 0.f, sb = 0.f;
+        for (int q = n.up_ptr[j]; q < n.up_ptr[j + 1]; q++) {
+            const int g = n.up_idx[q];
+            sa += va(g);
+            sb += vb(g);
+        }
+        a2 += sa;
+        b2 += sb;
+    }
+    o1a[mo + i] = a1;
+    o1b[mo + i] = b1;
+    o2a[mo + i] = a2;
+    o2b[mo + i] = b2;
+}
+
 // Manning discharge of a rectangular section of area A, hydraulic depth h and friction slope s
 __device__ __forceinline__ float manning_q(float area, float h, float s, float inv_man) {
     if (!(area > 0.f) || !(h > 0.f)) return 0.f;
@@ -856,10 +889,20 @@ int cmf_emu_features(const cmf_emu_net *net, const cmf_emu_member *mb, int nmemb
     cudaStream_t st = (cudaStream_t)stream;
     const dim3 blocks((n.N + 255) / 256, nmembers);
     const size_t plane = (size_t)nmembers * n.N;
-    k_emu_seed<<<blocks, 256, 0, st>>>(n, mb->qprev, mb->runoff, planes, planes + plane);
-    for (int h = 0; h < hops; h++)
-        k_emu_hop<<<blocks, 256, 0, st>>>(n, planes + (size_t)(2 * h) * plane, planes + (size_t)(2 * h + 1) * plane,
-                                          planes + (size_t)(2 * h + 2) * plane, planes + (size_t)(2 * h + 3) * plane);
+    auto pl = [&](int k) { return planes + (size_t)k * plane; };   // hop h: planes 2h+2 (outflow), 2h+3 (runoff)
+    int h = 0;
+    if (hops >= 2) {
+        k_emu_hop2<true><<<blocks, 256, 0, st>>>(n, nullptr, nullptr, mb->qprev, mb->runoff, pl(2), pl(3), pl(4), pl(5));
+        h = 2;
+    } else if (hops == 1) {
+        k_emu_seed<<<blocks, 256, 0, st>>>(n, mb->qprev, mb->runoff, pl(0), pl(1));
+        k_emu_hop<<<blocks, 256, 0, st>>>(n, pl(0), pl(1), pl(2), pl(3));
+        h = 1;
+    }
+    for (; h + 2 <= hops; h += 2)
+        k_emu_hop2<false><<<blocks, 256, 0, st>>>(n, pl(2 * h), pl(2 * h + 1), nullptr, nullptr, pl(2 * h + 2),
+                                                  pl(2 * h + 3), pl(2 * h + 4), pl(2 * h + 5));
+    if (h < hops) k_emu_hop<<<blocks, 256, 0, st>>>(n, pl(2 * h), pl(2 * h + 1), pl(2 * h + 2), pl(2 * h + 3));
     k_emu_assemble<<<blocks, 256, 0, st>>>(n, mb->rivsto, mb->fldsto, mb->levsto, mb->rivdph, mb->flddph, mb->fldfrc,
                                            mb->qprev, mb->runoff, planes, plane, hops, (__nv_bfloat16 *)X, ldx,
                                            rows_per_member);

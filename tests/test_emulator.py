@@ -165,6 +165,67 @@ def test_tcgen05_inference_matches_mma_sync_and_reference(R):
     assert np.allclose(a[:2048], ref[:, 0], rtol=2e-2, atol=2e-2 * float(np.abs(ref[:, 0]).max()))
 
 
+def _raw_i32(ptr, n, dev):
+    import torch
+
+    class _CAI:
+        def __init__(self):
+            self.__cuda_array_interface__ = {"shape": (n,), "typestr": "<i4", "data": (ptr, False), "version": 3}
+
+    return torch.as_tensor(_CAI(), device=dev)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("hops", [1, 2, 5, 8])
+def test_message_planes_equal_upstream_sums(case_dirs, hops):
+    """E2: hop h of the message passing is the fp32 sum, in the upstream-matrix order, of hop h-1 over
+    each cell's upstream cells (hop 0 = last-step outflow and runoff rounded to fp32) -- bit for bit,
+    whether the kernels take the hops one or two at a time; unused hop columns of X stay zero."""
+    import ctypes as C
+
+    import torch
+
+    from cmf_b200 import HostModel, PhysicsGPU
+    from cmf_b200 import emulator as E
+
+    h = HostModel(case_dirs["cfg1s"])
+    M, N = 3, h.dims.nseqall
+    p = PhysicsGPU(h, nmembers=M)
+    gr = h.map("grarea")
+    gens = E.runoff_generators(N, M, 3)
+    for _ in range(3):
+        p.put_runoff(E.runoff_step(gens, gr))
+        p.advance()
+    fe = E.Features(p, E.qref_from_host(h))
+    dev = fe.dev
+    planes = torch.full((2 * (hops + 1) * M * N,), float("nan"), dtype=torch.float32, device=dev)
+    X = torch.zeros(M * fe.Np, E.IN, dtype=torch.bfloat16, device=dev)
+    p.synchronize()
+    E.echeck(fe.lib.cmf_emu_features(C.byref(fe.net), C.byref(fe.mb), M, X.data_ptr(), E.IN, fe.Np, hops,
+                                     planes.data_ptr(), torch.cuda.current_stream(dev).cuda_stream), "features")
+    torch.cuda.synchronize()
+    up_ptr = _raw_i32(fe.net.up_ptr, N + 1, dev).cpu().numpy()
+    up_idx = _raw_i32(fe.net.up_idx, int(up_ptr[-1]), dev).cpu().numpy()
+    rows = np.repeat(np.arange(N), np.diff(up_ptr))
+    got = planes.cpu().numpy().reshape(2 * (hops + 1), M, N)
+    cur = [fe.qprev().cpu().numpy().astype(np.float32), fe.runoff_view().cpu().numpy().astype(np.float32)]
+    assert np.any(cur[0]) and np.any(cur[1])
+    for k in range(hops):
+        nxt = []
+        for v in cur:
+            out = np.zeros_like(v)
+            for m in range(M):
+                np.add.at(out[m], rows, v[m, up_idx])      # in order: ascending cell, then matrix order
+            nxt.append(out)
+        cur = nxt
+        for c in (0, 1):
+            assert np.array_equal(got[2 * k + 2 + c].view(np.int32), cur[c].view(np.int32)), (k, c)
+    x = X.float().cpu().numpy().reshape(M, fe.Np, E.IN)[:, :N]
+    assert not np.any(x[:, :, 14 + 2 * hops:30])
+    assert np.all(np.isfinite(x[:, :, :32]))
+    p.close()
+
+
 @pytest.mark.gpu
 def test_trained_emulator_beats_untrained_and_persistence(case_dirs):
     """E1-E5 on the config-1 laws: train on solver trajectories, then roll out 24 h from a plain
