@@ -1,4 +1,5 @@
-"""Builds libcmf_b200.so in-tree (sm_100a device code + the host model core).
+"""Builds libcmf_b200.so in-tree (sm_100a device code + the host model core) and libcmf_synth.so
+(host loops of the synthetic-case generator).
 
     python cama-flood_v4_b200/build.py            # build if sources changed
     python cama-flood_v4_b200/build.py --force
@@ -20,6 +21,10 @@ INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 
 SOURCES = ["cmf_engine.cu", "cmf_emu.cu", "cmf_host.cpp"]
 HEADERS = ["cmf_kernels.cuh"]
+SYNTH_LIB = os.path.join(LIBDIR, "libcmf_synth.so")
+SYNTH_SOURCE = "cmf_synth.cpp"
+# the generator's loops must round like numpy's element-wise operations: no contraction
+SYNTH_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-shared", "-ffp-contract=off", "-fno-fast-math"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
@@ -44,7 +49,21 @@ def _stale() -> bool:
     return any(os.path.getmtime(d) > t for d in deps)
 
 
+def build_synth(force: bool = False, verbose: bool = False) -> str:
+    src = os.path.join(CSRC, SYNTH_SOURCE)
+    deps = [src, __file__]
+    if not force and os.path.exists(SYNTH_LIB) and all(os.path.getmtime(d) <= os.path.getmtime(SYNTH_LIB) for d in deps):
+        return SYNTH_LIB
+    os.makedirs(LIBDIR, exist_ok=True)
+    cmd = ["g++", *SYNTH_FLAGS, "-o", SYNTH_LIB, src]
+    if verbose:
+        print(" ".join(cmd))
+    subprocess.run(cmd, check=True)
+    return SYNTH_LIB
+
+
 def build(force: bool = False, verbose: bool = False) -> str:
+    build_synth(force, verbose)
     if not force and not _stale():
         return LIB
     os.makedirs(LIBDIR, exist_ok=True)

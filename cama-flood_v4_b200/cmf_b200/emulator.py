@@ -476,13 +476,14 @@ class DeviceForcing:
 
     def fill(self, h: int, out) -> None:
         """Runoff of hour h into `out` ([M, N] device tensor, e.g. a context's runoff view) in one
-        pass: members m = j*K + k take field k, so the product broadcasts over j."""
+        pass: members m = j*K + k take field k, so the product broadcasts over j.  `out` may hold
+        the first M members of the ensemble only (M <= members)."""
         M, N = out.shape
         K = self.fields.shape[1]
-        if M % K == 0:
+        if M == self.factor.shape[0] and M % K == 0:
             self.torch.mul(self.fields[h].unsqueeze(0), self.factor.view(M // K, K, 1), out=out.view(M // K, K, N))
         else:
-            self.torch.mul(self.fields[h].index_select(0, self.idx), self.factor, out=out)
+            self.torch.mul(self.fields[h].index_select(0, self.idx[:M]), self.factor[:M], out=out)
 
     def hour(self, h: int):
         """[M, N] runoff of hour h (device; valid until the next call)."""

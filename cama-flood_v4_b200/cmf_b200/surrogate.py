@@ -19,7 +19,7 @@ from . import emulator as E
 def measure(host, device, members: int = 256, days: int = 2, judge_slots: int = 2, train_members: int = 8,
             train_hours: int = 96, train_iters: int = 6000, train_batch: int = 16384, train_noise: float = 0.02,
             cells_per_snapshot: int | None = 65536, seed: int = 100, gauges: int = 100, tol_rel: float = 0.05,
-            spinup: int = 24) -> dict:
+            spinup: int = 24, forcing_distinct: int = 8) -> dict:
     import torch
 
     from .model import PhysicsGPU
@@ -42,7 +42,7 @@ def measure(host, device, members: int = 256, days: int = 2, judge_slots: int = 
     G = river[np.argsort(-qref[river])][:gauges]
     Gt = torch.as_tensor(G, device=device)
     H = days * 24
-    forcing = E.DeviceForcing(host, members, spinup + H, seed + 1, device)
+    forcing = E.DeviceForcing(host, members, spinup + H, seed + 1, device, distinct=forcing_distinct)
     plain = PhysicsGPU(host, nmembers=members)
     pview = E.Features(plain, qref)                   # views only (gauge gather)
     stream = torch.cuda.current_stream(device)
@@ -118,6 +118,7 @@ def measure(host, device, members: int = 256, days: int = 2, judge_slots: int = 
         "train_loss_first_last": [hist[0][1], hist[-1][1]], "train_seconds": train_s,
         "training": f"{train_members} members x {train_hours} h of solver trajectories, {train_iters} Adam steps "
                     f"of {train_batch} rows, feature noise {train_noise}",
+        "forcing": f"{forcing_distinct} distinct hourly AR(1)-gamma fields, member factor lognormal(0, 0.3)",
         "features_ms": feat_ms, "mlp_fused_ms": mlp_ms, "mlp_rows": rows, "mlp_kernel": "tcgen05 (tensor memory)",
         "mlp_tflops": flops / (mlp_ms * 1e-3) / 1e12 if mlp_ms > 0 else None,
         "mlp_mma_sync_ms": mlp_ms_mma_sync,

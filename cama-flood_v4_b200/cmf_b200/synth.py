@@ -124,12 +124,81 @@ def _mouths(spec: CaseSpec, land: np.ndarray, rng: np.random.Generator) -> np.nd
     return mouths
 
 
+_SYNTH_LIB = None
+
+
+def _native():
+    """The generator's sequential loops in C++ (lib/libcmf_synth.so, built by build.py)."""
+    global _SYNTH_LIB
+    if _SYNTH_LIB is None:
+        import ctypes as C
+
+        path = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "lib", "libcmf_synth.so")
+        if not os.path.exists(path):
+            raise RuntimeError(f"{path} is missing: run cama-flood_v4_b200/build.py")
+        lib = C.CDLL(path)
+        P = C.c_void_p
+        lib.cmf_synth_grow_forest.argtypes = [C.c_int32, C.c_int32, P, P, C.c_int64, P, C.c_int64, P, P]
+        lib.cmf_synth_grow_forest.restype = C.c_int64
+        lib.cmf_synth_accumulate.argtypes = [C.c_int64, P, P, P]
+        lib.cmf_synth_accumulate.restype = None
+        lib.cmf_synth_elevation.argtypes = [C.c_int64, P, P, P, P, P]
+        lib.cmf_synth_elevation.restype = None
+        _SYNTH_LIB = lib
+    return _SYNTH_LIB
+
+
+def _ptr(a: np.ndarray) -> int:
+    assert a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data
+
+
 def _grow_forest(land: np.ndarray, mouths: np.ndarray, rng: np.random.Generator):
     """Randomised priority-first growth from the mouths over land (8-neighbour D8 tree).
 
     Returns (down, order): ``down`` holds the flat downstream index (-1 for mouths, -2 for
-    ocean or unreached) and ``order`` lists land cells parent-first.
-    """
+    ocean or unreached) and ``order`` lists land cells parent-first.  Native loop; the same
+    search as `_grow_forest_py` (identical output)."""
+    ny, nx = land.shape
+    ncell = nx * ny
+    landf = np.ascontiguousarray(land.ravel(), dtype=np.uint8)
+    mflat = np.ascontiguousarray(np.nonzero(mouths.ravel())[0], dtype=np.int64)
+    costs = rng.random(ncell * 8 + 16) + 0.05
+    down = np.empty(ncell, dtype=np.int64)
+    order = np.empty(ncell, dtype=np.int64)
+    n = _native().cmf_synth_grow_forest(nx, ny, _ptr(landf), _ptr(mflat), mflat.size, _ptr(costs), costs.size,
+                                        _ptr(down), _ptr(order))
+    if n < 0:
+        raise RuntimeError("cmf_synth_grow_forest: bad arguments")
+    return down, order[:n].copy()
+
+
+def _accumulate(order: np.ndarray, down: np.ndarray, upa: np.ndarray) -> None:
+    """upa[down[c]] += upa[c] in reverse visiting order (native; as `_accumulate_py`)."""
+    _native().cmf_synth_accumulate(order.size, _ptr(order), _ptr(down), _ptr(upa))
+
+
+def _elevation(order: np.ndarray, down: np.ndarray, slope: np.ndarray, length: np.ndarray, elev: np.ndarray) -> None:
+    """elev[c] = elev[down[c]] + slope[c] * length[c] in visiting order (native; as `_elevation_py`)."""
+    _native().cmf_synth_elevation(order.size, _ptr(order), _ptr(down), _ptr(slope), _ptr(length), _ptr(elev))
+
+
+def _accumulate_py(order, down, upa) -> None:
+    for c in order[::-1]:
+        d = down[c]
+        if d >= 0:
+            upa[d] += upa[c]
+
+
+def _elevation_py(order, down, slope, length, elev) -> None:
+    for c in order:
+        d = down[c]
+        if d >= 0:
+            elev[c] = elev[d] + slope[c] * length[c]
+
+
+def _grow_forest_py(land: np.ndarray, mouths: np.ndarray, rng: np.random.Generator):
+    """Python statement of the forest growth (the check of the native loop)."""
     ny, nx = land.shape
     ncell = nx * ny
     down = np.full(ncell, -2, dtype=np.int64)
@@ -210,20 +279,14 @@ def make_case(spec: CaseSpec) -> Case:
     ctmare[reached] = 2.25e8 * rng.lognormal(0.0, 0.2, size=int(reached.sum()))
     ctm32 = ctmare.astype(np.float32).astype(np.float64)
     upa = ctm32.copy()
-    for c in order[::-1]:
-        d = down[c]
-        if d >= 0:
-            upa[d] += upa[c]
+    _accumulate(order, down, upa)
     upa_km2 = upa * 1e-6
     rivlen = np.zeros(ncell)
     rivlen[reached] = 15000.0 * rng.lognormal(0.0, 0.5, size=int(reached.sum()))
     rivlen32 = rivlen.astype(np.float32).astype(np.float64)
     slope = rng.uniform(1e-5, 1e-3, size=ncell)
     elev = np.zeros(ncell)
-    for c in order:
-        d = down[c]
-        if d >= 0:
-            elev[c] = elev[d] + slope[c] * rivlen32[c]
+    _elevation(order, down, slope, rivlen32, elev)
     rivwth = np.where(reached, 5.0 * np.sqrt(upa_km2), 0.0)
     rivhgt = np.where(reached, 0.3 * np.power(np.maximum(upa_km2, 1e-12), 0.4) * spec.rivhgt_scale, 0.0)
     rivman = np.where(reached, 0.03, 0.0)
@@ -534,3 +597,17 @@ def spec_config2(n_domains: int = 8, n_min: int = 50_000, n_max: int = 2_000_000
         specs.append(sp)
     return specs
 
+
+
+def spec_config4(seed: int = 4, scale: float = 1.0) -> CaseSpec:
+    """7200x3600 grid, ~6M land cells (config-1 laws), 100k bifurcation channels x 5 levels, levees
+    on 10% of cells, 10k dams, hourly forcing.  ``scale`` shrinks the grid (and the channel and dam
+    counts with its area) for parity-size runs."""
+    nx = max(16, int(round(7200 * scale)))
+    ny = max(8, int(round(3600 * scale)))
+    frac = 6_000_000.0 / (7200 * 3600)
+    return CaseSpec(name="cfg4" if scale == 1.0 else f"cfg4s{scale:g}", nx=nx, ny=ny, land_frac=frac,
+                    mouth_prob=0.1, seed=seed, lpthout=True,
+                    npthout=max(4, int(round(100_000 * scale * scale))), npthlev=5,
+                    llevee=True, levee_frac=0.10, ldamout=True,
+                    ndam=max(2, int(round(10_000 * scale * scale))), dt=3600.0, ifrq_inp=1)

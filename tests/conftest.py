@@ -26,8 +26,9 @@ CASES = {
     "cfg0": lambda: synth.spec_config0(seed=0),
     "cfg1s": lambda: synth.spec_config1(seed=1, scale=0.1),
     "stress": lambda: _stress_spec(),
+    "cfg4s": lambda: synth.spec_config4(seed=4, scale=0.1),     # config-4 laws at 720x360
 }
-RUNOFF_SCALE = {"cfg0": 1.0, "cfg1s": 1.0, "stress": 40.0}
+RUNOFF_SCALE = {"cfg0": 1.0, "cfg1s": 1.0, "stress": 40.0, "cfg4s": 1.0}
 
 
 def _stress_spec():

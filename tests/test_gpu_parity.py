@@ -50,7 +50,7 @@ def _compare_state(g, o, tag, member=0, extra=()):
     assert not msgs, "; ".join(msgs)
 
 
-@pytest.mark.parametrize("name,nsteps,hourly", [("cfg0", 24 * 3, False), ("cfg1s", 48, True)])
+@pytest.mark.parametrize("name,nsteps,hourly", [("cfg0", 24 * 3, False), ("cfg1s", 48, True), ("cfg4s", 24, True)])
 def test_parity_vs_oracle(case_dirs, name, nsteps, hourly):
     """Free-running parity on the configured geometry laws (realistic flows)."""
     h, g, o = _models(case_dirs[name])
