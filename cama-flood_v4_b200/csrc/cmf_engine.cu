@@ -537,6 +537,33 @@ cmf_gpu_ctx *g_default = nullptr;
 extern "C" {
 
 int cmf_gpu_abi_version(void) { return CMF_GPU_ABI_VERSION; }
+
+namespace {
+__global__ void k_depth_powers(const double *x, int n, double *p73, double *p43) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    p73[i] = cmf::pow_depth<7>(x[i]);
+    p43[i] = cmf::pow_depth<4>(x[i]);
+}
+}  // namespace
+
+int cmf_gpu_depth_powers(const double *x, int32_t n, double *p73, double *p43) {
+    if (!x || n < 0) return set_err(CMF_E_ARG, "cmf_gpu_depth_powers: null input or negative count");
+    if (n == 0) return CMF_OK;
+    double *d = nullptr;
+    const size_t bytes = (size_t)n * sizeof(double);
+    CUDA_TRY(cudaMalloc(&d, 3 * bytes));
+    cudaError_t e = cudaMemcpy(d, x, bytes, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+        k_depth_powers<<<(unsigned)((n + 255) / 256), 256>>>(d, n, d + n, d + 2 * (size_t)n);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess && p73) e = cudaMemcpy(p73, d + n, bytes, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && p43) e = cudaMemcpy(p43, d + 2 * (size_t)n, bytes, cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    if (e != cudaSuccess) return set_err(CMF_E_CUDA, std::string("cmf_gpu_depth_powers: ") + cudaGetErrorString(e));
+    return CMF_OK;
+}
 const char *cmf_gpu_last_error(void) { return g_last_error.c_str(); }
 
 const char *cmf_gpu_strerror(int status) {

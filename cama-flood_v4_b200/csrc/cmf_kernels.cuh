@@ -16,8 +16,9 @@
 // phase is one kernel and the phases are ordered by the graph.
 //
 // Arithmetic follows the reference statement by statement, compiled with -fmad=false so no
-// multiply-add is fused: x**(-1) is 1/x, x**2 is x*x, x**0.5 is an IEEE square root and every other
-// non-integral power is pow().  Default-real literals of the reference are promoted float values
+// multiply-add is fused: x**(-1) is 1/x, x**2 is x*x, x**0.5 is an IEEE square root, the depth
+// powers of the flux formulas are correctly rounded (pow_depth) and every other non-integral power
+// is pow().  Default-real literals of the reference are promoted float values
 // (F(...) below).  All gathers sum in the reference's loop order (ascending upstream sequence);
 // there are no atomics on state, so results are independent of block size and timing.
 #pragma once
@@ -122,6 +123,44 @@ struct State {
 
 __device__ __forceinline__ double dmax(double a, double b) { return (a > b) ? a : b; }
 __device__ __forceinline__ double dmin(double a, double b) { return (a < b) ? a : b; }
+
+// x**(-7._JPRB/3._JPRB) and x**(-4._JPRB/3._JPRB) of the local-inertial flux formulas
+// (src/cmf_calc_outflw_mod.F90:74,106,133,162; src/cmf_calc_pthout_mod.F90:67;
+// src/cmf_ctrl_levee_mod.F90:553,573): pow(x, y) for the
+// doubles y nearest -7/3 and -4/3, correctly rounded, for the positive depths these formulas take.
+// The exponent is y = -K/3 + d with d its rounding offset (d = -0x1.5555555555555p-53 for K = 7,
+// +0x1.5555555555555p-54 for K = 4), so x^y = (x^(-1/3))^K * x^d:
+//   c0 = rcbrt(x); one Newton step for the inverse cube root, c = c0 (1 + r/3), r = 1 - x c0^3,
+//     with c0^3 formed exactly by Dekker's FMA products (c carried as a double-double);
+//   c^K in double-double (Dekker products; relative error about 2^-100);
+//   x^d = 1 + d ln x to first order (|d ln x| < 3e-15, so ln x to single precision suffices).
+// The sum is rounded once.  Outside (1e-300, 1e300) the general pow is used.
+struct DD {
+    double hi, lo;
+};
+__device__ __forceinline__ DD dd_mul(DD a, DD b) {
+    const double p = a.hi * b.hi;
+    double e = fma(a.hi, b.hi, -p);
+    e = e + (a.hi * b.lo + a.lo * b.hi);
+    return {p, e};
+}
+template <int K>
+__device__ __forceinline__ double pow_depth(double x) {
+    static_assert(K == 7 || K == 4, "exponents -7/3 and -4/3 only");
+    constexpr double y = -(double)K / 3.0;
+    constexpr double d = (K == 7) ? -0x1.5555555555555p-53 : 0x1.5555555555555p-54;
+    if (!(x > 1e-300 && x < 1e300)) return pow(x, y);
+    const double c0 = rcbrt(x);
+    const double p2 = c0 * c0, e2 = fma(c0, c0, -p2);
+    const double p3 = p2 * c0, e3 = fma(p2, c0, -p3);
+    const double t = fma(x, p3, -1.0);
+    const double r = -(t + x * (e3 + e2 * c0));
+    const DD c = {c0, c0 * (r * (1.0 / 3.0))};
+    const DD c2 = dd_mul(c, c), c4 = dd_mul(c2, c2);
+    const DD v = (K == 7) ? dd_mul(dd_mul(c4, c2), c) : c4;
+    const double corr = v.hi * (d * (double)logf((float)x));
+    return v.hi + (v.lo + corr);
+}
 
 // ------------------------------------------------------------------------------------------
 // stage schemes (one cell)
@@ -474,7 +513,7 @@ __device__ __forceinline__ void cell_outflow(const Net &n, const State &s, int m
             const double dflw_im = dmax(sqrt(dflw * dflw_pr), 1.E-6);
             const double dout_pr = s.rivout_pre[gi] * (1.0 / wth);
             const double dout = (wth * (dout_pr + (gdt * dflw_im) * dslp))
-                              * (1.0 / (1.0 + ((gdt * (man * man)) * fabs(dout_pr)) * pow(dflw_im, -7.0 / 3.0)));
+                              * (1.0 / (1.0 + ((gdt * (man * man)) * fabs(dout_pr)) * pow_depth<7>(dflw_im)));
             const double dvel = rivout_old * (1.0 / dare);
             const bool mask = (dflw_im > CMF_F(1.E-5) && dare > CMF_F(1.E-5));
             rout = mask ? dout : 0.0;
@@ -495,7 +534,7 @@ __device__ __forceinline__ void cell_outflow(const Net &n, const State &s, int m
             const double dare_im = dmax(sqrt(dare * dare_pr), 1.E-6);
             const double dout_pr = s.fldout_pre[gi];
             const double dout = (dout_pr + (gdt * dare_im) * dslp)
-                * (1.0 / (1.0 + (((gdt * (n.pmanfld * n.pmanfld)) * fabs(dout_pr)) * pow(dflw_im, -4.0 / 3.0)) * (1.0 / dare_im)));
+                * (1.0 / (1.0 + (((gdt * (n.pmanfld * n.pmanfld)) * fabs(dout_pr)) * pow_depth<4>(dflw_im)) * (1.0 / dare_im)));
             const bool mask = (dflw_im > 1.E-5 && dare > 1.E-5);
             fout = mask ? dout : 0.0;
             if (!(fout * rout > 0.0)) fout = 0.0;
@@ -514,7 +553,7 @@ __device__ __forceinline__ void cell_outflow(const Net &n, const State &s, int m
             const double dflw_im = dmax(sqrt(rivdph * rivdph_pre), 1.E-6);
             const double dout_pr = s.rivout_pre[gi] * (1.0 / wth);
             const double dout = (wth * (dout_pr + (gdt * dflw_im) * dslp))
-                              * (1.0 / (1.0 + ((gdt * (man * man)) * fabs(dout_pr)) * pow(dflw_im, -7.0 / 3.0)));
+                              * (1.0 / (1.0 + ((gdt * (man * man)) * fabs(dout_pr)) * pow_depth<7>(dflw_im)));
             const double dvel = rivout_old * (1.0 / dare);
             const bool mask = (dflw_im > CMF_F(1.E-5) && dare > CMF_F(1.E-5));
             rout = mask ? dout : 0.0;
@@ -532,7 +571,7 @@ __device__ __forceinline__ void cell_outflow(const Net &n, const State &s, int m
             const double dare_im = dmax(sqrt(dare * dare_pr), 1.E-6);
             const double dout_pr = s.fldout_pre[gi];
             const double dout = (dout_pr + (gdt * dare_im) * dslp)
-                * (1.0 / (1.0 + (((gdt * (n.pmanfld * n.pmanfld)) * fabs(dout_pr)) * pow(dflw_im, -4.0 / 3.0)) * (1.0 / dare_im)));
+                * (1.0 / (1.0 + (((gdt * (n.pmanfld * n.pmanfld)) * fabs(dout_pr)) * pow_depth<4>(dflw_im)) * (1.0 / dare_im)));
             const bool mask = (dflw_im > CMF_F(1.E-5) && dare > CMF_F(1.E-5));
             fout = mask ? dout : 0.0;
             if (!(fout * rout > 0.0)) fout = 0.0;
@@ -625,7 +664,7 @@ __device__ __forceinline__ void cell_outflow(const Net &n, const State &s, int m
 __device__ __forceinline__ double path_flux(double wth, double pre, double gdt, double dflw_im, double dslp, double man,
                                            bool recip) {
     const double dout_pr = recip ? pre * (1.0 / wth) : pre / wth;
-    return (wth * (dout_pr + (gdt * dflw_im) * dslp)) / (1.0 + ((gdt * (man * man)) * fabs(dout_pr)) * pow(dflw_im, -7.0 / 3.0));
+    return (wth * (dout_pr + (gdt * dflw_im) * dslp)) / (1.0 + ((gdt * (man * man)) * fabs(dout_pr)) * pow_depth<7>(dflw_im));
 }
 
 __device__ __forceinline__ void path_outflow(const Net &n, const State &s, int m, int p, double DT) {

@@ -345,6 +345,11 @@ void cmf_gpu_finalize(void);
 const char *cmf_gpu_strerror(int status);
 const char *cmf_gpu_last_error(void);
 int cmf_gpu_abi_version(void);
+/* Diagnostic: evaluates on the current device the two depth powers of the flux formulas,
+ * x**(-7._JPRB/3._JPRB) and x**(-4._JPRB/3._JPRB) (src/cmf_calc_outflw_mod.F90:74,106), exactly as
+ * the sub-step kernels do, for n host values x; results into host arrays p73 and p43 (either may
+ * be NULL).  Synchronous; allocates its own scratch. */
+int cmf_gpu_depth_powers(const double *x, int32_t n, double *p73, double *p43);
 
 /* ======================================================================================== */
 /* Host model core: the reference's CMF_DRV_INIT for a stand-alone (non-Fortran) host        */

@@ -182,3 +182,35 @@ def test_no_cpu_fallback_without_device(monkeypatch):
 
     lib = _abi.load()
     assert lib.cmf_gpu_physics_advance(3600.0, None, None, None) == -3   # no context: CMF_E_STATE
+
+
+def test_depth_powers_correctly_rounded():
+    """The flux formulas' DFLW_im**(-7._JPRB/3._JPRB) and **(-4._JPRB/3._JPRB) on the device equal
+    pow(x, y) correctly rounded (60-digit decimal reference) for depths from 1e-6 m to 2 km and
+    around 1; glibc's pow (the oracle's) differs from them by at most 1 ulp, rarely."""
+    import ctypes as C
+    from decimal import Decimal, localcontext
+
+    from cmf_b200 import _abi
+
+    import ctypes.util
+
+    lib = _abi.load()
+    lib.cmf_gpu_depth_powers.argtypes = [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p]
+    libm = C.CDLL(ctypes.util.find_library("m"))
+    libm.pow.restype = C.c_double
+    libm.pow.argtypes = [C.c_double, C.c_double]
+    rng = np.random.default_rng(0)
+    x = np.concatenate([np.exp(rng.uniform(np.log(1e-6), np.log(2e3), 4000)), 1.0 + rng.uniform(-1e-3, 1e-3, 500),
+                        [1e-6, 1.0000000000000002e-6, 1e-5, 0.5, 1.0, 2.0, 8.0, 27.0, 1e3]])
+    p73, p43 = np.empty_like(x), np.empty_like(x)
+    assert lib.cmf_gpu_depth_powers(x.ctypes.data, x.size, p73.ctypes.data, p43.ctypes.data) == 0
+    for got, y in ((p73, -7.0 / 3.0), (p43, -4.0 / 3.0)):
+        with localcontext() as ctx:
+            ctx.prec = 60
+            ref = np.array([float(Decimal(float(v)) ** Decimal(y)) for v in x])
+        bad = np.nonzero(got != ref)[0]
+        assert bad.size == 0, (y, x[bad[:5]], got[bad[:5]], ref[bad[:5]])
+        glibc = np.array([libm.pow(float(v), y) for v in x])      # the oracle's pow (numpy has its own)
+        ulps = np.abs(got.view(np.int64) - glibc.view(np.int64))
+        assert ulps.max() <= 1 and np.mean(ulps) < 0.01, (y, ulps.max(), np.mean(ulps))
