@@ -49,6 +49,7 @@ struct cmf_gpu_ctx {
     std::vector<void *> allocs;
     int block = 256;
     int ncell_blocks = 0, npath_blocks = 0;
+    bool small_cells = false;   // N x M <= kSmallCellMembers: the low-spill profile of k_flux/k_store
     int nlev = 0, ndam_placed = 0;
     size_t E = 0;
     // graph
@@ -334,13 +335,29 @@ void set_blocks(cmf_gpu_ctx *c, int block) {
     c->npath_blocks = c->net.P > 0 ? (c->net.P + block - 1) / block : 0;
 }
 
+// phase A and phase C in the context's occupancy profile
+void launch_flux(cmf_gpu_ctx *c, dim3 grid, int block) {
+    if (c->small_cells)
+        cmf::k_flux<cmf::kFluxMinBlocksSmall><<<grid, block, 0, c->stream>>>(c->net, c->st, c->ncell_blocks);
+    else
+        cmf::k_flux<cmf::kFluxMinBlocksWide><<<grid, block, 0, c->stream>>>(c->net, c->st, c->ncell_blocks);
+}
+void launch_store(cmf_gpu_ctx *c, dim3 grid, int block) {
+    if (c->small_cells)
+        cmf::k_store<cmf::kStoreMinBlocksSmall><<<grid, block, cmf::store_smem(block), c->stream>>>(c->net, c->st,
+                                                                                                   c->ncell_blocks);
+    else
+        cmf::k_store<cmf::kStoreMinBlocksWide><<<grid, block, cmf::store_smem(block), c->stream>>>(c->net, c->st,
+                                                                                                  c->ncell_blocks);
+}
+
 // Enqueue one sub-step (phases A, B, C and the control kernel).
 void enqueue_substep(cmf_gpu_ctx *c, int use_cond, cudaGraphConditionalHandle cond) {
     const dim3 gc(c->ncell_blocks, c->dims.nmembers);
     const dim3 gcp(c->ncell_blocks + c->npath_blocks, c->dims.nmembers);
-    cmf::k_flux<<<gcp, c->block, 0, c->stream>>>(c->net, c->st, c->ncell_blocks);
+    launch_flux(c, gcp, c->block);
     cmf::k_rate<<<gc, c->block, 0, c->stream>>>(c->net, c->st, 1, cond, use_cond);
-    cmf::k_store<<<gcp, c->block, cmf::store_smem(c->block), c->stream>>>(c->net, c->st, c->ncell_blocks);
+    launch_store(c, gcp, c->block);
 }
 void enqueue_substep(cmf_gpu_ctx *c, int use_cond) { enqueue_substep(c, use_cond, c->cond); }
 
@@ -453,9 +470,9 @@ int autotune(cmf_gpu_ctx *c) {
         float tot = 0.f;
         for (int rep = 0; rep < 4; rep++) {
             CUDA_TRY(cudaEventRecord(e0, c->stream));
-            cmf::k_flux<<<gcp, b, 0, c->stream>>>(c->net, c->st, c->ncell_blocks);
+            launch_flux(c, gcp, b);
             cmf::k_rate<<<gc, b, 0, c->stream>>>(c->net, c->st, 0, c->cond, 0);
-            cmf::k_store<<<gcp, b, cmf::store_smem(b), c->stream>>>(c->net, c->st, c->ncell_blocks);
+            launch_store(c, gcp, b);
             CUDA_TRY(cudaEventRecord(e1, c->stream));
             CUDA_TRY(cudaEventSynchronize(e1));
             float ms = 0.f;
@@ -609,6 +626,7 @@ int cmf_gpu_create(const cmf_dims *dims, const cmf_params *params, const cmf_map
         return fail(set_err(CMF_E_CUDA, "cudaStreamCreate failed"));
     if ((rc = build_net(c, maps))) return fail(rc);
     if ((rc = alloc_state(c))) return fail(rc);
+    c->small_cells = (size_t)dims->nseqall * (size_t)dims->nmembers <= cmf::kSmallCellMembers;
     if (opts->block_size > 0) {
         if (opts->block_size % 32 || opts->block_size > cmf::kCellThreads || opts->block_size < 64)
             return fail(set_err(CMF_E_ARG, "block_size must be a multiple of 32 in [64, 256]"));
@@ -722,11 +740,11 @@ int cmf_gpu_ctx_time_phases(cmf_gpu_ctx *c, double dt_def, int32_t reps, double 
         if ((rc = need(3 * (size_t)nt + 2))) break;
         CUDA_TRY(cudaEventRecord(ev[0], c->stream));
         for (int k = 0; k < nt; k++) {
-            cmf::k_flux<<<gcp, c->block, 0, c->stream>>>(c->net, c->st, c->ncell_blocks);
+            launch_flux(c, gcp, c->block);
             CUDA_TRY(cudaEventRecord(ev[3 * k + 1], c->stream));
             cmf::k_rate<<<gc, c->block, 0, c->stream>>>(c->net, c->st, 1, c->cond, 0);
             CUDA_TRY(cudaEventRecord(ev[3 * k + 2], c->stream));
-            cmf::k_store<<<gcp, c->block, cmf::store_smem(c->block), c->stream>>>(c->net, c->st, c->ncell_blocks);
+            launch_store(c, gcp, c->block);
             CUDA_TRY(cudaEventRecord(ev[3 * k + 3], c->stream));
         }
         enqueue_epilogue(c);

@@ -30,14 +30,15 @@
 namespace cmf {
 
 // Occupancy of the latency-bound cell kernels: at most kCellThreads threads per block and the
-// minimum resident blocks per SM (caps registers at 65536 / (threads x blocks)); measured on
-// 16 config-1 members, more resident warps beat the few spills this costs.
-#ifndef CMF_FLUX_MINB
-#define CMF_FLUX_MINB 6
-#endif
-#ifndef CMF_STORE_MINB
-#define CMF_STORE_MINB 5
-#endif
+// minimum resident blocks per SM (caps registers at 65536 / (threads x blocks)).  k_flux and
+// k_store come in two profiles, chosen per context by its cell-members (the engine's
+// `small_cells`): with many cell-members in flight more resident warps beat the spills they cost
+// (16 config-1 members: 22.2 ms per coupling step vs 24.4 ms with the small profile), while a
+// grid of about a wave or less runs best with fewer spills (one config-1 member: 2.04 vs 2.10 ms).
+// Both profiles execute the same arithmetic; only the register allocation differs.
+constexpr int kFluxMinBlocksWide = 6, kStoreMinBlocksWide = 5;
+constexpr int kFluxMinBlocksSmall = 5, kStoreMinBlocksSmall = 4;
+constexpr size_t kSmallCellMembers = size_t(1) << 19;   // cell-members up to which `small` applies
 #ifndef CMF_STAGE_MINB
 #define CMF_STAGE_MINB 6
 #endif
@@ -736,7 +737,8 @@ __device__ __forceinline__ void path_outflow(const Net &n, const State &s, int m
     s.pthsum_raw[(size_t)m * P + p] = sum;
 }
 
-__global__ void __launch_bounds__(kCellThreads, CMF_FLUX_MINB) k_flux(Net n, State s, int ncell_blocks) {
+template <int MinBlocks>
+__global__ void __launch_bounds__(kCellThreads, MinBlocks) k_flux(Net n, State s, int ncell_blocks) {
     const int m = blockIdx.y;
     const MemberCtl &c = s.ctl[m];
     const int k = s.loop->k;
@@ -797,7 +799,8 @@ __device__ __forceinline__ double scaled_pathsum(const Net &n, const double *sum
     return v >= 0.0 ? v * rate_m[n.pth_up[p]] : v * rate_m[n.pth_dn[p]];
 }
 
-__global__ void __launch_bounds__(kCellThreads, CMF_STORE_MINB) k_store(Net n, State s, int ncell_blocks) {
+template <int MinBlocks>
+__global__ void __launch_bounds__(kCellThreads, MinBlocks) k_store(Net n, State s, int ncell_blocks) {
     const int m = blockIdx.y;
     const MemberCtl &c = s.ctl[m];
     const int kk = s.loop->kcur;
