@@ -269,7 +269,6 @@ def gpu_arm(args) -> int:
 
     # ---- timed region: device-resident
     c0 = g.counters()
-    l0 = g.kernel_launches
     evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(K)]
     if ws > 1:
         dist.barrier()
@@ -557,7 +556,7 @@ def cfg4_arm(args) -> int:
                 cur.synchronize()
                 ctx.advance_device(1, None, 0)
             ctx.synchronize()
-            c0, l0 = ctx.counters(), ctx.kernel_launches
+            c0 = ctx.counters()
             ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(K)]
             for k in range(K):
                 forcing.fill(spin + W + k, v)
