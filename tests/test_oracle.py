@@ -55,10 +55,10 @@ def test_budget_identity_closes(case_dirs):
     (documented ~1e-10 km3 per step, doc/Note_HighPerformanceComputing.docx)."""
     from oracle import Oracle
 
-    for name in ("cfg0", "cfg1s"):
+    for name, steps in (("cfg0", 48), ("cfg1s", 48), ("cfg4s", 24)):
         o = Oracle(case_dirs[name])
         gr = o.d("grarea")
-        for r in runoff_series(gr, name, 48, hourly=(name == "cfg1s")):
+        for r in runoff_series(gr, name, steps, hourly=(name != "cfg0")):
             o.put_runoff(r)
             o.advance()
             b = o.budget()
