@@ -327,10 +327,24 @@ def runoff_step(gens, gr, scale: float = 1.0) -> np.ndarray:
     return np.stack([np.maximum((g.next().astype(np.float64) * scale * gr) / 86400000.0, 0.0) for g in gens])
 
 
+def snapshot_cells(rng: np.random.Generator, N: int, k: int, weights: np.ndarray | None = None) -> np.ndarray:
+    """min(k, N) distinct cells of N: uniformly (one `rng.choice` without replacement), or, with
+    `weights`, a weighted draw without replacement by Efraimidis-Spirakis keys (the k largest
+    log(u)/w; cells of weight 0 only when fewer than k cells weigh more)."""
+    k = min(k, N)
+    if weights is None:
+        return rng.choice(N, size=k, replace=False)
+    w = np.asarray(weights, dtype=np.float64)
+    with np.errstate(divide="ignore"):
+        keys = np.log(rng.random(N)) / w
+    return np.argpartition(-keys, k - 1)[:k]
+
+
 def generate_trajectories(host, members: int, hours: int, spinup: int, seed: int, cells_per_snapshot: int | None = None,
-                          residual: bool = True):
+                          residual: bool = True, cell_weights: np.ndarray | None = None):
     """E1: the plain GPU solver advances `members` members (different runoff seeds); returns feature
-    rows X [S, 64] (bf16) and targets t [S] (fp32)."""
+    rows X [S, 64] (bf16) and targets t [S] (fp32).  With `cells_per_snapshot`, each (hour, member)
+    snapshot keeps that many cells, drawn uniformly or in proportion to `cell_weights` [N]."""
     import torch
 
     from .model import PhysicsGPU
@@ -354,7 +368,7 @@ def generate_trajectories(host, members: int, hours: int, spinup: int, seed: int
         q1 = fe.qprev()                                                          # mean outflow over the step
         t = (residual_target(torch, q1, q0, fe.qref[None, :]) if residual else target_transform(torch, q1, fe.qref[None, :])).float()
         for m in range(members):
-            idx = np.arange(N) if cells_per_snapshot is None else rng.choice(N, size=min(cells_per_snapshot, N), replace=False)
+            idx = np.arange(N) if cells_per_snapshot is None else snapshot_cells(rng, N, cells_per_snapshot, cell_weights)
             it = torch.as_tensor(idx, device=fe.dev)
             Xs.append(X[m * fe.Np + it])
             ts.append(t[m][it])

@@ -19,7 +19,7 @@ from . import emulator as E
 def measure(host, device, members: int = 256, days: int = 2, judge_slots: int = 2, train_members: int = 8,
             train_hours: int = 96, train_iters: int = 6000, train_batch: int = 16384, train_noise: float = 0.02,
             cells_per_snapshot: int | None = 65536, seed: int = 100, gauges: int = 100, tol_rel: float = 0.05,
-            spinup: int = 24, forcing_distinct: int = 8) -> dict:
+            spinup: int = 24, forcing_distinct: int = 8, snapshot_weighting: str = "uniform") -> dict:
     import torch
 
     from .model import PhysicsGPU
@@ -27,8 +27,13 @@ def measure(host, device, members: int = 256, days: int = 2, judge_slots: int = 
     t0 = time.perf_counter()
     # the network predicts the step's transformed outflow itself (not its change), trained on rows
     # drawn with probability proportional to sqrt(discharge scale) so that large rivers are seen
+    # snapshot cells: uniform, or "discharge" -- in proportion to sqrt(discharge scale), so that the
+    # largest rivers of a multi-million-cell domain are in the training rows at all
+    if snapshot_weighting not in ("uniform", "discharge"):
+        raise ValueError(f"snapshot_weighting must be 'uniform' or 'discharge', not {snapshot_weighting!r}")
+    cw = np.sqrt(E.qref_from_host(host)) if snapshot_weighting == "discharge" else None
     X, t = E.generate_trajectories(host, members=train_members, hours=train_hours, spinup=12, seed=seed,
-                                   cells_per_snapshot=cells_per_snapshot, residual=False)
+                                   cells_per_snapshot=cells_per_snapshot, residual=False, cell_weights=cw)
     mlp = E.MLP(device, seed=0, lr=2e-3)
     mlp.residual = False
     hist = E.train(mlp, X, t, iters=train_iters, batch=train_batch, seed=0, weights=E.discharge_weights(X),
@@ -119,6 +124,7 @@ def measure(host, device, members: int = 256, days: int = 2, judge_slots: int = 
         "training": f"{train_members} members x {train_hours} h of solver trajectories, {train_iters} Adam steps "
                     f"of {train_batch} rows, feature noise {train_noise}",
         "forcing": f"{forcing_distinct} distinct hourly AR(1)-gamma fields, member factor lognormal(0, 0.3)",
+        "snapshot_weighting": snapshot_weighting,
         "features_ms": feat_ms, "mlp_fused_ms": mlp_ms, "mlp_rows": rows, "mlp_kernel": "tcgen05 (tensor memory)",
         "mlp_tflops": flops / (mlp_ms * 1e-3) / 1e12 if mlp_ms > 0 else None,
         "mlp_mma_sync_ms": mlp_ms_mma_sync,

@@ -314,3 +314,29 @@ def test_surrogate_controller_judges_resyncs_and_hands_back(case_dirs):
     truth = np.stack(truth)
     for m in sorted(ens.plain)[:2]:
         assert np.allclose(out[24:, m], truth[24:, m], rtol=1e-9, atol=1e-9)
+
+
+def test_snapshot_cells_uniform_and_weighted():
+    """Uniform snapshots are the plain draw without replacement (same generator calls as before the
+    helper); weighted snapshots are distinct, of the requested size, include the heavy cells, never
+    pick weight-0 cells while enough others remain, and follow the weights in frequency."""
+    from cmf_b200.emulator import snapshot_cells
+
+    N, k = 5000, 300
+    a = snapshot_cells(np.random.default_rng(3), N, k)
+    b = np.random.default_rng(3).choice(N, size=k, replace=False)
+    assert np.array_equal(a, b)
+    assert snapshot_cells(np.random.default_rng(0), 10, 50).size == 10
+    w = np.ones(N)
+    w[:20] = 1e6                        # 20 very heavy cells
+    w[100:200] = 0.0                    # never needed
+    hits = np.zeros(N)
+    rng = np.random.default_rng(1)
+    for _ in range(200):
+        idx = snapshot_cells(rng, N, k, w)
+        assert idx.size == k and np.unique(idx).size == k
+        assert not np.any((idx >= 100) & (idx < 200))
+        assert np.all(np.isin(np.arange(20), idx))
+        hits[idx] += 1
+    light = hits[np.r_[20:100, 200:N]] / 200.0
+    assert abs(light.mean() - (k - 20) / (N - 120)) < 0.005
