@@ -352,7 +352,8 @@ def gpu_arm(args) -> int:
 
         try:
             sur = surrogate.measure(h, dev, members=args.sur_members, days=args.sur_days,
-                                    snapshot_weighting=args.sur_snapshots)
+                                    snapshot_weighting=args.sur_snapshots,
+                                    trajectory_forcing=args.sur_traj_forcing or None)
         except Exception as e:       # reported, never silently replaced by another number
             sur = {"error": f"{type(e).__name__}: {e}"}
     out = 0
@@ -592,7 +593,8 @@ def cfg4_arm(args) -> int:
 
         try:
             sur = surrogate.measure(h, dev, members=Mmax, days=args.sur_days, forcing_distinct=2,
-                                    snapshot_weighting=args.sur_snapshots)
+                                    snapshot_weighting=args.sur_snapshots,
+                                    trajectory_forcing=args.sur_traj_forcing or None)
         except Exception as e:       # reported, never silently replaced by another number
             sur = {"error": f"{type(e).__name__}: {e}"}
     line = {
@@ -632,6 +634,8 @@ def main() -> int:
     ap.add_argument("--sur-days", type=int, default=2)
     ap.add_argument("--sur-snapshots", default="uniform", choices=["uniform", "discharge"],
                     help="training snapshot cells: uniform, or in proportion to sqrt(discharge scale)")
+    ap.add_argument("--sur-traj-forcing", type=int, default=0,
+                    help="K > 0: build the training trajectories' forcing on the device from K distinct fields")
     ap.add_argument("--launch-mode", type=int, default=0, choices=[0, 1],
                     help="0: CUDA graph with a device-side sub-step loop; 1: the same kernels as plain "
                          "launches from a host loop (what ncu can profile kernel by kernel)")

@@ -341,10 +341,14 @@ def snapshot_cells(rng: np.random.Generator, N: int, k: int, weights: np.ndarray
 
 
 def generate_trajectories(host, members: int, hours: int, spinup: int, seed: int, cells_per_snapshot: int | None = None,
-                          residual: bool = True, cell_weights: np.ndarray | None = None):
+                          residual: bool = True, cell_weights: np.ndarray | None = None,
+                          device_forcing: int | None = None):
     """E1: the plain GPU solver advances `members` members (different runoff seeds); returns feature
     rows X [S, 64] (bf16) and targets t [S] (fp32).  With `cells_per_snapshot`, each (hour, member)
-    snapshot keeps that many cells, drawn uniformly or in proportion to `cell_weights` [N]."""
+    snapshot keeps that many cells, drawn uniformly or in proportion to `cell_weights` [N].
+    Forcing: an independent host-generated AR(1)-gamma field per member (default), or, with
+    `device_forcing` = K, a `DeviceForcing` of K distinct fields built in HBM straight into the
+    context's runoff input (for large domains, where host generation dominates)."""
     import torch
 
     from .model import PhysicsGPU
@@ -352,19 +356,39 @@ def generate_trajectories(host, members: int, hours: int, spinup: int, seed: int
     phys = PhysicsGPU(host, nmembers=members)
     N = phys.N
     gr = host.map("grarea")
-    gens = runoff_generators(N, members, seed)
-    for _ in range(spinup):
-        phys.put_runoff(runoff_step(gens, gr))
-        phys.advance()
-    fe = Features(phys, qref_from_host(host))
+    if device_forcing:
+        fe = Features(phys, qref_from_host(host))
+        fo = DeviceForcing(host, members, spinup + hours, seed, fe.dev, distinct=device_forcing)
+        runv = fe.runoff_view()
+
+        def put(h):
+            fo.fill(h, runv)
+            torch.cuda.current_stream(fe.dev).synchronize()
+
+        def advance():
+            phys.advance_device(1, None, 0)            # runoff already in the context's input array
+            phys.synchronize()
+    else:
+        gens = runoff_generators(N, members, seed)
+
+        def put(h):
+            phys.put_runoff(runoff_step(gens, gr))
+
+        def advance():
+            phys.advance()
+    for h in range(spinup):
+        put(h)
+        advance()
+    if not device_forcing:
+        fe = Features(phys, qref_from_host(host))
     rng = np.random.default_rng(seed)
     Xs, ts = [], []
-    for _ in range(hours):
-        phys.put_runoff(runoff_step(gens, gr))
+    for h in range(hours):
+        put(spinup + h)
         X = fe.build().clone()                        # state at the start of the step + its runoff
         q0 = fe.qprev()
         torch.cuda.current_stream(fe.dev).synchronize()
-        phys.advance()
+        advance()
         q1 = fe.qprev()                                                          # mean outflow over the step
         t = (residual_target(torch, q1, q0, fe.qref[None, :]) if residual else target_transform(torch, q1, fe.qref[None, :])).float()
         for m in range(members):

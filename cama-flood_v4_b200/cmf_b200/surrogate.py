@@ -19,7 +19,8 @@ from . import emulator as E
 def measure(host, device, members: int = 256, days: int = 2, judge_slots: int = 2, train_members: int = 8,
             train_hours: int = 96, train_iters: int = 6000, train_batch: int = 16384, train_noise: float = 0.02,
             cells_per_snapshot: int | None = 65536, seed: int = 100, gauges: int = 100, tol_rel: float = 0.05,
-            spinup: int = 24, forcing_distinct: int = 8, snapshot_weighting: str = "uniform") -> dict:
+            spinup: int = 24, forcing_distinct: int = 8, snapshot_weighting: str = "uniform",
+            trajectory_forcing: int | None = None) -> dict:
     import torch
 
     from .model import PhysicsGPU
@@ -33,7 +34,8 @@ def measure(host, device, members: int = 256, days: int = 2, judge_slots: int = 
         raise ValueError(f"snapshot_weighting must be 'uniform' or 'discharge', not {snapshot_weighting!r}")
     cw = np.sqrt(E.qref_from_host(host)) if snapshot_weighting == "discharge" else None
     X, t = E.generate_trajectories(host, members=train_members, hours=train_hours, spinup=12, seed=seed,
-                                   cells_per_snapshot=cells_per_snapshot, residual=False, cell_weights=cw)
+                                   cells_per_snapshot=cells_per_snapshot, residual=False, cell_weights=cw,
+                                   device_forcing=trajectory_forcing)
     mlp = E.MLP(device, seed=0, lr=2e-3)
     mlp.residual = False
     hist = E.train(mlp, X, t, iters=train_iters, batch=train_batch, seed=0, weights=E.discharge_weights(X),
@@ -125,6 +127,8 @@ def measure(host, device, members: int = 256, days: int = 2, judge_slots: int = 
                     f"of {train_batch} rows, feature noise {train_noise}",
         "forcing": f"{forcing_distinct} distinct hourly AR(1)-gamma fields, member factor lognormal(0, 0.3)",
         "snapshot_weighting": snapshot_weighting,
+        "trajectory_forcing": (f"{trajectory_forcing} distinct fields built on the device" if trajectory_forcing
+                               else "host AR(1)-gamma field per member"),
         "features_ms": feat_ms, "mlp_fused_ms": mlp_ms, "mlp_rows": rows, "mlp_kernel": "tcgen05 (tensor memory)",
         "mlp_tflops": flops / (mlp_ms * 1e-3) / 1e12 if mlp_ms > 0 else None,
         "mlp_mma_sync_ms": mlp_ms_mma_sync,
