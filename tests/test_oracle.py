@@ -208,3 +208,226 @@ def test_oracle_serial_and_openmp_agree(case_dirs):
         assert a.advance() == b.advance()
     for f in ("rivsto", "fldsto", "rivout", "fldout", "levsto", "damsto"):
         assert np.array_equal(a.d(f).view(np.int64), b.d(f).view(np.int64)), f
+
+
+def _set_oracle_array(o, name, values):
+    """Writes into the oracle's own array (test access to its state)."""
+    import ctypes as C
+
+    n = C.c_int(0)
+    p = o.lib.orc_darray(o.h, name.encode(), C.byref(n))
+    assert n.value == len(values)
+    np.ctypeslib.as_array(p, shape=(n.value,))[:] = values
+
+
+def test_fldstg_def_known_answers_at_layer_boundaries(case_dirs):
+    """CMF_CALC_FLDSTG_DEF (src/cmf_calc_fldstg_mod.F90:21-110) restated here independently in
+    Python floats (left-to-right operation order, `**0.5` through libm pow as the reference) and
+    compared bit for bit with the oracle on storages at zero, exactly at and one ulp above the bank
+    (RIVSTOMAX), exactly on every layer boundary (the DO WHILE compares with `>`, so a storage equal
+    to FLDSTOMAX(I) stays in layer I), midway between boundaries, one ulp above and well beyond the
+    top layer (the saturated branch)."""
+    import math
+
+    from oracle import Oracle
+
+    o = Oracle(case_dirs["cfg0"])                       # no levee: the default stage scheme
+    N = o.d("rivsto").size
+    L = 10
+    smax, gr, ln, wth, elv = o.d("rivstomax"), o.d("grarea"), o.d("rivlen"), o.d("rivwth"), o.d("rivelv")
+    fsm, grd = o.d("fldstomax").reshape(L, N), o.d("fldgrd").reshape(L, N)
+    ncase = 2 * L + 5
+    tot = np.empty(N)
+    for i in range(N):
+        c = i % ncase
+        if c == 0:
+            v = 0.0
+        elif c == 1:
+            v = smax[i]
+        elif c == 2:
+            v = np.nextafter(smax[i], np.inf)
+        elif c == 3:
+            v = 1.5 * fsm[L - 1, i]
+        elif c == 4:
+            v = np.nextafter(fsm[L - 1, i], np.inf)
+        elif c < 5 + L:
+            v = fsm[c - 5, i]
+        else:
+            k = c - 5 - L
+            v = 0.5 * (fsm[k, i] + (fsm[k + 1, i] if k + 1 < L else 2.0 * fsm[L - 1, i]))
+        tot[i] = v
+    _set_oracle_array(o, "rivsto", tot)
+    _set_oracle_array(o, "fldsto", np.zeros(N))
+    o.physics_fldstg()
+    dfrcinc = 1.0 / 10.0
+    exp = {k: np.empty(N) for k in ("rivsto", "fldsto", "rivdph", "flddph", "fldfrc", "fldare", "sfcelv", "storge")}
+    for i in range(N):
+        psto = float(tot[i]) + 0.0
+        if psto > smax[i]:
+            I, dsto_fil, dwth_fil, ddph_fil = 1, float(smax[i]), float(wth[i]), 0.0
+            dwth_inc = float(gr[i]) / float(ln[i]) * dfrcinc
+            while psto > fsm[I - 1, i] and I <= L:
+                dsto_fil = float(fsm[I - 1, i])
+                dwth_fil = dwth_fil + dwth_inc
+                ddph_fil = ddph_fil + float(grd[I - 1, i]) * dwth_inc
+                I += 1
+                if I > L:
+                    break
+            dsto_add = psto - dsto_fil
+            if I > L:
+                dwth_add = 0.0
+                flddph = ddph_fil + dsto_add / dwth_fil / float(ln[i])
+            else:
+                g = float(grd[I - 1, i])
+                dwth_add = -dwth_fil + (dwth_fil * dwth_fil + 2.0 * dsto_add / float(ln[i]) / g) ** 0.5
+                flddph = ddph_fil + g * dwth_add
+            rivsto = min(float(smax[i]) + float(ln[i]) * float(wth[i]) * flddph, psto)
+            rivdph = rivsto / float(ln[i]) / float(wth[i])
+            fldsto = max(psto - rivsto, 0.0)
+            fldfrc = min(max((-float(wth[i]) + dwth_fil + dwth_add) / (dwth_inc * L), 0.0), 1.0)
+            fldare = float(gr[i]) * fldfrc
+        else:
+            rivsto, fldsto, flddph, fldfrc, fldare = psto, 0.0, 0.0, 0.0, 0.0
+            rivdph = max(psto / float(ln[i]) / float(wth[i]), 0.0)
+        for k, v in (("rivsto", rivsto), ("fldsto", fldsto), ("rivdph", rivdph), ("flddph", flddph),
+                     ("fldfrc", fldfrc), ("fldare", fldare), ("sfcelv", float(elv[i]) + rivdph),
+                     ("storge", rivsto + fldsto)):
+            exp[k][i] = v
+    assert math.isfinite(float(np.sum(exp["flddph"])))
+    for k, v in exp.items():
+        got = o.d(k)
+        bad = np.nonzero(got.view(np.int64) != v.view(np.int64))[0]
+        assert bad.size == 0, (k, bad[:5], got[bad[:5]], v[bad[:5]], [int(b) % ncase for b in bad[:5]])
+    # every branch was taken: in bank, each layer, saturated
+    layer = np.sum(tot[None, :] > fsm, axis=0)
+    assert np.any(tot <= smax) and np.all(np.isin(np.arange(L + 1), layer[tot > smax]))
+
+
+def _levee_stage_ref(psto, i, a, L):
+    """CMF_LEVEE_FLDSTG for one cell (src/cmf_ctrl_levee_mod.F90:271-490), Python floats."""
+    f = lambda k: float(a[k][i])                              # noqa: E731
+    fsm = lambda I: float(a["fsm"][I - 1, i])                 # noqa: E731
+    grd = lambda I: float(a["grd"][I - 1, i])                 # noqa: E731
+    fhg = lambda I: float(a["fhg"][I - 1, i])                 # noqa: E731
+    smax, ln, wth, gr = f("rivstomax"), f("rivlen"), f("rivwth"), f("grarea")
+    lbas, ltop, lfil = f("levbassto"), f("levtopsto"), f("levfilsto")
+    lhgt, lfrc, bash, ldst = f("levhgt"), f("levfrc"), f("bashgt"), f("levdst")
+    dsto = psto
+    winc = gr / ln * (1.0 / 10.0)
+    clamp = lambda x: min(max(x, 0.0), 1.0)                   # noqa: E731
+
+    def scan():
+        I, fil, wfil, dfil = 1, smax, wth, 0.0
+        while dsto > fsm(I) and I <= L:
+            fil = fsm(I)
+            wfil = wfil + winc
+            dfil = dfil + grd(I) * winc
+            I += 1
+            if I > L:
+                break
+        add = dsto - fil
+        if I <= L:
+            wadd = -wfil + (wfil * wfil + 2.0 * add / ln / grd(I)) ** 0.5
+            return wfil, wadd, dfil + grd(I) * wadd
+        return wfil, 0.0, dfil + add / wfil / ln
+
+    if not dsto > smax:                                       # case 0
+        return dict(rivsto=psto, fldsto=0.0, levsto=0.0, rivdph=max(dsto / ln / wth, 0.0), flddph=0.0,
+                    fldfrc=0.0, fldare=0.0, levdph=0.0)
+    if dsto < lbas:                                           # case 1
+        wfil, wadd, fdph = scan()
+        rs = smax + ln * wth * fdph
+        frc = clamp((-wth + wfil + wadd) / (winc * L))
+        return dict(rivsto=rs, fldsto=max(psto - rs, 0.0), levsto=0.0, rivdph=rs / ln / wth, flddph=fdph,
+                    fldfrc=frc, fldare=gr * frc, levdph=0.0)
+    if dsto < ltop:                                           # case 2
+        fdph = bash + (dsto - lbas) / (ldst + wth) / ln
+        rs = smax + ln * wth * fdph
+        return dict(rivsto=rs, fldsto=max(psto - rs, 0.0), levsto=0.0, rivdph=rs / ln / wth, flddph=fdph,
+                    fldfrc=lfrc, fldare=gr * lfrc, levdph=0.0)
+    if dsto < lfil:                                           # case 3
+        fdph = lhgt
+        rs = smax + ln * wth * fdph
+        fs = max(ltop - rs, 0.0)
+        ls = max(psto - rs - fs, 0.0)
+        I = int(lfrc * L) + 1
+        fil, wfil, dfil = ltop, 0.0, 0.0
+        while I <= L:
+            add = (ldst + wth) * (lhgt - fhg(I)) * ln
+            if dsto < fsm(I) + add:
+                break
+            fil = fsm(I) + add
+            wfil = winc * I - ldst
+            dfil = fhg(I) - bash
+            I += 1
+            if I > L:
+                break
+        add = dsto - fil
+        if I <= L:
+            wadd = -wfil + (wfil * wfil + 2.0 * add / ln / grd(I)) ** 0.5
+            ldph = bash + dfil + wadd * grd(I)
+            frc = clamp((wfil + ldst) / (winc * L))
+        else:
+            ldph = bash + dfil + add / wfil / ln
+            frc = 1.0
+        return dict(rivsto=rs, fldsto=fs, levsto=ls, rivdph=rs / ln / wth, flddph=fdph, fldfrc=frc,
+                    fldare=gr * frc, levdph=ldph)
+    wfil, wadd, fdph = scan()                                 # case 4
+    frc = (-wth + wfil + wadd) / (winc * L)
+    rs = smax + ln * wth * fdph
+    fs = max(ltop + (fdph - lhgt) * (ldst + wth) * ln - rs, 0.0)
+    return dict(rivsto=rs, fldsto=fs, levsto=max(psto - rs - fs, 0.0), rivdph=rs / ln / wth, flddph=fdph,
+                fldfrc=frc, fldare=gr * frc, levdph=fdph)
+
+
+def test_levee_stage_known_answers_at_case_boundaries(case_dirs):
+    """CMF_LEVEE_FLDSTG restated independently (above) and compared bit for bit with the oracle on
+    every levee cell at storages inside each of the five cases, exactly on the case boundaries
+    (LEVBASSTO, LEVTOPSTO, LEVFILSTO: the reference compares with `<`), and on and between the
+    protected-side layer boundaries of case 3; cells without a levee carry the 1e18 sentinels and
+    take case 1 (the default scheme without its MIN clamp)."""
+    from oracle import Oracle
+
+    o = Oracle(case_dirs["stress"])
+    N = o.d("rivsto").size
+    L = 10
+    a = {k: o.d(k) for k in ("rivstomax", "rivlen", "rivwth", "grarea", "levbassto", "levtopsto", "levfilsto",
+                             "levhgt", "levfrc", "bashgt", "levdst", "rivelv")}
+    a["fsm"], a["grd"], a["fhg"] = (o.d(k).reshape(L, N) for k in ("fldstomax", "fldgrd", "fldhgt"))
+    lev = np.nonzero(a["levbassto"] < 1e17)[0]
+    assert lev.size >= 20
+    rng = np.random.default_rng(9)
+    tot = np.empty(N)
+    on_layer = 0
+    for i in range(N):
+        if a["levbassto"][i] >= 1e17:
+            tot[i] = a["rivstomax"][i] * rng.uniform(0.5, 3.0)
+            continue
+        b, t, fl, s = a["levbassto"][i], a["levtopsto"][i], a["levfilsto"][i], a["rivstomax"][i]
+        cand = [0.5 * s, s, 0.5 * (s + b), b, np.nextafter(b, 0), 0.5 * (b + t), t, 0.5 * (t + fl), fl,
+                np.nextafter(fl, 0), 1.3 * fl]
+        # protected-side layer boundaries of case 3 (the values the EXIT test compares with)
+        ilev = int(a["levfrc"][i] * L) + 1
+        for I in range(ilev, L + 1):
+            add = (a["levdst"][i] + a["rivwth"][i]) * (a["levhgt"][i] - a["fhg"][I - 1, i]) * a["rivlen"][i]
+            v = a["fsm"][I - 1, i] + add
+            if t <= v < fl:
+                cand.append(v)
+        k = i % len(cand)
+        tot[i] = cand[k]
+        on_layer += k >= 11
+    _set_oracle_array(o, "rivsto", tot)
+    _set_oracle_array(o, "fldsto", np.zeros(N))
+    _set_oracle_array(o, "levsto", np.zeros(N))
+    o.physics_fldstg()
+    got = {k: o.d(k) for k in ("rivsto", "fldsto", "levsto", "rivdph", "flddph", "fldfrc", "fldare", "levdph")}
+    cases = np.zeros(5, dtype=int)
+    for i in range(N):
+        psto = float(tot[i]) + 0.0 + 0.0
+        exp = _levee_stage_ref(psto, i, a, L)
+        for k, v in exp.items():
+            assert np.float64(got[k][i]).view(np.int64) == np.float64(v).view(np.int64), (k, i, psto, got[k][i], v)
+        d = psto
+        cases[0 if not d > a["rivstomax"][i] else 1 if d < a["levbassto"][i] else 2 if d < a["levtopsto"][i]
+              else 3 if d < a["levfilsto"][i] else 4] += 1
+    assert np.all(cases > 0) and on_layer > 0, (cases, on_layer)
