@@ -133,9 +133,15 @@ def _native():
     if _SYNTH_LIB is None:
         import ctypes as C
 
-        path = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "lib", "libcmf_synth.so")
-        if not os.path.exists(path):
-            raise RuntimeError(f"{path} is missing: run cama-flood_v4_b200/build.py")
+        pkg = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+        path = os.path.join(pkg, "lib", "libcmf_synth.so")
+        if not os.path.exists(path):                  # host C++ only: build it in place (g++)
+            import importlib.util
+
+            spec = importlib.util.spec_from_file_location("cmf_build", os.path.join(pkg, "build.py"))
+            mod = importlib.util.module_from_spec(spec)
+            spec.loader.exec_module(mod)
+            mod.build_synth()
         lib = C.CDLL(path)
         P = C.c_void_p
         lib.cmf_synth_grow_forest.argtypes = [C.c_int32, C.c_int32, P, P, C.c_int64, P, C.c_int64, P, P]
