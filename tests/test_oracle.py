@@ -431,3 +431,68 @@ def test_levee_stage_known_answers_at_case_boundaries(case_dirs):
         cases[0 if not d > a["rivstomax"][i] else 1 if d < a["levbassto"][i] else 2 if d < a["levtopsto"][i]
               else 3 if d < a["levfilsto"][i] else 4] += 1
     assert np.all(cases > 0) and on_layer > 0, (cases, on_layer)
+
+
+def test_dam_rule_known_answers(case_dirs, tmp_path):
+    """Yamazaki-Funato reservoir operation (src/cmf_ctrl_damout_mod.F90:383-414, LDAMH22 off)
+    restated independently and compared bit for bit with the oracle's dam outflow after one sub-step
+    (LADPSTP off): every active dam's storage is set inside each of the four regimes and exactly on
+    their boundaries (ConVol, AdjVol, EmeVol; the reference compares with <= and >), half the dams
+    get local runoff above Qf (flood period), the rule's `**0.5`, `**3.0` and `**0.1` (a
+    single-precision exponent) go through libm pow as in the reference, then the limiter
+    min(Q, Vol/DT, (RIVSTO+FLDSTO)/DT) >= 0 and the LSPAMAT rescale of a positive outflow by the
+    cell's own rate."""
+    import shutil
+
+    from oracle import Oracle
+
+    d = str(tmp_path / "dams")
+    shutil.copytree(case_dirs["stress"], d)
+    nml = open(os.path.join(d, "input_cmf.nam")).read().replace("LADPSTP  = .TRUE.", "LADPSTP  = .FALSE.")
+    open(os.path.join(d, "input_cmf.nam"), "w").write(nml)
+    o = Oracle(d)
+    seq = o.i("damseq")                                  # 0-based cell of each dam
+    stat = o.i("damstat")
+    qn, qf, qa = o.d("dam_qn"), o.d("dam_qf"), o.d("dam_qa")
+    con, adj, eme = o.d("dam_convol"), o.d("dam_adjvol"), o.d("dam_emevol")
+    act = np.nonzero(stat > 0)[0]
+    assert act.size >= 8
+    N = o.d("rivsto").size
+    vols = lambda k: [0.3 * con[k], con[k], 0.5 * (con[k] + adj[k]), adj[k],     # noqa: E731
+                      0.5 * (adj[k] + eme[k]), eme[k], 1.2 * eme[k]]
+    damsto = o.d("damsto")
+    runoff = np.zeros(N)
+    for n, k in enumerate(act):
+        flood = n >= 7                                   # the first 7 dams dry, the others in flood
+        damsto[seq[k]] = vols(k)[n % 7 if not flood else (n - 4) % 7]
+        if flood:
+            runoff[seq[k]] = 2.0 * qf[k]                # inflow above Qf
+    _set_oracle_array(o, "damsto", damsto)
+    o.put_runoff(runoff)
+    dt_min = o.stage()
+    riv0, fld0, vol0 = o.d("rivsto"), o.d("fldsto"), o.d("damsto")
+    nt, DT = o.substeps(dt_min)
+    assert nt == 1
+    dinf_all, rate, rivout = o.d("daminf"), o.d("rate"), o.d("rivout")
+    f01 = float(np.float32(0.1))
+    regimes = set()
+    for k in act:
+        i = seq[k]
+        vol, dinf = float(vol0[i]), float(dinf_all[i])
+        if vol <= con[k]:
+            q, r = qn[k] * (vol / con[k]) ** 0.5, 1
+        elif vol <= adj[k]:
+            q, r = qn[k] + ((vol - con[k]) / (adj[k] - con[k])) ** 3.0 * (qa[k] - qn[k]), 2
+        elif vol <= eme[k]:
+            t = qa[k] + ((vol - adj[k]) / (eme[k] - adj[k])) ** f01 * (qf[k] - qa[k])
+            if dinf >= qf[k]:
+                q, r = max(qn[k] + ((vol - con[k]) / (eme[k] - con[k])) * (dinf - qn[k]), t), 3
+            else:
+                q, r = t, 30
+        else:
+            q, r = (dinf, 4) if dinf >= qf[k] else (qf[k], 40)
+        regimes.add(r)
+        q = max(min(q, vol / DT, (float(riv0[i]) + float(fld0[i])) / DT), 0.0)
+        exp = q * float(rate[i]) if q > 0.0 else 0.0
+        assert np.float64(rivout[i]).view(np.int64) == np.float64(exp).view(np.int64), (k, r, rivout[i], exp)
+    assert {1, 2, 3, 30, 4, 40} <= regimes, regimes
