@@ -496,3 +496,68 @@ def test_dam_rule_known_answers(case_dirs, tmp_path):
         exp = q * float(rate[i]) if q > 0.0 else 0.0
         assert np.float64(rivout[i]).view(np.int64) == np.float64(exp).view(np.int64), (k, r, rivout[i], exp)
     assert {1, 2, 3, 30, 4, 40} <= regimes, regimes
+
+
+def test_dam_rule_h22_known_answers(case_dirs, tmp_path):
+    """Hanazaki 2022 reservoir operation (src/cmf_ctrl_damout_mod.F90:354-377, LDAMH22 on) restated
+    independently and compared bit for bit with the oracle after one sub-step: storages in every
+    regime and on its boundaries (NorVol, ConVol, EmeVol), dry and flood inflow, the
+    single-precision literals 1. and 0.2 promoted to double, and R_VolUpa as the oracle holds it
+    (the reference assigns R_VolUpa(NDAM) inside its dam loop)."""
+    import shutil
+
+    from oracle import Oracle
+
+    d = str(tmp_path / "dams_h22")
+    shutil.copytree(case_dirs["stress"], d)
+    nml = open(os.path.join(d, "input_cmf.nam")).read()
+    nml = nml.replace("LADPSTP  = .TRUE.", "LADPSTP  = .FALSE.").replace("LDAMH22  = .FALSE.", "LDAMH22  = .TRUE.")
+    assert "LDAMH22  = .TRUE." in nml
+    open(os.path.join(d, "input_cmf.nam"), "w").write(nml)
+    o = Oracle(d)
+    seq, stat = o.i("damseq"), o.i("damstat")
+    qn, qf = o.d("dam_qn"), o.d("dam_qf")
+    nor, con, eme, rvu = o.d("dam_norvol"), o.d("dam_convol"), o.d("dam_emevol"), o.d("dam_r_volupa")
+    act = np.nonzero(stat > 0)[0]
+    vols = lambda k: [0.3 * nor[k], nor[k], 0.5 * (nor[k] + con[k]), con[k],      # noqa: E731
+                      0.5 * (con[k] + eme[k]), eme[k], 1.2 * eme[k]]
+    damsto = o.d("damsto")
+    runoff = np.zeros(damsto.size)
+    for n, k in enumerate(act):
+        flood = n >= 7
+        damsto[seq[k]] = vols(k)[n % 7 if not flood else (n - 4) % 7]
+        if flood:
+            runoff[seq[k]] = 2.0 * qf[k]
+    _set_oracle_array(o, "damsto", damsto)
+    o.put_runoff(runoff)
+    dt_min = o.stage()
+    riv0, fld0, vol0 = o.d("rivsto"), o.d("fldsto"), o.d("damsto")
+    nt, DT = o.substeps(dt_min)
+    assert nt == 1
+    dinf_all, rate, rivout = o.d("daminf"), o.d("rate"), o.d("rivout")
+    one, p2 = float(np.float32(1.0)), float(np.float32(0.2))
+    regimes = set()
+    for k in act:
+        i = seq[k]
+        vol, dinf = float(vol0[i]), float(dinf_all[i])
+        if vol <= nor[k]:
+            q, r = qn[k] * (vol / con[k]), 1
+        elif vol <= con[k]:
+            if qf[k] <= dinf:
+                q, r = qn[k] * 0.5 + (vol - nor[k]) / (con[k] - nor[k]) * (qf[k] - qn[k]), 2
+            else:
+                x = (vol - nor[k]) / (eme[k] - nor[k])
+                q, r = qn[k] * 0.5 + (x * x) * (qf[k] - qn[k]), 20
+        elif vol < eme[k]:
+            if qf[k] <= dinf:
+                q, r = qf[k] + max(one - rvu[k] / p2, 0.0) * (vol - con[k]) / (eme[k] - con[k]) * (dinf - qf[k]), 3
+            else:
+                x = (vol - nor[k]) / (eme[k] - nor[k])
+                q, r = qn[k] * 0.5 + (x * x) * (qf[k] - qn[k]), 30
+        else:
+            q, r = max(dinf, qf[k]), 4
+        regimes.add(r)
+        q = max(min(q, vol / DT, (float(riv0[i]) + float(fld0[i])) / DT), 0.0)
+        exp = q * float(rate[i]) if q > 0.0 else 0.0
+        assert np.float64(rivout[i]).view(np.int64) == np.float64(exp).view(np.int64), (k, r, rivout[i], exp)
+    assert {1, 2, 20, 3, 30, 4} <= regimes, regimes
