@@ -561,3 +561,148 @@ def test_dam_rule_h22_known_answers(case_dirs, tmp_path):
         exp = q * float(rate[i]) if q > 0.0 else 0.0
         assert np.float64(rivout[i]).view(np.int64) == np.float64(exp).view(np.int64), (k, r, rivout[i], exp)
     assert {1, 2, 20, 3, 30, 4} <= regimes, regimes
+
+
+def _one_substep_case(case_dirs, tmp_path, name, levee: bool):
+    """Copy of a case with LADPSTP off (one sub-step per outer step) and LLEVEE as given."""
+    import shutil
+
+    d = str(tmp_path / name)
+    shutil.copytree(case_dirs["stress"], d)
+    nml = open(os.path.join(d, "input_cmf.nam")).read().replace("LADPSTP  = .TRUE.", "LADPSTP  = .FALSE.")
+    if not levee:
+        nml = nml.replace("LLEVEE   = .TRUE.", "LLEVEE   = .FALSE.")
+    open(os.path.join(d, "input_cmf.nam"), "w").write(nml)
+    return d
+
+
+def test_bifurcation_flux_known_answers(case_dirs, tmp_path):
+    """CMF_CALC_PTHOUT (src/cmf_calc_pthout_mod.F90:20-97) and the LSPAMAT path rescale
+    (src/cmf_calc_outflw_mod.F90:494-517) restated independently and compared bit for bit with the
+    oracle's path flows and level sums after one sub-step (LADPSTP and LLEVEE off), from a state
+    with non-zero previous-step path flows."""
+    from oracle import Oracle
+
+    o = Oracle(_one_substep_case(case_dirs, tmp_path, "pth", levee=False))
+    gr = o.d("grarea")
+    forc = list(runoff_series(gr, "stress", 3, hourly=True))
+    for r in forc[:2]:
+        o.put_runoff(r)
+        o.advance()
+    o.put_runoff(forc[2])
+    dt_min = o.stage()
+    sfc, elv, dph_pre, stg = o.d("sfcelv"), o.d("rivelv"), o.d("rivdph_pre"), o.d("storge")
+    flw_pre = o.d("pthflw_pre")
+    nt, DT = o.substeps(dt_min)
+    assert nt == 1
+    up, dn, mask = o.i("pth_upst"), o.d("pth_dst"), o.i("i2mask")
+    down = o.i("pth_down")
+    P, Lp = up.size, o.d("pth_man").size
+    pelv, pwth, pman = o.d("pth_elv").reshape(Lp, P), o.d("pth_wth").reshape(Lp, P), o.d("pth_man")
+    flw_pre = flw_pre.reshape(Lp, P)
+    rate = o.d("rate")
+    got, got_sum = o.d("pthflw").reshape(Lp, P), o.d("pthflwsum")
+    sfc_pre = elv + dph_pre
+    g = 9.8 * DT
+    active = 0
+    for p in range(P):
+        u, d = int(up[p]) - 1, int(down[p]) - 1          # PTH_UPST / PTH_DOWN are 1-based
+        flw = [0.0] * Lp
+        skip = u < 0 or d < 0 or mask[u] > 0 or mask[d] > 0
+        if not skip:
+            dslp = (sfc[u] - sfc[d]) / dn[p]
+            dslp = max(-0.005, min(0.005, dslp))
+            for l in range(Lp):
+                dflw = max(max(sfc[u], sfc[d]) - pelv[l, p], 0.0)
+                dflw_pr = max(max(sfc_pre[u], sfc_pre[d]) - pelv[l, p], 0.0)
+                dflw_im = (dflw * dflw_pr) ** 0.5
+                dflw_im = max(dflw_im, (dflw * 0.01) ** 0.5)
+                if dflw_im > 1e-5:
+                    dout_pr = flw_pre[l, p] / pwth[l, p]
+                    flw[l] = pwth[l, p] * (dout_pr + g * dflw_im * dslp) / (
+                        1.0 + g * pman[l] ** 2.0 * abs(dout_pr) * dflw_im ** (-7.0 / 3.0))
+        s = 0.0
+        for l in range(Lp):
+            s = s + flw[l]
+        if s != 0.0:
+            rt = min(0.05 * min(stg[u], stg[d]) / abs(s * DT), 1.0)
+            flw = [f * rt for f in flw]
+            s = s * rt
+        if not skip:
+            flw = [f * (rate[u] if f >= 0.0 else rate[d]) for f in flw]
+            s = s * (rate[u] if s >= 0.0 else rate[d])
+            active += any(f != 0.0 for f in flw)
+        for l in range(Lp):
+            assert np.float64(got[l, p]).view(np.int64) == np.float64(flw[l]).view(np.int64), (p, l, got[l, p], flw[l])
+        assert np.float64(got_sum[p]).view(np.int64) == np.float64(s).view(np.int64), (p, got_sum[p], s)
+    assert active >= 5
+
+
+def test_levee_bifurcation_flux_known_answers(case_dirs, tmp_path):
+    """CMF_LEVEE_OPT_PTHOUT (src/cmf_ctrl_levee_mod.F90:497-603) and the LSPAMAT path rescale
+    restated independently and compared bit for bit with the oracle after one sub-step (LADPSTP off,
+    LLEVEE on): level 1 on the river surface with the semi-implicit depth (DFLW when that is not
+    positive), levels 2.. on the protected-side surface min(ELEVTN + LEVDPH, SFCELV) where LEVFRC < 1
+    with the explicit depth and PTH_WTH**(-1.) as a reciprocal; the flux skips I2MASK == 1 only,
+    the rescale any I2MASK > 0."""
+    from oracle import Oracle
+
+    o = Oracle(_one_substep_case(case_dirs, tmp_path, "pth_lev", levee=True))
+    gr = o.d("grarea")
+    forc = list(runoff_series(gr, "stress", 3, hourly=True))
+    for r in forc[:2]:
+        o.put_runoff(r)
+        o.advance()
+    o.put_runoff(forc[2])
+    dt_min = o.stage()
+    sfc, elv, dph_pre, stg = o.d("sfcelv"), o.d("rivelv"), o.d("rivdph_pre"), o.d("storge")
+    elevtn, levdph, levfrc = o.d("elevtn"), o.d("levdph"), o.d("levfrc")
+    flw_pre = o.d("pthflw_pre")
+    nt, DT = o.substeps(dt_min)
+    assert nt == 1
+    up, down, dst, mask = o.i("pth_upst"), o.i("pth_down"), o.d("pth_dst"), o.i("i2mask")
+    P, Lp = up.size, o.d("pth_man").size
+    assert Lp > 1
+    pelv, pwth, pman = o.d("pth_elv").reshape(Lp, P), o.d("pth_wth").reshape(Lp, P), o.d("pth_man")
+    flw_pre = flw_pre.reshape(Lp, P)
+    rate = o.d("rate")
+    got, got_sum = o.d("pthflw").reshape(Lp, P), o.d("pthflwsum")
+    sfc_pre = elv + dph_pre
+    sfc_lev = np.where(levfrc < 1.0, np.minimum(elevtn + levdph, sfc), sfc)
+    g = 9.8 * DT
+
+    def flux(wth, dout_pr, dflw_im, dslp, man):
+        return wth * (dout_pr + g * dflw_im * dslp) / (1.0 + g * man ** 2.0 * abs(dout_pr) * dflw_im ** (-7.0 / 3.0))
+
+    active = 0
+    for p in range(P):
+        u, d = int(up[p]) - 1, int(down[p]) - 1
+        flw = [0.0] * Lp
+        if not (u < 0 or d < 0 or mask[u] == 1 or mask[d] == 1):
+            dslp = max(-0.005, min(0.005, (sfc[u] - sfc[d]) / dst[p]))
+            dflw = max(max(sfc[u], sfc[d]) - pelv[0, p], 0.0)
+            dflw_pr = max(max(sfc_pre[u], sfc_pre[d]) - pelv[0, p], 0.0)
+            dflw_im = (dflw * dflw_pr) ** 0.5
+            if dflw_im <= 0.0:
+                dflw_im = dflw
+            if dflw_im > 1e-5:
+                flw[0] = flux(pwth[0, p], flw_pre[0, p] / pwth[0, p], dflw_im, dslp, pman[0])
+            for l in range(1, Lp):
+                dflw = max(max(sfc_lev[u], sfc_lev[d]) - pelv[l, p], 0.0)
+                if dflw > 1e-5:
+                    flw[l] = flux(pwth[l, p], flw_pre[l, p] * (1.0 / pwth[l, p]), dflw, dslp, pman[l])
+        s = 0.0
+        for l in range(Lp):
+            s = s + flw[l]
+        if s != 0.0:
+            rt = min(0.05 * min(stg[u], stg[d]) / abs(s * DT), 1.0)
+            flw = [f * rt for f in flw]
+            s = s * rt
+        if not (u < 0 or d < 0 or mask[u] > 0 or mask[d] > 0):
+            flw = [f * (rate[u] if f >= 0.0 else rate[d]) for f in flw]
+            s = s * (rate[u] if s >= 0.0 else rate[d])
+            active += any(f != 0.0 for f in flw[1:])
+        for l in range(Lp):
+            assert np.float64(got[l, p]).view(np.int64) == np.float64(flw[l]).view(np.int64), (p, l, got[l, p], flw[l])
+        assert np.float64(got_sum[p]).view(np.int64) == np.float64(s).view(np.int64), (p, got_sum[p], s)
+    assert active >= 3                                   # overland levels carry flow somewhere
