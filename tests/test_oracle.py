@@ -706,3 +706,88 @@ def test_levee_bifurcation_flux_known_answers(case_dirs, tmp_path):
             assert np.float64(got[l, p]).view(np.int64) == np.float64(flw[l]).view(np.int64), (p, l, got[l, p], flw[l])
         assert np.float64(got_sum[p]).view(np.int64) == np.float64(s).view(np.int64), (p, got_sum[p], s)
     assert active >= 3                                   # overland levels carry flow somewhere
+
+
+def test_outflow_known_answers_every_cell(case_dirs, tmp_path):
+    """CMF_CALC_OUTFLW (src/cmf_calc_outflw_mod.F90:44-182) -- river, floodplain and mouth branches,
+    their masks with single- (T4) and double-precision literals, the direction check and the 5 %
+    limiter with its single-precision floor (T5) -- and the LSPAMAT rescale restated independently
+    and compared bit for bit with the oracle's discharge and velocity of every cell after one
+    sub-step of a flooded case (LADPSTP off); cells under dam control are left to the dam tests."""
+    from oracle import Oracle
+
+    o = Oracle(_one_substep_case(case_dirs, tmp_path, "outflw", levee=True))
+    gr = o.d("grarea")
+    forc = list(runoff_series(gr, "stress", 4, hourly=True))
+    for r in forc[:3]:
+        o.put_runoff(r)
+        o.advance()
+    o.put_runoff(forc[3])
+    dt_min = o.stage()
+    st = {k: o.d(k) for k in ("rivdph", "rivdph_pre", "rivout_pre", "fldout_pre", "fldsto", "fldsto_pre", "flddph",
+                              "storge", "dwnelv")}
+    nt, DT = o.substeps(dt_min)
+    assert nt == 1
+    elv, hgt, dst, wth, man = o.d("rivelv"), o.d("rivhgt"), o.d("nxtdst"), o.d("rivwth"), o.d("rivman")
+    etn, ln = o.d("elevtn"), o.d("rivlen")
+    nxt, i1dam = o.i("i1next"), o.i("i1dam")            # river links 0-based in the oracle
+    rate, got_r, got_f, got_v = o.d("rate"), o.d("rivout"), o.d("fldout"), o.d("rivvel")
+    N, R = o.nseqall, o.nseqriv
+    g, pman, f5, f10 = 9.8 * DT, 0.10, float(np.float32(1e-5)), float(np.float32(1e-10))
+    sfc = elv + st["rivdph"]
+    sfc_pre = elv + st["rivdph_pre"]
+    fdph_pre = np.maximum(st["rivdph_pre"] - hgt, 0.0)
+    rout, fout, vel = np.zeros(N), np.zeros(N), np.zeros(N)
+    for i in range(N):
+        mouth = i >= R
+        dwn = st["dwnelv"][i] if mouth else sfc[nxt[i]]
+        dwn_pre = None if mouth else sfc_pre[nxt[i]]
+        inv_dst = (1.0 / 10000.0) if mouth else 1.0 / dst[i]
+        if mouth:
+            dslp = (sfc[i] - dwn) * inv_dst
+            dflw, dflw_pr = st["rivdph"][i], st["rivdph_pre"][i]
+        else:
+            dslp = (sfc[i] - dwn) * inv_dst
+            dflw = max(sfc[i], dwn) - elv[i]
+            dflw_pr = max(sfc_pre[i], dwn_pre) - elv[i]
+        dare = max(wth[i] * dflw, 1e-10)
+        dflw_im = max((dflw * dflw_pr) ** 0.5, 1e-6)
+        dout_pr = st["rivout_pre"][i] * (1.0 / wth[i])
+        q = wth[i] * (dout_pr + g * dflw_im * dslp) * (1.0 / (1.0 + g * (man[i] * man[i]) * abs(dout_pr)
+                                                           * dflw_im ** (-7.0 / 3.0)))
+        v = st["rivout_pre"][i] * (1.0 / dare)
+        ok = dflw_im > f5 and dare > f5
+        rout[i], vel[i] = (q, v) if ok else (0.0, 0.0)
+        # floodplain
+        fslp = max(-0.005, min(0.005, (sfc[i] - dwn) * inv_dst))
+        if mouth:
+            fdflw, fdflw_pr = sfc[i] - etn[i], sfc_pre[i] - etn[i]
+            fare = max(st["fldsto"][i] * (1.0 / ln[i]) - st["flddph"][i] * wth[i], 0.0)
+            fare_pr = max(st["fldsto_pre"][i] * (1.0 / ln[i]) - fdph_pre[i] * wth[i], 1e-6)
+        else:
+            fdflw = max(max(sfc[i], dwn) - etn[i], 0.0)
+            fdflw_pr = max(sfc_pre[i], dwn_pre) - etn[i]
+            fare = max(st["fldsto"][i] * (1.0 / ln[i]) - st["flddph"][i] * wth[i], 0.0)
+            fare_pr = max(st["fldsto_pre"][i] * (1.0 / ln[i]) - fdph_pre[i] * wth[i], 1e-6)
+        fim = max(max(fdflw * fdflw_pr, 0.0) ** 0.5, 1e-6)
+        aim = max((fare * fare_pr) ** 0.5, 1e-6)
+        fpr = st["fldout_pre"][i]
+        fq = (fpr + g * aim * fslp) * (1.0 / (1.0 + g * (pman * pman) * abs(fpr) * fim ** (-4.0 / 3.0) * (1.0 / aim)))
+        lim = (f5, f5) if mouth else (1e-5, 1e-5)
+        fout[i] = fq if (fim > lim[0] and fare > lim[1]) else 0.0
+        if not fout[i] * rout[i] > 0.0:
+            fout[i] = 0.0
+        if not mouth:                                    # limiter on river cells
+            dlim = max((-rout[i] - fout[i]) * DT, f10)
+            rt = min(0.05 * st["storge"][i] / dlim, 1.0)
+            rout[i], fout[i] = rout[i] * rt, fout[i] * rt
+    checked = 0
+    for i in range(N):
+        if i1dam[i] > 0:
+            continue
+        r = rate[i] if (i >= R or rout[i] > 0.0) else rate[nxt[i]]
+        er, ef = rout[i] * r, fout[i] * r
+        for name, a, b in (("rivout", got_r[i], er), ("fldout", got_f[i], ef), ("rivvel", got_v[i], vel[i])):
+            assert np.float64(a).view(np.int64) == np.float64(b).view(np.int64), (name, i, i >= R, a, b)
+        checked += 1
+    assert checked > 0.9 * N and np.count_nonzero(fout) > 10 and np.any(rout[R:] != 0.0)
