@@ -791,3 +791,65 @@ def test_outflow_known_answers_every_cell(case_dirs, tmp_path):
             assert np.float64(a).view(np.int64) == np.float64(b).view(np.int64), (name, i, i >= R, a, b)
         checked += 1
     assert checked > 0.9 * N and np.count_nonzero(fout) > 10 and np.any(rout[R:] != 0.0)
+
+
+def test_inflow_storage_update_and_stage_every_cell(case_dirs, tmp_path):
+    """The LSPAMAT inflow gathers (src/cmf_calc_outflw_mod.F90:481-489, 520-534), CMF_CALC_STONXT
+    (src/cmf_calc_stonxt_mod.F90:53-100: channel/floodplain borrowing, runoff split by the
+    pre-stage flooded fraction) and the levee stage that follows, restated independently (the stage
+    by `_levee_stage_ref`) and compared bit for bit with the oracle's inflows, path outflow, storages,
+    depths and fractions of every cell after one sub-step (LADPSTP off)."""
+    from oracle import Oracle
+
+    o = Oracle(_one_substep_case(case_dirs, tmp_path, "stonxt", levee=True))
+    gr = o.d("grarea")
+    forc = [20.0 * r for r in runoff_series(gr, "stress", 4, hourly=True)]   # a storm: protected sides flood
+    for r in forc[:3]:
+        o.put_runoff(r)
+        o.advance()
+    o.put_runoff(forc[3])
+    dt_min = o.stage()
+    pre = {k: o.d(k) for k in ("rivsto", "fldsto", "levsto", "fldfrc", "runoff")}
+    nt, DT = o.substeps(dt_min)
+    assert nt == 1
+    N, L = o.nseqall, 10
+    rout, fout, psum = o.d("rivout"), o.d("fldout"), o.d("pthflwsum")
+    upn, outn, infn = o.i("i1upn"), o.i("i1p_outn"), o.i("i1p_infn")
+    ups = o.i("i1upst").reshape(N, -1)
+    outs, infs = o.i("i1p_out").reshape(N, -1), o.i("i1p_inf").reshape(N, -1)
+    a = {k: o.d(k) for k in ("rivstomax", "rivlen", "rivwth", "grarea", "levbassto", "levtopsto", "levfilsto",
+                             "levhgt", "levfrc", "bashgt", "levdst")}
+    a["fsm"], a["grd"], a["fhg"] = (o.d(k).reshape(L, N) for k in ("fldstomax", "fldgrd", "fldhgt"))
+    got = {k: o.d(k) for k in ("rivinf", "fldinf", "pthout", "rivsto", "fldsto", "levsto", "rivdph", "flddph",
+                               "fldfrc", "fldare", "levdph")}
+    borrowed = 0
+    for i in range(N):
+        rinf = finf = pout = 0.0
+        for k in range(upn[i]):
+            j = ups[i, k]
+            rinf = rinf + rout[j]
+            finf = finf + fout[j]
+        for k in range(outn[i]):
+            pout = pout + psum[outs[i, k]]
+        for k in range(infn[i]):
+            pout = pout - psum[infs[i, k]]
+        rs = (pre["rivsto"][i] + rinf * DT) - rout[i] * DT
+        fs = pre["fldsto"][i]
+        if rs < 0.0:
+            fs = fs + rs
+            rs = 0.0
+            borrowed += 1
+        fs = ((fs + finf * DT) - fout[i] * DT) - pout * DT
+        if fs < 0.0:
+            rs = max(rs + fs, 0.0)
+            fs = 0.0
+            borrowed += 1
+        frc, roff = pre["fldfrc"][i], pre["runoff"][i]
+        rs = rs + (roff * (1.0 - frc)) * DT
+        fs = fs + (roff * frc) * DT
+        exp = _levee_stage_ref((rs + fs) + pre["levsto"][i], i, a, L)
+        exp.update(rivinf=rinf, fldinf=finf, pthout=pout)
+        for k, v in exp.items():
+            assert np.float64(got[k][i]).view(np.int64) == np.float64(v).view(np.int64), (k, i, got[k][i], v)
+    assert np.count_nonzero(got["pthout"]) > 0 and np.count_nonzero(got["levsto"]) > 0
+    assert np.count_nonzero(got["fldsto"]) > 0.5 * N
