@@ -638,45 +638,46 @@ def test_bifurcation_flux_known_answers(case_dirs, tmp_path):
     assert active >= 5
 
 
-def test_levee_bifurcation_flux_known_answers(case_dirs, tmp_path):
-    """CMF_LEVEE_OPT_PTHOUT (src/cmf_ctrl_levee_mod.F90:497-603) and the LSPAMAT path rescale
-    restated independently and compared bit for bit with the oracle after one sub-step (LADPSTP off,
-    LLEVEE on): level 1 on the river surface with the semi-implicit depth (DFLW when that is not
-    positive), levels 2.. on the protected-side surface min(ELEVTN + LEVDPH, SFCELV) where LEVFRC < 1
-    with the explicit depth and PTH_WTH**(-1.) as a reciprocal; the flux skips I2MASK == 1 only,
-    the rescale any I2MASK > 0."""
+_SUBSTEP_FIELDS = ("sfcelv", "rivdph", "rivdph_pre", "rivout_pre", "fldout_pre", "rivsto", "fldsto", "fldsto_pre",
+                   "flddph", "storge", "dwnelv", "levdph", "pthflw_pre")
+
+
+def _checked_substep(case_dirs, tmp_path, name, warm=3):
+    """Oracle on the flooded case with one sub-step per outer step and levees on, `warm` steps of
+    spin-up; returns (oracle after the checked sub-step, its post-stage state before the sub-step, DT)."""
     from oracle import Oracle
 
-    o = Oracle(_one_substep_case(case_dirs, tmp_path, "pth_lev", levee=True))
-    gr = o.d("grarea")
-    forc = list(runoff_series(gr, "stress", 3, hourly=True))
-    for r in forc[:2]:
+    o = Oracle(_one_substep_case(case_dirs, tmp_path, name, levee=True))
+    forc = list(runoff_series(o.d("grarea"), "stress", warm + 1, hourly=True))
+    for r in forc[:warm]:
         o.put_runoff(r)
         o.advance()
-    o.put_runoff(forc[2])
+    o.put_runoff(forc[warm])
     dt_min = o.stage()
-    sfc, elv, dph_pre, stg = o.d("sfcelv"), o.d("rivelv"), o.d("rivdph_pre"), o.d("storge")
-    elevtn, levdph, levfrc = o.d("elevtn"), o.d("levdph"), o.d("levfrc")
-    flw_pre = o.d("pthflw_pre")
+    st = {k: o.d(k) for k in _SUBSTEP_FIELDS}
     nt, DT = o.substeps(dt_min)
     assert nt == 1
+    return o, st, DT
+
+
+def _levee_pthout_restated(o, st, DT):
+    """CMF_LEVEE_OPT_PTHOUT (src/cmf_ctrl_levee_mod.F90:497-603) up to its 5 % limiter: path flows
+    [Lp][P] and level sums [P] before the LSPAMAT rescale, from the post-stage state `st`."""
     up, down, dst, mask = o.i("pth_upst"), o.i("pth_down"), o.d("pth_dst"), o.i("i2mask")
     P, Lp = up.size, o.d("pth_man").size
-    assert Lp > 1
     pelv, pwth, pman = o.d("pth_elv").reshape(Lp, P), o.d("pth_wth").reshape(Lp, P), o.d("pth_man")
-    flw_pre = flw_pre.reshape(Lp, P)
-    rate = o.d("rate")
-    got, got_sum = o.d("pthflw").reshape(Lp, P), o.d("pthflwsum")
-    sfc_pre = elv + dph_pre
-    sfc_lev = np.where(levfrc < 1.0, np.minimum(elevtn + levdph, sfc), sfc)
+    flw_pre = st["pthflw_pre"].reshape(Lp, P)
+    sfc, stg = st["sfcelv"], st["storge"]
+    sfc_pre = o.d("rivelv") + st["rivdph_pre"]
+    sfc_lev = np.where(o.d("levfrc") < 1.0, np.minimum(o.d("elevtn") + st["levdph"], sfc), sfc)
     g = 9.8 * DT
 
     def flux(wth, dout_pr, dflw_im, dslp, man):
         return wth * (dout_pr + g * dflw_im * dslp) / (1.0 + g * man ** 2.0 * abs(dout_pr) * dflw_im ** (-7.0 / 3.0))
 
-    active = 0
+    flows, sums = np.zeros((Lp, P)), np.zeros(P)
     for p in range(P):
-        u, d = int(up[p]) - 1, int(down[p]) - 1
+        u, d = int(up[p]) - 1, int(down[p]) - 1          # PTH_UPST / PTH_DOWN are 1-based
         flw = [0.0] * Lp
         if not (u < 0 or d < 0 or mask[u] == 1 or mask[d] == 1):
             dslp = max(-0.005, min(0.005, (sfc[u] - sfc[d]) / dst[p]))
@@ -698,40 +699,17 @@ def test_levee_bifurcation_flux_known_answers(case_dirs, tmp_path):
             rt = min(0.05 * min(stg[u], stg[d]) / abs(s * DT), 1.0)
             flw = [f * rt for f in flw]
             s = s * rt
-        if not (u < 0 or d < 0 or mask[u] > 0 or mask[d] > 0):
-            flw = [f * (rate[u] if f >= 0.0 else rate[d]) for f in flw]
-            s = s * (rate[u] if s >= 0.0 else rate[d])
-            active += any(f != 0.0 for f in flw[1:])
-        for l in range(Lp):
-            assert np.float64(got[l, p]).view(np.int64) == np.float64(flw[l]).view(np.int64), (p, l, got[l, p], flw[l])
-        assert np.float64(got_sum[p]).view(np.int64) == np.float64(s).view(np.int64), (p, got_sum[p], s)
-    assert active >= 3                                   # overland levels carry flow somewhere
+        flows[:, p], sums[p] = flw, s
+    return flows, sums
 
 
-def test_outflow_known_answers_every_cell(case_dirs, tmp_path):
-    """CMF_CALC_OUTFLW (src/cmf_calc_outflw_mod.F90:44-182) -- river, floodplain and mouth branches,
-    their masks with single- (T4) and double-precision literals, the direction check and the 5 %
-    limiter with its single-precision floor (T5) -- and the LSPAMAT rescale restated independently
-    and compared bit for bit with the oracle's discharge and velocity of every cell after one
-    sub-step of a flooded case (LADPSTP off); cells under dam control are left to the dam tests."""
-    from oracle import Oracle
-
-    o = Oracle(_one_substep_case(case_dirs, tmp_path, "outflw", levee=True))
-    gr = o.d("grarea")
-    forc = list(runoff_series(gr, "stress", 4, hourly=True))
-    for r in forc[:3]:
-        o.put_runoff(r)
-        o.advance()
-    o.put_runoff(forc[3])
-    dt_min = o.stage()
-    st = {k: o.d(k) for k in ("rivdph", "rivdph_pre", "rivout_pre", "fldout_pre", "fldsto", "fldsto_pre", "flddph",
-                              "storge", "dwnelv")}
-    nt, DT = o.substeps(dt_min)
-    assert nt == 1
+def _outflow_restated(o, st, DT):
+    """CMF_CALC_OUTFLW (src/cmf_calc_outflw_mod.F90:44-182) of every cell from the post-stage state
+    `st`: river and floodplain outflow after the 5 % limiter (before the LSPAMAT rescale; dam
+    operation not applied) and the velocity."""
     elv, hgt, dst, wth, man = o.d("rivelv"), o.d("rivhgt"), o.d("nxtdst"), o.d("rivwth"), o.d("rivman")
     etn, ln = o.d("elevtn"), o.d("rivlen")
-    nxt, i1dam = o.i("i1next"), o.i("i1dam")            # river links 0-based in the oracle
-    rate, got_r, got_f, got_v = o.d("rate"), o.d("rivout"), o.d("fldout"), o.d("rivvel")
+    nxt = o.i("i1next")                                  # river links 0-based in the oracle
     N, R = o.nseqall, o.nseqriv
     g, pman, f5, f10 = 9.8 * DT, 0.10, float(np.float32(1e-5)), float(np.float32(1e-10))
     sfc = elv + st["rivdph"]
@@ -743,11 +721,10 @@ def test_outflow_known_answers_every_cell(case_dirs, tmp_path):
         dwn = st["dwnelv"][i] if mouth else sfc[nxt[i]]
         dwn_pre = None if mouth else sfc_pre[nxt[i]]
         inv_dst = (1.0 / 10000.0) if mouth else 1.0 / dst[i]
+        dslp = (sfc[i] - dwn) * inv_dst
         if mouth:
-            dslp = (sfc[i] - dwn) * inv_dst
             dflw, dflw_pr = st["rivdph"][i], st["rivdph_pre"][i]
         else:
-            dslp = (sfc[i] - dwn) * inv_dst
             dflw = max(sfc[i], dwn) - elv[i]
             dflw_pr = max(sfc_pre[i], dwn_pre) - elv[i]
         dare = max(wth[i] * dflw, 1e-10)
@@ -762,25 +739,65 @@ def test_outflow_known_answers_every_cell(case_dirs, tmp_path):
         fslp = max(-0.005, min(0.005, (sfc[i] - dwn) * inv_dst))
         if mouth:
             fdflw, fdflw_pr = sfc[i] - etn[i], sfc_pre[i] - etn[i]
-            fare = max(st["fldsto"][i] * (1.0 / ln[i]) - st["flddph"][i] * wth[i], 0.0)
-            fare_pr = max(st["fldsto_pre"][i] * (1.0 / ln[i]) - fdph_pre[i] * wth[i], 1e-6)
         else:
             fdflw = max(max(sfc[i], dwn) - etn[i], 0.0)
             fdflw_pr = max(sfc_pre[i], dwn_pre) - etn[i]
-            fare = max(st["fldsto"][i] * (1.0 / ln[i]) - st["flddph"][i] * wth[i], 0.0)
-            fare_pr = max(st["fldsto_pre"][i] * (1.0 / ln[i]) - fdph_pre[i] * wth[i], 1e-6)
+        fare = max(st["fldsto"][i] * (1.0 / ln[i]) - st["flddph"][i] * wth[i], 0.0)
+        fare_pr = max(st["fldsto_pre"][i] * (1.0 / ln[i]) - fdph_pre[i] * wth[i], 1e-6)
         fim = max(max(fdflw * fdflw_pr, 0.0) ** 0.5, 1e-6)
         aim = max((fare * fare_pr) ** 0.5, 1e-6)
         fpr = st["fldout_pre"][i]
         fq = (fpr + g * aim * fslp) * (1.0 / (1.0 + g * (pman * pman) * abs(fpr) * fim ** (-4.0 / 3.0) * (1.0 / aim)))
-        lim = (f5, f5) if mouth else (1e-5, 1e-5)
-        fout[i] = fq if (fim > lim[0] and fare > lim[1]) else 0.0
+        lim = f5 if mouth else 1e-5                      # the mouth floodplain mask is a default-real literal
+        fout[i] = fq if (fim > lim and fare > lim) else 0.0
         if not fout[i] * rout[i] > 0.0:
             fout[i] = 0.0
         if not mouth:                                    # limiter on river cells
             dlim = max((-rout[i] - fout[i]) * DT, f10)
             rt = min(0.05 * st["storge"][i] / dlim, 1.0)
             rout[i], fout[i] = rout[i] * rt, fout[i] * rt
+    return rout, fout, vel
+
+
+def test_levee_bifurcation_flux_known_answers(case_dirs, tmp_path):
+    """CMF_LEVEE_OPT_PTHOUT (src/cmf_ctrl_levee_mod.F90:497-603) and the LSPAMAT path rescale
+    restated independently (`_levee_pthout_restated`) and compared bit for bit with the oracle after
+    one sub-step (LADPSTP off, LLEVEE on): level 1 on the river surface with the semi-implicit depth
+    (DFLW when that is not positive), levels 2.. on the protected-side surface
+    min(ELEVTN + LEVDPH, SFCELV) where LEVFRC < 1 with the explicit depth and PTH_WTH**(-1.) as a
+    reciprocal; the flux skips I2MASK == 1 only, the rescale any I2MASK > 0."""
+    o, st, DT = _checked_substep(case_dirs, tmp_path, "pth_lev")
+    flows, sums = _levee_pthout_restated(o, st, DT)
+    up, down, mask, rate = o.i("pth_upst"), o.i("pth_down"), o.i("i2mask"), o.d("rate")
+    Lp, P = flows.shape
+    assert Lp > 1
+    got, got_sum = o.d("pthflw").reshape(Lp, P), o.d("pthflwsum")
+    active = 0
+    for p in range(P):
+        u, d = int(up[p]) - 1, int(down[p]) - 1
+        flw, s = list(flows[:, p]), sums[p]
+        if not (u < 0 or d < 0 or mask[u] > 0 or mask[d] > 0):
+            flw = [f * (rate[u] if f >= 0.0 else rate[d]) for f in flw]
+            s = s * (rate[u] if s >= 0.0 else rate[d])
+            active += any(f != 0.0 for f in flw[1:])
+        for l in range(Lp):
+            assert np.float64(got[l, p]).view(np.int64) == np.float64(flw[l]).view(np.int64), (p, l, got[l, p], flw[l])
+        assert np.float64(got_sum[p]).view(np.int64) == np.float64(s).view(np.int64), (p, got_sum[p], s)
+    assert active >= 3                                   # overland levels carry flow somewhere
+
+
+def test_outflow_known_answers_every_cell(case_dirs, tmp_path):
+    """CMF_CALC_OUTFLW (src/cmf_calc_outflw_mod.F90:44-182) -- river, floodplain and mouth branches,
+    their masks with single- (T4) and double-precision literals, the direction check and the 5 %
+    limiter with its single-precision floor (T5) -- and the LSPAMAT rescale restated independently
+    (`_outflow_restated`) and compared bit for bit with the oracle's discharge and velocity of every
+    cell after one sub-step of a flooded case (LADPSTP off); cells under dam control are left to the
+    dam tests."""
+    o, st, DT = _checked_substep(case_dirs, tmp_path, "outflw")
+    rout, fout, vel = _outflow_restated(o, st, DT)
+    nxt, i1dam, rate = o.i("i1next"), o.i("i1dam"), o.d("rate")
+    got_r, got_f, got_v = o.d("rivout"), o.d("fldout"), o.d("rivvel")
+    N, R = o.nseqall, o.nseqriv
     checked = 0
     for i in range(N):
         if i1dam[i] > 0:
@@ -791,6 +808,40 @@ def test_outflow_known_answers_every_cell(case_dirs, tmp_path):
             assert np.float64(a).view(np.int64) == np.float64(b).view(np.int64), (name, i, i >= R, a, b)
         checked += 1
     assert checked > 0.9 * N and np.count_nonzero(fout) > 10 and np.any(rout[R:] != 0.0)
+
+
+def test_lspamat_rate_every_cell(case_dirs, tmp_path):
+    """LSPAMAT steps 1-2 (src/cmf_calc_outflw_mod.F90:410-451): storage out of each cell -- its own
+    positive outflows, the negative outflows of its upstream cells in I1UPST order, times DT, then
+    the positive outgoing and negative incoming path sums times DT -- and RATE =
+    min(STO / max(STOOUT, 1e-10), 1), from the restated outflows and path sums; compared bit for bit
+    with the oracle's rate wherever no dam-controlled cell feeds the sum."""
+    o, st, DT = _checked_substep(case_dirs, tmp_path, "rate")
+    rout, fout, _ = _outflow_restated(o, st, DT)
+    _, sums = _levee_pthout_restated(o, st, DT)
+    N = o.nseqall
+    i1dam, upn, outn, infn = o.i("i1dam"), o.i("i1upn"), o.i("i1p_outn"), o.i("i1p_infn")
+    ups, outs, infs = (o.i(k).reshape(N, -1) for k in ("i1upst", "i1p_out", "i1p_inf"))
+    got = o.d("rate")
+    checked = limited = 0
+    for i in range(N):
+        feeders = [i] + [int(ups[i, k]) for k in range(upn[i])]
+        if any(i1dam[j] > 0 for j in feeders):
+            continue
+        so = max(rout[i], 0.0) + max(fout[i], 0.0)
+        for k in range(upn[i]):
+            j = ups[i, k]
+            so = (so + max(-rout[j], 0.0)) + max(-fout[j], 0.0)
+        so = so * DT
+        for k in range(outn[i]):
+            so = so + max(sums[outs[i, k]], 0.0) * DT
+        for k in range(infn[i]):
+            so = so + max(-sums[infs[i, k]], 0.0) * DT
+        r = min((st["rivsto"][i] + st["fldsto"][i]) / max(so, 1e-10), 1.0)
+        assert np.float64(got[i]).view(np.int64) == np.float64(r).view(np.int64), (i, got[i], r)
+        checked += 1
+        limited += r < 1.0
+    assert checked > 0.9 * N and limited > 0
 
 
 def test_inflow_storage_update_and_stage_every_cell(case_dirs, tmp_path):
