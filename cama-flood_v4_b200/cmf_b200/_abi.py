@@ -28,7 +28,7 @@ class Opts(C.Structure):
     _fields_ = [(n, C.c_int32) for n in (
         "ladpstp", "lfldout", "lpthout", "ldamout", "llevee", "lspamat",
         "lkine", "lslpmix", "lstg_es", "lgdwdly", "lrosplit", "lwevap", "lupsinf", "lheatlink", "ltrace", "lslopemouth",
-        "ldamh22", "ldamyby", "ldiag", "launch_mode", "device", "block_size")]
+        "ldamh22", "ldamyby", "ldiag", "launch_mode", "device", "block_size", "ldiag_output")]
 
 
 MAP_FIELDS = [
@@ -69,6 +69,15 @@ class DiagPtrs(C.Structure):
     _fields_ = [(n, f64p) for n in DIAG_FIELDS]
 
 
+DIAG_OUT_FIELDS = ["rivout_oavg", "fldout_oavg", "outflw_oavg", "rivvel_oavg", "pthout_oavg",
+                   "gdwrtn_oavg", "runoff_oavg", "rofsub_oavg", "daminf_oavg",
+                   "storge_omax", "outflw_omax", "rivdph_omax", "pthflw_oavg", "nadd_out"]
+
+
+class DiagOutPtrs(C.Structure):
+    _fields_ = [(n, f64p) for n in DIAG_OUT_FIELDS]
+
+
 BUDGET_FIELDS = ["stopre", "stonxt", "stonew", "rivinf", "rivout", "stopre2", "stonew2", "rivsto", "fldsto",
                  "fldare", "levsto", "dam_miss"]
 
@@ -93,7 +102,8 @@ EXPORTS = [
     "cmf_gpu_init", "cmf_gpu_set_state", "cmf_gpu_get_state", "cmf_gpu_put_runoff", "cmf_gpu_physics_advance",
     "cmf_gpu_get_diag", "cmf_gpu_finalize", "cmf_gpu_strerror", "cmf_gpu_last_error", "cmf_gpu_abi_version",
     "cmf_host_load", "cmf_host_free", "cmf_host_describe", "cmf_host_state", "cmf_host_conv_resol", "cmf_host_grid",
-    "cmf_gpu_stage_noalloc",
+    "cmf_gpu_stage_noalloc", "cmf_gpu_ctx_nt_stats", "cmf_gpu_ctx_diag_output", "cmf_gpu_ctx_get_diag_output",
+    "cmf_gpu_diag_output", "cmf_gpu_get_diag_output",
 ]
 
 _lib = None
@@ -134,6 +144,11 @@ def load(build_if_missing: bool = True):
     lib.cmf_gpu_ctx_substeps.argtypes = [vp, C.c_double, C.c_double, i32p, f64p, C.POINTER(Budget)]
     lib.cmf_gpu_ctx_counters.argtypes = [vp, C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
     lib.cmf_gpu_ctx_time_phases.argtypes = [vp, C.c_double, C.c_int32, f64p]
+    lib.cmf_gpu_ctx_nt_stats.argtypes = [vp, C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.c_int32]
+    lib.cmf_gpu_ctx_diag_output.argtypes = [vp, C.c_int32]
+    lib.cmf_gpu_ctx_get_diag_output.argtypes = [vp, C.POINTER(DiagOutPtrs)]
+    lib.cmf_gpu_diag_output.argtypes = [C.c_int32]
+    lib.cmf_gpu_get_diag_output.argtypes = [C.POINTER(DiagOutPtrs)]
     lib.cmf_gpu_batch_create.argtypes = [C.POINTER(vp), C.c_int32, C.POINTER(vp)]
     lib.cmf_gpu_batch_launch.argtypes = [vp, C.c_double]
     lib.cmf_gpu_batch_advance.argtypes = [vp, C.c_double, i32p, f64p, C.POINTER(Budget)]

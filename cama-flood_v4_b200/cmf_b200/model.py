@@ -158,7 +158,7 @@ class PhysicsGPU:
     """A GPU context running ``nmembers`` members of the host model's network."""
 
     def __init__(self, host: HostModel, nmembers: int = 1, ldiag: bool = True, launch_mode: int = 0,
-                 device: int = 0, block_size: int = 0, opts_override: dict | None = None):
+                 device: int = 0, block_size: int = 0, opts_override: dict | None = None, ldiag_output: bool = False):
         self.lib = _abi.load()
         self.host = host
         dims = _abi.Dims.from_buffer_copy(host.dims)
@@ -168,6 +168,7 @@ class PhysicsGPU:
         opts.launch_mode = launch_mode
         opts.device = device
         opts.block_size = block_size
+        opts.ldiag_output = int(ldiag_output)
         for k, v in (opts_override or {}).items():
             setattr(opts, k, int(v))
         self.dims, self.opts = dims, opts
@@ -338,6 +339,15 @@ class PhysicsGPU:
         check(self.lib.cmf_gpu_ctx_counters(self.h, C.byref(a), C.byref(b), C.byref(c)), "counters")
         return {"member_substeps": a.value, "loop_iters": b.value, "outer_steps": c.value}
 
+    def nt_stats(self, nbins: int = 64) -> dict:
+        """NT histogram over (outer step, member) pairs since creation, and how many of them had
+        DT_DEF/DT_MIN - 0.01 within 1e-12 (relative) of an integer (NT hangs on DT_MIN's last bits)."""
+        near = C.c_int64()
+        hist = np.zeros(nbins, dtype=np.int64)
+        check(self.lib.cmf_gpu_ctx_nt_stats(self.h, C.byref(near), hist.ctypes.data_as(C.POINTER(C.c_int64)), nbins),
+              "nt_stats")
+        return {"near_boundary": near.value, "hist": hist}
+
     def time_phases(self, reps: int = 10, dt_def: float | None = None) -> dict:
         dt_def = self.host.dt if dt_def is None else dt_def
         ms = np.zeros(6)
@@ -371,6 +381,23 @@ class PhysicsGPU:
             out[n] = a
             setattr(dp, n, a.ctypes.data_as(_abi.f64p))
         check(self.lib.cmf_gpu_ctx_get_diag(self.h, C.byref(dp)), "get_diag")
+        return {k: v.reshape(self.M, -1) for k, v in out.items()}
+
+    def diag_output(self, op: str) -> None:
+        """CMF_DIAG_GETAVE_OUTPUT ("getave") or CMF_DIAG_RESET_OUTPUT ("reset") on the device; the
+        AVEMAX step runs inside every advance() when the context was made with ldiag_output."""
+        check(self.lib.cmf_gpu_ctx_diag_output(self.h, {"reset": 0, "getave": 2}[op]), "diag_output")
+
+    def get_diag_output(self) -> dict:
+        """The output-interval averages/maxima (D2*_oAVG, D2*_oMAX, D1PTHFLW_oAVG) and NADD_out."""
+        dp = _abi.DiagOutPtrs()
+        out = {}
+        for n in _abi.DIAG_OUT_FIELDS:
+            ln = self.M if n == "nadd_out" else (self.M * max(self.P * self.Lp, 1) if n == "pthflw_oavg" else self.M * self.N)
+            a = np.zeros(ln)
+            out[n] = a
+            setattr(dp, n, a.ctypes.data_as(_abi.f64p))
+        check(self.lib.cmf_gpu_ctx_get_diag_output(self.h, C.byref(dp)), "get_diag_output")
         return {k: v.reshape(self.M, -1) for k, v in out.items()}
 
     def get_diag_fields(self, out: dict) -> dict:

@@ -142,6 +142,7 @@ int build_net(cmf_gpu_ctx *c, const cmf_map_ptrs *mp) {
     n.pcadp = c->params.pcadp; n.pminslp = c->params.pminslp; n.dfrcinc = c->params.dfrcinc;
     n.ladpstp = c->opts.ladpstp; n.lfldout = c->opts.lfldout; n.lpthout = c->opts.lpthout;
     n.ldamout = c->opts.ldamout; n.llevee = c->opts.llevee; n.ldamh22 = c->opts.ldamh22; n.ldiag = c->opts.ldiag;
+    n.ldiag_out = c->opts.ldiag && c->opts.ldiag_output;
     // ---- network
     std::vector<int> next(N, -1);
     for (int i = 0; i < R; i++) {
@@ -322,6 +323,15 @@ int alloc_state(cmf_gpu_ctx *c) {
         if ((rc = c->alloc(p, dg ? MN : 1))) return rc;
     if ((rc = c->alloc(&s.a_daminf, (dg && c->opts.ldamout) ? MN : 1))) return rc;
     if ((rc = c->alloc(&s.a_pthflw, dg ? MPL : 1)) || (rc = c->alloc(&s.a_pthsum, dg ? MP : 1))) return rc;
+    // output-interval accumulators (zeroed by alloc: CMF_DIAG_INIT leaves them at zero, NADD_out = 0)
+    const bool dout = c->net.ldiag_out;
+    double **oarr[] = {&s.o_rivout, &s.o_fldout, &s.o_outflw, &s.o_rivvel, &s.o_pthout, &s.o_runoff,
+                       &s.om_storge, &s.om_outflw, &s.om_rivdph};
+    for (double **p : oarr)
+        if ((rc = c->alloc(p, dout ? MN : 1))) return rc;
+    if ((rc = c->alloc(&s.o_daminf, (dout && c->opts.ldamout) ? MN : 1)) || (rc = c->alloc(&s.o_pthflw, dout ? MPL : 1)) ||
+        (rc = c->alloc(&s.o_nadd, c->dims.nmembers)))
+        return rc;
     if ((rc = c->alloc(&s.ctl, c->dims.nmembers)) || (rc = c->alloc(&s.loop, 1))) return rc;
     // budget partials sized for the smallest block the autotuner may pick (64 threads)
     const size_t nblk_max = (size_t)(c->dims.nseqall + 63) / 64;
@@ -540,9 +550,17 @@ int finish_outer(cmf_gpu_ctx *c, int32_t *nt_out, double *dt_out, cmf_budget *b)
     }
     if (c->opts.launch_mode == 0) c->launches += 3LL * ntmax;
     if (err) {
+        int bad = -1;
+        for (size_t m = 0; m < c->hctl.size(); m++)
+            if (c->hctl[m].err && bad < 0) bad = (int)m;
         for (auto &x : c->hctl) x.err = 0;
         CUDA_TRY(cudaMemcpyAsync(c->st.ctl, c->hctl.data(), c->hctl.size() * sizeof(cmf::MemberCtl), cudaMemcpyHostToDevice, c->stream));
-        return set_err(CMF_E_NT_CAP, "adaptive sub-step count is not finite or above the cap (DT_MIN non-finite or tiny)");
+        CUDA_TRY(cudaStreamSynchronize(c->stream));
+        if (err == cmf::kErrNonFinite)
+            return set_err(CMF_E_NONFINITE, "member " + std::to_string(bad) +
+                                                ": a sub-step produced a non-finite storage (NaN or infinite runoff or state)");
+        return set_err(CMF_E_NT_CAP, "member " + std::to_string(bad) +
+                                         ": adaptive sub-step count is not finite or above the cap (DT_MIN non-finite or tiny)");
     }
     return CMF_OK;
 }
@@ -562,7 +580,30 @@ __global__ void k_depth_powers(const double *x, int n, double *p73, double *p43)
     p73[i] = cmf::pow_depth<7>(x[i]);
     p43[i] = cmf::pow_depth<4>(x[i]);
 }
+__global__ void k_cfl_keys(const double *rivdph, const double *ddst, int n, double pgrv, double pcadp, double *key) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    key[i] = cmf::cfl_key(pcadp, ddst[i], pgrv, rivdph[i]);
+}
 }  // namespace
+
+int cmf_gpu_cfl_keys(const double *rivdph, const double *ddst, int32_t n, double pgrv, double pcadp, double *key) {
+    if (!rivdph || !ddst || !key || n < 0) return set_err(CMF_E_ARG, "cmf_gpu_cfl_keys: null array or negative count");
+    if (n == 0) return CMF_OK;
+    double *d = nullptr;
+    const size_t bytes = (size_t)n * sizeof(double);
+    CUDA_TRY(cudaMalloc(&d, 3 * bytes));
+    cudaError_t e = cudaMemcpy(d, rivdph, bytes, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(d + n, ddst, bytes, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+        k_cfl_keys<<<(unsigned)((n + 255) / 256), 256>>>(d, d + n, n, pgrv, pcadp, d + 2 * (size_t)n);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpy(key, d + 2 * (size_t)n, bytes, cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    if (e != cudaSuccess) return set_err(CMF_E_CUDA, std::string("cmf_gpu_cfl_keys: ") + cudaGetErrorString(e));
+    return CMF_OK;
+}
 
 int cmf_gpu_depth_powers(const double *x, int32_t n, double *p73, double *p43) {
     if (!x || n < 0) return set_err(CMF_E_ARG, "cmf_gpu_depth_powers: null input or negative count");
@@ -593,6 +634,7 @@ const char *cmf_gpu_strerror(int status) {
         case CMF_E_CUDA: return "CUDA runtime error";
         case CMF_E_NT_CAP: return "adaptive sub-step count not finite or above the cap";
         case CMF_E_NO_DEVICE: return "no usable CUDA device (sm_100a required)";
+        case CMF_E_NONFINITE: return "non-finite storage after a sub-step";
         default: return "unknown status";
     }
 }
@@ -696,6 +738,75 @@ int cmf_gpu_ctx_counters(cmf_gpu_ctx *c, int64_t *member_substeps, int64_t *loop
     if (member_substeps) *member_substeps = lc.member_substeps;
     if (loop_iters) *loop_iters = lc.loop_iters;
     if (outer_steps) *outer_steps = lc.outer_steps;
+    return CMF_OK;
+}
+
+int cmf_gpu_ctx_diag_output(cmf_gpu_ctx *c, int32_t op) {
+    if (!c) return set_err(CMF_E_STATE, "no context");
+    if (!c->net.ldiag_out) return set_err(CMF_E_UNSUPPORTED, "output diagnostics need opts.ldiag and opts.ldiag_output");
+    CUDA_TRY(cudaSetDevice(c->device));
+    const size_t MN = (size_t)c->dims.nmembers * c->dims.nseqall;
+    const size_t MPL = (size_t)c->dims.nmembers * c->net.P * c->net.Lp;
+    cmf::State &s = c->st;
+    if (op == CMF_DIAG_OUT_RESET) {
+        // CMF_DIAG_RESET_OUTPUT, src/cmf_calc_diag_mod.F90:222-266
+        for (double *p : {s.o_rivout, s.o_fldout, s.o_outflw, s.o_rivvel, s.o_pthout, s.o_runoff, s.om_storge, s.om_outflw,
+                          s.om_rivdph})
+            CUDA_TRY(cudaMemsetAsync(p, 0, MN * sizeof(double), c->stream));
+        if (c->opts.ldamout) CUDA_TRY(cudaMemsetAsync(s.o_daminf, 0, MN * sizeof(double), c->stream));
+        if (MPL) CUDA_TRY(cudaMemsetAsync(s.o_pthflw, 0, MPL * sizeof(double), c->stream));
+        CUDA_TRY(cudaMemsetAsync(s.o_nadd, 0, (size_t)c->dims.nmembers * sizeof(double), c->stream));
+        return CMF_OK;
+    }
+    if (op == CMF_DIAG_OUT_GETAVE) {
+        const int pl_blocks = MPL ? (int)((c->net.P * c->net.Lp + c->block - 1) / c->block) : 0;
+        const dim3 g(c->ncell_blocks + pl_blocks, c->dims.nmembers);
+        cmf::k_diag_getave_output<<<g, c->block, 0, c->stream>>>(c->net, c->st, c->ncell_blocks);
+        CUDA_TRY(cudaGetLastError());
+        c->launches += 1;
+        return CMF_OK;
+    }
+    return set_err(CMF_E_ARG, "cmf_gpu_ctx_diag_output: op must be CMF_DIAG_OUT_RESET or CMF_DIAG_OUT_GETAVE "
+                              "(AVEMAX runs inside every outer step)");
+}
+
+int cmf_gpu_ctx_get_diag_output(cmf_gpu_ctx *c, const cmf_diag_out_ptrs *p) {
+    if (!c || !p) return set_err(CMF_E_ARG, "null argument");
+    if (!c->net.ldiag_out) return set_err(CMF_E_UNSUPPORTED, "output diagnostics need opts.ldiag and opts.ldiag_output");
+    CUDA_TRY(cudaSetDevice(c->device));
+    const size_t MN = (size_t)c->dims.nmembers * c->dims.nseqall;
+    const size_t MPL = (size_t)c->dims.nmembers * c->net.P * c->net.Lp;
+    const cmf::State &s = c->st;
+    struct { double *dst; const double *src; size_t n; } t[] = {
+        {p->rivout_oavg, s.o_rivout, MN}, {p->fldout_oavg, s.o_fldout, MN}, {p->outflw_oavg, s.o_outflw, MN},
+        {p->rivvel_oavg, s.o_rivvel, MN}, {p->pthout_oavg, s.o_pthout, MN}, {p->runoff_oavg, s.o_runoff, MN},
+        {p->daminf_oavg, c->opts.ldamout ? s.o_daminf : nullptr, MN}, {p->storge_omax, s.om_storge, MN},
+        {p->outflw_omax, s.om_outflw, MN}, {p->rivdph_omax, s.om_rivdph, MN}, {p->pthflw_oavg, s.o_pthflw, MPL},
+        {p->nadd_out, s.o_nadd, (size_t)c->dims.nmembers}};
+    int rc;
+    for (auto &x : t) {
+        if (!x.dst || !x.src || !x.n) continue;
+        if ((rc = d2h(c, x.dst, x.src, x.n))) return rc;
+    }
+    // GDWRTN/ROFSUB are zero without groundwater delay or LROSPLIT (both refused)
+    if (p->gdwrtn_oavg) std::memset(p->gdwrtn_oavg, 0, MN * sizeof(double));
+    if (p->rofsub_oavg) std::memset(p->rofsub_oavg, 0, MN * sizeof(double));
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    return CMF_OK;
+}
+
+int cmf_gpu_ctx_nt_stats(cmf_gpu_ctx *c, int64_t *near_boundary, int64_t *hist, int32_t nbins) {
+    if (!c) return set_err(CMF_E_STATE, "no context");
+    if (hist && nbins < 1) return set_err(CMF_E_ARG, "cmf_gpu_ctx_nt_stats: nbins must be positive");
+    CUDA_TRY(cudaSetDevice(c->device));
+    cmf::LoopCtl lc{};
+    CUDA_TRY(cudaMemcpyAsync(&lc, c->st.loop, sizeof lc, cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    if (near_boundary) *near_boundary = lc.near_int;
+    if (hist) {
+        for (int k = 0; k < nbins; k++) hist[k] = 0;
+        for (int k = 0; k < cmf::kNtHist; k++) hist[std::min(k, nbins - 1)] += lc.nt_hist[k];
+    }
     return CMF_OK;
 }
 
@@ -1205,6 +1316,12 @@ int cmf_gpu_physics_advance(double dt_def, int32_t *nt_out, double *dt_out, cmf_
 int cmf_gpu_get_diag(const cmf_diag_ptrs *dg) {
     return g_default ? cmf_gpu_ctx_get_diag(g_default, dg) : set_err(CMF_E_STATE, "cmf_gpu_init not called");
 }
+int cmf_gpu_diag_output(int32_t op) {
+    return g_default ? cmf_gpu_ctx_diag_output(g_default, op) : set_err(CMF_E_STATE, "cmf_gpu_init not called");
+}
+int cmf_gpu_get_diag_output(const cmf_diag_out_ptrs *dg) {
+    return g_default ? cmf_gpu_ctx_get_diag_output(g_default, dg) : set_err(CMF_E_STATE, "cmf_gpu_init not called");
+}
 void cmf_gpu_finalize(void) {
     if (g_default) cmf_gpu_destroy(g_default);
     g_default = nullptr;
@@ -1237,11 +1354,8 @@ __global__ void k_noalloc_stage(cmf::Net n, cmf::State s, double *blockmin) {
     if (i < n.N) {
         const cmf::StageOut o = cmf::stage_def(n, i, s.rivsto[i], s.fldsto[i]);
         cmf::store_stage(n, s, i, i, o);
-        if (n.ladpstp && n.i2mask[i] == 0) {
-            const double ddph = cmf::dmax(o.rivdph, 0.01);
-            const double ddst = (i < n.R) ? n.nxtdst[i] : n.pdstmth;
-            key = (n.pcadp * ddst) * pow(n.pgrv * ddph, -0.5);
-        }
+        if (n.ladpstp && n.i2mask[i] == 0)
+            key = cmf::cfl_key(n.pcadp, (i < n.R) ? n.nxtdst[i] : n.pdstmth, n.pgrv, o.rivdph);
     }
     for (int o = 16; o > 0; o >>= 1) key = cmf::dmin(key, __shfl_down_sync(0xffffffffu, key, o));
     __shared__ double wmin[32];

@@ -581,7 +581,7 @@ int cmf_host_describe(const cmf_host_model *hm, cmf_dims *dims, cmf_params *para
         opts->llevee = n.llevee; opts->lspamat = n.lspamat; opts->lkine = n.lkine; opts->lslpmix = n.lslpmix;
         opts->lstg_es = n.lstg_es; opts->lgdwdly = n.lgdwdly; opts->lrosplit = n.lrosplit; opts->lwevap = n.lwevap;
         opts->lupsinf = n.lupsinf; opts->ldamh22 = n.ldamh22; opts->ldamyby = n.ldamyby;
-        opts->ldiag = 1; opts->launch_mode = 0; opts->device = 0; opts->block_size = 0;
+        opts->ldiag = 1; opts->launch_mode = 0; opts->device = 0; opts->block_size = 0; opts->ldiag_output = 0;
     }
     if (dt) *dt = n.dt;
     return CMF_OK;

@@ -48,6 +48,9 @@ constexpr int kBudgets = 12;       // stopre stonxt stonew rivinf rivout stopre2
 // dynamic shared memory of k_store: the last sub-step's budget terms, kBudgets per thread
 inline size_t store_smem(int block) { return (size_t)kBudgets * block * sizeof(double); }
 constexpr int kNtCap = 10000;      // bound of the device-side sub-step loop
+// MemberCtl.err codes (mapped to the ABI's positive statuses by the engine)
+constexpr int kErrNtCap = 2;       // DT_MIN non-finite or NT above kNtCap: no sub-step ran
+constexpr int kErrNonFinite = 3;   // a sub-step produced a non-finite storage
 
 struct MemberCtl {
     double dt_def;                 // DT at entry (DT_DEF)
@@ -62,6 +65,8 @@ struct MemberCtl {
     double budget[kBudgets];       // last finished sub-step
 };
 
+constexpr int kNtHist = 64;       // NT histogram bins (the last one holds NT >= kNtHist-1)
+
 struct LoopCtl {
     int k;            // sub-step counter of the device-side loop (advanced by k_rate)
     int kcur;         // the sub-step the running k_flux/k_rate/k_store work on (set by k_flux)
@@ -71,6 +76,9 @@ struct LoopCtl {
     long long member_substeps;   // sum over outer steps and members of NT (throughput accounting)
     long long loop_iters;        // sum over outer steps of NTmax (kernel-launch accounting)
     long long outer_steps;
+    long long near_int;          // (outer step, member) pairs whose DT_DEF/DT_MIN-0.01 lay within
+                                 // 1e-12 (relative) of an integer: NT there hangs on DT_MIN's last bits
+    long long nt_hist[kNtHist];  // (outer step, member) pairs by NT
 };
 
 // Static data shared by all members (device pointers).
@@ -101,6 +109,7 @@ struct Net {
     const double *__restrict__ emevol, *__restrict__ norvol, *__restrict__ adjvol, *__restrict__ r_volupa;
     double pgrv, pmanfld, pdstmth, pcadp, pminslp, dfrcinc;
     int ladpstp, lfldout, lpthout, ldamout, llevee, ldamh22, ldiag;
+    int ldiag_out;   // CMF_DIAG_AVEMAX_OUTPUT after every outer step, fused into its last sub-step
 };
 
 // Per-member state, member-major [M][N] (paths [M][Lp][P] / [M][P]).
@@ -117,6 +126,9 @@ struct State {
     // sub-step diagnostics
     double *a_rivout, *a_fldout, *a_outflw, *a_rivvel, *a_pthout, *a_runoff, *a_daminf;
     double *m_storge, *m_outflw, *m_rivdph, *a_pthflw, *a_pthsum;
+    // output-interval averages and maxima (D2*_oAVG, D2*_oMAX, D1PTHFLW_oAVG, NADD_out per member)
+    double *o_rivout, *o_fldout, *o_outflw, *o_rivvel, *o_pthout, *o_runoff, *o_daminf;
+    double *om_storge, *om_outflw, *om_rivdph, *o_pthflw, *o_nadd;
     MemberCtl *ctl;
     LoopCtl *loop;
     double *partials;                         // [M][nblk][kBudgets]
@@ -161,6 +173,28 @@ __device__ __forceinline__ double pow_depth(double x) {
     const DD v = (K == 7) ? dd_mul(dd_mul(c4, c2), c) : c4;
     const double corr = v.hi * (d * (double)logf((float)x));
     return v.hi + (v.lo + corr);
+}
+
+// (PGRV*DDPH)**(-0.5) of CALC_ADPSTP (src/cmf_ctrl_physics_mod.F90:193,201), correctly rounded.
+// NT is INT(DT_DEF/DT_MIN - 0.01) + 1, so a last-bit change of the minimum can move NT; the
+// oracle's glibc pow is correctly rounded for all but rare arguments, and so is this:
+//   r0 = rsqrt(x) (within an ulp or two); the residual e = 1 - x r0^2 from exact FMA products
+//   (r0^2 = p + pe exactly, x p - 1 rounded once at ~2^-51 magnitude); then one Newton step with
+//   its second-order term, x^-1/2 = r0 (1 + e/2 + 3e^2/8 + O(e^3)), added to r0 and rounded once.
+// Relative error before the final rounding is about 2^-100.  Outside (1e-300, 1e300) pow is used.
+__device__ __forceinline__ double rsqrt_cr(double x) {
+    if (!(x > 1e-300 && x < 1e300)) return pow(x, -0.5);
+    const double r0 = rsqrt(x);
+    const double p = r0 * r0, pe = fma(r0, r0, -p);
+    const double t = fma(x, p, -1.0);
+    const double e = -(t + x * pe);
+    return r0 + r0 * (e * (0.5 + 0.375 * e));
+}
+
+// CFL key of one cell, PCADP*DDST*(PGRV*DDPH)**(-0.5) (src/cmf_ctrl_physics_mod.F90:190-202)
+__device__ __forceinline__ double cfl_key(double pcadp, double ddst, double pgrv, double rivdph) {
+    const double ddph = (rivdph > 0.01) ? rivdph : 0.01;
+    return (pcadp * ddst) * rsqrt_cr(pgrv * ddph);
 }
 
 // ------------------------------------------------------------------------------------------
@@ -397,11 +431,7 @@ __global__ void __launch_bounds__(kCellThreads, CMF_STAGE_MINB) k_stage(Net n, S
         const StageOut o = n.llevee ? stage_levee(n, i, s.rivsto[gi], s.fldsto[gi], s.levsto[gi])
                                     : stage_def(n, i, s.rivsto[gi], s.fldsto[gi]);
         store_stage(n, s, gi, i, o);
-        if (n.ladpstp && n.i2mask[i] == 0) {
-            const double ddph = dmax(o.rivdph, 0.01);
-            const double ddst = (i < n.R) ? n.nxtdst[i] : n.pdstmth;
-            key = (n.pcadp * ddst) * pow(n.pgrv * ddph, -0.5);
-        }
+        if (n.ladpstp && n.i2mask[i] == 0) key = cfl_key(n.pcadp, (i < n.R) ? n.nxtdst[i] : n.pdstmth, n.pgrv, o.rivdph);
     }
     if (n.ladpstp) {
         for (int o = 16; o > 0; o >>= 1) key = dmin(key, __shfl_down_sync(0xffffffffu, key, o));
@@ -423,7 +453,7 @@ __global__ void __launch_bounds__(kCellThreads, CMF_STAGE_MINB) k_stage(Net n, S
 __global__ void k_ntdt(Net n, State s, cudaGraphConditionalHandle h, int use_cond) {
     __shared__ int smax[32];
     int ntmax = 1;
-    long long ntsum = 0;
+    long long ntsum = 0, near = 0;
     for (int m = threadIdx.x; m < n.M; m += blockDim.x) {
         MemberCtl &c = s.ctl[m];
         const double dt_def = c.dt_def;
@@ -434,11 +464,12 @@ __global__ void k_ntdt(Net n, State s, cudaGraphConditionalHandle h, int use_con
             c.dt_min = dt_min;
             const double x = dt_def * (1.0 / dt_min) - CMF_F(0.01);
             if (!(x >= 0.0) || x > (double)(kNtCap - 1)) {
-                c.err = 2;           // non-finite or oversized NT: refuse to loop
+                c.err = kErrNtCap;   // non-finite or oversized NT: refuse to loop
                 nt = 0;
             } else {
                 nt = (int)x + 1;
                 dt = dt_def * (double)(1.0f / (float)nt);
+                if (fabs(x - rint(x)) <= 1e-12 * dmax(x, 1.0)) near++;
             }
             c.dtmin_bits = (unsigned long long)__double_as_longlong(dt_def);
         } else {
@@ -450,21 +481,24 @@ __global__ void k_ntdt(Net n, State s, cudaGraphConditionalHandle h, int use_con
         c.nadd = 0.0;
         ntmax = max(ntmax, nt);
         ntsum += nt;
+        atomicAdd((unsigned long long *)&s.loop->nt_hist[min(nt, kNtHist - 1)], 1ull);
     }
-    __shared__ long long ssum[32];
+    __shared__ long long ssum[32], snear[32];
     for (int o = 16; o > 0; o >>= 1) {
         ntmax = max(ntmax, __shfl_down_sync(0xffffffffu, ntmax, o));
         ntsum += __shfl_down_sync(0xffffffffu, ntsum, o);
+        near += __shfl_down_sync(0xffffffffu, near, o);
     }
-    if ((threadIdx.x & 31) == 0) { smax[threadIdx.x >> 5] = ntmax; ssum[threadIdx.x >> 5] = ntsum; }
+    if ((threadIdx.x & 31) == 0) { smax[threadIdx.x >> 5] = ntmax; ssum[threadIdx.x >> 5] = ntsum; snear[threadIdx.x >> 5] = near; }
     __syncthreads();
     if (threadIdx.x == 0) {
         int v = 1;
-        long long tot = 0;
-        for (int w = 0; w < (int)((blockDim.x + 31) >> 5); w++) { v = max(v, smax[w]); tot += ssum[w]; }
+        long long tot = 0, nr = 0;
+        for (int w = 0; w < (int)((blockDim.x + 31) >> 5); w++) { v = max(v, smax[w]); tot += ssum[w]; nr += snear[w]; }
         v = min(v, kNtCap);
         s.loop->k = 0;
         s.loop->ntmax = v;
+        s.loop->near_int += nr;
         s.loop->member_substeps += tot;
         s.loop->loop_iters += v;
         s.loop->outer_steps += 1;
@@ -656,7 +690,10 @@ __device__ __forceinline__ void cell_outflow(const Net &n, const State &s, int m
     if (last) s.rivvel[gi] = rvel;
     if (n.ldiag) {
         double a = first ? rvel * DT : s.a_rivvel[gi] + rvel * DT;
-        if (last) a = a / (nadd_before(k, DT) + DT);
+        if (last) {
+            a = a / (nadd_before(k, DT) + DT);
+            if (n.ldiag_out) s.o_rivvel[gi] = s.o_rivvel[gi] + a * c.dt_def;   // CMF_DIAG_AVEMAX_OUTPUT
+        }
         s.a_rivvel[gi] = a;
     }
 }
@@ -828,7 +865,11 @@ __global__ void __launch_bounds__(kCellThreads, MinBlocks) k_store(Net n, State 
             s.pthflw_pre[o] = f;
             if (n.ldiag) {
                 double a = first ? f * DT : s.a_pthflw[o] + f * DT;
-                if (last) { a = a / (nadd + DT); asum = asum + a; }
+                if (last) {
+                    a = a / (nadd + DT);
+                    asum = asum + a;
+                    if (n.ldiag_out) s.o_pthflw[o] = s.o_pthflw[o] + a * c.dt_def;
+                }
                 s.a_pthflw[o] = a;
             }
         }
@@ -914,6 +955,9 @@ __global__ void __launch_bounds__(kCellThreads, MinBlocks) k_store(Net n, State 
         bput(2, n.llevee ? (rs + fs) + levsto : rs + fs);
         // stage scheme, :125
         const StageOut o = n.llevee ? stage_levee(n, i, rs, fs, levsto) : stage_def(n, i, rs, fs);
+        // CMF_CheckNanB-style probe (src/cmf_utils_mod.F90:807-815) on the new storage: a NaN or
+        // infinite runoff or state surfaces as a positive status instead of a silent NaN state
+        if (!isfinite((o.rivsto + o.fldsto) + o.levsto)) s.ctl[m].err = kErrNonFinite;
         store_stage(n, s, gi, i, o, last);
         bput(5, n.llevee ? (rs + fs) + levsto : rs + fs);
         bput(6, n.llevee ? (o.rivsto + o.fldsto) + o.levsto : o.rivsto + o.fldsto);
@@ -930,28 +974,43 @@ __global__ void __launch_bounds__(kCellThreads, MinBlocks) k_store(Net n, State 
         // CMF_DIAG_AVEMAX_ADPSTP / GETAVE_ADPSTP, src/cmf_calc_diag_mod.F90:104-221
         if (n.ldiag) {
             const double na = nadd + DT;
-            auto acc = [&](double *a, double v) {
+            // CMF_DIAG_AVEMAX_OUTPUT (src/cmf_calc_diag_mod.F90:272-318) on the last sub-step: the
+            // output interval accumulates the finished sub-step average times DT_DEF
+            const bool out = last && n.ldiag_out;
+            const double ddef = c.dt_def;
+            auto acc = [&](double *a, double *oa, double v) {
                 double x = first ? v * DT : a[gi] + v * DT;
                 if (last) x = x / na;
                 a[gi] = x;
+                if (out) oa[gi] = oa[gi] + x * ddef;
             };
-            acc(s.a_rivout, rout);
-            acc(s.a_fldout, fout);
-            acc(s.a_outflw, outflw);
-            acc(s.a_pthout, pout);        // D2PTHINF is never written by the reference (always 0)
+            acc(s.a_rivout, s.o_rivout, rout);
+            acc(s.a_fldout, s.o_fldout, fout);
+            acc(s.a_outflw, s.o_outflw, outflw);
+            acc(s.a_pthout, s.o_pthout, pout);        // D2PTHINF is never written by the reference (always 0)
             if (last) {
                 // runoff and DT are constant over the outer step: the same running sum of
                 // runoff*DT the accumulator would hold, rebuilt in registers on the last sub-step
                 const double rdt = runoff * DT;
                 double a = rdt;
                 for (int k = 1; k < c.nt; k++) a = a + rdt;
-                s.a_runoff[gi] = a / na;
+                a = a / na;
+                s.a_runoff[gi] = a;
+                if (out) s.o_runoff[gi] = s.o_runoff[gi] + a * ddef;
             }
-            if (n.ldamout) acc(s.a_daminf, s.daminf[gi]);
+            if (n.ldamout) acc(s.a_daminf, s.o_daminf, s.daminf[gi]);
             const double stg = n.llevee ? (o.rivsto + o.fldsto) + o.levsto : o.rivsto + o.fldsto;
-            s.m_outflw[gi] = first ? dmax(0.0, fabs(outflw)) : dmax(s.m_outflw[gi], fabs(outflw));
-            s.m_rivdph[gi] = first ? dmax(0.0, o.rivdph) : dmax(s.m_rivdph[gi], o.rivdph);
-            s.m_storge[gi] = first ? dmax(0.0, stg) : dmax(s.m_storge[gi], stg);
+            const double mo = first ? dmax(0.0, fabs(outflw)) : dmax(s.m_outflw[gi], fabs(outflw));
+            const double md = first ? dmax(0.0, o.rivdph) : dmax(s.m_rivdph[gi], o.rivdph);
+            const double ms = first ? dmax(0.0, stg) : dmax(s.m_storge[gi], stg);
+            s.m_outflw[gi] = mo;
+            s.m_rivdph[gi] = md;
+            s.m_storge[gi] = ms;
+            if (out) {
+                s.om_outflw[gi] = dmax(s.om_outflw[gi], fabs(mo));
+                s.om_rivdph[gi] = dmax(s.om_rivdph[gi], md);
+                s.om_storge[gi] = dmax(s.om_storge[gi], ms);
+            }
         }
     }
     // per-block budget partials of the last sub-step (the only one the caller observes);
@@ -993,6 +1052,32 @@ __global__ void __launch_bounds__(kBudgetThreads) k_budget(Net n, State s, int n
         double t = 0.0;
         for (int j = 0; j < kBudgetThreads / 32; j++) t = t + w[j];
         s.ctl[m].budget[k] = t;
+        if (k == 0 && n.ldiag_out) s.o_nadd[m] = s.o_nadd[m] + s.ctl[m].dt_def;   // NADD_out = NADD_out + DT
+    }
+}
+
+// CMF_DIAG_GETAVE_OUTPUT (src/cmf_calc_diag_mod.F90:324-356): the output-interval sums divided by
+// NADD_out in place (maxima untouched).  Cells on blocks [0, ncell_blocks), path levels after them.
+__global__ void k_diag_getave_output(Net n, State s, int ncell_blocks) {
+    const int m = blockIdx.y;
+    const double na = s.o_nadd[m];
+    if ((int)blockIdx.x < ncell_blocks) {
+        const int i = blockIdx.x * blockDim.x + threadIdx.x;
+        if (i >= n.N) return;
+        const size_t gi = (size_t)m * n.N + i;
+        s.o_rivout[gi] = s.o_rivout[gi] / na;
+        s.o_fldout[gi] = s.o_fldout[gi] / na;
+        s.o_outflw[gi] = s.o_outflw[gi] / na;
+        s.o_rivvel[gi] = s.o_rivvel[gi] / na;
+        s.o_pthout[gi] = s.o_pthout[gi] / na;
+        s.o_runoff[gi] = s.o_runoff[gi] / na;
+        if (n.ldamout) s.o_daminf[gi] = s.o_daminf[gi] / na;
+    } else {
+        const int q = (blockIdx.x - ncell_blocks) * blockDim.x + threadIdx.x;
+        const size_t PL = (size_t)n.P * n.Lp;
+        if ((size_t)q >= PL) return;
+        const size_t o = (size_t)m * PL + q;
+        s.o_pthflw[o] = s.o_pthflw[o] / na;
     }
 }
 

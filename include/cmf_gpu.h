@@ -31,7 +31,7 @@
 extern "C" {
 #endif
 
-#define CMF_GPU_ABI_VERSION 1
+#define CMF_GPU_ABI_VERSION 2
 
 /* ---- status codes ------------------------------------------------------------------------ */
 #define CMF_OK                0
@@ -42,6 +42,7 @@ extern "C" {
 #define CMF_E_CUDA            1  /* CUDA runtime error (message via cmf_gpu_last_error)          */
 #define CMF_E_NT_CAP          2  /* adaptive sub-step count above the cap (non-finite DT_MIN)     */
 #define CMF_E_NO_DEVICE       3  /* no CUDA device or the sm_100a kernels cannot run on it       */
+#define CMF_E_NONFINITE       4  /* a sub-step produced a NaN/infinite storage (NaN runoff...)   */
 
 /* ---- dimensions (src/yos_cmf_map.F90, src/yos_cmf_input.F90) ----------------------------- */
 typedef struct cmf_dims {
@@ -80,6 +81,9 @@ typedef struct cmf_opts {
                             1: host-driven launches (reads NT back before the sub-steps)          */
     int32_t device;      /* CUDA device ordinal                                                   */
     int32_t block_size;  /* 0: autotune; else threads per block for the cell kernels (64..256)   */
+    int32_t ldiag_output;/* accumulate the output-interval averages/maxima (D2*_oAVG, D2*_oMAX) on
+                            the device: CMF_DIAG_AVEMAX_OUTPUT after every outer step, as
+                            CMF_DRV_ADVANCE calls it (src/cmf_drv_advance_mod.F90:114); needs ldiag */
 } cmf_opts;
 
 /* ---- static maps: Fortran module arrays (read-only, host memory) ------------------------- */
@@ -132,6 +136,15 @@ typedef struct cmf_diag_ptrs {
     double *pthflw_aavg, *pthflwsum_aavg;
 } cmf_diag_ptrs;
 
+/* ---- output-interval averages and maxima (src/yos_cmf_diag.F90:82-103); NULL entries skipped */
+typedef struct cmf_diag_out_ptrs {
+    double *rivout_oavg, *fldout_oavg, *outflw_oavg, *rivvel_oavg, *pthout_oavg;
+    double *gdwrtn_oavg, *runoff_oavg, *rofsub_oavg, *daminf_oavg;
+    double *storge_omax, *outflw_omax, *rivdph_omax;
+    double *pthflw_oavg;                      /* D1PTHFLW_oAVG (NPTHOUT,NPTHLEV)                 */
+    double *nadd_out;                         /* NADD_out, one value per member                 */
+} cmf_diag_out_ptrs;
+
 /* ---- water budget of the last sub-step (CALC_WATBAL, src/cmf_ctrl_physics_mod.F90:216-248) */
 typedef struct cmf_budget {
     double stopre, stonxt, stonew, rivinf, rivout;       /* P0GLB* written by CMF_CALC_STONXT      */
@@ -183,6 +196,23 @@ int32_t cmf_gpu_ctx_block_size(cmf_gpu_ctx *ctx);
 /* Device-side counters since creation: sum over outer steps and members of NT, sum over outer
  * steps of max NT (sub-step loop iterations) and the number of outer steps. */
 int cmf_gpu_ctx_counters(cmf_gpu_ctx *ctx, int64_t *member_substeps, int64_t *loop_iters, int64_t *outer_steps);
+/* Output-interval diagnostics on the device (needs opts.ldiag_output; src/cmf_calc_diag_mod.F90:
+ * 222-356).  CMF_DIAG_AVEMAX_OUTPUT runs inside every outer step (fused into its last sub-step),
+ * as CMF_DRV_ADVANCE calls it after every CMF_PHYSICS_ADVANCE (src/cmf_drv_advance_mod.F90:114).
+ * op CMF_DIAG_OUT_GETAVE divides the sums by NADD_out in place (CMF_DIAG_GETAVE_OUTPUT, :123),
+ * op CMF_DIAG_OUT_RESET zeroes them and NADD_out (CMF_DIAG_RESET_OUTPUT, :143).  Enqueued on the
+ * context's stream.  cmf_gpu_ctx_get_diag_output copies the oAVG/oMAX arrays to the host
+ * (synchronous; [nmembers][NSEQMAX], pthflw_oavg [nmembers][NPTHLEV][NPTHOUT]). */
+#define CMF_DIAG_OUT_RESET  0
+#define CMF_DIAG_OUT_GETAVE 2
+int cmf_gpu_ctx_diag_output(cmf_gpu_ctx *ctx, int32_t op);
+int cmf_gpu_ctx_get_diag_output(cmf_gpu_ctx *ctx, const cmf_diag_out_ptrs *dg);
+/* Adaptive-step statistics since creation: near_boundary = (outer step, member) pairs whose
+ * DT_DEF/DT_MIN - 0.01 (the argument of INT in CALC_ADPSTP, src/cmf_ctrl_physics_mod.F90:205)
+ * lay within 1e-12 (relative) of an integer, where NT depends on the last bits of DT_MIN;
+ * hist[k] = pairs with NT == k for k < nbins-1, hist[nbins-1] = pairs with NT >= nbins-1.
+ * Either pointer may be NULL. */
+int cmf_gpu_ctx_nt_stats(cmf_gpu_ctx *ctx, int64_t *near_boundary, int64_t *hist, int32_t nbins);
 /* Measurement helper: runs `reps` outer steps kernel by kernel with CUDA events between kernels
  * on the context's stream (advances the state), timing every sub-step.  ms_out[6] receives the mean
  * duration per launch of the stage/CFL and NT/DT kernels (once per outer step), of the flux, rate
@@ -341,6 +371,10 @@ int cmf_gpu_get_state(const cmf_state_ptrs *st);
 int cmf_gpu_put_runoff(const double *runoff, const double *rofsub);
 int cmf_gpu_physics_advance(double dt_def, int32_t *nt_out, double *dt_out, cmf_budget *budget_out);
 int cmf_gpu_get_diag(const cmf_diag_ptrs *dg);
+/* replace CMF_DIAG_GETAVE_OUTPUT / CMF_DIAG_RESET_OUTPUT at src/cmf_drv_advance_mod.F90:123,143
+ * (AVEMAX at :114 runs inside cmf_gpu_physics_advance when opts.ldiag_output is set) */
+int cmf_gpu_diag_output(int32_t op);
+int cmf_gpu_get_diag_output(const cmf_diag_out_ptrs *dg);
 void cmf_gpu_finalize(void);
 const char *cmf_gpu_strerror(int status);
 const char *cmf_gpu_last_error(void);
@@ -350,6 +384,11 @@ int cmf_gpu_abi_version(void);
  * the sub-step kernels do, for n host values x; results into host arrays p73 and p43 (either may
  * be NULL).  Synchronous; allocates its own scratch. */
 int cmf_gpu_depth_powers(const double *x, int32_t n, double *p73, double *p43);
+/* Diagnostic: the CFL key of CALC_ADPSTP, PCADP*DDST*(PGRV*MAX(RIVDPH,0.01))**(-0.5)
+ * (src/cmf_ctrl_physics_mod.F90:190-202), evaluated on the current device exactly as the stage
+ * kernels do (the inverse square root correctly rounded), for n host values; key is a host
+ * array.  Synchronous; allocates its own scratch. */
+int cmf_gpu_cfl_keys(const double *rivdph, const double *ddst, int32_t n, double pgrv, double pcadp, double *key);
 
 /* ======================================================================================== */
 /* Host model core: the reference's CMF_DRV_INIT for a stand-alone (non-Fortran) host        */

@@ -89,6 +89,10 @@ typedef struct {
     double nadd_adp;
     double *rivout_a, *fldout_a, *outflw_a, *rivvel_a, *pthout_a, *gdwrtn_a, *runoff_a, *rofsub_a;
     double *daminf_a, *storge_m, *outflw_m, *rivdph_m, *pthflw_a, *pthflwsum_a;
+    /* ---- output-interval averages (src/yos_cmf_diag.F90:82-103) */
+    double nadd_out;
+    double *rivout_o, *fldout_o, *outflw_o, *rivvel_o, *pthout_o, *gdwrtn_o, *runoff_o, *rofsub_o, *daminf_o;
+    double *storge_om, *outflw_om, *rivdph_om, *pthflw_o;
     /* ---- budgets (src/yos_cmf_diag.F90 P0GLB*) */
     double glbstopre, glbstonxt, glbstonew, glbrivinf, glbrivout;
     double glbstopre2, glbstonew2, glbrivsto, glbfldsto, glblevsto, glbfldare;
@@ -443,6 +447,10 @@ static void prog_diag_init(orc_model *m) {
     m->pthout_a = dalloc(N); m->gdwrtn_a = dalloc(N); m->runoff_a = dalloc(N); m->rofsub_a = dalloc(N);
     m->daminf_a = dalloc(N); m->storge_m = dalloc(N); m->outflw_m = dalloc(N); m->rivdph_m = dalloc(N);
     m->pthflw_a = dalloc(PL); m->pthflwsum_a = dalloc(m->npthout);
+    m->rivout_o = dalloc(N); m->fldout_o = dalloc(N); m->outflw_o = dalloc(N); m->rivvel_o = dalloc(N);
+    m->pthout_o = dalloc(N); m->gdwrtn_o = dalloc(N); m->runoff_o = dalloc(N); m->rofsub_o = dalloc(N);
+    m->daminf_o = dalloc(N); m->storge_om = dalloc(N); m->outflw_om = dalloc(N); m->rivdph_om = dalloc(N);
+    m->pthflw_o = dalloc(PL); m->nadd_out = 0.0;
     /* STORAGE_SEA_SURFACE, :129-176 */
     for (int i = m->nseqriv; i < m->nseqall; i++) {
         double dseaelv = m->dwnelv[i];
@@ -1226,6 +1234,59 @@ static void diag_getave_adpstp(orc_model *m) {
         }
 }
 
+/* Output-interval averages and maxima, src/cmf_calc_diag_mod.F90:222-356.  CMF_DRV_ADVANCE calls
+ * AVEMAX after every CMF_PHYSICS_ADVANCE (src/cmf_drv_advance_mod.F90:114), GETAVE before an output
+ * write (:123) and RESET after it (:143); DT there is DT_DEF again (src/cmf_ctrl_physics_mod.F90:145). */
+static void diag_reset_output(orc_model *m) {
+    int N = m->nseqmax, PL = m->npthout * m->npthlev;
+    m->nadd_out = 0.0;
+    for (int i = 0; i < N; i++) {
+        m->rivout_o[i] = m->fldout_o[i] = m->outflw_o[i] = m->rivvel_o[i] = m->pthout_o[i] = 0.0;
+        m->gdwrtn_o[i] = m->runoff_o[i] = m->rofsub_o[i] = 0.0;
+        m->storge_om[i] = m->outflw_om[i] = m->rivdph_om[i] = 0.0;
+    }
+    if (m->ldamout) for (int i = 0; i < N; i++) m->daminf_o[i] = 0.0;
+    for (int k = 0; k < PL; k++) m->pthflw_o[k] = 0.0;
+}
+static void diag_avemax_output(orc_model *m) {
+    int N = m->nseqmax, PL = m->npthout * m->npthlev;
+    double DT = m->dt;
+    m->nadd_out = m->nadd_out + DT;
+    OMP_FOR
+    for (int i = 0; i < N; i++) {
+        m->rivout_o[i] = m->rivout_o[i] + m->rivout_a[i] * DT;
+        m->fldout_o[i] = m->fldout_o[i] + m->fldout_a[i] * DT;
+        m->rivvel_o[i] = m->rivvel_o[i] + m->rivvel_a[i] * DT;
+        m->outflw_o[i] = m->outflw_o[i] + m->outflw_a[i] * DT;
+        m->pthout_o[i] = m->pthout_o[i] + m->pthout_a[i] * DT;
+        m->gdwrtn_o[i] = m->gdwrtn_o[i] + m->gdwrtn_a[i] * DT;
+        m->runoff_o[i] = m->runoff_o[i] + m->runoff_a[i] * DT;
+        m->rofsub_o[i] = m->rofsub_o[i] + m->rofsub_a[i] * DT;
+        m->outflw_om[i] = dmax(m->outflw_om[i], fabs(m->outflw_m[i]));
+        m->rivdph_om[i] = dmax(m->rivdph_om[i], m->rivdph_m[i]);
+        m->storge_om[i] = dmax(m->storge_om[i], m->storge_m[i]);
+    }
+    if (m->ldamout) for (int i = 0; i < N; i++) m->daminf_o[i] = m->daminf_o[i] + m->daminf_a[i] * DT;
+    for (int k = 0; k < PL; k++) m->pthflw_o[k] = m->pthflw_o[k] + m->pthflw_a[k] * DT;
+}
+static void diag_getave_output(orc_model *m) {
+    int N = m->nseqmax, PL = m->npthout * m->npthlev;
+    double n = m->nadd_out;
+    for (int i = 0; i < N; i++) {
+        m->rivout_o[i] /= n; m->fldout_o[i] /= n; m->outflw_o[i] /= n; m->rivvel_o[i] /= n;
+        m->pthout_o[i] /= n; m->gdwrtn_o[i] /= n; m->runoff_o[i] /= n; m->rofsub_o[i] /= n;
+        if (m->ldamout) m->daminf_o[i] /= n;
+    }
+    for (int k = 0; k < PL; k++) m->pthflw_o[k] /= n;
+}
+/* op 0: CMF_DIAG_RESET_OUTPUT, 1: CMF_DIAG_AVEMAX_OUTPUT, 2: CMF_DIAG_GETAVE_OUTPUT */
+void orc_diag_output(orc_model *m, int op) {
+    if (op == 0) diag_reset_output(m);
+    else if (op == 1) diag_avemax_output(m);
+    else if (op == 2) diag_getave_output(m);
+}
+double orc_nadd_out(const orc_model *m) { return m->nadd_out; }
+
 /* ============================================================================ ADVANCE */
 /* CMF_PHYSICS_ADVANCE, src/cmf_ctrl_physics_mod.F90:21-153, split where the reference places
  * CMF_MPI_ADPSTP (:200-202): orc_stage returns this domain's DT_MIN, orc_substeps takes the
@@ -1626,6 +1687,10 @@ double *orc_darray(orc_model *m, const char *name, int *len) {
         {"rivvel_aavg", m->rivvel_a, N}, {"pthout_aavg", m->pthout_a, N}, {"runoff_aavg", m->runoff_a, N},
         {"daminf_aavg", m->daminf_a, N}, {"storge_amax", m->storge_m, N}, {"outflw_amax", m->outflw_m, N},
         {"rivdph_amax", m->rivdph_m, N}, {"pthflw_aavg", m->pthflw_a, PL}, {"pthflwsum_aavg", m->pthflwsum_a, P},
+        {"rivout_oavg", m->rivout_o, N}, {"fldout_oavg", m->fldout_o, N}, {"outflw_oavg", m->outflw_o, N},
+        {"rivvel_oavg", m->rivvel_o, N}, {"pthout_oavg", m->pthout_o, N}, {"runoff_oavg", m->runoff_o, N},
+        {"daminf_oavg", m->daminf_o, N}, {"storge_omax", m->storge_om, N}, {"outflw_omax", m->outflw_om, N},
+        {"rivdph_omax", m->rivdph_om, N}, {"pthflw_oavg", m->pthflw_o, PL},
         {"dam_fldvol", m->fldvol, m->ndam}, {"dam_convol", m->convol, m->ndam}, {"dam_emevol", m->emevol, m->ndam},
         {"dam_adjvol", m->adjvol, m->ndam}, {"dam_qn", m->qn, m->ndam}, {"dam_qf", m->qf, m->ndam}, {"dam_qa", m->qa, m->ndam},
         {"dam_norvol", m->norvol, m->ndam}, {"dam_r_volupa", m->r_volupa, m->ndam},

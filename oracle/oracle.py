@@ -54,6 +54,9 @@ def _lib(omp: bool = False):
     lib.orc_roff_interp.argtypes = [C.c_void_p, C.POINTER(C.c_double), C.c_int, C.c_int, C.c_int, C.POINTER(C.c_int),
                                     C.POINTER(C.c_int), C.POINTER(C.c_double)]
     lib.orc_update_boundary.argtypes = [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double)]
+    lib.orc_diag_output.argtypes = [C.c_void_p, C.c_int]
+    lib.orc_nadd_out.argtypes = [C.c_void_p]
+    lib.orc_nadd_out.restype = C.c_double
     _LIBS[key] = lib
     return lib
 
@@ -144,6 +147,14 @@ class Oracle:
         keep = [None if a is None else np.ascontiguousarray(a, dtype=np.float64) for a in (sealev, meansl)]
         ptr = [None if a is None else a.ctypes.data_as(C.POINTER(C.c_double)) for a in keep]
         self.lib.orc_update_boundary(self.h, ptr[0], ptr[1])
+
+    def diag_output(self, op: str) -> None:
+        """CMF_DIAG_RESET_OUTPUT / CMF_DIAG_AVEMAX_OUTPUT / CMF_DIAG_GETAVE_OUTPUT
+        (src/cmf_calc_diag_mod.F90:222-356): op = "reset", "avemax" or "getave"."""
+        self.lib.orc_diag_output(self.h, {"reset": 0, "avemax": 1, "getave": 2}[op])
+
+    def nadd_out(self) -> float:
+        return float(self.lib.orc_nadd_out(self.h))
 
     def budget(self) -> dict:
         b = (C.c_double * 15)()

@@ -39,6 +39,29 @@ def _stress_spec():
     return s
 
 
+# Full-size cases of the benchmarked configurations (generated on first use only: config 1 is a
+# 1440x720 grid of 299,157 cells, about 100 MB of map files).
+FULL_CASES = {
+    "cfg0": lambda: synth.spec_config0(seed=0),
+    "cfg1": lambda: synth.spec_config1(seed=1),
+}
+
+
+@pytest.fixture(scope="session")
+def full_case_dir(tmp_path_factory):
+    base = tmp_path_factory.mktemp("full_cases")
+    made = {}
+
+    def get(name: str) -> str:
+        if name not in made:
+            d = os.path.join(str(base), name)
+            synth.write_case(synth.make_case(FULL_CASES[name]()), d)
+            made[name] = d
+        return made[name]
+
+    return get
+
+
 @pytest.fixture(scope="session")
 def case_dirs(tmp_path_factory):
     base = tmp_path_factory.mktemp("cases")

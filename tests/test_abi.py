@@ -46,7 +46,8 @@ def test_ctypes_structs_match_header():
 
     for cname, py in [("cmf_dims", _abi.Dims), ("cmf_params", _abi.Params), ("cmf_opts", _abi.Opts),
                       ("cmf_map_ptrs", _abi.MapPtrs), ("cmf_state_ptrs", _abi.StatePtrs),
-                      ("cmf_diag_ptrs", _abi.DiagPtrs), ("cmf_budget", _abi.Budget)]:
+                      ("cmf_diag_ptrs", _abi.DiagPtrs), ("cmf_budget", _abi.Budget),
+                      ("cmf_diag_out_ptrs", _abi.DiagOutPtrs)]:
         assert _struct_fields(cname) == [f[0] for f in py._fields_], cname
 
 
@@ -54,7 +55,7 @@ def test_abi_version_and_errors_without_device():
     from cmf_b200 import _abi
 
     lib = _abi.load()
-    assert lib.cmf_gpu_abi_version() == 1
+    assert lib.cmf_gpu_abi_version() == 2
     assert lib.cmf_gpu_strerror(-2) == b"option combination not supported by the GPU path"
     assert lib.cmf_gpu_set_state(None) == -3        # no default context yet: CMF_E_STATE
 

@@ -161,3 +161,69 @@ def test_gpu_regions_with_host_min_equal_whole_domain(case_dirs, tmp_path):
         for h, p in zip(hs, gs):
             g[(h.i1seqy - 1) * h.nx + (h.i1seqx - 1)] = p.get_state()[f][0]
         assert np.array_equal(g[flat_w].view(np.int64), sw[f][0].view(np.int64)), f
+
+
+def _gpu_region_worker(rank, world, port, region_dirs, out_dir):
+    """One rank of the product's split outer step: cmf_gpu_ctx_stage -> 8-byte MIN all-reduce over
+    gloo (CMF_MPI_ADPSTP, src/cmf_ctrl_mpi_mod.F90:261-281) -> cmf_gpu_ctx_substeps."""
+    import torch
+    import torch.distributed as dist
+    import sys
+
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    sys.path[:0] = [os.path.join(root, "cama-flood_v4_b200")]
+    from cmf_b200 import HostModel, PhysicsGPU
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=120))
+    h = HostModel(region_dirs[rank])
+    g = PhysicsGPU(h, device=0)
+    nts = []
+    for k in range(NSTEPS):
+        g.put_runoff(h.conv_resol(_grid_runoff(h.nx, h.ny, k)))
+        local = float(g.stage()[0])
+        t = torch.tensor([local], dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MIN)
+        nt, dt, _ = g.substeps(float(t.item()))
+        nts.append((int(nt[0]), float(dt[0])))
+    flat = (h.i1seqy - 1) * h.nx + (h.i1seqx - 1)
+    st = g.get_state()
+    grids = {}
+    for f in ("rivsto", "fldsto", "rivout", "fldout", "levsto", "damsto"):
+        a = np.full(h.nx * h.ny, np.nan)
+        a[flat] = st[f][0]
+        grids[f] = a
+    np.savez(os.path.join(out_dir, f"gpu_rank{rank}.npz"), nts=np.array(nts), **grids)
+    g.close()
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+@pytest.mark.gpu
+def test_gloo_two_ranks_product_split_equal_whole_domain(case_dirs, tmp_path):
+    """World size 2 over gloo, both ranks on the one GPU (their kernels never wait on each other;
+    the only exchange is the host-side MIN of DT_MIN): the product's split API per rank reproduces
+    the whole-domain GPU run bit for bit, NT and DT included."""
+    import torch.multiprocessing as mp
+
+    from cmf_b200 import HostModel, PhysicsGPU, regions
+
+    dirs = regions.split_case(case_dirs["cfg1s"], 2, str(tmp_path))
+    mp.start_processes(_gpu_region_worker, args=(2, _free_port(), dirs, str(tmp_path)), nprocs=2, join=True,
+                       start_method="spawn")
+    hw = HostModel(case_dirs["cfg1s"])
+    gw = PhysicsGPU(hw)
+    ref = []
+    for k in range(NSTEPS):
+        gw.put_runoff(hw.conv_resol(_grid_runoff(hw.nx, hw.ny, k)))
+        nt, dt, _ = gw.advance()
+        ref.append((int(nt[0]), float(dt[0])))
+    parts = [dict(np.load(os.path.join(str(tmp_path), f"gpu_rank{r}.npz"))) for r in (0, 1)]
+    for p in parts:
+        assert [(int(a), float(b)) for a, b in p["nts"]] == ref
+    flat = (hw.i1seqy - 1) * hw.nx + (hw.i1seqx - 1)
+    sw = gw.get_state()
+    for f in ("rivsto", "fldsto", "rivout", "fldout", "levsto", "damsto"):
+        merged = np.where(np.isnan(parts[0][f]), parts[1][f], parts[0][f])[flat]
+        assert np.array_equal(merged.view(np.int64), sw[f][0].view(np.int64)), f

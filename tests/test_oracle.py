@@ -904,3 +904,47 @@ def test_inflow_storage_update_and_stage_every_cell(case_dirs, tmp_path):
             assert np.float64(got[k][i]).view(np.int64) == np.float64(v).view(np.int64), (k, i, got[k][i], v)
     assert np.count_nonzero(got["pthout"]) > 0 and np.count_nonzero(got["levsto"]) > 0
     assert np.count_nonzero(got["fldsto"]) > 0.5 * N
+
+
+def test_output_interval_diagnostics_known_answer(case_dirs):
+    """CMF_DIAG_AVEMAX/GETAVE/RESET_OUTPUT (src/cmf_calc_diag_mod.F90:222-356) in the oracle: after
+    each outer step the output sums gain aAVG*DT (DT = DT_DEF again, src/cmf_ctrl_physics_mod.F90:145)
+    and the maxima the step's aMAX; GETAVE divides by NADD_out = sum of DT; RESET zeroes everything.
+    Restated here in numpy with the same operation order, bit for bit."""
+    from oracle import Oracle
+
+    o = Oracle(case_dirs["cfg1s"])
+    gr = o.d("grarea")
+    avg = ["rivout", "fldout", "outflw", "rivvel", "pthout", "runoff", "daminf"]
+    mx = ["storge", "outflw", "rivdph"]
+    sums = {k: np.zeros(o.nseqmax) for k in avg}
+    sums["pthflw"] = np.zeros(o.npthout * o.npthlev)
+    mxs = {k: np.zeros(o.nseqmax) for k in mx}
+    nadd = 0.0
+    series = list(runoff_series(gr, "cfg1s", 9, hourly=True))
+    for k, r in enumerate(series):
+        o.put_runoff(r)
+        o.advance()
+        o.diag_output("avemax")
+        nadd = nadd + 3600.0
+        for a in avg:
+            sums[a] = sums[a] + o.d(a + "_aavg") * 3600.0
+        sums["pthflw"] = sums["pthflw"] + o.d("pthflw_aavg") * 3600.0
+        for a in mx:
+            mxs[a] = np.where(mxs[a] > np.abs(o.d(a + "_amax")) if a == "outflw" else mxs[a] > o.d(a + "_amax"),
+                              mxs[a], np.abs(o.d(a + "_amax")) if a == "outflw" else o.d(a + "_amax"))
+        if k == 5:
+            assert o.nadd_out() == nadd
+            o.diag_output("getave")
+            for a in avg:
+                assert np.array_equal(o.d(a + "_oavg"), sums[a] / nadd), a
+            assert np.array_equal(o.d("pthflw_oavg"), sums["pthflw"] / nadd)
+            for a in mx:
+                assert np.array_equal(o.d(a + "_omax"), mxs[a]), a
+            o.diag_output("reset")
+            assert o.nadd_out() == 0.0 and not np.any(o.d("rivout_oavg")) and not np.any(o.d("storge_omax"))
+            sums = {a: np.zeros_like(v) for a, v in sums.items()}
+            mxs = {a: np.zeros_like(v) for a, v in mxs.items()}
+            nadd = 0.0
+    assert o.nadd_out() == 3 * 3600.0
+    assert np.array_equal(o.d("outflw_oavg"), sums["outflw"])     # not yet averaged
