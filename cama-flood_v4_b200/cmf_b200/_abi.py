@@ -103,7 +103,7 @@ EXPORTS = [
     "cmf_gpu_get_diag", "cmf_gpu_finalize", "cmf_gpu_strerror", "cmf_gpu_last_error", "cmf_gpu_abi_version",
     "cmf_host_load", "cmf_host_free", "cmf_host_describe", "cmf_host_state", "cmf_host_conv_resol", "cmf_host_grid",
     "cmf_gpu_stage_noalloc", "cmf_gpu_ctx_nt_stats", "cmf_gpu_ctx_diag_output", "cmf_gpu_ctx_get_diag_output",
-    "cmf_gpu_diag_output", "cmf_gpu_get_diag_output",
+    "cmf_gpu_diag_output", "cmf_gpu_get_diag_output", "cmf_gpu_ctx_persist_selftest", "cmf_gpu_ctx_launch_mode",
 ]
 
 _lib = None
@@ -145,6 +145,8 @@ def load(build_if_missing: bool = True):
     lib.cmf_gpu_ctx_counters.argtypes = [vp, C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
     lib.cmf_gpu_ctx_time_phases.argtypes = [vp, C.c_double, C.c_int32, f64p]
     lib.cmf_gpu_ctx_nt_stats.argtypes = [vp, C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.c_int32]
+    lib.cmf_gpu_ctx_persist_selftest.argtypes = [vp, C.c_int64]
+    lib.cmf_gpu_ctx_launch_mode.argtypes = [vp]
     lib.cmf_gpu_ctx_diag_output.argtypes = [vp, C.c_int32]
     lib.cmf_gpu_ctx_get_diag_output.argtypes = [vp, C.POINTER(DiagOutPtrs)]
     lib.cmf_gpu_diag_output.argtypes = [C.c_int32]

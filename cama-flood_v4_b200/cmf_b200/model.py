@@ -366,6 +366,29 @@ class PhysicsGPU:
     def block_size(self) -> int:
         return int(self.lib.cmf_gpu_ctx_block_size(self.h))
 
+    @property
+    def launch_mode(self) -> int:
+        """0: graph of phase kernels, 1: host-driven phase kernels, 2: persistent kernel."""
+        return int(self.lib.cmf_gpu_ctx_launch_mode(self.h))
+
+    def schedule(self) -> dict:
+        """The launch schedule the context runs (chosen by the autotuner unless forced)."""
+        if self.launch_mode == 2:
+            return {"kernels": "one persistent cooperative kernel per coupling step (grid barriers between phases, "
+                               "tiles of 256 cells streamed by bulk asynchronous copies)"}
+        return {"kernels": "stage, NT/DT, {flux, rate, store} x NT, budget", "block_size": self.block_size}
+
+    def launches_per_step(self) -> int:
+        """Kernel launches per outer step outside the sub-step loop."""
+        return 1 if self.launch_mode == 2 else 3
+
+    def launches_per_substep(self) -> int:
+        return 0 if self.launch_mode == 2 else 3
+
+    def persist_selftest(self, wait_ns: int = 2_000_000) -> int:
+        """Status of the persistent kernel's bounded-wait check (CMF_E_BARRIER = 5 when it works)."""
+        return int(self.lib.cmf_gpu_ctx_persist_selftest(self.h, int(wait_ns)))
+
     def get_diag(self) -> dict:
         dp = _abi.DiagPtrs()
         out = {}

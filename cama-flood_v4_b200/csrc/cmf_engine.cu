@@ -17,6 +17,7 @@
 
 #include "../../include/cmf_gpu.h"
 #include "cmf_kernels.cuh"
+#include "cmf_persist.cuh"
 
 namespace {
 
@@ -49,6 +50,8 @@ struct cmf_gpu_ctx {
     std::vector<void *> allocs;
     int block = 256;
     int ncell_blocks = 0, npath_blocks = 0;
+    int persist_grid = 0;       // co-resident CTAs of the persistent kernel (0: it cannot run here)
+    bool persist = false;       // outer steps run as one persistent cooperative launch
     bool small_cells = false;   // N x M <= kSmallCellMembers: the low-spill profile of k_flux/k_store
     int nlev = 0, ndam_placed = 0;
     size_t E = 0;
@@ -68,12 +71,14 @@ struct cmf_gpu_ctx {
     void *rgrid = nullptr;
     size_t rgrid_bytes = 0;
 
+    // every device array gets 16 bytes of zeroed slack after its end: the persistent kernel's bulk
+    // copies fetch 16-byte aligned ranges, which may end up to 16 bytes past the last element
     template <class T>
     int alloc(T **p, size_t n) {
         void *q = nullptr;
         if (n == 0) n = 1;
-        CUDA_TRY(cudaMalloc(&q, n * sizeof(T)));
-        CUDA_TRY(cudaMemsetAsync(q, 0, n * sizeof(T), stream));
+        CUDA_TRY(cudaMalloc(&q, n * sizeof(T) + 16));
+        CUDA_TRY(cudaMemsetAsync(q, 0, n * sizeof(T) + 16, stream));
         allocs.push_back(q);
         *p = static_cast<T *>(q);
         return CMF_OK;
@@ -439,7 +444,39 @@ int sync_dt_def(cmf_gpu_ctx *c, double dt_def) {
     return CMF_OK;
 }
 
+// ---- persistent schedule: one cooperative launch per outer step --------------------------------
+int persist_setup(cmf_gpu_ctx *c) {
+    CUDA_TRY(cudaFuncSetAttribute(cmf::k_persist, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cmf::kPersistSmem));
+    int per_sm = 0, nsm = 0;
+    CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cmf::k_persist, cmf::kTile, cmf::kPersistSmem));
+    CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device));
+    int coop = 0;
+    CUDA_TRY(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, c->device));
+    c->persist_grid = coop ? per_sm * nsm : 0;
+    return CMF_OK;
+}
+
+cmf::PersistArgs persist_args(const cmf_gpu_ctx *c) {
+    cmf::PersistArgs a{};
+    a.tpm = (c->dims.nseqall + cmf::kTile - 1) / cmf::kTile;
+    a.ppm = c->net.P > 0 ? (c->net.P + cmf::kTile - 1) / cmf::kTile : 0;
+    a.wait_ns = cmf::kWaitNsDefault;
+    a.selftest = 0;
+    return a;
+}
+
+int launch_persist(cmf_gpu_ctx *c, cmf::PersistArgs a) {
+    if (c->persist_grid < 1) return set_err(CMF_E_UNSUPPORTED, "the persistent kernel cannot be co-resident on this device");
+    CUDA_TRY(cudaMemsetAsync(&c->st.loop->bar, 0, sizeof(unsigned), c->stream));
+    void *args[] = {&c->net, &c->st, &a};
+    CUDA_TRY(cudaLaunchCooperativeKernel((const void *)cmf::k_persist, dim3(c->persist_grid), dim3(cmf::kTile), args,
+                                         cmf::kPersistSmem, c->stream));
+    c->launches += 1;
+    return CMF_OK;
+}
+
 int launch_outer(cmf_gpu_ctx *c) {
+    if (c->persist) return launch_persist(c, persist_args(c));
     if (c->opts.launch_mode == 0) {
         CUDA_TRY(cudaGraphLaunch(c->exec, c->stream));
         c->launches += 3;   // prologue and epilogue; the loop body adds 3 per sub-step (counted on read-back)
@@ -533,6 +570,17 @@ int d2h(cmf_gpu_ctx *c, T *dst, const T *src, size_t n) {
 int finish_outer(cmf_gpu_ctx *c, int32_t *nt_out, double *dt_out, cmf_budget *b) {
     int rc = read_ctl(c);
     if (rc) return rc;
+    if (c->persist) {
+        int berr = 0;
+        CUDA_TRY(cudaMemcpyAsync(&berr, &c->st.loop->bar_err, sizeof berr, cudaMemcpyDeviceToHost, c->stream));
+        CUDA_TRY(cudaStreamSynchronize(c->stream));
+        if (berr) {
+            CUDA_TRY(cudaMemsetAsync(&c->st.loop->bar_err, 0, sizeof(int), c->stream));
+            CUDA_TRY(cudaStreamSynchronize(c->stream));
+            return set_err(CMF_E_BARRIER, berr == 2 ? "persistent kernel: a bulk copy did not complete within its bound"
+                                                    : "persistent kernel: a grid barrier did not complete within its bound");
+        }
+    }
     int err = 0;
     int ntmax = 0;
     for (size_t m = 0; m < c->hctl.size(); m++) {
@@ -548,7 +596,7 @@ int finish_outer(cmf_gpu_ctx *c, int32_t *nt_out, double *dt_out, cmf_budget *b)
             b[m].fldare = x.budget[9]; b[m].levsto = x.budget[10]; b[m].dam_miss = x.budget[11];
         }
     }
-    if (c->opts.launch_mode == 0) c->launches += 3LL * ntmax;
+    if (c->opts.launch_mode == 0 && !c->persist) c->launches += 3LL * ntmax;
     if (err) {
         int bad = -1;
         for (size_t m = 0; m < c->hctl.size(); m++)
@@ -635,6 +683,7 @@ const char *cmf_gpu_strerror(int status) {
         case CMF_E_NT_CAP: return "adaptive sub-step count not finite or above the cap";
         case CMF_E_NO_DEVICE: return "no usable CUDA device (sm_100a required)";
         case CMF_E_NONFINITE: return "non-finite storage after a sub-step";
+        case CMF_E_BARRIER: return "a bounded device-side wait ran out";
         default: return "unknown status";
     }
 }
@@ -676,10 +725,15 @@ int cmf_gpu_create(const cmf_dims *dims, const cmf_params *params, const cmf_map
     } else if ((rc = autotune(c))) {
         return fail(rc);
     }
+    if ((rc = persist_setup(c))) return fail(rc);
+    if (opts->launch_mode == 2) {
+        if (c->persist_grid < 1) return fail(set_err(CMF_E_UNSUPPORTED, "launch_mode 2: the persistent kernel cannot run here"));
+        c->persist = true;
+    }
     if ((rc = zero_state(c))) return fail(rc);
     c->dt_def_dev = -1.0;
     if ((rc = sync_dt_def(c, 86400.0))) return fail(rc);
-    if (opts->launch_mode == 0 && (rc = build_graph(c))) return fail(rc);
+    if ((opts->launch_mode == 0 || c->persist) && (rc = build_graph(c))) return fail(rc);
     if (cudaStreamSynchronize(c->stream) != cudaSuccess) return fail(set_err(CMF_E_CUDA, cudaGetErrorString(cudaGetLastError())));
     *out = c;
     return CMF_OK;
@@ -794,6 +848,27 @@ int cmf_gpu_ctx_get_diag_output(cmf_gpu_ctx *c, const cmf_diag_out_ptrs *p) {
     CUDA_TRY(cudaStreamSynchronize(c->stream));
     return CMF_OK;
 }
+
+int cmf_gpu_ctx_persist_selftest(cmf_gpu_ctx *c, int64_t wait_ns) {
+    if (!c) return set_err(CMF_E_STATE, "no context");
+    if (wait_ns < 1000 || wait_ns > 2000000000LL) return set_err(CMF_E_ARG, "wait_ns must lie in [1 us, 2 s]");
+    CUDA_TRY(cudaSetDevice(c->device));
+    cmf::PersistArgs a = persist_args(c);
+    a.wait_ns = (unsigned long long)wait_ns;
+    a.selftest = 1;
+    int rc = launch_persist(c, a);
+    if (rc) return rc;
+    int berr = 0;
+    CUDA_TRY(cudaMemcpyAsync(&berr, &c->st.loop->bar_err, sizeof berr, cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    CUDA_TRY(cudaGetLastError());
+    if (!berr) return set_err(CMF_E_STATE, "persistent self-test: the barrier completed although it could not");
+    CUDA_TRY(cudaMemsetAsync(&c->st.loop->bar_err, 0, sizeof(int), c->stream));
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    return set_err(CMF_E_BARRIER, "persistent self-test: the grid barrier ran out its bound and the kernel returned");
+}
+
+int32_t cmf_gpu_ctx_launch_mode(cmf_gpu_ctx *c) { return c ? (c->persist ? 2 : c->opts.launch_mode) : -1; }
 
 int cmf_gpu_ctx_nt_stats(cmf_gpu_ctx *c, int64_t *near_boundary, int64_t *hist, int32_t nbins) {
     if (!c) return set_err(CMF_E_STATE, "no context");
@@ -937,7 +1012,9 @@ int cmf_gpu_ctx_advance_device(cmf_gpu_ctx *c, double dt_def, int32_t ksteps, co
     for (int k = 0; k < ksteps; k++) {
         if (runoff_dev)
             CUDA_TRY(cudaMemcpyAsync(c->st.runoff, runoff_dev + (size_t)k * stride, MN * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
-        if (c->opts.launch_mode == 0) {
+        if (c->persist) {
+            if ((rc = launch_persist(c, persist_args(c)))) return rc;
+        } else if (c->opts.launch_mode == 0) {
             CUDA_TRY(cudaGraphLaunch(c->exec, c->stream));
             c->launches += 3;
         } else {
@@ -1352,7 +1429,7 @@ __global__ void k_noalloc_stage(cmf::Net n, cmf::State s, double *blockmin) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     double key = 1.0e308;
     if (i < n.N) {
-        const cmf::StageOut o = cmf::stage_def(n, i, s.rivsto[i], s.fldsto[i]);
+        const cmf::StageOut o = cmf::stage_def(n, cmf::OwnG{n, s}, i, s.rivsto[i], s.fldsto[i]);
         cmf::store_stage(n, s, i, i, o);
         if (n.ladpstp && n.i2mask[i] == 0)
             key = cmf::cfl_key(n.pcadp, (i < n.R) ? n.nxtdst[i] : n.pdstmth, n.pgrv, o.rivdph);

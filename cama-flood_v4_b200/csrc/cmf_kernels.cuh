@@ -79,6 +79,8 @@ struct LoopCtl {
     long long near_int;          // (outer step, member) pairs whose DT_DEF/DT_MIN-0.01 lay within
                                  // 1e-12 (relative) of an integer: NT there hangs on DT_MIN's last bits
     long long nt_hist[kNtHist];  // (outer step, member) pairs by NT
+    unsigned bar;                // grid-barrier arrival count of the persistent kernel (zeroed per launch)
+    int bar_err;                 // set when a bounded wait of the persistent kernel ran out
 };
 
 // Static data shared by all members (device pointers).
@@ -136,6 +138,35 @@ struct State {
 
 __device__ __forceinline__ double dmax(double a, double b) { return (a > b) ? a : b; }
 __device__ __forceinline__ double dmin(double a, double b) { return (a < b) ? a : b; }
+
+// Own-cell reads of the per-cell code go through an accessor.  OwnG reads the arrays in global
+// memory (the phase kernels); the persistent kernel's accessors read the same values from the
+// shared-memory tiles its bulk copies filled.  The arithmetic is shared, so both produce the same
+// bits.  Static maps are indexed by the cell i, member state by g = m*N + i; reads of another
+// cell (downstream, upstream, path ends) always go to global memory through Net/State.
+#define CMF_OWN_STATIC(name) \
+    __device__ __forceinline__ double name(int i) const { return n.name[i]; }
+#define CMF_OWN_STATE(name) \
+    __device__ __forceinline__ double name(size_t g) const { return s.name[g]; }
+struct OwnG {
+    const Net &n;
+    const State &s;
+    CMF_OWN_STATIC(rivelv) CMF_OWN_STATIC(elevtn) CMF_OWN_STATIC(nxtdst) CMF_OWN_STATIC(rivwth)
+    CMF_OWN_STATIC(rivhgt) CMF_OWN_STATIC(rivlen) CMF_OWN_STATIC(rivman) CMF_OWN_STATIC(grarea)
+    CMF_OWN_STATIC(rivstomax)
+    __device__ __forceinline__ int next(int i) const { return n.next[i]; }
+    __device__ __forceinline__ int up_lo(int i) const { return n.up_ptr[i]; }
+    __device__ __forceinline__ int up_hi(int i) const { return n.up_ptr[i + 1]; }
+    __device__ __forceinline__ int i1dam(int i) const { return n.i1dam[i]; }
+    CMF_OWN_STATE(rivsto) CMF_OWN_STATE(fldsto) CMF_OWN_STATE(levsto) CMF_OWN_STATE(rivdph)
+    CMF_OWN_STATE(rivdph_pre) CMF_OWN_STATE(rivout_pre) CMF_OWN_STATE(fldout_pre) CMF_OWN_STATE(fldsto_pre)
+    CMF_OWN_STATE(flddph) CMF_OWN_STATE(fldfrc) CMF_OWN_STATE(storge) CMF_OWN_STATE(runoff)
+    CMF_OWN_STATE(rivout_raw) CMF_OWN_STATE(fldout_raw) CMF_OWN_STATE(rate)
+    CMF_OWN_STATE(a_rivvel) CMF_OWN_STATE(a_rivout) CMF_OWN_STATE(a_fldout) CMF_OWN_STATE(a_outflw)
+    CMF_OWN_STATE(a_pthout) CMF_OWN_STATE(m_outflw) CMF_OWN_STATE(m_rivdph) CMF_OWN_STATE(m_storge)
+};
+#undef CMF_OWN_STATIC
+#undef CMF_OWN_STATE
 
 // x**(-7._JPRB/3._JPRB) and x**(-4._JPRB/3._JPRB) of the local-inertial flux formulas
 // (src/cmf_calc_outflw_mod.F90:74,106,133,162; src/cmf_calc_pthout_mod.F90:67;
@@ -205,16 +236,17 @@ struct StageOut {
 };
 
 // CMF_CALC_FLDSTG_DEF body, src/cmf_calc_fldstg_mod.F90:46-97
-__device__ __forceinline__ StageOut stage_def(const Net &n, int i, double rivsto, double fldsto) {
+template <class Own>
+__device__ __forceinline__ StageOut stage_def(const Net &n, const Own &w, int i, double rivsto, double fldsto) {
     StageOut o;
     const int N = n.N, L = n.L;
     const double pstoall = rivsto + fldsto;
-    const double rsm = n.rivstomax[i];
+    const double rsm = w.rivstomax(i);
     o.levsto = 0.0;
     o.levdph = 0.0;
     if (pstoall > rsm) {
-        const double len = n.rivlen[i], wth = n.rivwth[i];
-        const double inc = (n.grarea[i] / len) * n.dfrcinc;
+        const double len = w.rivlen(i), wth = w.rivwth(i);
+        const double inc = (w.grarea(i) / len) * n.dfrcinc;
         int I = 0;   // 0-based layer
         double sfil = rsm, wfil = wth, dfil = 0.0;
         while (I < L) {
@@ -244,10 +276,10 @@ __device__ __forceinline__ StageOut stage_def(const Net &n, int i, double rivsto
         frc = dmax(frc, 0.0);
         frc = dmin(frc, 1.0);
         o.fldfrc = frc;
-        o.fldare = n.grarea[i] * frc;
+        o.fldare = w.grarea(i) * frc;
     } else {
         o.rivsto = pstoall;
-        o.rivdph = dmax((pstoall / n.rivlen[i]) / n.rivwth[i], 0.0);
+        o.rivdph = dmax((pstoall / w.rivlen(i)) / w.rivwth(i), 0.0);
         o.fldsto = 0.0;
         o.flddph = 0.0;
         o.fldfrc = 0.0;
@@ -257,13 +289,16 @@ __device__ __forceinline__ StageOut stage_def(const Net &n, int i, double rivsto
 }
 
 // CMF_LEVEE_FLDSTG body, src/cmf_ctrl_levee_mod.F90:301-461
-__device__ __forceinline__ StageOut stage_levee(const Net &n, int i, double rivsto, double fldsto, double levsto) {
+template <class Own>
+__device__ __forceinline__ StageOut stage_levee(const Net &n, const Own &w, int i, double rivsto, double fldsto,
+                                                double levsto) {
     StageOut o;
     const int N = n.N, L = n.L;
     const double pstoall = (rivsto + fldsto) + levsto;
-    const double rsm = n.rivstomax[i];
-    const double len = n.rivlen[i], wth = n.rivwth[i];
-    const double inc = (n.grarea[i] / len) * n.dfrcinc;
+    const double rsm = w.rivstomax(i);
+    const double len = w.rivlen(i), wth = w.rivwth(i);
+    const double inc = (w.grarea(i) / len) * n.dfrcinc;
+    const double grarea = w.grarea(i);
     const int lv = n.lev_id[i];
     const double lbas = lv >= 0 ? n.levbassto[lv] : 1.E18;
     if (pstoall > rsm) {
@@ -291,7 +326,7 @@ __device__ __forceinline__ StageOut stage_levee(const Net &n, int i, double rivs
             frc = dmax(frc, 0.0);
             frc = dmin(frc, 1.0);
             o.fldfrc = frc;
-            o.fldare = n.grarea[i] * frc;
+            o.fldare = grarea * frc;
             o.levsto = 0.0;
             o.levdph = 0.0;
         } else {
@@ -305,7 +340,7 @@ __device__ __forceinline__ StageOut stage_levee(const Net &n, int i, double rivs
                 o.rivdph = (o.rivsto / len) / wth;
                 o.fldsto = dmax(pstoall - o.rivsto, 0.0);
                 o.fldfrc = lfrc;
-                o.fldare = n.grarea[i] * lfrc;
+                o.fldare = grarea * lfrc;
                 o.levsto = 0.0;
                 o.levdph = 0.0;
             } else if (pstoall < lfil) {                                            // case 3
@@ -334,12 +369,12 @@ __device__ __forceinline__ StageOut stage_levee(const Net &n, int i, double rivs
                     frc = dmax(frc, 0.0);
                     frc = dmin(frc, 1.0);
                     o.fldfrc = frc;
-                    o.fldare = n.grarea[i] * frc;
+                    o.fldare = grarea * frc;
                 } else {
                     const double dadd = ((pstoall - sfil) / wfil) / len;
                     o.levdph = (bhgt + dfil) + dadd;
                     o.fldfrc = 1.0;
-                    o.fldare = n.grarea[i] * 1.0;
+                    o.fldare = grarea * 1.0;
                 }
             } else {                                                                // case 4
                 int I = 0;
@@ -359,7 +394,7 @@ __device__ __forceinline__ StageOut stage_levee(const Net &n, int i, double rivs
                     o.flddph = dfil + ((pstoall - sfil) / wfil) / len;
                 }
                 o.fldfrc = ((-wth + wfil) + wadd) / (inc * (double)L);
-                o.fldare = n.grarea[i] * o.fldfrc;
+                o.fldare = grarea * o.fldfrc;
                 o.rivsto = rsm + (len * wth) * o.flddph;
                 o.rivdph = (o.rivsto / len) / wth;
                 const double sadd = ((o.flddph - lhgt) * (ldst + wth)) * len;
@@ -428,8 +463,9 @@ __global__ void __launch_bounds__(kCellThreads, CMF_STAGE_MINB) k_stage(Net n, S
     double key = 1.0e308;
     if (i < n.N) {
         const size_t gi = (size_t)m * n.N + i;
-        const StageOut o = n.llevee ? stage_levee(n, i, s.rivsto[gi], s.fldsto[gi], s.levsto[gi])
-                                    : stage_def(n, i, s.rivsto[gi], s.fldsto[gi]);
+        const OwnG w{n, s};
+        const StageOut o = n.llevee ? stage_levee(n, w, i, s.rivsto[gi], s.fldsto[gi], s.levsto[gi])
+                                    : stage_def(n, w, i, s.rivsto[gi], s.fldsto[gi]);
         store_stage(n, s, gi, i, o);
         if (n.ladpstp && n.i2mask[i] == 0) key = cfl_key(n.pcadp, (i < n.R) ? n.nxtdst[i] : n.pdstmth, n.pgrv, o.rivdph);
     }
@@ -518,26 +554,28 @@ __device__ __forceinline__ double nadd_before(int k, double dt) {
     return a;
 }
 
-__device__ __forceinline__ void cell_outflow(const Net &n, const State &s, int m, int i, double DT, const MemberCtl &c,
-                                             int k) {
+template <class Own>
+__device__ __forceinline__ void cell_outflow(const Net &n, const State &s, const Own &w, int m, int i, double DT,
+                                             const MemberCtl &c, int k, bool split) {
     const size_t base = (size_t)m * n.N, gi = base + i;
     const double gdt = n.pgrv * DT;
-    const double rivelv = n.rivelv[i];
-    const double rivdph = s.rivdph[gi], rivdph_pre = s.rivdph_pre[gi];
+    const double rivelv = w.rivelv(i);
+    const double rivdph = w.rivdph(gi), rivdph_pre = w.rivdph_pre(gi);
     const double sfc = rivelv + rivdph;
     const double sfc_pre = rivelv + rivdph_pre;
-    const double flddph_pre = dmax(rivdph_pre - n.rivhgt[i], 0.0);
-    const double wth = n.rivwth[i];
-    const double man = n.rivman[i];
-    const double rivout_old = s.loop->split ? s.rivout_cur[gi] : s.rivout_pre[gi];
+    const double flddph_pre = dmax(rivdph_pre - w.rivhgt(i), 0.0);
+    const double wth = w.rivwth(i);
+    const double man = w.rivman(i);
+    const double rivout_pre = w.rivout_pre(gi);
+    const double rivout_old = split ? s.rivout_cur[gi] : rivout_pre;
     double rout, fout = 0.0, rvel;
     if (i < n.R) {
-        const int j = n.next[i];
+        const int j = w.next(i);
         const size_t gj = base + j;
         const double rj = n.rivelv[j];
         const double dwn = rj + s.rivdph[gj];
         const double dwn_pre = rj + s.rivdph_pre[gj];
-        const double inv_dst = 1.0 / n.nxtdst[i];
+        const double inv_dst = 1.0 / w.nxtdst(i);
         // river
         {
             const double dsfc = dmax(sfc, dwn);
@@ -546,7 +584,7 @@ __device__ __forceinline__ void cell_outflow(const Net &n, const State &s, int m
             const double dare = dmax(wth * dflw, 1.E-10);
             const double dflw_pr = dmax(sfc_pre, dwn_pre) - rivelv;
             const double dflw_im = dmax(sqrt(dflw * dflw_pr), 1.E-6);
-            const double dout_pr = s.rivout_pre[gi] * (1.0 / wth);
+            const double dout_pr = rivout_pre * (1.0 / wth);
             const double dout = (wth * (dout_pr + (gdt * dflw_im) * dslp))
                               * (1.0 / (1.0 + ((gdt * (man * man)) * fabs(dout_pr)) * pow_depth<7>(dflw_im)));
             const double dvel = rivout_old * (1.0 / dare);
@@ -555,19 +593,19 @@ __device__ __forceinline__ void cell_outflow(const Net &n, const State &s, int m
             rvel = mask ? dvel : 0.0;
         }
         if (n.lfldout) {
-            const double len = n.rivlen[i], elv = n.elevtn[i];
+            const double len = w.rivlen(i), elv = w.elevtn(i);
             const double dsfc = dmax(sfc, dwn);
             double dslp = (sfc - dwn) * inv_dst;
             dslp = dmax(-0.005, dmin(0.005, dslp));
             const double dflw = dmax(dsfc - elv, 0.0);
-            double dare = s.fldsto[gi] * (1.0 / len);
-            dare = dmax(dare - s.flddph[gi] * wth, 0.0);
+            double dare = w.fldsto(gi) * (1.0 / len);
+            dare = dmax(dare - w.flddph(gi) * wth, 0.0);
             const double dflw_pr = dmax(sfc_pre, dwn_pre) - elv;
             const double dflw_im = dmax(sqrt(dmax(dflw * dflw_pr, 0.0)), 1.E-6);
-            double dare_pr = s.fldsto_pre[gi] * (1.0 / len);
+            double dare_pr = w.fldsto_pre(gi) * (1.0 / len);
             dare_pr = dmax(dare_pr - flddph_pre * wth, 1.E-6);
             const double dare_im = dmax(sqrt(dare * dare_pr), 1.E-6);
-            const double dout_pr = s.fldout_pre[gi];
+            const double dout_pr = w.fldout_pre(gi);
             const double dout = (dout_pr + (gdt * dare_im) * dslp)
                 * (1.0 / (1.0 + (((gdt * (n.pmanfld * n.pmanfld)) * fabs(dout_pr)) * pow_depth<4>(dflw_im)) * (1.0 / dare_im)));
             const bool mask = (dflw_im > 1.E-5 && dare > 1.E-5);
@@ -576,7 +614,7 @@ __device__ __forceinline__ void cell_outflow(const Net &n, const State &s, int m
         }
         // storage-change limiter (v423), :176-182
         const double dlim = dmax((-rout - fout) * DT, CMF_F(1.E-10));
-        const double rate = dmin((0.05 * s.storge[gi]) / dlim, 1.0);
+        const double rate = dmin((0.05 * w.storge(gi)) / dlim, 1.0);
         rout = rout * rate;
         fout = fout * rate;
     } else {
@@ -586,7 +624,7 @@ __device__ __forceinline__ void cell_outflow(const Net &n, const State &s, int m
             const double dslp = (sfc - dwn) * inv_dst;
             const double dare = dmax(wth * rivdph, 1.E-10);
             const double dflw_im = dmax(sqrt(rivdph * rivdph_pre), 1.E-6);
-            const double dout_pr = s.rivout_pre[gi] * (1.0 / wth);
+            const double dout_pr = rivout_pre * (1.0 / wth);
             const double dout = (wth * (dout_pr + (gdt * dflw_im) * dslp))
                               * (1.0 / (1.0 + ((gdt * (man * man)) * fabs(dout_pr)) * pow_depth<7>(dflw_im)));
             const double dvel = rivout_old * (1.0 / dare);
@@ -595,16 +633,16 @@ __device__ __forceinline__ void cell_outflow(const Net &n, const State &s, int m
             rvel = mask ? dvel : 0.0;
         }
         if (n.lfldout) {
-            const double len = n.rivlen[i], elv = n.elevtn[i];
+            const double len = w.rivlen(i), elv = w.elevtn(i);
             double dslp = (sfc - dwn) * inv_dst;
             dslp = dmax(-0.005, dmin(0.005, dslp));
             const double dflw = sfc - elv;
-            const double dare = dmax(s.fldsto[gi] * (1.0 / len) - s.flddph[gi] * wth, 0.0);
+            const double dare = dmax(w.fldsto(gi) * (1.0 / len) - w.flddph(gi) * wth, 0.0);
             const double dflw_pr = sfc_pre - elv;
             const double dflw_im = dmax(sqrt(dmax(dflw * dflw_pr, 0.0)), 1.E-6);
-            const double dare_pr = dmax(s.fldsto_pre[gi] * (1.0 / len) - flddph_pre * wth, 1.E-6);
+            const double dare_pr = dmax(w.fldsto_pre(gi) * (1.0 / len) - flddph_pre * wth, 1.E-6);
             const double dare_im = dmax(sqrt(dare * dare_pr), 1.E-6);
-            const double dout_pr = s.fldout_pre[gi];
+            const double dout_pr = w.fldout_pre(gi);
             const double dout = (dout_pr + (gdt * dare_im) * dslp)
                 * (1.0 / (1.0 + (((gdt * (n.pmanfld * n.pmanfld)) * fabs(dout_pr)) * pow_depth<4>(dflw_im)) * (1.0 / dare_im)));
             const bool mask = (dflw_im > CMF_F(1.E-5) && dare > CMF_F(1.E-5));
@@ -614,7 +652,7 @@ __device__ __forceinline__ void cell_outflow(const Net &n, const State &s, int m
     }
     // reservoir operation, CMF_DAMOUT_CALC (src/cmf_ctrl_damout_mod.F90:316-498)
     if (n.ldamout) {
-        const int code = n.i1dam[i];
+        const int code = w.i1dam(i);
         if (code > 0) {
             rout = 0.0;
             fout = 0.0;
@@ -689,7 +727,7 @@ __device__ __forceinline__ void cell_outflow(const Net &n, const State &s, int m
     const bool first = (k == 0), last = (k == c.nt - 1);
     if (last) s.rivvel[gi] = rvel;
     if (n.ldiag) {
-        double a = first ? rvel * DT : s.a_rivvel[gi] + rvel * DT;
+        double a = first ? rvel * DT : w.a_rivvel(gi) + rvel * DT;
         if (last) {
             a = a / (nadd_before(k, DT) + DT);
             if (n.ldiag_out) s.o_rivvel[gi] = s.o_rivvel[gi] + a * c.dt_def;   // CMF_DIAG_AVEMAX_OUTPUT
@@ -784,7 +822,7 @@ __global__ void __launch_bounds__(kCellThreads, MinBlocks) k_flux(Net n, State s
     const double DT = c.dt;
     if ((int)blockIdx.x < ncell_blocks) {
         const int i = blockIdx.x * blockDim.x + threadIdx.x;
-        if (i < n.N) cell_outflow(n, s, m, i, DT, c, k);
+        if (i < n.N) cell_outflow(n, s, OwnG{n, s}, m, i, DT, c, k, s.loop->split != 0);
     } else {
         const int p = (blockIdx.x - ncell_blocks) * blockDim.x + threadIdx.x;
         if (p < n.P) path_outflow(n, s, m, p, DT);
@@ -794,6 +832,26 @@ __global__ void __launch_bounds__(kCellThreads, MinBlocks) k_flux(Net n, State s
 // ------------------------------------------------------------------------------------------
 // phase B: P2STOOUT and D2RATE, src/cmf_calc_outflw_mod.F90:410-451
 // ------------------------------------------------------------------------------------------
+template <class Own>
+__device__ __forceinline__ void cell_rate(const Net &n, const State &s, const Own &w, int m, int i, double DT) {
+    const size_t base = (size_t)m * n.N, gi = base + i;
+    double so = dmax(w.rivout_raw(gi), 0.0) + dmax(w.fldout_raw(gi), 0.0);
+    const int u1 = w.up_hi(i);
+    for (int k = w.up_lo(i); k < u1; k++) {
+        const int j = n.up_idx[k];
+        so = (so + dmax(-s.rivout_raw[base + j], 0.0)) + dmax(-s.fldout_raw[base + j], 0.0);
+    }
+    so = so * DT;
+    if (n.lpthout) {
+        const double *sum = s.pthsum_raw + (size_t)m * n.P;
+        for (int k = n.pout_ptr[i]; k < n.pout_ptr[i + 1]; k++) so = so + dmax(sum[n.pout_idx[k]], 0.0) * DT;
+        for (int k = n.pinf_ptr[i]; k < n.pinf_ptr[i + 1]; k++) so = so + dmax(-sum[n.pinf_idx[k]], 0.0) * DT;
+    }
+    const double dout = dmax(so, 1.E-10);
+    const double dsto = w.rivsto(gi) + w.fldsto(gi);
+    s.rate[gi] = dmin(dsto / dout, 1.0);
+}
+
 // advance != 0: block (0,0) also moves the loop counter to the next sub-step and sets the WHILE
 // condition (every k_flux block has read the counter; k_rate and k_store read `kcur`)
 __global__ void k_rate(Net n, State s, int advance, cudaGraphConditionalHandle h, int use_cond) {
@@ -809,22 +867,7 @@ __global__ void k_rate(Net n, State s, int advance, cudaGraphConditionalHandle h
     if (k >= c.nt) return;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n.N) return;
-    const double DT = c.dt;
-    const size_t base = (size_t)m * n.N, gi = base + i;
-    double so = dmax(s.rivout_raw[gi], 0.0) + dmax(s.fldout_raw[gi], 0.0);
-    for (int k = n.up_ptr[i]; k < n.up_ptr[i + 1]; k++) {
-        const int j = n.up_idx[k];
-        so = (so + dmax(-s.rivout_raw[base + j], 0.0)) + dmax(-s.fldout_raw[base + j], 0.0);
-    }
-    so = so * DT;
-    if (n.lpthout) {
-        const double *sum = s.pthsum_raw + (size_t)m * n.P;
-        for (int k = n.pout_ptr[i]; k < n.pout_ptr[i + 1]; k++) so = so + dmax(sum[n.pout_idx[k]], 0.0) * DT;
-        for (int k = n.pinf_ptr[i]; k < n.pinf_ptr[i + 1]; k++) so = so + dmax(-sum[n.pinf_idx[k]], 0.0) * DT;
-    }
-    const double dout = dmax(so, 1.E-10);
-    const double dsto = s.rivsto[gi] + s.fldsto[gi];
-    s.rate[gi] = dmin(dsto / dout, 1.0);
+    cell_rate(n, s, OwnG{n, s}, m, i, c.dt);
 }
 
 // ------------------------------------------------------------------------------------------
@@ -834,6 +877,185 @@ __device__ __forceinline__ double scaled_pathsum(const Net &n, const double *sum
     const double v = sum_raw[p];
     if (n.pth_skip[p] & 1) return v;
     return v >= 0.0 ? v * rate_m[n.pth_up[p]] : v * rate_m[n.pth_dn[p]];
+}
+
+// bifurcation paths in phase C: LSPAMAT path rescale (:494-517), CALC_VARS_PRE copy, diagnostics
+__device__ __forceinline__ void path_rescale(const Net &n, const State &s, int m, int p, double DT, bool first, bool last,
+                                             double nadd, double dt_def) {
+    const int P = n.P, Lp = n.Lp;
+    const size_t base = (size_t)m * n.N;
+    const size_t pb = (size_t)m * Lp * P;
+    const double *rate_m = s.rate + base;
+    const bool sk = n.pth_skip[p] & 1;
+    const int u = n.pth_up[p], d = n.pth_dn[p];
+    double asum = 0.0;
+    for (int l = 0; l < Lp; l++) {
+        const size_t o = pb + (size_t)l * P + p;
+        double f = s.pthflw_raw[o];
+        if (!sk) f = (f >= 0.0) ? f * rate_m[u] : f * rate_m[d];
+        s.pthflw_pre[o] = f;
+        if (n.ldiag) {
+            double a = first ? f * DT : s.a_pthflw[o] + f * DT;
+            if (last) {
+                a = a / (nadd + DT);
+                asum = asum + a;
+                if (n.ldiag_out) s.o_pthflw[o] = s.o_pthflw[o] + a * dt_def;
+            }
+            s.a_pthflw[o] = a;
+        }
+    }
+    s.pthsum[(size_t)m * P + p] = scaled_pathsum(n, s.pthsum_raw + (size_t)m * P, rate_m, p);
+    if (n.ldiag && last) s.a_pthsum[(size_t)m * P + p] = asum;
+}
+
+// one cell in phase C; `bput(k, v)` receives the last sub-step's budget term k
+template <class Own, class BPut>
+__device__ __forceinline__ void cell_store(const Net &n, const State &s, const Own &w, int m, int i, double DT,
+                                           bool first, bool last, double nadd, const MemberCtl &c, BPut bput) {
+    const size_t base = (size_t)m * n.N;
+    const size_t gi = base + i;
+    const double *rate_m = s.rate + base;
+    const double rate_i = w.rate(gi);
+    // own outflow after the LSPAMAT rescale (:456-473)
+    double rout = w.rivout_raw(gi), fout = w.fldout_raw(gi);
+    if (i < n.R) {
+        const double r = (rout > 0.0) ? rate_i : rate_m[w.next(i)];
+        rout = rout * r;
+        fout = fout * r;
+    } else {
+        rout = rout * rate_i;
+        fout = fout * rate_i;
+    }
+    // inflow from the upstream cells, rescaled on the fly (:481-489); next(j) == i
+    double rinf = 0.0, finf = 0.0;
+    const int u1 = w.up_hi(i);
+    for (int k = w.up_lo(i); k < u1; k++) {
+        const int j = n.up_idx[k];
+        const double rj = s.rivout_raw[base + j], fj = s.fldout_raw[base + j];
+        const double r = (rj > 0.0) ? rate_m[j] : rate_i;
+        rinf = rinf + rj * r;
+        finf = finf + fj * r;
+    }
+    double pout = 0.0;
+    if (n.lpthout) {
+        const double *sum = s.pthsum_raw + (size_t)m * n.P;
+        for (int k = n.pout_ptr[i]; k < n.pout_ptr[i + 1]; k++) pout = pout + scaled_pathsum(n, sum, rate_m, n.pout_idx[k]);
+        for (int k = n.pinf_ptr[i]; k < n.pinf_ptr[i + 1]; k++) pout = pout - scaled_pathsum(n, sum, rate_m, n.pinf_idx[k]);
+    }
+    const double runoff = w.runoff(gi);
+    // CMF_DAMOUT_WATBAL, src/cmf_ctrl_damout_mod.F90:516-535
+    double dmiss = 0.0;
+    if (n.ldamout) {
+        const int d = n.dam_id[i];
+        if (d >= 0) {
+            const double inflow = (rinf + finf) + runoff;
+            const double outflw = rout + fout;
+            const double s0 = s.damsto[gi];
+            const double s1 = (s0 + inflow * DT) - outflw * DT;
+            s.damsto[gi] = s1;
+            dmiss = ((s0 - s1) + inflow * DT) - outflw * DT;
+        }
+    }
+    bput(11, dmiss);
+    // CALC_VARS_PRE, src/cmf_ctrl_physics_mod.F90:254-277
+    const double rivsto0 = w.rivsto(gi), fldsto0 = w.fldsto(gi);
+    s.rivout_pre[gi] = rout;
+    s.fldout_pre[gi] = fout;
+    s.rivdph_pre[gi] = w.rivdph(gi);
+    s.fldsto_pre[gi] = fldsto0;
+    // CMF_CALC_STONXT, src/cmf_calc_stonxt_mod.F90:53-100
+    bput(0, rivsto0 + fldsto0);
+    bput(3, rinf * DT + finf * DT);
+    bput(4, (rout * DT + fout * DT) + pout * DT);
+    double rs = (rivsto0 + rinf * DT) - rout * DT;
+    double fs = fldsto0;
+    if (rs < 0.0) { fs = fs + rs; rs = 0.0; }
+    fs = ((fs + finf * DT) - fout * DT) - pout * DT;
+    if (fs < 0.0) { rs = dmax(rs + fs, 0.0); fs = 0.0; }
+    bput(1, rs + fs);
+    const double outflw = rout + fout;
+    const double frc = w.fldfrc(gi);
+    rs = rs + (runoff * (1.0 - frc)) * DT;       // D2GDWRTN is zero without groundwater delay
+    fs = fs + (runoff * frc) * DT;
+    double levsto = n.llevee ? w.levsto(gi) : 0.0;
+    bput(2, n.llevee ? (rs + fs) + levsto : rs + fs);
+    // stage scheme, :125
+    const StageOut o = n.llevee ? stage_levee(n, w, i, rs, fs, levsto) : stage_def(n, w, i, rs, fs);
+    // CMF_CheckNanB-style probe (src/cmf_utils_mod.F90:807-815) on the new storage: a NaN or
+    // infinite runoff or state surfaces as a positive status instead of a silent NaN state
+    if (!isfinite((o.rivsto + o.fldsto) + o.levsto)) s.ctl[m].err = kErrNonFinite;
+    store_stage(n, s, gi, i, o, last);
+    bput(5, n.llevee ? (rs + fs) + levsto : rs + fs);
+    bput(6, n.llevee ? (o.rivsto + o.fldsto) + o.levsto : o.rivsto + o.fldsto);
+    bput(7, o.rivsto);
+    bput(8, o.fldsto);
+    bput(9, o.fldare);
+    bput(10, o.levsto);
+    if (last) {   // diagnostics read by nothing inside the sub-step loop
+        s.rivinf[gi] = rinf;
+        s.fldinf[gi] = finf;
+        s.pthout[gi] = pout;
+        s.outflw[gi] = outflw;
+    }
+    // CMF_DIAG_AVEMAX_ADPSTP / GETAVE_ADPSTP, src/cmf_calc_diag_mod.F90:104-221
+    if (n.ldiag) {
+        const double na = nadd + DT;
+        // CMF_DIAG_AVEMAX_OUTPUT (src/cmf_calc_diag_mod.F90:272-318) on the last sub-step: the
+        // output interval accumulates the finished sub-step average times DT_DEF
+        const bool out = last && n.ldiag_out;
+        const double ddef = c.dt_def;
+        auto acc = [&](double prev, double *a, double *oa, double v) {
+            double x = first ? v * DT : prev + v * DT;
+            if (last) x = x / na;
+            a[gi] = x;
+            if (out) oa[gi] = oa[gi] + x * ddef;
+        };
+        acc(first ? 0.0 : w.a_rivout(gi), s.a_rivout, s.o_rivout, rout);
+        acc(first ? 0.0 : w.a_fldout(gi), s.a_fldout, s.o_fldout, fout);
+        acc(first ? 0.0 : w.a_outflw(gi), s.a_outflw, s.o_outflw, outflw);
+        acc(first ? 0.0 : w.a_pthout(gi), s.a_pthout, s.o_pthout, pout);   // D2PTHINF is never written (always 0)
+        if (last) {
+            // runoff and DT are constant over the outer step: the same running sum of
+            // runoff*DT the accumulator would hold, rebuilt in registers on the last sub-step
+            const double rdt = runoff * DT;
+            double a = rdt;
+            for (int k = 1; k < c.nt; k++) a = a + rdt;
+            a = a / na;
+            s.a_runoff[gi] = a;
+            if (out) s.o_runoff[gi] = s.o_runoff[gi] + a * ddef;
+        }
+        if (n.ldamout) acc(first ? 0.0 : s.a_daminf[gi], s.a_daminf, s.o_daminf, s.daminf[gi]);
+        const double stg = n.llevee ? (o.rivsto + o.fldsto) + o.levsto : o.rivsto + o.fldsto;
+        const double mo = first ? dmax(0.0, fabs(outflw)) : dmax(w.m_outflw(gi), fabs(outflw));
+        const double md = first ? dmax(0.0, o.rivdph) : dmax(w.m_rivdph(gi), o.rivdph);
+        const double ms = first ? dmax(0.0, stg) : dmax(w.m_storge(gi), stg);
+        s.m_outflw[gi] = mo;
+        s.m_rivdph[gi] = md;
+        s.m_storge[gi] = ms;
+        if (out) {
+            s.om_outflw[gi] = dmax(s.om_outflw[gi], fabs(mo));
+            s.om_rivdph[gi] = dmax(s.om_rivdph[gi], md);
+            s.om_storge[gi] = dmax(s.om_storge[gi], ms);
+        }
+    }
+}
+
+// per-block budget partials of the last sub-step (the only one the caller observes);
+// fixed-shape tree -> deterministic; layout [m][k][block] for a coalesced final reduction.
+// Every thread of the block calls it (it holds block barriers); bt: this thread's kBudgets terms,
+// stride bstride apart in shared memory.
+__device__ __forceinline__ void store_budget_partials(const State &s, int m, int blk, int ncell_blocks, const double *bt,
+                                                      int bstride, double *red) {
+    __syncthreads();
+    double b[kBudgets];
+#pragma unroll
+    for (int k = 0; k < kBudgets; k++) b[k] = bt[k * bstride];
+    block_sum<kBudgets>(b, red);
+    if (threadIdx.x == 0) {
+        double *dst = s.partials + (size_t)m * kBudgets * ncell_blocks + blk;
+#pragma unroll
+        for (int k = 0; k < kBudgets; k++) dst[(size_t)k * ncell_blocks] = b[k];
+    }
 }
 
 template <int MinBlocks>
@@ -847,34 +1069,9 @@ __global__ void __launch_bounds__(kCellThreads, MinBlocks) k_store(Net n, State 
     const bool first = (kk == 0);
     const bool last = (kk == c.nt - 1);
     const double nadd = last ? nadd_before(kk, DT) : 0.0;   // only the averages of the last sub-step need it
-    const size_t base = (size_t)m * n.N;
     if ((int)blockIdx.x >= ncell_blocks) {
-        // bifurcation paths: LSPAMAT path rescale (:494-517), CALC_VARS_PRE copy, diagnostics
         const int p = (blockIdx.x - ncell_blocks) * blockDim.x + threadIdx.x;
-        if (p >= n.P) return;
-        const int P = n.P, Lp = n.Lp;
-        const size_t pb = (size_t)m * Lp * P;
-        const double *rate_m = s.rate + base;
-        const bool sk = n.pth_skip[p] & 1;
-        const int u = n.pth_up[p], d = n.pth_dn[p];
-        double asum = 0.0;
-        for (int l = 0; l < Lp; l++) {
-            const size_t o = pb + (size_t)l * P + p;
-            double f = s.pthflw_raw[o];
-            if (!sk) f = (f >= 0.0) ? f * rate_m[u] : f * rate_m[d];
-            s.pthflw_pre[o] = f;
-            if (n.ldiag) {
-                double a = first ? f * DT : s.a_pthflw[o] + f * DT;
-                if (last) {
-                    a = a / (nadd + DT);
-                    asum = asum + a;
-                    if (n.ldiag_out) s.o_pthflw[o] = s.o_pthflw[o] + a * c.dt_def;
-                }
-                s.a_pthflw[o] = a;
-            }
-        }
-        s.pthsum[(size_t)m * P + p] = scaled_pathsum(n, s.pthsum_raw + (size_t)m * P, rate_m, p);
-        if (n.ldiag && last) s.a_pthsum[(size_t)m * P + p] = asum;
+        if (p < n.P) path_rescale(n, s, m, p, DT, first, last, nadd, c.dt_def);
         return;
     }
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -887,146 +1084,10 @@ __global__ void __launch_bounds__(kCellThreads, MinBlocks) k_store(Net n, State 
     if (last && i >= n.N)
 #pragma unroll
         for (int k = 0; k < kBudgets; k++) bt[k * bstride] = 0.0;
-    if (i < n.N) {
-        const size_t gi = base + i;
-        const double *rate_m = s.rate + base;
-        const double rate_i = rate_m[i];
-        // own outflow after the LSPAMAT rescale (:456-473)
-        double rout = s.rivout_raw[gi], fout = s.fldout_raw[gi];
-        if (i < n.R) {
-            const double r = (rout > 0.0) ? rate_i : rate_m[n.next[i]];
-            rout = rout * r;
-            fout = fout * r;
-        } else {
-            rout = rout * rate_i;
-            fout = fout * rate_i;
-        }
-        // inflow from the upstream cells, rescaled on the fly (:481-489); next(j) == i
-        double rinf = 0.0, finf = 0.0;
-        for (int k = n.up_ptr[i]; k < n.up_ptr[i + 1]; k++) {
-            const int j = n.up_idx[k];
-            const double rj = s.rivout_raw[base + j], fj = s.fldout_raw[base + j];
-            const double r = (rj > 0.0) ? rate_m[j] : rate_i;
-            rinf = rinf + rj * r;
-            finf = finf + fj * r;
-        }
-        double pout = 0.0;
-        if (n.lpthout) {
-            const double *sum = s.pthsum_raw + (size_t)m * n.P;
-            for (int k = n.pout_ptr[i]; k < n.pout_ptr[i + 1]; k++) pout = pout + scaled_pathsum(n, sum, rate_m, n.pout_idx[k]);
-            for (int k = n.pinf_ptr[i]; k < n.pinf_ptr[i + 1]; k++) pout = pout - scaled_pathsum(n, sum, rate_m, n.pinf_idx[k]);
-        }
-        const double runoff = s.runoff[gi];
-        // CMF_DAMOUT_WATBAL, src/cmf_ctrl_damout_mod.F90:516-535
-        double dmiss = 0.0;
-        if (n.ldamout) {
-            const int d = n.dam_id[i];
-            if (d >= 0) {
-                const double inflow = (rinf + finf) + runoff;
-                const double outflw = rout + fout;
-                const double s0 = s.damsto[gi];
-                const double s1 = (s0 + inflow * DT) - outflw * DT;
-                s.damsto[gi] = s1;
-                dmiss = ((s0 - s1) + inflow * DT) - outflw * DT;
-            }
-        }
-        bput(11, dmiss);
-        // CALC_VARS_PRE, src/cmf_ctrl_physics_mod.F90:254-277
-        const double rivsto0 = s.rivsto[gi], fldsto0 = s.fldsto[gi];
-        s.rivout_pre[gi] = rout;
-        s.fldout_pre[gi] = fout;
-        s.rivdph_pre[gi] = s.rivdph[gi];
-        s.fldsto_pre[gi] = fldsto0;
-        // CMF_CALC_STONXT, src/cmf_calc_stonxt_mod.F90:53-100
-        bput(0, rivsto0 + fldsto0);
-        bput(3, rinf * DT + finf * DT);
-        bput(4, (rout * DT + fout * DT) + pout * DT);
-        double rs = (rivsto0 + rinf * DT) - rout * DT;
-        double fs = fldsto0;
-        if (rs < 0.0) { fs = fs + rs; rs = 0.0; }
-        fs = ((fs + finf * DT) - fout * DT) - pout * DT;
-        if (fs < 0.0) { rs = dmax(rs + fs, 0.0); fs = 0.0; }
-        bput(1, rs + fs);
-        const double outflw = rout + fout;
-        const double frc = s.fldfrc[gi];
-        rs = rs + (runoff * (1.0 - frc)) * DT;       // D2GDWRTN is zero without groundwater delay
-        fs = fs + (runoff * frc) * DT;
-        double levsto = n.llevee ? s.levsto[gi] : 0.0;
-        bput(2, n.llevee ? (rs + fs) + levsto : rs + fs);
-        // stage scheme, :125
-        const StageOut o = n.llevee ? stage_levee(n, i, rs, fs, levsto) : stage_def(n, i, rs, fs);
-        // CMF_CheckNanB-style probe (src/cmf_utils_mod.F90:807-815) on the new storage: a NaN or
-        // infinite runoff or state surfaces as a positive status instead of a silent NaN state
-        if (!isfinite((o.rivsto + o.fldsto) + o.levsto)) s.ctl[m].err = kErrNonFinite;
-        store_stage(n, s, gi, i, o, last);
-        bput(5, n.llevee ? (rs + fs) + levsto : rs + fs);
-        bput(6, n.llevee ? (o.rivsto + o.fldsto) + o.levsto : o.rivsto + o.fldsto);
-        bput(7, o.rivsto);
-        bput(8, o.fldsto);
-        bput(9, o.fldare);
-        bput(10, o.levsto);
-        if (last) {   // diagnostics read by nothing inside the sub-step loop
-            s.rivinf[gi] = rinf;
-            s.fldinf[gi] = finf;
-            s.pthout[gi] = pout;
-            s.outflw[gi] = outflw;
-        }
-        // CMF_DIAG_AVEMAX_ADPSTP / GETAVE_ADPSTP, src/cmf_calc_diag_mod.F90:104-221
-        if (n.ldiag) {
-            const double na = nadd + DT;
-            // CMF_DIAG_AVEMAX_OUTPUT (src/cmf_calc_diag_mod.F90:272-318) on the last sub-step: the
-            // output interval accumulates the finished sub-step average times DT_DEF
-            const bool out = last && n.ldiag_out;
-            const double ddef = c.dt_def;
-            auto acc = [&](double *a, double *oa, double v) {
-                double x = first ? v * DT : a[gi] + v * DT;
-                if (last) x = x / na;
-                a[gi] = x;
-                if (out) oa[gi] = oa[gi] + x * ddef;
-            };
-            acc(s.a_rivout, s.o_rivout, rout);
-            acc(s.a_fldout, s.o_fldout, fout);
-            acc(s.a_outflw, s.o_outflw, outflw);
-            acc(s.a_pthout, s.o_pthout, pout);        // D2PTHINF is never written by the reference (always 0)
-            if (last) {
-                // runoff and DT are constant over the outer step: the same running sum of
-                // runoff*DT the accumulator would hold, rebuilt in registers on the last sub-step
-                const double rdt = runoff * DT;
-                double a = rdt;
-                for (int k = 1; k < c.nt; k++) a = a + rdt;
-                a = a / na;
-                s.a_runoff[gi] = a;
-                if (out) s.o_runoff[gi] = s.o_runoff[gi] + a * ddef;
-            }
-            if (n.ldamout) acc(s.a_daminf, s.o_daminf, s.daminf[gi]);
-            const double stg = n.llevee ? (o.rivsto + o.fldsto) + o.levsto : o.rivsto + o.fldsto;
-            const double mo = first ? dmax(0.0, fabs(outflw)) : dmax(s.m_outflw[gi], fabs(outflw));
-            const double md = first ? dmax(0.0, o.rivdph) : dmax(s.m_rivdph[gi], o.rivdph);
-            const double ms = first ? dmax(0.0, stg) : dmax(s.m_storge[gi], stg);
-            s.m_outflw[gi] = mo;
-            s.m_rivdph[gi] = md;
-            s.m_storge[gi] = ms;
-            if (out) {
-                s.om_outflw[gi] = dmax(s.om_outflw[gi], fabs(mo));
-                s.om_rivdph[gi] = dmax(s.om_rivdph[gi], md);
-                s.om_storge[gi] = dmax(s.om_storge[gi], ms);
-            }
-        }
-    }
-    // per-block budget partials of the last sub-step (the only one the caller observes);
-    // fixed-shape tree -> deterministic; layout [m][k][block] for a coalesced final reduction
+    if (i < n.N) cell_store(n, s, OwnG{n, s}, m, i, DT, first, last, nadd, c, bput);
     if (last) {
         __shared__ double red[32 * kBudgets];
-        __syncthreads();
-        double b[kBudgets];
-#pragma unroll
-        for (int k = 0; k < kBudgets; k++) b[k] = bt[k * bstride];
-        block_sum<kBudgets>(b, red);
-        if (threadIdx.x == 0) {
-            double *dst = s.partials + (size_t)m * kBudgets * ncell_blocks + blockIdx.x;
-#pragma unroll
-            for (int k = 0; k < kBudgets; k++) dst[(size_t)k * ncell_blocks] = b[k];
-        }
+        store_budget_partials(s, m, blockIdx.x, ncell_blocks, bt, bstride, red);
     }
 }
 

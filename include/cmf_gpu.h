@@ -43,6 +43,7 @@ extern "C" {
 #define CMF_E_NT_CAP          2  /* adaptive sub-step count above the cap (non-finite DT_MIN)     */
 #define CMF_E_NO_DEVICE       3  /* no CUDA device or the sm_100a kernels cannot run on it       */
 #define CMF_E_NONFINITE       4  /* a sub-step produced a NaN/infinite storage (NaN runoff...)   */
+#define CMF_E_BARRIER         5  /* a bounded device-side wait (grid barrier, bulk copy) ran out */
 
 /* ---- dimensions (src/yos_cmf_map.F90, src/yos_cmf_input.F90) ----------------------------- */
 typedef struct cmf_dims {
@@ -78,7 +79,9 @@ typedef struct cmf_opts {
     int32_t ldamyby;     /* refused: year-by-year dam activation                                  */
     int32_t ldiag;       /* accumulate the CMF_DIAG_*_ADPSTP averages/maxima on the device       */
     int32_t launch_mode; /* 0: one CUDA graph per coupling step with a device-side sub-step loop;
-                            1: host-driven launches (reads NT back before the sub-steps)          */
+                            1: host-driven launches (reads NT back before the sub-steps);
+                            2: one persistent cooperative kernel per coupling step (grid barriers
+                               between the phases, tiles streamed by bulk asynchronous copies)    */
     int32_t device;      /* CUDA device ordinal                                                   */
     int32_t block_size;  /* 0: autotune; else threads per block for the cell kernels (64..256)   */
     int32_t ldiag_output;/* accumulate the output-interval averages/maxima (D2*_oAVG, D2*_oMAX) on
@@ -207,6 +210,14 @@ int cmf_gpu_ctx_counters(cmf_gpu_ctx *ctx, int64_t *member_substeps, int64_t *lo
 #define CMF_DIAG_OUT_GETAVE 2
 int cmf_gpu_ctx_diag_output(cmf_gpu_ctx *ctx, int32_t op);
 int cmf_gpu_ctx_get_diag_output(cmf_gpu_ctx *ctx, const cmf_diag_out_ptrs *dg);
+/* Check of the persistent kernel's bounded waits (launch_mode 2 contexts, or any context whose
+ * device can run it): launches the kernel with a grid barrier that one arrival short of its count
+ * can never complete and a bound of wait_ns; every CTA gives up after about that time and the
+ * kernel returns.  Returns CMF_E_BARRIER when the bound worked (the context stays usable: its
+ * error word is cleared), another status otherwise.  No state changes. */
+int cmf_gpu_ctx_persist_selftest(cmf_gpu_ctx *ctx, int64_t wait_ns);
+/* The schedule the context runs: 0 graph, 1 host-driven, 2 persistent. */
+int32_t cmf_gpu_ctx_launch_mode(cmf_gpu_ctx *ctx);
 /* Adaptive-step statistics since creation: near_boundary = (outer step, member) pairs whose
  * DT_DEF/DT_MIN - 0.01 (the argument of INT in CALC_ADPSTP, src/cmf_ctrl_physics_mod.F90:205)
  * lay within 1e-12 (relative) of an integer, where NT depends on the last bits of DT_MIN;
