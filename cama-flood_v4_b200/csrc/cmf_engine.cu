@@ -184,6 +184,16 @@ int build_net(cmf_gpu_ctx *c, const cmf_map_ptrs *mp) {
         if (!a.src) return set_err(CMF_E_ARG, "a required map pointer is NULL");
         if ((rc = c->upload_raw(a.dst, a.src, a.cnt))) return rc;
     }
+    // reciprocals the outflow formulas take (x**(-1._JPRB)), correctly rounded once here
+    {
+        std::vector<double> inv(N);
+        struct { const double *__restrict__ *dst; const double *src; } recips[] = {
+            {&n.inv_nxtdst, mp->nxtdst}, {&n.inv_rivwth, mp->rivwth}, {&n.inv_rivlen, mp->rivlen}};
+        for (auto &r : recips) {
+            for (int i = 0; i < N; i++) inv[i] = 1.0 / r.src[i];
+            if ((rc = c->upload(r.dst, inv))) return rc;
+        }
+    }
     // layer tables: (NSEQMAX,1,NLFP) -> [L][N]
     auto layers = [&](const double *src, std::vector<double> &out) {
         out.assign((size_t)L * N, 0.0);

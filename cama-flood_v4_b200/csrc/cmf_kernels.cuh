@@ -93,6 +93,9 @@ struct Net {
     const double *__restrict__ rivelv, *__restrict__ elevtn, *__restrict__ nxtdst, *__restrict__ rivwth;
     const double *__restrict__ rivhgt, *__restrict__ rivlen, *__restrict__ rivman, *__restrict__ grarea;
     const double *__restrict__ rivstomax, *__restrict__ dwnelv;
+    // D2NXTDST**(-1), D2RIVWTH**(-1), D2RIVLEN**(-1) of the outflow formulas, computed once at init
+    // (the same correctly rounded reciprocal the reference evaluates every time)
+    const double *__restrict__ inv_nxtdst, *__restrict__ inv_rivwth, *__restrict__ inv_rivlen;
     const double *__restrict__ fldstomax, *__restrict__ fldgrd, *__restrict__ fldhgt;   // [L][N]
     // bifurcation paths
     const int *__restrict__ pth_up, *__restrict__ pth_dn;   // [P] 0-based, -1 outside domain
@@ -153,7 +156,7 @@ struct OwnG {
     const State &s;
     CMF_OWN_STATIC(rivelv) CMF_OWN_STATIC(elevtn) CMF_OWN_STATIC(nxtdst) CMF_OWN_STATIC(rivwth)
     CMF_OWN_STATIC(rivhgt) CMF_OWN_STATIC(rivlen) CMF_OWN_STATIC(rivman) CMF_OWN_STATIC(grarea)
-    CMF_OWN_STATIC(rivstomax)
+    CMF_OWN_STATIC(rivstomax) CMF_OWN_STATIC(inv_nxtdst) CMF_OWN_STATIC(inv_rivwth) CMF_OWN_STATIC(inv_rivlen)
     __device__ __forceinline__ int next(int i) const { return n.next[i]; }
     __device__ __forceinline__ int up_lo(int i) const { return n.up_ptr[i]; }
     __device__ __forceinline__ int up_hi(int i) const { return n.up_ptr[i + 1]; }
@@ -167,6 +170,7 @@ struct OwnG {
 };
 #undef CMF_OWN_STATIC
 #undef CMF_OWN_STATE
+
 
 // x**(-7._JPRB/3._JPRB) and x**(-4._JPRB/3._JPRB) of the local-inertial flux formulas
 // (src/cmf_calc_outflw_mod.F90:74,106,133,162; src/cmf_calc_pthout_mod.F90:67;
@@ -554,6 +558,13 @@ __device__ __forceinline__ double nadd_before(int k, double dt) {
     return a;
 }
 
+// Exact shortcuts (the same bits as evaluating every expression):
+//  - merge(DOUT, 0, Mask) discards DOUT when Mask is false, so the floodplain flux is evaluated only
+//    where its area term passes the mask (most cells carry no floodplain water);
+//  - min(a/b, 1) with b > 0 is 1 whenever a >= b (a correctly rounded quotient of a >= b is >= 1),
+//    so the limiter rates skip the division in the common case; a NaN a still takes the division.
+__device__ __forceinline__ double rate_min1(double a, double b) { return (a >= b) ? 1.0 : dmin(a / b, 1.0); }
+
 template <class Own>
 __device__ __forceinline__ void cell_outflow(const Net &n, const State &s, const Own &w, int m, int i, double DT,
                                              const MemberCtl &c, int k, bool split) {
@@ -563,8 +574,8 @@ __device__ __forceinline__ void cell_outflow(const Net &n, const State &s, const
     const double rivdph = w.rivdph(gi), rivdph_pre = w.rivdph_pre(gi);
     const double sfc = rivelv + rivdph;
     const double sfc_pre = rivelv + rivdph_pre;
-    const double flddph_pre = dmax(rivdph_pre - w.rivhgt(i), 0.0);
     const double wth = w.rivwth(i);
+    const double inv_wth = w.inv_rivwth(i);
     const double man = w.rivman(i);
     const double rivout_pre = w.rivout_pre(gi);
     const double rivout_old = split ? s.rivout_cur[gi] : rivout_pre;
@@ -575,7 +586,7 @@ __device__ __forceinline__ void cell_outflow(const Net &n, const State &s, const
         const double rj = n.rivelv[j];
         const double dwn = rj + s.rivdph[gj];
         const double dwn_pre = rj + s.rivdph_pre[gj];
-        const double inv_dst = 1.0 / w.nxtdst(i);
+        const double inv_dst = w.inv_nxtdst(i);
         // river
         {
             const double dsfc = dmax(sfc, dwn);
@@ -584,7 +595,7 @@ __device__ __forceinline__ void cell_outflow(const Net &n, const State &s, const
             const double dare = dmax(wth * dflw, 1.E-10);
             const double dflw_pr = dmax(sfc_pre, dwn_pre) - rivelv;
             const double dflw_im = dmax(sqrt(dflw * dflw_pr), 1.E-6);
-            const double dout_pr = rivout_pre * (1.0 / wth);
+            const double dout_pr = rivout_pre * inv_wth;
             const double dout = (wth * (dout_pr + (gdt * dflw_im) * dslp))
                               * (1.0 / (1.0 + ((gdt * (man * man)) * fabs(dout_pr)) * pow_depth<7>(dflw_im)));
             const double dvel = rivout_old * (1.0 / dare);
@@ -593,28 +604,31 @@ __device__ __forceinline__ void cell_outflow(const Net &n, const State &s, const
             rvel = mask ? dvel : 0.0;
         }
         if (n.lfldout) {
-            const double len = w.rivlen(i), elv = w.elevtn(i);
-            const double dsfc = dmax(sfc, dwn);
-            double dslp = (sfc - dwn) * inv_dst;
-            dslp = dmax(-0.005, dmin(0.005, dslp));
-            const double dflw = dmax(dsfc - elv, 0.0);
-            double dare = w.fldsto(gi) * (1.0 / len);
+            const double inv_len = w.inv_rivlen(i);
+            double dare = w.fldsto(gi) * inv_len;
             dare = dmax(dare - w.flddph(gi) * wth, 0.0);
-            const double dflw_pr = dmax(sfc_pre, dwn_pre) - elv;
-            const double dflw_im = dmax(sqrt(dmax(dflw * dflw_pr, 0.0)), 1.E-6);
-            double dare_pr = w.fldsto_pre(gi) * (1.0 / len);
-            dare_pr = dmax(dare_pr - flddph_pre * wth, 1.E-6);
-            const double dare_im = dmax(sqrt(dare * dare_pr), 1.E-6);
-            const double dout_pr = w.fldout_pre(gi);
-            const double dout = (dout_pr + (gdt * dare_im) * dslp)
-                * (1.0 / (1.0 + (((gdt * (n.pmanfld * n.pmanfld)) * fabs(dout_pr)) * pow_depth<4>(dflw_im)) * (1.0 / dare_im)));
-            const bool mask = (dflw_im > 1.E-5 && dare > 1.E-5);
-            fout = mask ? dout : 0.0;
-            if (!(fout * rout > 0.0)) fout = 0.0;
+            if (dare > 1.E-5) {
+                const double elv = w.elevtn(i);
+                const double dsfc = dmax(sfc, dwn);
+                double dslp = (sfc - dwn) * inv_dst;
+                dslp = dmax(-0.005, dmin(0.005, dslp));
+                const double dflw = dmax(dsfc - elv, 0.0);
+                const double dflw_pr = dmax(sfc_pre, dwn_pre) - elv;
+                const double dflw_im = dmax(sqrt(dmax(dflw * dflw_pr, 0.0)), 1.E-6);
+                const double flddph_pre = dmax(rivdph_pre - w.rivhgt(i), 0.0);
+                double dare_pr = w.fldsto_pre(gi) * inv_len;
+                dare_pr = dmax(dare_pr - flddph_pre * wth, 1.E-6);
+                const double dare_im = dmax(sqrt(dare * dare_pr), 1.E-6);
+                const double dout_pr = w.fldout_pre(gi);
+                const double dout = (dout_pr + (gdt * dare_im) * dslp)
+                    * (1.0 / (1.0 + (((gdt * (n.pmanfld * n.pmanfld)) * fabs(dout_pr)) * pow_depth<4>(dflw_im)) * (1.0 / dare_im)));
+                fout = (dflw_im > 1.E-5) ? dout : 0.0;
+                if (!(fout * rout > 0.0)) fout = 0.0;
+            }
         }
         // storage-change limiter (v423), :176-182
         const double dlim = dmax((-rout - fout) * DT, CMF_F(1.E-10));
-        const double rate = dmin((0.05 * w.storge(gi)) / dlim, 1.0);
+        const double rate = rate_min1(0.05 * w.storge(gi), dlim);
         rout = rout * rate;
         fout = fout * rate;
     } else {
@@ -624,7 +638,7 @@ __device__ __forceinline__ void cell_outflow(const Net &n, const State &s, const
             const double dslp = (sfc - dwn) * inv_dst;
             const double dare = dmax(wth * rivdph, 1.E-10);
             const double dflw_im = dmax(sqrt(rivdph * rivdph_pre), 1.E-6);
-            const double dout_pr = rivout_pre * (1.0 / wth);
+            const double dout_pr = rivout_pre * inv_wth;
             const double dout = (wth * (dout_pr + (gdt * dflw_im) * dslp))
                               * (1.0 / (1.0 + ((gdt * (man * man)) * fabs(dout_pr)) * pow_depth<7>(dflw_im)));
             const double dvel = rivout_old * (1.0 / dare);
@@ -633,21 +647,24 @@ __device__ __forceinline__ void cell_outflow(const Net &n, const State &s, const
             rvel = mask ? dvel : 0.0;
         }
         if (n.lfldout) {
-            const double len = w.rivlen(i), elv = w.elevtn(i);
-            double dslp = (sfc - dwn) * inv_dst;
-            dslp = dmax(-0.005, dmin(0.005, dslp));
-            const double dflw = sfc - elv;
-            const double dare = dmax(w.fldsto(gi) * (1.0 / len) - w.flddph(gi) * wth, 0.0);
-            const double dflw_pr = sfc_pre - elv;
-            const double dflw_im = dmax(sqrt(dmax(dflw * dflw_pr, 0.0)), 1.E-6);
-            const double dare_pr = dmax(w.fldsto_pre(gi) * (1.0 / len) - flddph_pre * wth, 1.E-6);
-            const double dare_im = dmax(sqrt(dare * dare_pr), 1.E-6);
-            const double dout_pr = w.fldout_pre(gi);
-            const double dout = (dout_pr + (gdt * dare_im) * dslp)
-                * (1.0 / (1.0 + (((gdt * (n.pmanfld * n.pmanfld)) * fabs(dout_pr)) * pow_depth<4>(dflw_im)) * (1.0 / dare_im)));
-            const bool mask = (dflw_im > CMF_F(1.E-5) && dare > CMF_F(1.E-5));
-            fout = mask ? dout : 0.0;
-            if (!(fout * rout > 0.0)) fout = 0.0;
+            const double inv_len = w.inv_rivlen(i);
+            const double dare = dmax(w.fldsto(gi) * inv_len - w.flddph(gi) * wth, 0.0);
+            if (dare > CMF_F(1.E-5)) {
+                const double elv = w.elevtn(i);
+                double dslp = (sfc - dwn) * inv_dst;
+                dslp = dmax(-0.005, dmin(0.005, dslp));
+                const double dflw = sfc - elv;
+                const double dflw_pr = sfc_pre - elv;
+                const double dflw_im = dmax(sqrt(dmax(dflw * dflw_pr, 0.0)), 1.E-6);
+                const double flddph_pre = dmax(rivdph_pre - w.rivhgt(i), 0.0);
+                const double dare_pr = dmax(w.fldsto_pre(gi) * inv_len - flddph_pre * wth, 1.E-6);
+                const double dare_im = dmax(sqrt(dare * dare_pr), 1.E-6);
+                const double dout_pr = w.fldout_pre(gi);
+                const double dout = (dout_pr + (gdt * dare_im) * dslp)
+                    * (1.0 / (1.0 + (((gdt * (n.pmanfld * n.pmanfld)) * fabs(dout_pr)) * pow_depth<4>(dflw_im)) * (1.0 / dare_im)));
+                fout = (dflw_im > CMF_F(1.E-5)) ? dout : 0.0;
+                if (!(fout * rout > 0.0)) fout = 0.0;
+            }
         }
     }
     // reservoir operation, CMF_DAMOUT_CALC (src/cmf_ctrl_damout_mod.F90:316-498)
@@ -727,12 +744,14 @@ __device__ __forceinline__ void cell_outflow(const Net &n, const State &s, const
     const bool first = (k == 0), last = (k == c.nt - 1);
     if (last) s.rivvel[gi] = rvel;
     if (n.ldiag) {
-        double a = first ? rvel * DT : w.a_rivvel(gi) + rvel * DT;
+        const double prev = first ? 0.0 : w.a_rivvel(gi);
+        double a = first ? rvel * DT : prev + rvel * DT;
         if (last) {
             a = a / (nadd_before(k, DT) + DT);
             if (n.ldiag_out) s.o_rivvel[gi] = s.o_rivvel[gi] + a * c.dt_def;   // CMF_DIAG_AVEMAX_OUTPUT
         }
-        s.a_rivvel[gi] = a;
+        // unchanged bits (a dry cell adds +0): no store needed
+        if (first || last || __double_as_longlong(a) != __double_as_longlong(prev)) s.a_rivvel[gi] = a;
     }
 }
 
@@ -802,7 +821,7 @@ __device__ __forceinline__ void path_outflow(const Net &n, const State &s, int m
     }
     for (int l = 0; l < Lp; l++) sum = sum + (l < 8 ? flw[l] : s.pthflw_raw[pb + (size_t)l * P + p]);
     if (sum != 0.0) {
-        const double rate = dmin((0.05 * dmin(s.storge[base + u], s.storge[base + d])) / fabs(sum * DT), 1.0);
+        const double rate = rate_min1(0.05 * dmin(s.storge[base + u], s.storge[base + d]), fabs(sum * DT));
         for (int l = 0; l < Lp; l++) {
             const size_t o = pb + (size_t)l * P + p;
             s.pthflw_raw[o] = (l < 8 ? flw[l] : s.pthflw_raw[o]) * rate;
@@ -849,7 +868,7 @@ __device__ __forceinline__ void cell_rate(const Net &n, const State &s, const Ow
     }
     const double dout = dmax(so, 1.E-10);
     const double dsto = w.rivsto(gi) + w.fldsto(gi);
-    s.rate[gi] = dmin(dsto / dout, 1.0);
+    s.rate[gi] = rate_min1(dsto, dout);
 }
 
 // advance != 0: block (0,0) also moves the loop counter to the next sub-step and sets the WHILE
@@ -916,8 +935,8 @@ __device__ __forceinline__ void cell_store(const Net &n, const State &s, const O
     const size_t gi = base + i;
     const double *rate_m = s.rate + base;
     const double rate_i = w.rate(gi);
-    // own outflow after the LSPAMAT rescale (:456-473)
     double rout = w.rivout_raw(gi), fout = w.fldout_raw(gi);
+    // own outflow after the LSPAMAT rescale (:456-473)
     if (i < n.R) {
         const double r = (rout > 0.0) ? rate_i : rate_m[w.next(i)];
         rout = rout * r;
@@ -937,10 +956,13 @@ __device__ __forceinline__ void cell_store(const Net &n, const State &s, const O
         finf = finf + fj * r;
     }
     double pout = 0.0;
+    bool has_path = false;
     if (n.lpthout) {
         const double *sum = s.pthsum_raw + (size_t)m * n.P;
-        for (int k = n.pout_ptr[i]; k < n.pout_ptr[i + 1]; k++) pout = pout + scaled_pathsum(n, sum, rate_m, n.pout_idx[k]);
-        for (int k = n.pinf_ptr[i]; k < n.pinf_ptr[i + 1]; k++) pout = pout - scaled_pathsum(n, sum, rate_m, n.pinf_idx[k]);
+        const int o0 = n.pout_ptr[i], o1 = n.pout_ptr[i + 1], f0 = n.pinf_ptr[i], f1 = n.pinf_ptr[i + 1];
+        has_path = (o1 > o0) || (f1 > f0);
+        for (int k = o0; k < o1; k++) pout = pout + scaled_pathsum(n, sum, rate_m, n.pout_idx[k]);
+        for (int k = f0; k < f1; k++) pout = pout - scaled_pathsum(n, sum, rate_m, n.pinf_idx[k]);
     }
     const double runoff = w.runoff(gi);
     // CMF_DAMOUT_WATBAL, src/cmf_ctrl_damout_mod.F90:516-535
@@ -977,7 +999,7 @@ __device__ __forceinline__ void cell_store(const Net &n, const State &s, const O
     const double frc = w.fldfrc(gi);
     rs = rs + (runoff * (1.0 - frc)) * DT;       // D2GDWRTN is zero without groundwater delay
     fs = fs + (runoff * frc) * DT;
-    double levsto = n.llevee ? w.levsto(gi) : 0.0;
+    const double levsto = n.llevee ? w.levsto(gi) : 0.0;
     bput(2, n.llevee ? (rs + fs) + levsto : rs + fs);
     // stage scheme, :125
     const StageOut o = n.llevee ? stage_levee(n, w, i, rs, fs, levsto) : stage_def(n, w, i, rs, fs);
@@ -1004,16 +1026,23 @@ __device__ __forceinline__ void cell_store(const Net &n, const State &s, const O
         // output interval accumulates the finished sub-step average times DT_DEF
         const bool out = last && n.ldiag_out;
         const double ddef = c.dt_def;
+        // a store is skipped when the sub-step leaves the accumulator's bits unchanged (a zero
+        // discharge added to a running sum, a maximum that did not move): the array holds the same
+        // bits either way
+        auto same = [](double a, double b) { return __double_as_longlong(a) == __double_as_longlong(b); };
         auto acc = [&](double prev, double *a, double *oa, double v) {
             double x = first ? v * DT : prev + v * DT;
             if (last) x = x / na;
-            a[gi] = x;
+            if (first || last || !same(x, prev)) a[gi] = x;
             if (out) oa[gi] = oa[gi] + x * ddef;
         };
         acc(first ? 0.0 : w.a_rivout(gi), s.a_rivout, s.o_rivout, rout);
         acc(first ? 0.0 : w.a_fldout(gi), s.a_fldout, s.o_fldout, fout);
         acc(first ? 0.0 : w.a_outflw(gi), s.a_outflw, s.o_outflw, outflw);
-        acc(first ? 0.0 : w.a_pthout(gi), s.a_pthout, s.o_pthout, pout);   // D2PTHINF is never written (always 0)
+        // D2PTHOUT_aAVG: D2PTHINF is never written by the reference (always 0), and a cell without
+        // bifurcation channels adds +0 every sub-step, so its average (and output average) stays at
+        // the +0 the arrays were created with: nothing to read or write
+        if (has_path) acc(first ? 0.0 : w.a_pthout(gi), s.a_pthout, s.o_pthout, pout);
         if (last) {
             // runoff and DT are constant over the outer step: the same running sum of
             // runoff*DT the accumulator would hold, rebuilt in registers on the last sub-step
@@ -1026,12 +1055,14 @@ __device__ __forceinline__ void cell_store(const Net &n, const State &s, const O
         }
         if (n.ldamout) acc(first ? 0.0 : s.a_daminf[gi], s.a_daminf, s.o_daminf, s.daminf[gi]);
         const double stg = n.llevee ? (o.rivsto + o.fldsto) + o.levsto : o.rivsto + o.fldsto;
-        const double mo = first ? dmax(0.0, fabs(outflw)) : dmax(w.m_outflw(gi), fabs(outflw));
-        const double md = first ? dmax(0.0, o.rivdph) : dmax(w.m_rivdph(gi), o.rivdph);
-        const double ms = first ? dmax(0.0, stg) : dmax(w.m_storge(gi), stg);
-        s.m_outflw[gi] = mo;
-        s.m_rivdph[gi] = md;
-        s.m_storge[gi] = ms;
+        const double pmo = first ? 0.0 : w.m_outflw(gi), pmd = first ? 0.0 : w.m_rivdph(gi);
+        const double pms = first ? 0.0 : w.m_storge(gi);
+        const double mo = dmax(pmo, fabs(outflw));
+        const double md = dmax(pmd, o.rivdph);
+        const double ms = dmax(pms, stg);
+        if (first || !same(mo, pmo)) s.m_outflw[gi] = mo;
+        if (first || !same(md, pmd)) s.m_rivdph[gi] = md;
+        if (first || !same(ms, pms)) s.m_storge[gi] = ms;
         if (out) {
             s.om_outflw[gi] = dmax(s.om_outflw[gi], fabs(mo));
             s.om_rivdph[gi] = dmax(s.om_rivdph[gi], md);

@@ -27,7 +27,8 @@ constexpr unsigned long long kWaitNsDefault = 1000000000ull;   // bound of every
 
 // tile slots of each phase (doubles: member state then static maps; ints)
 enum SlotA { A_RIVDPH, A_RIVDPH_PRE, A_RIVOUT_PRE, A_FLDSTO, A_FLDDPH, A_FLDSTO_PRE, A_FLDOUT_PRE, A_STORGE, A_A_RIVVEL,
-             A_NSTATE, A_RIVELV = A_NSTATE, A_RIVHGT, A_RIVWTH, A_RIVMAN, A_NXTDST, A_RIVLEN, A_ELEVTN, A_ND };
+             A_NSTATE, A_RIVELV = A_NSTATE, A_RIVHGT, A_RIVWTH, A_RIVMAN, A_INV_NXTDST, A_INV_RIVLEN, A_ELEVTN,
+             A_INV_RIVWTH, A_ND };
 enum SlotAI { AI_NEXT, AI_I1DAM, A_NI };
 enum SlotB { B_RIVOUT_RAW, B_FLDOUT_RAW, B_RIVSTO, B_FLDSTO, B_ND, B_NSTATE = B_ND };
 enum SlotBI { BI_UP, B_NI };
@@ -153,8 +154,9 @@ struct OwnTA {
     __device__ __forceinline__ double rivhgt(int i) const { return v.sx(A_RIVHGT, i); }
     __device__ __forceinline__ double rivwth(int i) const { return v.sx(A_RIVWTH, i); }
     __device__ __forceinline__ double rivman(int i) const { return v.sx(A_RIVMAN, i); }
-    __device__ __forceinline__ double nxtdst(int i) const { return v.sx(A_NXTDST, i); }
-    __device__ __forceinline__ double rivlen(int i) const { return v.sx(A_RIVLEN, i); }
+    __device__ __forceinline__ double inv_nxtdst(int i) const { return v.sx(A_INV_NXTDST, i); }
+    __device__ __forceinline__ double inv_rivlen(int i) const { return v.sx(A_INV_RIVLEN, i); }
+    __device__ __forceinline__ double inv_rivwth(int i) const { return v.sx(A_INV_RIVWTH, i); }
     __device__ __forceinline__ double elevtn(int i) const { return v.sx(A_ELEVTN, i); }
     __device__ __forceinline__ int next(int i) const { return v.ix(AI_NEXT, i); }
     __device__ __forceinline__ int i1dam(int i) const { return v.ix(AI_I1DAM, i); }
@@ -469,8 +471,9 @@ __global__ void __launch_bounds__(kTile, 2) k_persist(Net n, State s, PersistArg
     fa.st[A_FLDSTO] = s.fldsto; fa.st[A_FLDDPH] = s.flddph; fa.st[A_FLDSTO_PRE] = s.fldsto_pre;
     fa.st[A_FLDOUT_PRE] = s.fldout_pre; fa.st[A_STORGE] = s.storge; fa.st[A_A_RIVVEL] = n.ldiag ? s.a_rivvel : nullptr;
     fa.sx[A_RIVELV - A_NSTATE] = n.rivelv; fa.sx[A_RIVHGT - A_NSTATE] = n.rivhgt; fa.sx[A_RIVWTH - A_NSTATE] = n.rivwth;
-    fa.sx[A_RIVMAN - A_NSTATE] = n.rivman; fa.sx[A_NXTDST - A_NSTATE] = n.nxtdst; fa.sx[A_RIVLEN - A_NSTATE] = n.rivlen;
-    fa.sx[A_ELEVTN - A_NSTATE] = n.elevtn;
+    fa.sx[A_RIVMAN - A_NSTATE] = n.rivman; fa.sx[A_INV_NXTDST - A_NSTATE] = n.inv_nxtdst;
+    fa.sx[A_INV_RIVLEN - A_NSTATE] = n.inv_rivlen; fa.sx[A_ELEVTN - A_NSTATE] = n.elevtn;
+    fa.sx[A_INV_RIVWTH - A_NSTATE] = n.inv_rivwth;
     fa.iv[AI_NEXT] = n.next; fa.iv[AI_I1DAM] = n.ldamout ? n.i1dam : nullptr;
     ra.nst = B_NSTATE; ra.nsx = 0; ra.niv = B_NI; ra.iv_extra = 1;
     ra.st[B_RIVOUT_RAW] = s.rivout_raw; ra.st[B_FLDOUT_RAW] = s.fldout_raw; ra.st[B_RIVSTO] = s.rivsto;
