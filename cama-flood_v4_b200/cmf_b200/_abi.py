@@ -86,6 +86,12 @@ class Budget(C.Structure):
     _fields_ = [(n, C.c_double) for n in BUDGET_FIELDS]
 
 
+class Schedule(C.Structure):
+    _fields_ = [("mode", C.c_int32), ("flux_block", C.c_int32), ("rate_block", C.c_int32), ("store_block", C.c_int32),
+                ("profile", C.c_int32), ("tuned", C.c_int32), ("candidates", C.c_int32),
+                ("best_us_per_substep", C.c_double), ("worst_us_per_substep", C.c_double)]
+
+
 class StageDevArgs(C.Structure):
     _fields_ = [("nseqall", C.c_int32), ("nseqriv", C.c_int32), ("nlfp", C.c_int32), ("ladpstp", C.c_int32),
                 ("dt_def", C.c_double), ("pgrv", C.c_double), ("pdstmth", C.c_double), ("pcadp", C.c_double),
@@ -104,6 +110,7 @@ EXPORTS = [
     "cmf_host_load", "cmf_host_free", "cmf_host_describe", "cmf_host_state", "cmf_host_conv_resol", "cmf_host_grid",
     "cmf_gpu_stage_noalloc", "cmf_gpu_ctx_nt_stats", "cmf_gpu_ctx_diag_output", "cmf_gpu_ctx_get_diag_output",
     "cmf_gpu_diag_output", "cmf_gpu_get_diag_output", "cmf_gpu_ctx_persist_selftest", "cmf_gpu_ctx_launch_mode",
+    "cmf_gpu_ctx_get_schedule", "cmf_gpu_ctx_set_schedule",
 ]
 
 _lib = None
@@ -146,6 +153,9 @@ def load(build_if_missing: bool = True):
     lib.cmf_gpu_ctx_time_phases.argtypes = [vp, C.c_double, C.c_int32, f64p]
     lib.cmf_gpu_ctx_nt_stats.argtypes = [vp, C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.c_int32]
     lib.cmf_gpu_ctx_persist_selftest.argtypes = [vp, C.c_int64]
+    lib.cmf_gpu_ctx_get_schedule.argtypes = [vp, C.POINTER(Schedule)]
+    lib.cmf_gpu_ctx_set_schedule.argtypes = [vp, C.POINTER(Schedule)]
+    lib.cmf_gpu_schedule_cache_clear.restype = None
     lib.cmf_gpu_ctx_launch_mode.argtypes = [vp]
     lib.cmf_gpu_ctx_diag_output.argtypes = [vp, C.c_int32]
     lib.cmf_gpu_ctx_get_diag_output.argtypes = [vp, C.POINTER(DiagOutPtrs)]

@@ -372,11 +372,20 @@ class PhysicsGPU:
         return int(self.lib.cmf_gpu_ctx_launch_mode(self.h))
 
     def schedule(self) -> dict:
-        """The launch schedule the context runs (chosen by the autotuner unless forced)."""
-        if self.launch_mode == 2:
-            return {"kernels": "one persistent cooperative kernel per coupling step (grid barriers between phases, "
-                               "tiles of 256 cells streamed by bulk asynchronous copies)"}
-        return {"kernels": "stage, NT/DT, {flux, rate, store} x NT, budget", "block_size": self.block_size}
+        """The launch schedule the context runs (chosen by the online autotuner unless fixed)."""
+        q = _abi.Schedule()
+        check(self.lib.cmf_gpu_ctx_get_schedule(self.h, C.byref(q)), "get_schedule")
+        d = {f: getattr(q, f) for f, _ in _abi.Schedule._fields_}
+        d["kernels"] = ("one persistent cooperative kernel per coupling step (grid barriers between phases, tiles "
+                        "of 256 cells streamed by bulk asynchronous copies)" if q.mode == 2 else
+                        "graph: stage, NT/DT, {flux, rate, store} x NT, budget")
+        return d
+
+    def set_schedule(self, mode: int = 0, flux_block: int = 128, rate_block: int = 128, store_block: int = 128,
+                     profile: int = 1) -> None:
+        q = _abi.Schedule(mode=mode, flux_block=flux_block, rate_block=rate_block, store_block=store_block,
+                          profile=profile)
+        check(self.lib.cmf_gpu_ctx_set_schedule(self.h, C.byref(q)), "set_schedule")
 
     def launches_per_step(self) -> int:
         """Kernel launches per outer step outside the sub-step loop."""

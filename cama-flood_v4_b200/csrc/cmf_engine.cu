@@ -10,6 +10,9 @@
 
 #include <algorithm>
 #include <chrono>
+#include <map>
+#include <mutex>
+#include <tuple>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -39,6 +42,35 @@ constexpr int kImis = -9999;
 
 }  // namespace
 
+// Launch schedule of one outer step: the graph of phase kernels with a block size per kernel and
+// an occupancy profile (wide: more resident warps, fewer registers; small: fewer spills), or the
+// persistent kernel.  Every schedule computes the same bits (no atomics on state, budgets from
+// per-warp partials), so the autotuner may switch between them at any outer step.
+struct Sched {
+    int mode = 0;               // 0 graph of phase kernels, 2 persistent kernel
+    int bf = 256, br = 256, bs = 256;
+    int prof = 0;               // 0 wide, 1 small
+    bool operator==(const Sched &o) const {
+        return mode == o.mode && bf == o.bf && br == o.br && bs == o.bs && prof == o.prof;
+    }
+};
+inline int nblk(int n, int b) { return n > 0 ? (n + b - 1) / b : 0; }
+
+// Online autotuner: after `warm` outer steps on the starting schedule (so that the state is
+// spun up: flooded cells, levees and dams active), every candidate runs `reps` real outer steps,
+// timed with CUDA events and normalised by the sub-step count; the fastest is kept for good and
+// cached per network shape for later contexts.  The trajectory is not affected (same bits).
+struct Tuner {
+    bool active = false;
+    int warm = 0, reps = 2, cand = 0, rep = 0;
+    std::vector<Sched> cands;
+    std::vector<double> ms, sub;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    long long iters0 = 0;
+    double best_us = 0.0, worst_us = 0.0;
+    int timed = 0;              // candidates timed (0: the schedule was fixed by the caller or the cache)
+};
+
 struct cmf_gpu_ctx {
     cmf_dims dims{};
     cmf_params params{};
@@ -48,11 +80,10 @@ struct cmf_gpu_ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
     std::vector<void *> allocs;
-    int block = 256;
-    int ncell_blocks = 0, npath_blocks = 0;
+    Sched sched;                // the launch schedule of the outer step
     int persist_grid = 0;       // co-resident CTAs of the persistent kernel (0: it cannot run here)
     bool persist = false;       // outer steps run as one persistent cooperative launch
-    bool small_cells = false;   // N x M <= kSmallCellMembers: the low-spill profile of k_flux/k_store
+    Tuner tune;                 // online autotuner state
     int nlev = 0, ndam_placed = 0;
     size_t E = 0;
     // graph
@@ -348,55 +379,59 @@ int alloc_state(cmf_gpu_ctx *c) {
         (rc = c->alloc(&s.o_nadd, c->dims.nmembers)))
         return rc;
     if ((rc = c->alloc(&s.ctl, c->dims.nmembers)) || (rc = c->alloc(&s.loop, 1))) return rc;
-    // budget partials sized for the smallest block the autotuner may pick (64 threads)
-    const size_t nblk_max = (size_t)(c->dims.nseqall + 63) / 64;
-    if ((rc = c->alloc(&s.partials, (size_t)c->dims.nmembers * nblk_max * cmf::kBudgets))) return rc;
+    // budget partials: one per warp of 32 cells, per member and budget
+    if ((rc = c->alloc(&s.partials, (size_t)c->dims.nmembers * cmf::budget_warps(c->dims.nseqall) * cmf::kBudgets)))
+        return rc;
     return CMF_OK;
 }
 
-void set_blocks(cmf_gpu_ctx *c, int block) {
-    c->block = block;
-    c->ncell_blocks = (c->dims.nseqall + block - 1) / block;
-    c->npath_blocks = c->net.P > 0 ? (c->net.P + block - 1) / block : 0;
+// phase A and phase C in the schedule's occupancy profile; grids cover the cells of every member,
+// then (phases A and C) the bifurcation paths
+void launch_flux(cmf_gpu_ctx *c) {
+    const Sched &q = c->sched;
+    const int nc = nblk(c->dims.nseqall, q.bf);
+    const dim3 g(nc + nblk(c->net.P, q.bf), c->dims.nmembers);
+    if (q.prof)
+        cmf::k_flux<cmf::kFluxMinBlocksSmall><<<g, q.bf, 0, c->stream>>>(c->net, c->st, nc);
+    else
+        cmf::k_flux<cmf::kFluxMinBlocksWide><<<g, q.bf, 0, c->stream>>>(c->net, c->st, nc);
+}
+void launch_rate(cmf_gpu_ctx *c, int advance, cudaGraphConditionalHandle cond, int use_cond) {
+    const dim3 g(nblk(c->dims.nseqall, c->sched.br), c->dims.nmembers);
+    cmf::k_rate<<<g, c->sched.br, 0, c->stream>>>(c->net, c->st, advance, cond, use_cond);
+}
+void launch_store(cmf_gpu_ctx *c) {
+    const Sched &q = c->sched;
+    const int nc = nblk(c->dims.nseqall, q.bs);
+    const dim3 g(nc + nblk(c->net.P, q.bs), c->dims.nmembers);
+    if (q.prof)
+        cmf::k_store<cmf::kStoreMinBlocksSmall><<<g, q.bs, cmf::store_smem(q.bs), c->stream>>>(c->net, c->st, nc);
+    else
+        cmf::k_store<cmf::kStoreMinBlocksWide><<<g, q.bs, cmf::store_smem(q.bs), c->stream>>>(c->net, c->st, nc);
+}
+constexpr int kStageBlock = 256;   // stage + CFL kernel (once per outer step)
+void launch_stage(cmf_gpu_ctx *c) {
+    const dim3 g(nblk(c->dims.nseqall, kStageBlock), c->dims.nmembers);
+    cmf::k_stage<<<g, kStageBlock, 0, c->stream>>>(c->net, c->st);
 }
 
-// phase A and phase C in the context's occupancy profile
-void launch_flux(cmf_gpu_ctx *c, dim3 grid, int block) {
-    if (c->small_cells)
-        cmf::k_flux<cmf::kFluxMinBlocksSmall><<<grid, block, 0, c->stream>>>(c->net, c->st, c->ncell_blocks);
-    else
-        cmf::k_flux<cmf::kFluxMinBlocksWide><<<grid, block, 0, c->stream>>>(c->net, c->st, c->ncell_blocks);
-}
-void launch_store(cmf_gpu_ctx *c, dim3 grid, int block) {
-    if (c->small_cells)
-        cmf::k_store<cmf::kStoreMinBlocksSmall><<<grid, block, cmf::store_smem(block), c->stream>>>(c->net, c->st,
-                                                                                                   c->ncell_blocks);
-    else
-        cmf::k_store<cmf::kStoreMinBlocksWide><<<grid, block, cmf::store_smem(block), c->stream>>>(c->net, c->st,
-                                                                                                  c->ncell_blocks);
-}
-
-// Enqueue one sub-step (phases A, B, C and the control kernel).
+// Enqueue one sub-step (phases A, B, C).
 void enqueue_substep(cmf_gpu_ctx *c, int use_cond, cudaGraphConditionalHandle cond) {
-    const dim3 gc(c->ncell_blocks, c->dims.nmembers);
-    const dim3 gcp(c->ncell_blocks + c->npath_blocks, c->dims.nmembers);
-    launch_flux(c, gcp, c->block);
-    cmf::k_rate<<<gc, c->block, 0, c->stream>>>(c->net, c->st, 1, cond, use_cond);
-    launch_store(c, gcp, c->block);
+    launch_flux(c);
+    launch_rate(c, 1, cond, use_cond);
+    launch_store(c);
 }
 void enqueue_substep(cmf_gpu_ctx *c, int use_cond) { enqueue_substep(c, use_cond, c->cond); }
 
 void enqueue_prologue(cmf_gpu_ctx *c, int use_cond, cudaGraphConditionalHandle cond) {
-    const dim3 gc(c->ncell_blocks, c->dims.nmembers);
-    cmf::k_stage<<<gc, c->block, 0, c->stream>>>(c->net, c->st);
+    launch_stage(c);
     cmf::k_ntdt<<<1, 256, 0, c->stream>>>(c->net, c->st, cond, use_cond);
 }
 void enqueue_prologue(cmf_gpu_ctx *c, int use_cond) { enqueue_prologue(c, use_cond, c->cond); }
 
 // after the sub-step loop: the budgets of every member's last sub-step
 void enqueue_epilogue(cmf_gpu_ctx *c) {
-    cmf::k_budget<<<dim3(c->dims.nmembers, cmf::kBudgets), cmf::kBudgetThreads, 0, c->stream>>>(c->net, c->st,
-                                                                                           c->ncell_blocks);
+    cmf::k_budget<<<dim3(c->dims.nmembers, cmf::kBudgets), cmf::kBudgetThreads, 0, c->stream>>>(c->net, c->st);
 }
 
 // Captures one context's outer step (prologue, then a WHILE node around the sub-step body) into
@@ -485,63 +520,109 @@ int launch_persist(cmf_gpu_ctx *c, cmf::PersistArgs a) {
     return CMF_OK;
 }
 
-int launch_outer(cmf_gpu_ctx *c) {
-    if (c->persist) return launch_persist(c, persist_args(c));
-    if (c->opts.launch_mode == 0) {
-        CUDA_TRY(cudaGraphLaunch(c->exec, c->stream));
-        c->launches += 3;   // prologue and epilogue; the loop body adds 3 per sub-step (counted on read-back)
+int read_loop(cmf_gpu_ctx *c, cmf::LoopCtl *lc) {
+    CUDA_TRY(cudaMemcpyAsync(lc, c->st.loop, sizeof *lc, cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    return CMF_OK;
+}
+
+int build_graph(cmf_gpu_ctx *c);
+
+// Installs a schedule: the persistent flag and, for graph launches, the graph of the phase kernels.
+int apply_sched(cmf_gpu_ctx *c, const Sched &q) {
+    const bool rebuild = c->opts.launch_mode == 0 && q.mode == 0 && (!c->exec || !(q == c->sched) || c->persist);
+    c->sched = q;
+    c->persist = q.mode == 2;
+    if (rebuild) return build_graph(c);
+    return CMF_OK;
+}
+
+using SchedKey = std::tuple<int, int, int, int, int, int, int>;
+std::map<SchedKey, Sched> g_sched_cache;
+std::mutex g_sched_mu;
+SchedKey sched_key(const cmf_gpu_ctx *c) {
+    const int flags = c->opts.llevee | (c->opts.ldamout << 1) | (c->opts.lpthout << 2) | (c->opts.ldiag << 3) |
+                      (c->net.ldiag_out << 4) | (c->opts.lfldout << 5);
+    return SchedKey{c->device, c->dims.nseqall, c->dims.nseqriv, c->dims.nmembers, c->net.P, c->net.Lp, flags};
+}
+
+// before an outer step: the tuner's schedule for it, and the start of its timing
+int tune_begin(cmf_gpu_ctx *c, bool &trial) {
+    trial = false;
+    Tuner &t = c->tune;
+    if (!t.active) return CMF_OK;
+    if (t.warm > 0) {
+        t.warm--;
         return CMF_OK;
     }
-    enqueue_prologue(c, 0);
-    CUDA_TRY(cudaGetLastError());
+    int rc;
+    if (t.rep == 0 && (rc = apply_sched(c, t.cands[t.cand]))) return rc;
     cmf::LoopCtl lc;
-    CUDA_TRY(cudaMemcpyAsync(&lc, c->st.loop, sizeof lc, cudaMemcpyDeviceToHost, c->stream));
-    CUDA_TRY(cudaStreamSynchronize(c->stream));
-    for (int k = 0; k < lc.ntmax; k++) enqueue_substep(c, 0);
-    enqueue_epilogue(c);
-    CUDA_TRY(cudaGetLastError());
-    c->launches += 3 + 3LL * lc.ntmax;
+    if ((rc = read_loop(c, &lc))) return rc;
+    t.iters0 = lc.loop_iters;
+    CUDA_TRY(cudaEventRecord(t.e0, c->stream));
+    trial = true;
     return CMF_OK;
+}
+
+// after a timed outer step: time per sub-step of the candidate; after the last candidate, the
+// fastest schedule is installed and cached
+int tune_end(cmf_gpu_ctx *c, bool trial) {
+    if (!trial) return CMF_OK;
+    Tuner &t = c->tune;
+    CUDA_TRY(cudaEventRecord(t.e1, c->stream));
+    CUDA_TRY(cudaEventSynchronize(t.e1));
+    float ms = 0.f;
+    CUDA_TRY(cudaEventElapsedTime(&ms, t.e0, t.e1));
+    cmf::LoopCtl lc;
+    int rc;
+    if ((rc = read_loop(c, &lc))) return rc;
+    const double sub = (double)std::max(1LL, lc.loop_iters - t.iters0);
+    const double per = ms / sub;
+    if (t.rep == 0 || per < t.ms[t.cand]) t.ms[t.cand] = per;       // best of the repetitions
+    if (++t.rep < t.reps) return CMF_OK;
+    t.rep = 0;
+    if (++t.cand < (int)t.cands.size()) return CMF_OK;
+    size_t best = 0, worst = 0;
+    for (size_t k = 1; k < t.cands.size(); k++) {
+        if (t.ms[k] < t.ms[best]) best = k;
+        if (t.ms[k] > t.ms[worst]) worst = k;
+    }
+    t.best_us = t.ms[best] * 1e3;
+    t.worst_us = t.ms[worst] * 1e3;
+    t.timed = (int)t.cands.size();
+    t.active = false;
+    if ((rc = apply_sched(c, t.cands[best]))) return rc;
+    std::lock_guard<std::mutex> lk(g_sched_mu);
+    g_sched_cache[sched_key(c)] = t.cands[best];
+    return CMF_OK;
+}
+
+int launch_outer(cmf_gpu_ctx *c) {
+    bool trial = false;
+    int rc;
+    if ((rc = tune_begin(c, trial))) return rc;
+    if (c->persist) {
+        if ((rc = launch_persist(c, persist_args(c)))) return rc;
+    } else if (c->opts.launch_mode == 0) {
+        CUDA_TRY(cudaGraphLaunch(c->exec, c->stream));
+        c->launches += 3;   // prologue and epilogue; the loop body adds 3 per sub-step (counted on read-back)
+    } else {
+        enqueue_prologue(c, 0);
+        CUDA_TRY(cudaGetLastError());
+        cmf::LoopCtl lc;
+        if ((rc = read_loop(c, &lc))) return rc;
+        for (int k = 0; k < lc.ntmax; k++) enqueue_substep(c, 0);
+        enqueue_epilogue(c);
+        CUDA_TRY(cudaGetLastError());
+        c->launches += 3 + 3LL * lc.ntmax;
+    }
+    return tune_end(c, trial);
 }
 
 int read_ctl(cmf_gpu_ctx *c) {
     CUDA_TRY(cudaMemcpyAsync(c->hctl.data(), c->st.ctl, c->hctl.size() * sizeof(cmf::MemberCtl), cudaMemcpyDeviceToHost, c->stream));
     CUDA_TRY(cudaStreamSynchronize(c->stream));
-    return CMF_OK;
-}
-
-int autotune(cmf_gpu_ctx *c) {
-    // times one sub-step (phases A, B, C) of the zero state for each candidate block size
-    const int cands[] = {128, 256};   // the cell kernels are built for at most cmf::kCellThreads
-    std::vector<cmf::MemberCtl> probe(c->dims.nmembers);
-    for (auto &m : probe) { m = cmf::MemberCtl{}; m.dt_def = 3600.0; m.dt = 600.0; m.nt = 1; m.it = 0; }
-    CUDA_TRY(cudaMemcpyAsync(c->st.ctl, probe.data(), probe.size() * sizeof(cmf::MemberCtl), cudaMemcpyHostToDevice, c->stream));
-    cudaEvent_t e0, e1;
-    CUDA_TRY(cudaEventCreate(&e0));
-    CUDA_TRY(cudaEventCreate(&e1));
-    float best = 1e30f;
-    int best_b = 256;
-    for (int b : cands) {
-        set_blocks(c, b);
-        const dim3 gc(c->ncell_blocks, c->dims.nmembers), gcp(c->ncell_blocks + c->npath_blocks, c->dims.nmembers);
-        float tot = 0.f;
-        for (int rep = 0; rep < 4; rep++) {
-            CUDA_TRY(cudaEventRecord(e0, c->stream));
-            launch_flux(c, gcp, b);
-            cmf::k_rate<<<gc, b, 0, c->stream>>>(c->net, c->st, 0, c->cond, 0);
-            launch_store(c, gcp, b);
-            CUDA_TRY(cudaEventRecord(e1, c->stream));
-            CUDA_TRY(cudaEventSynchronize(e1));
-            float ms = 0.f;
-            CUDA_TRY(cudaEventElapsedTime(&ms, e0, e1));
-            if (rep > 0) tot += ms;
-        }
-        c->launches += 12;
-        if (tot < best) { best = tot; best_b = b; }
-    }
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
-    set_blocks(c, best_b);
     return CMF_OK;
 }
 
@@ -624,6 +705,7 @@ int finish_outer(cmf_gpu_ctx *c, int32_t *nt_out, double *dt_out, cmf_budget *b)
 }
 
 cmf_gpu_ctx *g_default = nullptr;
+constexpr int kTuneWarm = 4;   // outer steps before the autotuner's first candidate
 
 }  // namespace
 
@@ -727,23 +809,55 @@ int cmf_gpu_create(const cmf_dims *dims, const cmf_params *params, const cmf_map
         return fail(set_err(CMF_E_CUDA, "cudaStreamCreate failed"));
     if ((rc = build_net(c, maps))) return fail(rc);
     if ((rc = alloc_state(c))) return fail(rc);
-    c->small_cells = (size_t)dims->nseqall * (size_t)dims->nmembers <= cmf::kSmallCellMembers;
-    if (opts->block_size > 0) {
-        if (opts->block_size % 32 || opts->block_size > cmf::kCellThreads || opts->block_size < 64)
-            return fail(set_err(CMF_E_ARG, "block_size must be a multiple of 32 in [64, 256]"));
-        set_blocks(c, opts->block_size);
-    } else if ((rc = autotune(c))) {
-        return fail(rc);
-    }
     if ((rc = persist_setup(c))) return fail(rc);
+    if (opts->launch_mode < 0 || opts->launch_mode > 2) return fail(set_err(CMF_E_ARG, "launch_mode must be 0, 1 or 2"));
+    if (opts->block_size && (opts->block_size % 32 || opts->block_size > cmf::kCellThreads || opts->block_size < 64))
+        return fail(set_err(CMF_E_ARG, "block_size must be a multiple of 32 in [64, 256]"));
+    // starting schedule: phase kernels at 128 threads, the low-spill profile for grids of about a
+    // wave (the rule of thumb the autotuner then checks against the alternatives)
+    Sched q;
+    q.bf = q.br = q.bs = opts->block_size > 0 ? opts->block_size : 128;
+    q.prof = (size_t)dims->nseqall * (size_t)dims->nmembers <= cmf::kSmallCellMembers ? 1 : 0;
     if (opts->launch_mode == 2) {
         if (c->persist_grid < 1) return fail(set_err(CMF_E_UNSUPPORTED, "launch_mode 2: the persistent kernel cannot run here"));
-        c->persist = true;
+        q.mode = 2;
     }
     if ((rc = zero_state(c))) return fail(rc);
     c->dt_def_dev = -1.0;
     if ((rc = sync_dt_def(c, 86400.0))) return fail(rc);
-    if ((opts->launch_mode == 0 || c->persist) && (rc = build_graph(c))) return fail(rc);
+    if ((rc = apply_sched(c, q))) return fail(rc);
+    if (opts->launch_mode == 0 && opts->block_size == 0) {
+        bool cached = false;
+        {
+            std::lock_guard<std::mutex> lk(g_sched_mu);
+            auto it = g_sched_cache.find(sched_key(c));
+            if (it != g_sched_cache.end()) { q = it->second; cached = true; }
+        }
+        if (cached) {
+            if ((rc = apply_sched(c, q))) return fail(rc);
+        } else {
+            Tuner &t = c->tune;
+            for (int bf : {128, 256})
+                for (int bs : {128, 256})
+                    for (int prof : {0, 1}) {
+                        Sched k;
+                        k.bf = k.br = bf;
+                        k.bs = bs;
+                        k.prof = prof;
+                        t.cands.push_back(k);
+                    }
+            if (c->persist_grid > 0) {
+                Sched k;
+                k.mode = 2;
+                t.cands.push_back(k);
+            }
+            t.ms.assign(t.cands.size(), 0.0);
+            t.warm = kTuneWarm;
+            if (cudaEventCreate(&t.e0) != cudaSuccess || cudaEventCreate(&t.e1) != cudaSuccess)
+                return fail(set_err(CMF_E_CUDA, "cudaEventCreate failed"));
+            t.active = true;
+        }
+    }
     if (cudaStreamSynchronize(c->stream) != cudaSuccess) return fail(set_err(CMF_E_CUDA, cudaGetErrorString(cudaGetLastError())));
     *out = c;
     return CMF_OK;
@@ -755,6 +869,8 @@ int cmf_gpu_destroy(cmf_gpu_ctx *c) {
     if (c->stream) cudaStreamSynchronize(c->stream);
     if (c->exec) cudaGraphExecDestroy(c->exec);
     if (c->graph) cudaGraphDestroy(c->graph);
+    if (c->tune.e0) cudaEventDestroy(c->tune.e0);
+    if (c->tune.e1) cudaEventDestroy(c->tune.e1);
     for (void *p : c->allocs) cudaFree(p);
     if (c->rgrid) cudaFree(c->rgrid);
     if (c->stream) cudaStreamDestroy(c->stream);
@@ -823,9 +939,9 @@ int cmf_gpu_ctx_diag_output(cmf_gpu_ctx *c, int32_t op) {
         return CMF_OK;
     }
     if (op == CMF_DIAG_OUT_GETAVE) {
-        const int pl_blocks = MPL ? (int)((c->net.P * c->net.Lp + c->block - 1) / c->block) : 0;
-        const dim3 g(c->ncell_blocks + pl_blocks, c->dims.nmembers);
-        cmf::k_diag_getave_output<<<g, c->block, 0, c->stream>>>(c->net, c->st, c->ncell_blocks);
+        const int b = 256, nc = nblk(c->dims.nseqall, b);
+        const dim3 g(nc + (MPL ? nblk(c->net.P * c->net.Lp, b) : 0), c->dims.nmembers);
+        cmf::k_diag_getave_output<<<g, b, 0, c->stream>>>(c->net, c->st, nc);
         CUDA_TRY(cudaGetLastError());
         c->launches += 1;
         return CMF_OK;
@@ -916,11 +1032,10 @@ int cmf_gpu_ctx_time_phases(cmf_gpu_ctx *c, double dt_def, int32_t reps, double 
         }
         return CMF_OK;
     };
-    const dim3 gc(c->ncell_blocks, c->dims.nmembers), gcp(c->ncell_blocks + c->npath_blocks, c->dims.nmembers);
     for (int r = 0; r < reps && !rc; r++) {
         if ((rc = need(3))) break;
         CUDA_TRY(cudaEventRecord(ev[0], c->stream));
-        cmf::k_stage<<<gc, c->block, 0, c->stream>>>(c->net, c->st);
+        launch_stage(c);
         CUDA_TRY(cudaEventRecord(ev[1], c->stream));
         cmf::k_ntdt<<<1, 256, 0, c->stream>>>(c->net, c->st, c->cond, 0);
         CUDA_TRY(cudaEventRecord(ev[2], c->stream));
@@ -936,11 +1051,11 @@ int cmf_gpu_ctx_time_phases(cmf_gpu_ctx *c, double dt_def, int32_t reps, double 
         if ((rc = need(3 * (size_t)nt + 2))) break;
         CUDA_TRY(cudaEventRecord(ev[0], c->stream));
         for (int k = 0; k < nt; k++) {
-            launch_flux(c, gcp, c->block);
+            launch_flux(c);
             CUDA_TRY(cudaEventRecord(ev[3 * k + 1], c->stream));
-            cmf::k_rate<<<gc, c->block, 0, c->stream>>>(c->net, c->st, 1, c->cond, 0);
+            launch_rate(c, 1, c->cond, 0);
             CUDA_TRY(cudaEventRecord(ev[3 * k + 2], c->stream));
-            launch_store(c, gcp, c->block);
+            launch_store(c);
             CUDA_TRY(cudaEventRecord(ev[3 * k + 3], c->stream));
         }
         enqueue_epilogue(c);
@@ -1022,15 +1137,7 @@ int cmf_gpu_ctx_advance_device(cmf_gpu_ctx *c, double dt_def, int32_t ksteps, co
     for (int k = 0; k < ksteps; k++) {
         if (runoff_dev)
             CUDA_TRY(cudaMemcpyAsync(c->st.runoff, runoff_dev + (size_t)k * stride, MN * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
-        if (c->persist) {
-            if ((rc = launch_persist(c, persist_args(c)))) return rc;
-        } else if (c->opts.launch_mode == 0) {
-            CUDA_TRY(cudaGraphLaunch(c->exec, c->stream));
-            c->launches += 3;
-        } else {
-            // host-driven: the same kernels as plain launches (reads NTmax back once per step)
-            if ((rc = launch_outer(c))) return rc;
-        }
+        if ((rc = launch_outer(c))) return rc;
     }
     return CMF_OK;
 }
@@ -1210,8 +1317,9 @@ int cmf_gpu_ctx_calc_outpre(cmf_gpu_ctx *c) {
     const double dt = c->dt_def_dev > 0.0 ? c->dt_def_dev : 86400.0;
     int rc = cmf_gpu_ctx_stage(c, dt, nullptr);
     if (rc) return rc;
-    const dim3 g(c->ncell_blocks + c->npath_blocks, c->dims.nmembers);
-    cmf::k_outpre<<<g, c->block, 0, c->stream>>>(c->net, c->st, c->ncell_blocks);
+    const int b = 256, nc = nblk(c->dims.nseqall, b);
+    const dim3 g(nc + nblk(c->net.P, b), c->dims.nmembers);
+    cmf::k_outpre<<<g, b, 0, c->stream>>>(c->net, c->st, nc);
     CUDA_TRY(cudaGetLastError());
     c->launches += 1;
     CUDA_TRY(cudaStreamSynchronize(c->stream));
@@ -1293,15 +1401,55 @@ int cmf_gpu_ctx_put_runoff_grid(cmf_gpu_ctx *c, const void *grid, int32_t is_flo
 
 void *cmf_gpu_ctx_stream(cmf_gpu_ctx *c) { return c ? (void *)c->stream : nullptr; }
 int64_t cmf_gpu_ctx_kernel_launches(cmf_gpu_ctx *c) { return c ? c->launches : 0; }
-int32_t cmf_gpu_ctx_block_size(cmf_gpu_ctx *c) { return c ? c->block : 0; }
+int32_t cmf_gpu_ctx_block_size(cmf_gpu_ctx *c) { return c ? c->sched.bf : 0; }
+
+int cmf_gpu_ctx_get_schedule(cmf_gpu_ctx *c, cmf_schedule *out) {
+    if (!c || !out) return set_err(CMF_E_ARG, "null argument");
+    const Sched &q = c->sched;
+    out->mode = q.mode;
+    out->flux_block = q.bf;
+    out->rate_block = q.br;
+    out->store_block = q.bs;
+    out->profile = q.prof;
+    out->tuned = c->tune.active ? -1 : (c->tune.timed > 0 ? 1 : 0);
+    out->candidates = c->tune.timed;
+    out->best_us_per_substep = c->tune.best_us;
+    out->worst_us_per_substep = c->tune.worst_us;
+    return CMF_OK;
+}
+
+void cmf_gpu_schedule_cache_clear(void) {
+    std::lock_guard<std::mutex> lk(g_sched_mu);
+    g_sched_cache.clear();
+}
+
+int cmf_gpu_ctx_set_schedule(cmf_gpu_ctx *c, const cmf_schedule *q) {
+    if (!c || !q) return set_err(CMF_E_ARG, "null argument");
+    if (c->opts.launch_mode == 1) return set_err(CMF_E_UNSUPPORTED, "launch_mode 1 contexts run the phase kernels from the host");
+    Sched k;
+    k.mode = q->mode;
+    k.bf = q->flux_block;
+    k.br = q->rate_block;
+    k.bs = q->store_block;
+    k.prof = q->profile;
+    if (k.mode != 0 && k.mode != 2) return set_err(CMF_E_ARG, "schedule mode must be 0 (graph) or 2 (persistent)");
+    if (k.mode == 2 && c->persist_grid < 1) return set_err(CMF_E_UNSUPPORTED, "the persistent kernel cannot run here");
+    for (int b : {k.bf, k.br, k.bs})
+        if (b % 32 || b < 64 || b > cmf::kCellThreads) return set_err(CMF_E_ARG, "block sizes must be multiples of 32 in [64, 256]");
+    if (k.prof != 0 && k.prof != 1) return set_err(CMF_E_ARG, "profile must be 0 or 1");
+    CUDA_TRY(cudaSetDevice(c->device));
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    c->tune.active = false;
+    c->tune.timed = 0;
+    return apply_sched(c, k);
+}
 
 int cmf_gpu_ctx_stage(cmf_gpu_ctx *c, double dt_def, double *dt_min_local) {
     if (!c) return set_err(CMF_E_STATE, "no context");
     CUDA_TRY(cudaSetDevice(c->device));
     int rc;
     if ((rc = sync_dt_def(c, dt_def))) return rc;
-    const dim3 gc(c->ncell_blocks, c->dims.nmembers);
-    cmf::k_stage<<<gc, c->block, 0, c->stream>>>(c->net, c->st);
+    launch_stage(c);
     CUDA_TRY(cudaGetLastError());
     c->launches += 1;
     if ((rc = read_ctl(c))) return rc;

@@ -1071,23 +1071,21 @@ __device__ __forceinline__ void cell_store(const Net &n, const State &s, const O
     }
 }
 
-// per-block budget partials of the last sub-step (the only one the caller observes);
-// fixed-shape tree -> deterministic; layout [m][k][block] for a coalesced final reduction.
-// Every thread of the block calls it (it holds block barriers); bt: this thread's kBudgets terms,
-// stride bstride apart in shared memory.
-__device__ __forceinline__ void store_budget_partials(const State &s, int m, int blk, int ncell_blocks, const double *bt,
-                                                      int bstride, double *red) {
-    __syncthreads();
-    double b[kBudgets];
+// Budget partials of the last sub-step (the only one the caller observes), one per warp of 32
+// consecutive cells: a fixed butterfly over the warp, so the partials -- and the budgets k_budget
+// sums from them in a fixed order -- are the same whatever block size or schedule ran the cells.
+// Layout [m][k][warp] for a coalesced final reduction.  Every lane of the warp calls it.
+__device__ __forceinline__ void warp_budget_partials(const State &s, int m, int warp, int nwarps, double (&b)[kBudgets]) {
 #pragma unroll
-    for (int k = 0; k < kBudgets; k++) b[k] = bt[k * bstride];
-    block_sum<kBudgets>(b, red);
-    if (threadIdx.x == 0) {
-        double *dst = s.partials + (size_t)m * kBudgets * ncell_blocks + blk;
+    for (int k = 0; k < kBudgets; k++)
+        for (int o = 16; o > 0; o >>= 1) b[k] = b[k] + __shfl_down_sync(0xffffffffu, b[k], o);
+    if ((threadIdx.x & 31) == 0 && warp < nwarps) {     // warps past the last cell hold no cells
+        double *dst = s.partials + (size_t)m * kBudgets * nwarps + warp;
 #pragma unroll
-        for (int k = 0; k < kBudgets; k++) dst[(size_t)k * ncell_blocks] = b[k];
+        for (int k = 0; k < kBudgets; k++) dst[(size_t)k * nwarps] = b[k];
     }
 }
+__host__ __device__ inline int budget_warps(int N) { return (N + 31) / 32; }
 
 template <int MinBlocks>
 __global__ void __launch_bounds__(kCellThreads, MinBlocks) k_store(Net n, State s, int ncell_blocks) {
@@ -1117,8 +1115,10 @@ __global__ void __launch_bounds__(kCellThreads, MinBlocks) k_store(Net n, State 
         for (int k = 0; k < kBudgets; k++) bt[k * bstride] = 0.0;
     if (i < n.N) cell_store(n, s, OwnG{n, s}, m, i, DT, first, last, nadd, c, bput);
     if (last) {
-        __shared__ double red[32 * kBudgets];
-        store_budget_partials(s, m, blockIdx.x, ncell_blocks, bt, bstride, red);
+        double b[kBudgets];
+#pragma unroll
+        for (int k = 0; k < kBudgets; k++) b[k] = bt[k * bstride];
+        warp_budget_partials(s, m, i >> 5, budget_warps(n.N), b);
     }
 }
 
@@ -1126,15 +1126,16 @@ __global__ void __launch_bounds__(kCellThreads, MinBlocks) k_store(Net n, State 
 // k_budget: after the sub-step loop, the budgets of every member's last sub-step
 // ------------------------------------------------------------------------------------------
 // grid (members, kBudgets), kBudgetThreads threads: block (m, k) reduces budget k of member m over
-// the block partials its last sub-step wrote -- thread t sums partials t, t+T, ... in order, then a
+// the warp partials its last sub-step wrote -- thread t sums partials t, t+T, ... in order, then a
 // fixed warp tree and a fixed tree over the warps: the same sums whatever the timing
 constexpr int kBudgetThreads = 256;
-__global__ void __launch_bounds__(kBudgetThreads) k_budget(Net n, State s, int ncell_blocks) {
+__global__ void __launch_bounds__(kBudgetThreads) k_budget(Net n, State s) {
     const int m = blockIdx.x, k = blockIdx.y;
     if (s.ctl[m].nt < 1) return;                        // refused step (NT cap): no sub-step ran
-    const double *src = s.partials + ((size_t)m * kBudgets + k) * ncell_blocks;
+    const int nw = budget_warps(n.N);
+    const double *src = s.partials + ((size_t)m * kBudgets + k) * nw;
     double x = 0.0;
-    for (int b = threadIdx.x; b < ncell_blocks; b += kBudgetThreads) x = x + src[b];
+    for (int b = threadIdx.x; b < nw; b += kBudgetThreads) x = x + src[b];
     for (int o = 16; o > 0; o >>= 1) x = x + __shfl_down_sync(0xffffffffu, x, o);
     __shared__ double w[kBudgetThreads / 32];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;

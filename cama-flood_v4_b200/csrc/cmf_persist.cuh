@@ -316,12 +316,13 @@ __device__ __forceinline__ bool run_cell_phase(Pipe &pp, const PhaseArrays &pa, 
     return true;
 }
 
-__device__ __forceinline__ void budget_reduce(const Net &n, const State &s, int m, int k, int nblk) {
+__device__ __forceinline__ void budget_reduce(const Net &n, const State &s, int m, int k) {
     // k_budget's tree (kBudgetThreads == kTile threads): the same sums as the phase-kernel path
     if (s.ctl[m].nt < 1) return;
-    const double *src = s.partials + ((size_t)m * kBudgets + k) * nblk;
+    const int nw = budget_warps(n.N);
+    const double *src = s.partials + ((size_t)m * kBudgets + k) * nw;
     double x = 0.0;
-    for (int b = threadIdx.x; b < nblk; b += kBudgetThreads) x = x + src[b];
+    for (int b = threadIdx.x; b < nw; b += kBudgetThreads) x = x + src[b];
     for (int o = 16; o > 0; o >>= 1) x = x + __shfl_down_sync(0xffffffffu, x, o);
     __shared__ double w[kBudgetThreads / 32];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -402,7 +403,6 @@ __device__ __forceinline__ void ntdt_block(const Net &n, const State &s) {
 __global__ void __launch_bounds__(kTile, 2) k_persist(Net n, State s, PersistArgs pa) {
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ int sflag;
-    __shared__ double red[32 * kBudgets];
     const unsigned G = gridDim.x, b = blockIdx.x;
     GridBar gb{&s.loop->bar, &s.loop->bar_err, G, 0u, pa.wait_ns, &sflag};
     if (pa.selftest) {
@@ -527,14 +527,7 @@ __global__ void __launch_bounds__(kTile, 2) k_persist(Net n, State s, PersistArg
                 for (int q = 0; q < kBudgets; q++) bl[q] = 0.0;
                 auto bput = [&](int q, double val) { if (last) bl[q] = val; };
                 if (i < tg.i1) cell_store(n, s, OwnTC{v}, tg.m, i, DT, first, last, nadd, c, bput);
-                if (last) {
-                    block_sum<kBudgets>(bl, red);
-                    if (threadIdx.x == 0) {
-                        double *dst = s.partials + (size_t)tg.m * kBudgets * tpm + tg.j;
-#pragma unroll
-                        for (int q = 0; q < kBudgets; q++) dst[(size_t)q * tpm] = bl[q];
-                    }
-                }
+                if (last) warp_budget_partials(s, tg.m, i >> 5, budget_warps(N), bl);
             }))
             return;
         for (int t = p0; t < p1; t++) {
@@ -549,7 +542,7 @@ __global__ void __launch_bounds__(kTile, 2) k_persist(Net n, State s, PersistArg
         if (!gb.sync()) return;
     }
     // ---- budgets of every member's last sub-step (k_budget)
-    for (int r = b; r < M * kBudgets; r += G) budget_reduce(n, s, r / kBudgets, r % kBudgets, tpm);
+    for (int r = b; r < M * kBudgets; r += G) budget_reduce(n, s, r / kBudgets, r % kBudgets);
     if (b == 0 && threadIdx.x == 0) s.loop->split = 0;
 }
 

@@ -83,7 +83,8 @@ typedef struct cmf_opts {
                             2: one persistent cooperative kernel per coupling step (grid barriers
                                between the phases, tiles streamed by bulk asynchronous copies)    */
     int32_t device;      /* CUDA device ordinal                                                   */
-    int32_t block_size;  /* 0: autotune; else threads per block for the cell kernels (64..256)   */
+    int32_t block_size;  /* 0: the online autotuner picks the schedule (launch_mode 0); else
+                            threads per block of the phase kernels (64..256)                     */
     int32_t ldiag_output;/* accumulate the output-interval averages/maxima (D2*_oAVG, D2*_oMAX) on
                             the device: CMF_DIAG_AVEMAX_OUTPUT after every outer step, as
                             CMF_DRV_ADVANCE calls it (src/cmf_drv_advance_mod.F90:114); needs ldiag */
@@ -194,8 +195,28 @@ int cmf_gpu_ctx_last_nt(cmf_gpu_ctx *ctx, int32_t *nt_out, double *dt_out);
 void *cmf_gpu_ctx_stream(cmf_gpu_ctx *ctx);
 /* Number of kernels this context launched so far (graph launches count their kernel nodes). */
 int64_t cmf_gpu_ctx_kernel_launches(cmf_gpu_ctx *ctx);
-/* Block size the autotuner chose for the cell kernels. */
+/* Threads per block of the flux kernel in the current schedule. */
 int32_t cmf_gpu_ctx_block_size(cmf_gpu_ctx *ctx);
+
+/* Launch schedule of the outer step.  Every schedule computes the same bits (states, NT/DT and the
+ * budgets, which are summed from per-warp partials), so it is a pure performance choice.  A
+ * launch_mode 0 context with block_size 0 is tuned online: after 4 outer steps on a starting
+ * schedule, each candidate (flux/rate block 128 or 256 x store block 128 or 256 x occupancy
+ * profile, and the persistent kernel) runs 2 real outer steps timed with CUDA events (best time
+ * per sub-step kept); the fastest is installed and cached per network shape for later contexts in
+ * the process.  cmf_gpu_ctx_set_schedule fixes a schedule (and stops tuning). */
+typedef struct cmf_schedule {
+    int32_t mode;                 /* 0 graph of phase kernels, 2 persistent cooperative kernel     */
+    int32_t flux_block, rate_block, store_block;   /* threads per block of the phase kernels     */
+    int32_t profile;              /* 0 more resident warps (fewer registers), 1 fewer spills       */
+    int32_t tuned;                /* 1 chosen by the autotuner, 0 fixed or cached, -1 still tuning  */
+    int32_t candidates;           /* candidates the autotuner timed                                */
+    double best_us_per_substep, worst_us_per_substep;
+} cmf_schedule;
+int cmf_gpu_ctx_get_schedule(cmf_gpu_ctx *ctx, cmf_schedule *out);
+int cmf_gpu_ctx_set_schedule(cmf_gpu_ctx *ctx, const cmf_schedule *sched);
+/* Forgets the cached schedules, so that the next contexts tune again. */
+void cmf_gpu_schedule_cache_clear(void);
 /* Device-side counters since creation: sum over outer steps and members of NT, sum over outer
  * steps of max NT (sub-step loop iterations) and the number of outer steps. */
 int cmf_gpu_ctx_counters(cmf_gpu_ctx *ctx, int64_t *member_substeps, int64_t *loop_iters, int64_t *outer_steps);

@@ -47,7 +47,7 @@ def test_ctypes_structs_match_header():
     for cname, py in [("cmf_dims", _abi.Dims), ("cmf_params", _abi.Params), ("cmf_opts", _abi.Opts),
                       ("cmf_map_ptrs", _abi.MapPtrs), ("cmf_state_ptrs", _abi.StatePtrs),
                       ("cmf_diag_ptrs", _abi.DiagPtrs), ("cmf_budget", _abi.Budget),
-                      ("cmf_diag_out_ptrs", _abi.DiagOutPtrs)]:
+                      ("cmf_diag_out_ptrs", _abi.DiagOutPtrs), ("cmf_schedule", _abi.Schedule)]:
         assert _struct_fields(cname) == [f[0] for f in py._fields_], cname
 
 
