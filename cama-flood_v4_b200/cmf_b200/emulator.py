@@ -47,6 +47,7 @@ def _emu_lib():
     if not getattr(lib, "_emu_ready", False):
         vp, i, f, d = C.c_void_p, C.c_int, C.c_float, C.c_double
         lib.cmf_emu_gemm.argtypes = [i, i, i, vp, i, i, vp, i, i, vp, i, vp, i, vp, i, i, i, vp]
+        lib.cmf_emu_gemm_mma.argtypes = [i, i, i, vp, i, i, vp, i, i, vp, i, vp, i, vp, i, i, i, vp]
         lib.cmf_emu_relu_bwd.argtypes = [i, vp, vp, vp, vp, vp]
         lib.cmf_emu_colsum.argtypes = [i, i, vp, vp, vp]
         lib.cmf_emu_mse_grad.argtypes = [i, i, i, vp, vp, vp, vp, vp, vp]
@@ -59,6 +60,7 @@ def _emu_lib():
         lib.cmf_emu_mlp_tc_pack_bytes.restype = C.c_size_t
         lib.cmf_emu_mlp_tc_pack.argtypes = [vp, vp, vp, vp, i, vp, vp]
         lib.cmf_emu_mlp_tc.argtypes = [vp, i, i, vp, vp, vp, vp, vp, vp, vp]
+        lib.cmf_emu_mlp_tc_set_wait_limit.argtypes = [C.c_int32]
         lib.cmf_emu_last_error.restype = C.c_char_p
         lib.cmf_gpu_ctx_emu_views.argtypes = [vp, C.c_int32, C.POINTER(EmuNet), C.POINTER(EmuMember)]
         lib.cmf_gpu_ctx_copy_member.argtypes = [vp, C.c_int32, vp, C.c_int32]

@@ -545,7 +545,11 @@ constexpr int kTcA = kTcWBytes;                       // activations: 128 rows x
 constexpr int kTcBias = kTcA + kTcRows * 128 * 2;     // b0 b1 b2 (3 x 128 floats), b3[0]
 constexpr int kTcMisc = kTcBias + (3 * 128 + 4) * 4;  // mbarrier (8 B), TMEM address (4 B)
 constexpr int kTcSmem = kTcMisc + 16;
-constexpr int kTcWaitLimit = 1 << 20;
+#ifndef CMF_TC_WAIT_LIMIT
+#define CMF_TC_WAIT_LIMIT (1 << 20)
+#endif
+constexpr int kTcWaitLimit = CMF_TC_WAIT_LIMIT;        // polls of an MMA completion before giving up
+int g_tc_wait_limit = kTcWaitLimit;                   // host side: the bound the next launches use
 
 __device__ int g_mlp_tc_status;                       // 0 ok; 1: an MMA completion wait ran out
 
@@ -597,8 +601,8 @@ __device__ __forceinline__ void umma_commit(uint32_t mbar) {
 }
 
 // bounded wait on an mbarrier phase; false when the limit ran out
-__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity) {
-    for (int i = 0; i < kTcWaitLimit; i++) {
+__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity, int limit) {
+    for (int i = 0; i < limit; i++) {
         uint32_t ok;
         asm volatile(
             "{\n\t.reg .pred p;\n\t"
@@ -660,7 +664,8 @@ __device__ __forceinline__ void tc_epilogue_hidden(uint32_t tmem_row, int col0, 
 __global__ void __launch_bounds__(kTcThreads, 2) k_mlp_tc(const __nv_bfloat16 *__restrict__ X, int ldx, int rows,
                                                         const uint4 *__restrict__ wimg, const float *__restrict__ b0,
                                                         const float *__restrict__ b1, const float *__restrict__ b2,
-                                                        const float *__restrict__ b3, float *__restrict__ y) {
+                                                        const float *__restrict__ b3, float *__restrict__ y,
+                                                        int wait_limit) {
     extern __shared__ __align__(1024) unsigned char sm[];
     unsigned char *sA = sm + kTcA;
     float *sb = reinterpret_cast<float *>(sm + kTcBias);
@@ -728,7 +733,7 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_mlp_tc(const __nv_bfloat16 *_
                 }
                 umma_commit(mb);
             }
-            const bool ok = mbar_wait(mb, phase);
+            const bool ok = mbar_wait(mb, phase, wait_limit);
             if (__syncthreads_or(ok ? 0 : 1)) { failed = true; break; }   // block-uniform exit
             phase ^= 1u;
             tc_fence_after();
@@ -751,13 +756,172 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_mlp_tc(const __nv_bfloat16 *_
     }
     if (failed) {
         if (tid == 0) atomicExch(&g_mlp_tc_status, 1);
-        mbar_wait(mb, phase);                                 // one more bounded wait for the MMA phase in flight
+        // the MMA of this phase may still be in flight: wait for it (full bound, whatever the
+        // launch's bound was) before the accumulator columns are released
+        mbar_wait(mb, phase, kTcWaitLimit);
         tc_fence_before();
         __syncthreads();
         tc_fence_after();
     }
     if (warp == 0)
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(tmem), "r"(kTcCols) : "memory");
+}
+
+// ------------------------------------------------------------------------------------------
+// Training GEMM on the 5th-generation tensor cores: the contract of k_gemm (C (+)= op(A) op(B),
+// bias + ReLU, fp32 and/or bf16 output, or split-K atomic accumulation), with the products on
+// tcgen05.  CTA tile 128 rows x NT columns (NT = 128, or 64 when N is not a multiple of 128); K in
+// chunks of 64 staged into two shared-memory buffers in the canonical K-major no-swizzle layout
+// (operands stored transposed in global memory are written element by element); one thread issues
+// the chunk's MMAs (M=128, N=NT, K=16, bf16 x bf16 -> fp32) into a tensor-memory accumulator and
+// commits them to the buffer's mbarrier, which completes (bounded wait) before the buffer is refilled.
+// Epilogue: thread t owns row t (TMEM lane t) and reads its NT accumulator columns 32 at a time.
+// ------------------------------------------------------------------------------------------
+constexpr int kGThreads = 128;                          // = rows of the tile = TMEM lanes
+constexpr int kGK = 64;                                 // K per staged chunk
+constexpr int kGTileBytes = 128 * kGK * 2;              // one 128-row operand chunk (bf16)
+constexpr int kGBuf = 2 * kGTileBytes;                  // A and B chunks of one buffer
+constexpr int kGSmem = 2 * kGBuf + 64;                  // two buffers, two mbarriers, TMEM address
+
+// stages rows [r0, r0 + 128) (rows >= rmax zero) x k [k0, k0 + kc) of an operand whose element
+// (r, k) is at P[r * ld + k] (kmajor) or P[k * ld + r] (r contiguous) into the canonical layout
+__device__ __forceinline__ void gemm_stage(unsigned char *dst, int R, const __nv_bfloat16 *__restrict__ P, int ld,
+                                           bool kmajor, int r0, int rmax, int k0, int kc) {
+    const int tid = threadIdx.x;
+    if (kmajor) {
+        const int cpr = kc / 8;                          // 16-byte chunks per row
+        for (int e = tid; e < R * cpr; e += kGThreads) {
+            const int r = e / cpr, kq = e - r * cpr;
+            uint4 v = make_uint4(0u, 0u, 0u, 0u);
+            if (r0 + r < rmax) v = *reinterpret_cast<const uint4 *>(P + (size_t)(r0 + r) * ld + k0 + kq * 8);
+            *reinterpret_cast<uint4 *>(dst + canon_off(r, kq * 8, R)) = v;
+        }
+    } else {
+        const int cpk = R / 8;                           // 16-byte chunks along r per k
+        for (int e = tid; e < kc * cpk; e += kGThreads) {
+            const int k = e / cpk, rq = e - k * cpk;
+            uint4 v = make_uint4(0u, 0u, 0u, 0u);
+            if (r0 + rq * 8 < rmax) v = *reinterpret_cast<const uint4 *>(P + (size_t)(k0 + k) * ld + r0 + rq * 8);
+            const __nv_bfloat16 *h = reinterpret_cast<const __nv_bfloat16 *>(&v);
+#pragma unroll
+            for (int j = 0; j < 8; j++) *reinterpret_cast<__nv_bfloat16 *>(dst + canon_off(rq * 8 + j, k, R)) = h[j];
+        }
+    }
+}
+
+template <int NT>
+__global__ void __launch_bounds__(kGThreads) k_gemm_tc(int M, int N, int K, const __nv_bfloat16 *__restrict__ A, int lda,
+                                                       int transA, const __nv_bfloat16 *__restrict__ B, int ldb, int transB,
+                                                       float *C, int ldc, __nv_bfloat16 *Cb, int ldcb,
+                                                       const float *__restrict__ bias, int relu, int accumulate,
+                                                       int k_per_split, int wait_limit) {
+    extern __shared__ __align__(1024) unsigned char sm[];
+    uint64_t *mbar = reinterpret_cast<uint64_t *>(sm + 2 * kGBuf);
+    uint32_t *tslot = reinterpret_cast<uint32_t *>(sm + 2 * kGBuf + 16);
+    const int tid = threadIdx.x, warp = tid >> 5;
+    const int m0 = blockIdx.x * 128, n0 = blockIdx.y * NT;
+    const int kbeg = blockIdx.z * k_per_split, kend = min(K, kbeg + k_per_split);
+    if (tid == 0) {
+        for (int b = 0; b < 2; b++) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_u32(&mbar[b])) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" :: "r"(smem_u32(tslot)), "r"(NT)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tslot;
+    const uint32_t idesc = umma_idesc_bf16_f32(128, NT);
+    uint32_t phase[2] = {0u, 0u};
+    bool issued[2] = {false, false};
+    bool failed = false;
+    int chunk = 0;
+    for (int k0 = kbeg; k0 < kend; k0 += kGK, chunk++) {
+        const int buf = chunk & 1;
+        unsigned char *sA = sm + buf * kGBuf, *sB = sA + kGTileBytes;
+        if (issued[buf]) {   // the MMAs that read this buffer two chunks ago must have finished
+            const bool ok = mbar_wait(smem_u32(&mbar[buf]), phase[buf], wait_limit);
+            if (__syncthreads_or(ok ? 0 : 1)) { failed = true; break; }   // block-uniform
+            phase[buf] ^= 1u;
+            issued[buf] = false;
+            tc_fence_after();
+        }
+        const int kc = min(kGK, kend - k0);             // a multiple of 32
+        gemm_stage(sA, 128, A, lda, !transA, m0, M, k0, kc);
+        gemm_stage(sB, NT, B, ldb, transB != 0, n0, N, k0, kc);
+        fence_async_smem();
+        tc_fence_before();
+        __syncthreads();
+        if (tid == 0) {
+            tc_fence_after();
+            for (int s = 0; s < kc / 16; s++) {
+                const uint64_t ad = umma_smem_desc(smem_u32(sA) + 2 * s * (128 * 16), 128 * 16, 128);
+                const uint64_t bd = umma_smem_desc(smem_u32(sB) + 2 * s * (NT * 16), NT * 16, 128);
+                umma_bf16(tmem, ad, bd, idesc, (chunk > 0 || s > 0) ? 1u : 0u);
+            }
+            umma_commit(smem_u32(&mbar[buf]));
+        }
+        issued[buf] = true;
+    }
+    // the outstanding commits, oldest first (after a failure: drain them with the full bound
+    // before the accumulator columns are released)
+    for (int q = 0; q < 2; q++) {
+        const int b = (chunk + q) & 1;
+        if (!issued[b]) continue;
+        const bool ok = mbar_wait(smem_u32(&mbar[b]), phase[b], failed ? kTcWaitLimit : wait_limit);
+        if (__syncthreads_or(ok ? 0 : 1)) failed = true;
+        phase[b] ^= 1u;
+    }
+    tc_fence_after();
+    if (failed) {
+        if (tid == 0) atomicExch(&g_mlp_tc_status, 1);
+    } else {
+        const uint32_t trow = tmem + ((uint32_t)(32 * warp) << 16);
+        const int row = m0 + tid;
+        const bool vec = ((ldc & 3) == 0) && (((uintptr_t)C & 15) == 0);
+#pragma unroll 1
+        for (int c0 = 0; c0 < NT; c0 += 32) {
+            uint32_t v[32];
+            tmem_ld32(trow + c0, v);
+            tmem_wait_ld();
+            if (row >= M) continue;
+            const int col = n0 + c0;
+            float x[32];
+#pragma unroll
+            for (int j = 0; j < 32; j++) x[j] = __uint_as_float(v[j]);
+            if (accumulate) {
+#pragma unroll
+                for (int j = 0; j < 32; j++) atomicAdd(&C[(size_t)row * ldc + col + j], x[j]);
+                continue;
+            }
+#pragma unroll
+            for (int j = 0; j < 32; j++) {
+                if (bias) x[j] += bias[col + j];
+                if (relu) x[j] = fmaxf(x[j], 0.f);
+            }
+            if (C) {
+                float *dst = C + (size_t)row * ldc + col;
+                if (vec) {
+#pragma unroll
+                    for (int j = 0; j < 32; j += 4) *reinterpret_cast<float4 *>(dst + j) = make_float4(x[j], x[j + 1], x[j + 2], x[j + 3]);
+                } else {
+#pragma unroll
+                    for (int j = 0; j < 32; j++) dst[j] = x[j];
+                }
+            }
+            if (Cb) {
+#pragma unroll
+                for (int j = 0; j < 32; j++) Cb[(size_t)row * ldcb + col + j] = __float2bfloat16_rn(x[j]);
+            }
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(tmem), "r"(NT) : "memory");
 }
 
 }  // namespace
@@ -770,6 +934,38 @@ int cmf_emu_gemm(int M, int N, int K, const void *A, int lda, int transA, const 
                  int ldc, void *Cb, int ldcb, const float *bias, int relu, int accumulate, int ksplit, void *stream) {
     if (M % TM || N % TN || K % TK || M <= 0 || N <= 0 || K <= 0)
         return emu_err(CMF_E_ARG, "cmf_emu_gemm: M,N must be multiples of 64 and K of 32");
+    if ((lda % 8) || (ldb % 8) || ((uintptr_t)A & 15) || ((uintptr_t)B & 15))
+        return emu_err(CMF_E_ARG, "cmf_emu_gemm: lda, ldb must be multiples of 8 and A, B 16-byte aligned");
+    int dev = 0, major = 0;
+    EMU_TRY(cudaGetDevice(&dev));
+    EMU_TRY(cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev));
+    if (major != 10) return emu_err(CMF_E_NO_DEVICE, "cmf_emu_gemm: needs an sm_100 device");
+    if (ksplit < 1) ksplit = 1;
+    const int kps = ((K / ksplit + kGK - 1) / kGK) * kGK;   // whole chunks per split
+    const int splits = (K + kps - 1) / kps;
+    if (splits > 1 && !accumulate) return emu_err(CMF_E_ARG, "cmf_emu_gemm: split-K needs accumulate=1");
+    cudaStream_t st = (cudaStream_t)stream;
+    if (N % 128 == 0) {
+        EMU_TRY(cudaFuncSetAttribute(k_gemm_tc<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, kGSmem));
+        dim3 grid((M + 127) / 128, N / 128, splits);
+        k_gemm_tc<128><<<grid, kGThreads, kGSmem, st>>>(M, N, K, (const __nv_bfloat16 *)A, lda, transA, (const __nv_bfloat16 *)B,
+                                                       ldb, transB, C, ldc, (__nv_bfloat16 *)Cb, ldcb, bias, relu, accumulate,
+                                                       kps, g_tc_wait_limit);
+    } else {
+        EMU_TRY(cudaFuncSetAttribute(k_gemm_tc<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, kGSmem));
+        dim3 grid((M + 127) / 128, N / 64, splits);
+        k_gemm_tc<64><<<grid, kGThreads, kGSmem, st>>>(M, N, K, (const __nv_bfloat16 *)A, lda, transA, (const __nv_bfloat16 *)B,
+                                                      ldb, transB, C, ldc, (__nv_bfloat16 *)Cb, ldcb, bias, relu, accumulate,
+                                                      kps, g_tc_wait_limit);
+    }
+    EMU_TRY(cudaGetLastError());
+    return CMF_OK;
+}
+
+int cmf_emu_gemm_mma(int M, int N, int K, const void *A, int lda, int transA, const void *B, int ldb, int transB, float *C,
+                     int ldc, void *Cb, int ldcb, const float *bias, int relu, int accumulate, int ksplit, void *stream) {
+    if (M % TM || N % TN || K % TK || M <= 0 || N <= 0 || K <= 0)
+        return emu_err(CMF_E_ARG, "cmf_emu_gemm_mma: M,N must be multiples of 64 and K of 32");
     if (ksplit < 1) ksplit = 1;
     int kps = ((K / ksplit + TK - 1) / TK) * TK;
     const int splits = (K + kps - 1) / kps;
@@ -866,7 +1062,7 @@ int cmf_emu_mlp_tc(const void *X, int ldx, int rows, const void *pack, const flo
     const int ntiles = (rows + kTcRows - 1) / kTcRows;
     const int grid = ntiles < 2 * sms ? ntiles : 2 * sms;
     k_mlp_tc<<<grid, kTcThreads, kTcSmem, (cudaStream_t)stream>>>((const __nv_bfloat16 *)X, ldx, rows, (const uint4 *)pack,
-                                                                  b0, b1, b2, b3, y);
+                                                                  b0, b1, b2, b3, y, g_tc_wait_limit);
     EMU_TRY(cudaGetLastError());
     return CMF_OK;
 }
@@ -874,7 +1070,16 @@ int cmf_emu_mlp_tc(const void *X, int ldx, int rows, const void *pack, const flo
 int cmf_emu_mlp_tc_status(void) {
     int v = 0;
     if (cudaMemcpyFromSymbol(&v, g_mlp_tc_status, sizeof v) != cudaSuccess) return emu_err(CMF_E_CUDA, "cmf_emu_mlp_tc_status: read failed");
-    return v ? CMF_E_CUDA : CMF_OK;
+    if (!v) return CMF_OK;
+    const int zero = 0;                                       // clear on read: the next check starts clean
+    if (cudaMemcpyToSymbol(g_mlp_tc_status, &zero, sizeof zero) != cudaSuccess)
+        return emu_err(CMF_E_CUDA, "cmf_emu_mlp_tc_status: reset failed");
+    return emu_err(CMF_E_CUDA, "cmf_emu_mlp_tc: an MMA completion wait ran out its bound (the kernel returned early)");
+}
+
+int cmf_emu_mlp_tc_set_wait_limit(int32_t limit) {
+    g_tc_wait_limit = limit < 0 ? kTcWaitLimit : limit;
+    return CMF_OK;
 }
 
 // Features of every member: X rows [M][rows_per_member][ldx] bf16 (columns 0..31 written);

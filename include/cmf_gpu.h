@@ -345,11 +345,17 @@ int cmf_gpu_ctx_emu_views(cmf_gpu_ctx *ctx, int32_t member, cmf_emu_net *net, cm
 /* Device-to-device copy of one member's prognostic state and last-step averages between two
  * contexts of the same network (hand-over between the emulator and the judging plain solver). */
 int cmf_gpu_ctx_copy_member(cmf_gpu_ctx *dst, int32_t dst_member, cmf_gpu_ctx *src, int32_t src_member);
-/* BF16 tensor-core GEMM, fp32 accumulate: C[M,N] (+)= op(A)[M,K] op(B)[K,N]; epilogue bias+ReLU,
- * fp32 and/or bf16 output, or atomic accumulation for split-K (ksplit > 1). M,N % 64, K % 32. */
+/* BF16 GEMM on the tcgen05 tensor cores (accumulator in tensor memory), fp32 accumulate:
+ * C[M,N] (+)= op(A)[M,K] op(B)[K,N]; epilogue bias+ReLU, fp32 and/or bf16 output, or atomic
+ * accumulation for split-K (ksplit > 1).  M,N % 64, K % 32, lda/ldb % 8, A and B 16-byte aligned.
+ * A launch that gives up a bounded MMA wait reports through cmf_emu_mlp_tc_status. */
 int cmf_emu_gemm(int M, int N, int K, const void *A, int lda, int transA, const void *B, int ldb, int transB,
                  float *C, int ldc, void *Cb, int ldcb, const float *bias, int relu, int accumulate, int ksplit,
                  void *stream);
+/* The same contract on the legacy mma.sync tiles (kept as the cross-check of cmf_emu_gemm). */
+int cmf_emu_gemm_mma(int M, int N, int K, const void *A, int lda, int transA, const void *B, int ldb, int transB,
+                     float *C, int ldc, void *Cb, int ldcb, const float *bias, int relu, int accumulate, int ksplit,
+                     void *stream);
 int cmf_emu_relu_bwd(int n, const float *dA, const void *act, void *dZ, float *dZf, void *stream);
 int cmf_emu_colsum(int rows, int cols, const float *X, float *out, void *stream);
 /* MSE gradient on column 0 of Y (rows padded, `valid` real rows): dY fp32 + bf16, loss partials
@@ -384,13 +390,19 @@ int cmf_emu_mlp_fused(const void *X, int ldx, int rows, const void *pack, const 
  * column 0 is the output); cmf_emu_mlp_tc maps X rows (bf16, ldx >= 32 and a multiple of 8, X
  * 16-byte aligned, columns 32.. ignored) to y[rows].  Rounding points as the layer-by-layer
  * chain; fp32 accumulation order is the tensor core's.  cmf_emu_mlp_tc_status() reports (after
- * the stream is synchronised) whether any launch gave up waiting for an MMA (CMF_E_CUDA). */
+ * the stream is synchronised) whether any launch since the last report gave up waiting for an MMA
+ * (CMF_E_CUDA), and clears the report. */
 size_t cmf_emu_mlp_tc_pack_bytes(void);
 int cmf_emu_mlp_tc_pack(const void *W0, const void *W1, const void *W2, const void *W3, int ldw3, void *pack,
                         void *stream);
 int cmf_emu_mlp_tc(const void *X, int ldx, int rows, const void *pack, const float *b0, const float *b1,
                    const float *b2, const float *b3, float *y, void *stream);
 int cmf_emu_mlp_tc_status(void);
+/* Diagnostic: bound (polls) of the MMA completion waits of later cmf_emu_mlp_tc launches; a
+ * negative value restores the default.  With 0 every launch gives up at its first wait, reports
+ * through cmf_emu_mlp_tc_status (which clears the report when it returns it) and still waits for
+ * its MMA in flight, with the default bound, before releasing tensor memory. */
+int cmf_emu_mlp_tc_set_wait_limit(int32_t limit);
 const char *cmf_emu_last_error(void);
 
 /* ======================================================================================== */

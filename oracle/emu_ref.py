@@ -17,9 +17,10 @@ def to_bf16(x: np.ndarray) -> np.ndarray:
     return r.astype(np.uint32).view(np.float32)
 
 
-def forward(X, W, b, bf16=True):
-    q = to_bf16 if bf16 else (lambda v: v)
-    dt = np.float32 if bf16 else np.float64
+def forward(X, W, b, bf16=True, acc64=False):
+    """acc64 (with bf16): the bf16 rounding points of the GPU chain, products accumulated in float64."""
+    q = (lambda v: to_bf16(v).astype(np.float64)) if (bf16 and acc64) else (to_bf16 if bf16 else (lambda v: v))
+    dt = np.float32 if (bf16 and not acc64) else np.float64
     acts = [q(X.astype(dt))]
     a = acts[0]
     for li in range(3):
@@ -30,10 +31,10 @@ def forward(X, W, b, bf16=True):
     return Y, acts
 
 
-def loss_and_grads(X, t, W, b, bf16=True):
-    q = to_bf16 if bf16 else (lambda v: v)
-    dt = np.float32 if bf16 else np.float64
-    Y, acts = forward(X, W, b, bf16)
+def loss_and_grads(X, t, W, b, bf16=True, acc64=False):
+    q = (lambda v: to_bf16(v).astype(np.float64)) if (bf16 and acc64) else (to_bf16 if bf16 else (lambda v: v))
+    dt = np.float32 if (bf16 and not acc64) else np.float64
+    Y, acts = forward(X, W, b, bf16, acc64)
     R = X.shape[0]
     e = Y[:, 0] - t.astype(dt)
     loss = float(np.sum(e.astype(np.float64) ** 2) / R)

@@ -52,27 +52,50 @@ def test_nse_known_answers():
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("ta,tb,ks", [(0, 0, 1), (1, 0, 1), (0, 1, 1), (1, 0, 4)])
-def test_gemm_kernel_matches_numpy(ta, tb, ks):
+@pytest.mark.parametrize("ta,tb,ks,M,N,K", [(0, 0, 1, 128, 64, 256), (1, 0, 1, 128, 64, 256), (0, 1, 1, 128, 64, 256),
+                                          (1, 0, 4, 128, 64, 256), (0, 0, 1, 384, 128, 96), (1, 0, 3, 64, 128, 1024),
+                                          (0, 1, 1, 192, 128, 128), (1, 1, 2, 64, 64, 160)])
+def test_gemm_kernel_matches_numpy(ta, tb, ks, M, N, K):
+    """The tcgen05 GEMM (products in tensor memory) against float64 numpy and against the legacy
+    mma.sync tiles on the same bf16 operands: every transpose combination, split-K accumulation,
+    tiles of 64 and 128 columns, 64-row problems (half a tcgen05 tile) and K chunks of 32."""
     import torch
 
     from cmf_b200.emulator import _emu_lib, echeck
     from emu_ref import to_bf16
 
     lib = _emu_lib()
-    rng = np.random.default_rng(ta * 2 + tb + ks)
-    M, N, K = 128, 64, 256
+    rng = np.random.default_rng(ta * 2 + tb + ks + M + N + K)
     A = to_bf16(rng.standard_normal((K, M) if ta else (M, K)))
     B = to_bf16(rng.standard_normal((N, K) if tb else (K, N)))
     dev = torch.device("cuda", 0)
     tA = torch.tensor(A, device=dev).to(torch.bfloat16)
     tB = torch.tensor(B, device=dev).to(torch.bfloat16)
-    C = torch.zeros(M, N, device=dev)
-    echeck(lib.cmf_emu_gemm(M, N, K, tA.data_ptr(), A.shape[1], ta, tB.data_ptr(), B.shape[1], tb, C.data_ptr(), N,
-                            None, 0, None, 0, 1 if ks > 1 else 0, ks, None), "gemm")
+    bias = torch.tensor(rng.standard_normal(N).astype(np.float32), device=dev)
+    acc = 1 if ks > 1 else 0
+    out = {}
+    for name, fn in (("tc", lib.cmf_emu_gemm), ("mma", lib.cmf_emu_gemm_mma)):
+        C = torch.zeros(M, N, device=dev)
+        echeck(fn(M, N, K, tA.data_ptr(), A.shape[1], ta, tB.data_ptr(), B.shape[1], tb, C.data_ptr(), N,
+                  None, 0, None, 0, acc, ks, None), name)
+        out[name] = C
+        if not acc:   # epilogue: bias + ReLU into fp32 and bf16
+            Cr = torch.zeros(M, N, device=dev)
+            Cb = torch.zeros(M, N, dtype=torch.bfloat16, device=dev)
+            echeck(fn(M, N, K, tA.data_ptr(), A.shape[1], ta, tB.data_ptr(), B.shape[1], tb, Cr.data_ptr(), N,
+                      Cb.data_ptr(), N, bias.data_ptr(), 1, 0, 1, None), name)
+            out[name + "_relu"] = (Cr, Cb)
     torch.cuda.synchronize()
+    assert lib.cmf_emu_mlp_tc_status() == 0
     ref = (A.T if ta else A).astype(np.float64) @ (B.T if tb else B).astype(np.float64)
-    assert np.allclose(C.cpu().numpy(), ref, rtol=1e-5, atol=1e-3)
+    for name in ("tc", "mma"):
+        assert np.allclose(out[name].cpu().numpy(), ref, rtol=1e-5, atol=1e-3), name
+    assert np.allclose(out["tc"].cpu().numpy(), out["mma"].cpu().numpy(), rtol=1e-5, atol=1e-4)
+    if not acc:
+        rr = np.maximum(ref + bias.cpu().numpy()[None, :].astype(np.float64), 0.0)
+        Cr, Cb = out["tc_relu"]
+        assert np.allclose(Cr.cpu().numpy(), rr, rtol=1e-5, atol=1e-3)
+        assert np.allclose(Cb.float().cpu().numpy(), to_bf16(Cr.cpu().numpy()))
 
 
 @pytest.mark.gpu
@@ -93,14 +116,19 @@ def test_training_kernels_gradients_match_cpu_reference():
     t = rng.standard_normal(R).astype(np.float32)
     loss = mlp.loss_and_grad(torch.tensor(X, device=dev).to(torch.bfloat16), torch.tensor(t, device=dev), R)
     torch.cuda.synchronize()
-    rloss, gW, gb = loss_and_grads(X, t, [w.astype(np.float32) for w in W], [v.astype(np.float32) for v in b], bf16=True)
-    assert abs(float(loss) - rloss) <= 1e-3 * abs(rloss)
+    # reference with the GPU chain's rounding points (bf16 inputs, weights, activations and dZ) and
+    # float64 accumulation: the remaining differences are the fp32 accumulation order of the tensor
+    # cores and the rare bf16 roundings such a difference flips
+    rloss, gW, gb = loss_and_grads(X, t, [w.astype(np.float32) for w in W], [v.astype(np.float32) for v in b], bf16=True,
+                                   acc64=True)
+    assert abs(float(loss) - rloss) <= 1e-4 * abs(rloss)
     for li in range(4):
         g = mlp.gW[li].cpu().numpy()
         err = np.linalg.norm(g - gW[li]) / max(np.linalg.norm(gW[li]), 1e-30)
-        assert err < 2e-2, (li, err)
         e2 = np.linalg.norm(mlp.gb[li].cpu().numpy() - gb[li]) / max(np.linalg.norm(gb[li]), 1e-30)
-        assert e2 < 2e-2, (li, e2)
+        print(f"layer {li}: relative gradient error W {err:.2e}, b {e2:.2e}")
+        assert err < 2e-3, (li, err)
+        assert e2 < 2e-3, (li, e2)
 
 
 @pytest.mark.gpu
@@ -163,6 +191,42 @@ def test_tcgen05_inference_matches_mma_sync_and_reference(R):
     assert np.median(np.abs(a - m)) <= 1e-3 * scale
     ref, _ = forward(X[:2048], [w.astype(np.float32) for w in W], [v.astype(np.float32) for v in b], bf16=True)
     assert np.allclose(a[:2048], ref[:, 0], rtol=2e-2, atol=2e-2 * float(np.abs(ref[:, 0]).max()))
+
+
+@pytest.mark.gpu
+def test_tcgen05_bounded_wait_reports_and_recovers():
+    """With the MMA completion bound set to 0 every tcgen05 launch gives up at its first wait: the
+    kernel still drains its MMA in flight and frees its tensor memory, returns, and the status
+    reports CMF_E_CUDA once (cleared on read).  With the default bound restored the next launch is
+    correct again."""
+    import torch
+
+    from cmf_b200.emulator import MLP, _emu_lib
+
+    lib = _emu_lib()
+    dev = torch.device("cuda", 0)
+    rng = np.random.default_rng(5)
+    mlp = MLP(dev, seed=3)
+    W, b = _rand_params(rng, 0.2)
+    mlp.load({"W": W, "b": b})
+    X = torch.tensor(rng.standard_normal((4096, 64)) * 2.0, device=dev).to(torch.bfloat16)
+    X[:, 30:] = 0
+    ref = mlp.infer(X)
+    torch.cuda.synchronize()
+    assert lib.cmf_emu_mlp_tc_status() == 0
+    try:
+        assert lib.cmf_emu_mlp_tc_set_wait_limit(0) == 0
+        mlp.infer_tc(X)
+        torch.cuda.synchronize()
+        assert lib.cmf_emu_mlp_tc_status() == 1          # CMF_E_CUDA: a wait ran out
+        assert lib.cmf_emu_mlp_tc_status() == 0          # cleared on read
+    finally:
+        lib.cmf_emu_mlp_tc_set_wait_limit(-1)
+    y = mlp.infer_tc(X)
+    torch.cuda.synchronize()
+    assert lib.cmf_emu_mlp_tc_status() == 0
+    scale = float(ref.abs().max())
+    assert float((y - ref).abs().max()) <= 2e-2 * scale
 
 
 def _raw_i32(ptr, n, dev):
