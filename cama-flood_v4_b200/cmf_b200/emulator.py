@@ -550,7 +550,9 @@ class SurrogateEnsemble:
     """E4: ensemble advanced by the emulator with plain-solver judging and hand-back."""
 
     def __init__(self, host, mlp: MLP, members: int, judge_slots: int, gauges: np.ndarray, tol_rel: float = 0.05,
-                 resync_hours: int = 24):
+                 resync_hours: int = 24, schedule: dict | None = None):
+        """schedule: launch schedule for the judging plain solver (PhysicsGPU.set_schedule keys), e.g. the
+        one the plain ensemble tuned; without it the judge runs phase kernels at 128 threads."""
         import torch
 
         from .model import PhysicsGPU
@@ -559,8 +561,11 @@ class SurrogateEnsemble:
         self.host = host
         self.mlp = mlp
         self.M = members
-        self.emu = PhysicsGPU(host, nmembers=members)
-        self.judge = PhysicsGPU(host, nmembers=judge_slots)
+        self.emu = PhysicsGPU(host, nmembers=members, block_size=128)     # stage scheme only: no tuning
+        self.judge = PhysicsGPU(host, nmembers=judge_slots, block_size=128)
+        if schedule:
+            self.judge.set_schedule(**{k: schedule[k] for k in ("mode", "flux_block", "rate_block", "store_block",
+                                                                 "profile")})
         self.fe = Features(self.emu, qref_from_host(host))
         self.jfe = Features(self.judge, qref_from_host(host))
         self.lib = _emu_lib()

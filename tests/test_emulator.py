@@ -127,8 +127,8 @@ def test_training_kernels_gradients_match_cpu_reference():
         err = np.linalg.norm(g - gW[li]) / max(np.linalg.norm(gW[li]), 1e-30)
         e2 = np.linalg.norm(mlp.gb[li].cpu().numpy() - gb[li]) / max(np.linalg.norm(gb[li]), 1e-30)
         print(f"layer {li}: relative gradient error W {err:.2e}, b {e2:.2e}")
-        assert err < 2e-3, (li, err)
-        assert e2 < 2e-3, (li, e2)
+        assert err < 1e-4, (li, err)
+        assert e2 < 1e-4, (li, e2)
 
 
 @pytest.mark.gpu
