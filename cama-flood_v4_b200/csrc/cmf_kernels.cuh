@@ -31,14 +31,15 @@ namespace cmf {
 
 // Occupancy of the latency-bound cell kernels: at most kCellThreads threads per block and the
 // minimum resident blocks per SM (caps registers at 65536 / (threads x blocks)).  k_flux and
-// k_store come in two profiles, chosen per context by its cell-members (the engine's
-// `small_cells`): with many cell-members in flight more resident warps beat the spills they cost
-// (16 config-1 members: 22.2 ms per coupling step vs 24.4 ms with the small profile), while a
-// grid of about a wave or less runs best with fewer spills (one config-1 member: 2.04 vs 2.10 ms).
-// Both profiles execute the same arithmetic; only the register allocation differs.
+// k_store come in two profiles, one of the dimensions the engine's autotuner searches: with many
+// cell-members in flight more resident warps beat the spills they cost (`wide`: 40/48 registers;
+// 16 config-1 members 22.2 vs 24.4 ms per coupling step), while a grid of about two waves runs
+// best with few spills (`small`: 64/64 registers, k_flux spill-free; one config-1 member 1.91 ms
+// vs 1.95 ms with k_flux at 48).  Both profiles execute the same arithmetic; only the register
+// allocation differs.
 constexpr int kFluxMinBlocksWide = 6, kStoreMinBlocksWide = 5;
-constexpr int kFluxMinBlocksSmall = 5, kStoreMinBlocksSmall = 4;
-constexpr size_t kSmallCellMembers = size_t(1) << 19;   // cell-members up to which `small` applies
+constexpr int kFluxMinBlocksSmall = 4, kStoreMinBlocksSmall = 4;
+constexpr size_t kSmallCellMembers = size_t(1) << 19;   // untuned start: `small` up to this many cell-members
 #ifndef CMF_STAGE_MINB
 #define CMF_STAGE_MINB 6
 #endif
@@ -148,7 +149,7 @@ __device__ __forceinline__ double dmin(double a, double b) { return (a < b) ? a 
 // bits.  Static maps are indexed by the cell i, member state by g = m*N + i; reads of another
 // cell (downstream, upstream, path ends) always go to global memory through Net/State.
 #define CMF_OWN_STATIC(name) \
-    __device__ __forceinline__ double name(int i) const { return n.name[i]; }
+    __device__ __forceinline__ double name(int i) const { return __ldg(&n.name[i]); }
 #define CMF_OWN_STATE(name) \
     __device__ __forceinline__ double name(size_t g) const { return s.name[g]; }
 struct OwnG {
@@ -157,10 +158,10 @@ struct OwnG {
     CMF_OWN_STATIC(rivelv) CMF_OWN_STATIC(elevtn) CMF_OWN_STATIC(nxtdst) CMF_OWN_STATIC(rivwth)
     CMF_OWN_STATIC(rivhgt) CMF_OWN_STATIC(rivlen) CMF_OWN_STATIC(rivman) CMF_OWN_STATIC(grarea)
     CMF_OWN_STATIC(rivstomax) CMF_OWN_STATIC(inv_nxtdst) CMF_OWN_STATIC(inv_rivwth) CMF_OWN_STATIC(inv_rivlen)
-    __device__ __forceinline__ int next(int i) const { return n.next[i]; }
-    __device__ __forceinline__ int up_lo(int i) const { return n.up_ptr[i]; }
-    __device__ __forceinline__ int up_hi(int i) const { return n.up_ptr[i + 1]; }
-    __device__ __forceinline__ int i1dam(int i) const { return n.i1dam[i]; }
+    __device__ __forceinline__ int next(int i) const { return __ldg(&n.next[i]); }
+    __device__ __forceinline__ int up_lo(int i) const { return __ldg(&n.up_ptr[i]); }
+    __device__ __forceinline__ int up_hi(int i) const { return __ldg(&n.up_ptr[i + 1]); }
+    __device__ __forceinline__ int i1dam(int i) const { return __ldg(&n.i1dam[i]); }
     CMF_OWN_STATE(rivsto) CMF_OWN_STATE(fldsto) CMF_OWN_STATE(levsto) CMF_OWN_STATE(rivdph)
     CMF_OWN_STATE(rivdph_pre) CMF_OWN_STATE(rivout_pre) CMF_OWN_STATE(fldout_pre) CMF_OWN_STATE(fldsto_pre)
     CMF_OWN_STATE(flddph) CMF_OWN_STATE(fldfrc) CMF_OWN_STATE(storge) CMF_OWN_STATE(runoff)
@@ -254,11 +255,11 @@ __device__ __forceinline__ StageOut stage_def(const Net &n, const Own &w, int i,
         int I = 0;   // 0-based layer
         double sfil = rsm, wfil = wth, dfil = 0.0;
         while (I < L) {
-            const double smax = n.fldstomax[(size_t)I * N + i];
+            const double smax = __ldg(&n.fldstomax[(size_t)I * N + i]);
             if (!(pstoall > smax)) break;
             sfil = smax;
             wfil = wfil + inc;
-            dfil = dfil + n.fldgrd[(size_t)I * N + i] * inc;
+            dfil = dfil + __ldg(&n.fldgrd[(size_t)I * N + i]) * inc;
             I++;
         }
         double wadd;
@@ -266,7 +267,7 @@ __device__ __forceinline__ StageOut stage_def(const Net &n, const Own &w, int i,
             wadd = 0.0;
             o.flddph = dfil + ((pstoall - sfil) / wfil) / len;
         } else {
-            const double gr = n.fldgrd[(size_t)I * N + i];
+            const double gr = __ldg(&n.fldgrd[(size_t)I * N + i]);
             const double sadd = pstoall - sfil;
             wadd = -wfil + sqrt(wfil * wfil + ((2.0 * sadd) / len) / gr);
             o.flddph = dfil + gr * wadd;
@@ -303,20 +304,20 @@ __device__ __forceinline__ StageOut stage_levee(const Net &n, const Own &w, int 
     const double len = w.rivlen(i), wth = w.rivwth(i);
     const double inc = (w.grarea(i) / len) * n.dfrcinc;
     const double grarea = w.grarea(i);
-    const int lv = n.lev_id[i];
-    const double lbas = lv >= 0 ? n.levbassto[lv] : 1.E18;
+    const int lv = __ldg(&n.lev_id[i]);
+    const double lbas = lv >= 0 ? __ldg(&n.levbassto[lv]) : 1.E18;
     if (pstoall > rsm) {
         if (pstoall < lbas) {                                                       // case 1
             int I = 0;
             double sfil = rsm, wfil = wth, dfil = 0.0, wadd;
             while (I < L) {
-                const double smax = n.fldstomax[(size_t)I * N + i];
+                const double smax = __ldg(&n.fldstomax[(size_t)I * N + i]);
                 if (!(pstoall > smax)) break;
-                sfil = smax; wfil = wfil + inc; dfil = dfil + n.fldgrd[(size_t)I * N + i] * inc;
+                sfil = smax; wfil = wfil + inc; dfil = dfil + __ldg(&n.fldgrd[(size_t)I * N + i]) * inc;
                 I++;
             }
             if (I < L) {
-                const double gr = n.fldgrd[(size_t)I * N + i];
+                const double gr = __ldg(&n.fldgrd[(size_t)I * N + i]);
                 wadd = -wfil + sqrt(wfil * wfil + ((2.0 * (pstoall - sfil)) / len) / gr);
                 o.flddph = dfil + gr * wadd;
             } else {
@@ -334,8 +335,8 @@ __device__ __forceinline__ StageOut stage_levee(const Net &n, const Own &w, int 
             o.levsto = 0.0;
             o.levdph = 0.0;
         } else {
-            const double lhgt = n.levhgt[lv], lfrc = n.levfrc[lv], bhgt = n.bashgt[lv], ldst = n.levdst[lv];
-            const double ltop = n.levtopsto[lv], lfil = n.levfilsto[lv];
+            const double lhgt = __ldg(&n.levhgt[lv]), lfrc = __ldg(&n.levfrc[lv]), bhgt = __ldg(&n.bashgt[lv]), ldst = __ldg(&n.levdst[lv]);
+            const double ltop = __ldg(&n.levtopsto[lv]), lfil = __ldg(&n.levfilsto[lv]);
             if (pstoall < ltop) {                                                   // case 2
                 const double sadd = pstoall - lbas;
                 const double wadd = ldst + wth;
@@ -357,15 +358,15 @@ __device__ __forceinline__ StageOut stage_levee(const Net &n, const Own &w, int 
                 double sfil = ltop, wfil = 0.0, dfil = 0.0, sadd;
                 int I = ilev;                                   // 1-based
                 while (I <= L) {
-                    sadd = ((ldst + wth) * (lhgt - n.fldhgt[(size_t)(I - 1) * N + i])) * len;
-                    if (pstoall < n.fldstomax[(size_t)(I - 1) * N + i] + sadd) break;
-                    sfil = n.fldstomax[(size_t)(I - 1) * N + i] + sadd;
+                    sadd = ((ldst + wth) * (lhgt - __ldg(&n.fldhgt[(size_t)(I - 1) * N + i]))) * len;
+                    if (pstoall < __ldg(&n.fldstomax[(size_t)(I - 1) * N + i]) + sadd) break;
+                    sfil = __ldg(&n.fldstomax[(size_t)(I - 1) * N + i]) + sadd;
                     wfil = inc * (double)I - ldst;
-                    dfil = n.fldhgt[(size_t)(I - 1) * N + i] - bhgt;
+                    dfil = __ldg(&n.fldhgt[(size_t)(I - 1) * N + i]) - bhgt;
                     I++;
                 }
                 if (I <= L) {
-                    const double gr = n.fldgrd[(size_t)(I - 1) * N + i];
+                    const double gr = __ldg(&n.fldgrd[(size_t)(I - 1) * N + i]);
                     const double wadd = -wfil + sqrt(wfil * wfil + ((2.0 * (pstoall - sfil)) / len) / gr);
                     const double dadd = wadd * gr;
                     o.levdph = (bhgt + dfil) + dadd;
@@ -384,13 +385,13 @@ __device__ __forceinline__ StageOut stage_levee(const Net &n, const Own &w, int 
                 int I = 0;
                 double sfil = rsm, wfil = wth, dfil = 0.0, wadd;
                 while (I < L) {
-                    const double smax = n.fldstomax[(size_t)I * N + i];
+                    const double smax = __ldg(&n.fldstomax[(size_t)I * N + i]);
                     if (!(pstoall > smax)) break;
-                    sfil = smax; wfil = wfil + inc; dfil = dfil + n.fldgrd[(size_t)I * N + i] * inc;
+                    sfil = smax; wfil = wfil + inc; dfil = dfil + __ldg(&n.fldgrd[(size_t)I * N + i]) * inc;
                     I++;
                 }
                 if (I < L) {
-                    const double gr = n.fldgrd[(size_t)I * N + i];
+                    const double gr = __ldg(&n.fldgrd[(size_t)I * N + i]);
                     wadd = -wfil + sqrt(wfil * wfil + ((2.0 * (pstoall - sfil)) / len) / gr);
                     o.flddph = dfil + gr * wadd;
                 } else {
@@ -426,7 +427,7 @@ __device__ __forceinline__ void store_stage(const Net &n, const State &s, size_t
     s.fldfrc[gi] = o.fldfrc;
     if (diag_out) {
         s.fldare[gi] = o.fldare;
-        s.sfcelv[gi] = n.rivelv[i] + o.rivdph;
+        s.sfcelv[gi] = __ldg(&n.rivelv[i]) + o.rivdph;
     }
     if (n.llevee) {
         s.levsto[gi] = o.levsto;
@@ -471,7 +472,7 @@ __global__ void __launch_bounds__(kCellThreads, CMF_STAGE_MINB) k_stage(Net n, S
         const StageOut o = n.llevee ? stage_levee(n, w, i, s.rivsto[gi], s.fldsto[gi], s.levsto[gi])
                                     : stage_def(n, w, i, s.rivsto[gi], s.fldsto[gi]);
         store_stage(n, s, gi, i, o);
-        if (n.ladpstp && n.i2mask[i] == 0) key = cfl_key(n.pcadp, (i < n.R) ? n.nxtdst[i] : n.pdstmth, n.pgrv, o.rivdph);
+        if (n.ladpstp && __ldg(&n.i2mask[i]) == 0) key = cfl_key(n.pcadp, (i < n.R) ? __ldg(&n.nxtdst[i]) : n.pdstmth, n.pgrv, o.rivdph);
     }
     if (n.ladpstp) {
         for (int o = 16; o > 0; o >>= 1) key = dmin(key, __shfl_down_sync(0xffffffffu, key, o));
@@ -565,6 +566,55 @@ __device__ __forceinline__ double nadd_before(int k, double dt) {
 //    so the limiter rates skip the division in the common case; a NaN a still takes the division.
 __device__ __forceinline__ double rate_min1(double a, double b) { return (a >= b) ? 1.0 : dmin(a / b, 1.0); }
 
+// CMF_DIAG_AVEMAX_ADPSTP (src/cmf_calc_diag_mod.F90:104-161) of the sub-step before this one,
+// carried into this sub-step's phase A, which reads that sub-step's results anyway: its D2RIVOUT and
+// D2FLDOUT are this sub-step's D2*OUT_PRE, its D2RIVDPH and D2STORGE the state it left, its D2DAMINF
+// the inflow phase A is about to replace.  Every addition and maximum is the reference's, in its
+// order, so each accumulator holds the bits phase C of that sub-step would have stored.  Phase C
+// still forms the last sub-step's terms (and the division by NADD), and D2PTHOUT_aAVG, whose
+// per-cell path sum phase A does not see.  The accumulators are read after phase A's own stores:
+// read at its top they would hold 16 registers across the outflow arithmetic and spill (measured
+// slower).
+struct DiagPrev {
+    double rivout, fldout, outflw, daminf, dinf, mout, mdph, msto;
+};
+__device__ __forceinline__ DiagPrev diag_carry_load(const Net &n, const State &s, size_t gi, bool first) {
+    DiagPrev p;
+    p.rivout = first ? 0.0 : s.a_rivout[gi];
+    p.fldout = first ? 0.0 : s.a_fldout[gi];
+    p.outflw = first ? 0.0 : s.a_outflw[gi];
+    p.mout = first ? 0.0 : s.m_outflw[gi];
+    p.mdph = first ? 0.0 : s.m_rivdph[gi];
+    p.msto = first ? 0.0 : s.m_storge[gi];
+    p.dinf = n.ldamout ? s.daminf[gi] : 0.0;
+    p.daminf = (first || !n.ldamout) ? 0.0 : s.a_daminf[gi];
+    return p;
+}
+__device__ __forceinline__ bool same_bits(double a, double b) {
+    return __double_as_longlong(a) == __double_as_longlong(b);
+}
+__device__ __forceinline__ void diag_carry_store(const Net &n, const State &s, size_t gi, double DT, bool first,
+                                                 const DiagPrev &p, double rivout, double fldout, double rivdph,
+                                                 double storge) {
+    // a store is skipped when the sub-step leaves the accumulator's bits unchanged (a zero discharge
+    // added to a running sum, a maximum that did not move): the array holds the same bits either way
+    auto acc = [&](double prev, double *a, double v) {
+        const double x = first ? v * DT : prev + v * DT;
+        if (first || !same_bits(x, prev)) a[gi] = x;
+    };
+    const double outflw = rivout + fldout;
+    acc(p.rivout, s.a_rivout, rivout);
+    acc(p.fldout, s.a_fldout, fldout);
+    acc(p.outflw, s.a_outflw, outflw);
+    if (n.ldamout) acc(p.daminf, s.a_daminf, p.dinf);
+    const double mo = dmax(p.mout, fabs(outflw));
+    const double md = dmax(p.mdph, rivdph);
+    const double ms = dmax(p.msto, storge);
+    if (first || !same_bits(mo, p.mout)) s.m_outflw[gi] = mo;
+    if (first || !same_bits(md, p.mdph)) s.m_rivdph[gi] = md;
+    if (first || !same_bits(ms, p.msto)) s.m_storge[gi] = ms;
+}
+
 template <class Own>
 __device__ __forceinline__ void cell_outflow(const Net &n, const State &s, const Own &w, int m, int i, double DT,
                                              const MemberCtl &c, int k, bool split) {
@@ -579,11 +629,13 @@ __device__ __forceinline__ void cell_outflow(const Net &n, const State &s, const
     const double man = w.rivman(i);
     const double rivout_pre = w.rivout_pre(gi);
     const double rivout_old = split ? s.rivout_cur[gi] : rivout_pre;
+    const double fldout_pre = w.fldout_pre(gi), storge = w.storge(gi);
+    const bool carry = n.ldiag && k > 0;   // diagnostics of sub-step k-1 (diag_carry_store)
     double rout, fout = 0.0, rvel;
     if (i < n.R) {
         const int j = w.next(i);
         const size_t gj = base + j;
-        const double rj = n.rivelv[j];
+        const double rj = __ldg(&n.rivelv[j]);
         const double dwn = rj + s.rivdph[gj];
         const double dwn_pre = rj + s.rivdph_pre[gj];
         const double inv_dst = w.inv_nxtdst(i);
@@ -619,7 +671,7 @@ __device__ __forceinline__ void cell_outflow(const Net &n, const State &s, const
                 double dare_pr = w.fldsto_pre(gi) * inv_len;
                 dare_pr = dmax(dare_pr - flddph_pre * wth, 1.E-6);
                 const double dare_im = dmax(sqrt(dare * dare_pr), 1.E-6);
-                const double dout_pr = w.fldout_pre(gi);
+                const double dout_pr = fldout_pre;
                 const double dout = (dout_pr + (gdt * dare_im) * dslp)
                     * (1.0 / (1.0 + (((gdt * (n.pmanfld * n.pmanfld)) * fabs(dout_pr)) * pow_depth<4>(dflw_im)) * (1.0 / dare_im)));
                 fout = (dflw_im > 1.E-5) ? dout : 0.0;
@@ -628,12 +680,12 @@ __device__ __forceinline__ void cell_outflow(const Net &n, const State &s, const
         }
         // storage-change limiter (v423), :176-182
         const double dlim = dmax((-rout - fout) * DT, CMF_F(1.E-10));
-        const double rate = rate_min1(0.05 * w.storge(gi), dlim);
+        const double rate = rate_min1(0.05 * storge, dlim);
         rout = rout * rate;
         fout = fout * rate;
     } else {
         const double inv_dst = 1.0 / n.pdstmth;
-        const double dwn = n.dwnelv[i];
+        const double dwn = __ldg(&n.dwnelv[i]);
         {
             const double dslp = (sfc - dwn) * inv_dst;
             const double dare = dmax(wth * rivdph, 1.E-10);
@@ -659,7 +711,7 @@ __device__ __forceinline__ void cell_outflow(const Net &n, const State &s, const
                 const double flddph_pre = dmax(rivdph_pre - w.rivhgt(i), 0.0);
                 const double dare_pr = dmax(w.fldsto_pre(gi) * inv_len - flddph_pre * wth, 1.E-6);
                 const double dare_im = dmax(sqrt(dare * dare_pr), 1.E-6);
-                const double dout_pr = w.fldout_pre(gi);
+                const double dout_pr = fldout_pre;
                 const double dout = (dout_pr + (gdt * dare_im) * dslp)
                     * (1.0 / (1.0 + (((gdt * (n.pmanfld * n.pmanfld)) * fabs(dout_pr)) * pow_depth<4>(dflw_im)) * (1.0 / dare_im)));
                 fout = (dflw_im > CMF_F(1.E-5)) ? dout : 0.0;
@@ -674,12 +726,12 @@ __device__ __forceinline__ void cell_outflow(const Net &n, const State &s, const
             rout = 0.0;
             fout = 0.0;
             double dinf = s.runoff[gi];
-            const int d = n.dam_id[i];
+            const int d = __ldg(&n.dam_id[i]);
             if (d >= 0) {
                 // UPDATE_INFLOW 1b: inflow from the dam's upstream cells, in ascending sequence
-                for (int k = n.up_ptr[i]; k < n.up_ptr[i + 1]; k++) {
-                    const int j = n.up_idx[k];
-                    const int cj = n.i1dam[j];
+                for (int k = __ldg(&n.up_ptr[i]); k < __ldg(&n.up_ptr[i + 1]); k++) {
+                    const int j = __ldg(&n.up_idx[k]);
+                    const int cj = __ldg(&n.i1dam[j]);
                     if (cj == 10 || cj == 11) {
                         const double fpre = n.lfldout ? s.fldout_pre[base + j] : 0.0;
                         dinf = (dinf + s.rivout_pre[base + j]) + fpre;
@@ -689,9 +741,9 @@ __device__ __forceinline__ void cell_outflow(const Net &n, const State &s, const
             s.daminf[gi] = dinf;
             if (code == 10 && i < n.R) {
                 // UPDATE_INFLOW 1c: kinematic outflow upstream of a dam
-                const int j = n.next[i];
+                const int j = __ldg(&n.next[i]);
                 const double p23 = CMF_F(2. / 3.);
-                double dslope = (n.elevtn[i] - n.elevtn[j]) * (1.0 / n.nxtdst[i]);
+                double dslope = (__ldg(&n.elevtn[i]) - __ldg(&n.elevtn[j])) * (1.0 / __ldg(&n.nxtdst[i]));
                 dslope = dmax(dslope, n.pminslp);
                 const double dph = rivdph;
                 const double dvel = ((1.0 / man) * sqrt(dslope)) * pow(dph, p23);
@@ -701,27 +753,27 @@ __device__ __forceinline__ void cell_outflow(const Net &n, const State &s, const
                 const double slope_f = dmin(0.005, dslope);
                 const double fdph = s.flddph[gi];
                 const double dvel_f = ((1.0 / n.pmanfld) * sqrt(slope_f)) * pow(fdph, p23);
-                double dare_f = s.fldsto[gi] * (1.0 / n.rivlen[i]);
+                double dare_f = s.fldsto[gi] * (1.0 / __ldg(&n.rivlen[i]));
                 dare_f = dmax(dare_f - fdph * wth, 0.0);
                 fout = dmin(dare_f * dvel_f, s.fldsto[gi] / DT);
             }
-            if (d >= 0 && n.dam_stat[d] > 0) {
+            if (d >= 0 && __ldg(&n.dam_stat[d]) > 0) {
                 const double vol = s.damsto[gi];
-                const double qn = n.qn[d], qf = n.qf[d], qa = n.qa[d], con = n.convol[d], eme = n.emevol[d];
+                const double qn = __ldg(&n.qn[d]), qf = __ldg(&n.qf[d]), qa = __ldg(&n.qa[d]), con = __ldg(&n.convol[d]), eme = __ldg(&n.emevol[d]);
                 double q = 0.0;
                 if (n.ldamh22) {
-                    const double nor = n.norvol[d];
+                    const double nor = __ldg(&n.norvol[d]);
                     if (vol <= nor) q = qn * (vol / con);
                     else if (nor < vol && vol <= con) {
                         if (qf <= dinf) q = qn * CMF_F(0.5) + ((vol - nor) / (con - nor)) * (qf - qn);
                         else { const double r = (vol - nor) / (eme - nor); q = qn * CMF_F(0.5) + (r * r) * (qf - qn); }
                     } else if (con < vol && vol < eme) {
                         if (qf <= dinf)
-                            q = qf + ((dmax(CMF_F(1.) - n.r_volupa[d] / CMF_F(0.2), 0.0) * (vol - con)) / (eme - con)) * (dinf - qf);
+                            q = qf + ((dmax(CMF_F(1.) - __ldg(&n.r_volupa[d]) / CMF_F(0.2), 0.0) * (vol - con)) / (eme - con)) * (dinf - qf);
                         else { const double r = (vol - nor) / (eme - nor); q = qn * CMF_F(0.5) + (r * r) * (qf - qn); }
                     } else q = dmax(dinf, qf);
                 } else {
-                    const double adj = n.adjvol[d];
+                    const double adj = __ldg(&n.adjvol[d]);
                     if (vol <= con) q = qn * sqrt(vol / con);
                     else if (vol > con && vol <= adj) q = qn + pow((vol - con) / (adj - con), 3.0) * (qa - qn);
                     else if (vol > adj && vol <= eme) {
@@ -739,6 +791,7 @@ __device__ __forceinline__ void cell_outflow(const Net &n, const State &s, const
     }
     s.rivout_raw[gi] = rout;
     s.fldout_raw[gi] = fout;
+    if (carry) diag_carry_store(n, s, gi, DT, k == 1, diag_carry_load(n, s, gi, k == 1), rivout_pre, fldout_pre, rivdph, storge);
     // D2RIVVEL is observed after the last sub-step; its sub-step average is accumulated here
     // (CMF_DIAG_AVEMAX_ADPSTP, src/cmf_calc_diag_mod.F90:104-161) instead of in phase C
     const bool first = (k == 0), last = (k == c.nt - 1);
@@ -767,7 +820,7 @@ __device__ __forceinline__ void path_outflow(const Net &n, const State &s, int m
     const size_t pb = (size_t)m * Lp * P;
     const size_t base = (size_t)m * n.N;
     const double gdt = n.pgrv * DT;
-    const int skip = n.pth_skip[p];
+    const int skip = __ldg(&n.pth_skip[p]);
     double sum = 0.0;
     double flw[8];
     const bool skipped = n.llevee ? (skip & 2) : (skip & 1);
@@ -776,44 +829,44 @@ __device__ __forceinline__ void path_outflow(const Net &n, const State &s, int m
         s.pthsum_raw[(size_t)m * P + p] = 0.0;
         return;
     }
-    const int u = n.pth_up[p], d = n.pth_dn[p];
-    const double su = n.rivelv[u] + s.rivdph[base + u], sd = n.rivelv[d] + s.rivdph[base + d];
-    const double spu = n.rivelv[u] + s.rivdph_pre[base + u], spd = n.rivelv[d] + s.rivdph_pre[base + d];
-    double dslp = (su - sd) / n.pth_dst[p];
+    const int u = __ldg(&n.pth_up[p]), d = __ldg(&n.pth_dn[p]);
+    const double su = __ldg(&n.rivelv[u]) + s.rivdph[base + u], sd = __ldg(&n.rivelv[d]) + s.rivdph[base + d];
+    const double spu = __ldg(&n.rivelv[u]) + s.rivdph_pre[base + u], spd = __ldg(&n.rivelv[d]) + s.rivdph_pre[base + d];
+    double dslp = (su - sd) / __ldg(&n.pth_dst[p]);
     dslp = dmax(-0.005, dmin(0.005, dslp));
     if (!n.llevee) {
         for (int l = 0; l < Lp; l++) {
             const size_t o = (size_t)l * P + p;
-            const double elv = n.pth_elv[o];
+            const double elv = __ldg(&n.pth_elv[o]);
             const double dflw = dmax(dmax(su, sd) - elv, 0.0);
             const double dflw_pr = dmax(dmax(spu, spd) - elv, 0.0);
             double dflw_im = sqrt(dflw * dflw_pr);
             dflw_im = dmax(dflw_im, sqrt(dflw * 0.01));
-            const double f = (dflw_im > 1.E-5) ? path_flux(n.pth_wth[o], s.pthflw_pre[pb + o], gdt, dflw_im, dslp, n.pth_man[l], false) : 0.0;
+            const double f = (dflw_im > 1.E-5) ? path_flux(__ldg(&n.pth_wth[o]), s.pthflw_pre[pb + o], gdt, dflw_im, dslp, __ldg(&n.pth_man[l]), false) : 0.0;
             if (l < 8) flw[l] = f;
             s.pthflw_raw[pb + o] = f;
         }
     } else {
         // level 1: river channel, semi-implicit depth
         {
-            const double elv = n.pth_elv[p];
+            const double elv = __ldg(&n.pth_elv[p]);
             const double dflw = dmax(dmax(su, sd) - elv, 0.0);
             const double dflw_pr = dmax(dmax(spu, spd) - elv, 0.0);
             double dflw_im = sqrt(dflw * dflw_pr);
             if (dflw_im <= 0.0) dflw_im = dflw;
-            const double f = (dflw_im > 1.E-5) ? path_flux(n.pth_wth[p], s.pthflw_pre[pb + p], gdt, dflw_im, dslp, n.pth_man[0], false) : 0.0;
+            const double f = (dflw_im > 1.E-5) ? path_flux(__ldg(&n.pth_wth[p]), s.pthflw_pre[pb + p], gdt, dflw_im, dslp, __ldg(&n.pth_man[0]), false) : 0.0;
             flw[0] = f;
             s.pthflw_raw[pb + p] = f;
         }
         if (Lp > 1) {
-            const int lu = n.lev_id[u], ld = n.lev_id[d];
+            const int lu = __ldg(&n.lev_id[u]), ld = __ldg(&n.lev_id[d]);
             double slu = su, sld = sd;
-            if (lu >= 0 && n.levfrc[lu] < 1.0) slu = dmin(n.elevtn[u] + s.levdph[base + u], su);
-            if (ld >= 0 && n.levfrc[ld] < 1.0) sld = dmin(n.elevtn[d] + s.levdph[base + d], sd);
+            if (lu >= 0 && __ldg(&n.levfrc[lu]) < 1.0) slu = dmin(__ldg(&n.elevtn[u]) + s.levdph[base + u], su);
+            if (ld >= 0 && __ldg(&n.levfrc[ld]) < 1.0) sld = dmin(__ldg(&n.elevtn[d]) + s.levdph[base + d], sd);
             for (int l = 1; l < Lp; l++) {
                 const size_t o = (size_t)l * P + p;
-                const double dflw = dmax(dmax(slu, sld) - n.pth_elv[o], 0.0);
-                const double f = (dflw > 1.E-5) ? path_flux(n.pth_wth[o], s.pthflw_pre[pb + o], gdt, dflw, dslp, n.pth_man[l], true) : 0.0;
+                const double dflw = dmax(dmax(slu, sld) - __ldg(&n.pth_elv[o]), 0.0);
+                const double f = (dflw > 1.E-5) ? path_flux(__ldg(&n.pth_wth[o]), s.pthflw_pre[pb + o], gdt, dflw, dslp, __ldg(&n.pth_man[l]), true) : 0.0;
                 if (l < 8) flw[l] = f;
                 s.pthflw_raw[pb + o] = f;
             }
@@ -857,14 +910,14 @@ __device__ __forceinline__ void cell_rate(const Net &n, const State &s, const Ow
     double so = dmax(w.rivout_raw(gi), 0.0) + dmax(w.fldout_raw(gi), 0.0);
     const int u1 = w.up_hi(i);
     for (int k = w.up_lo(i); k < u1; k++) {
-        const int j = n.up_idx[k];
+        const int j = __ldg(&n.up_idx[k]);
         so = (so + dmax(-s.rivout_raw[base + j], 0.0)) + dmax(-s.fldout_raw[base + j], 0.0);
     }
     so = so * DT;
     if (n.lpthout) {
         const double *sum = s.pthsum_raw + (size_t)m * n.P;
-        for (int k = n.pout_ptr[i]; k < n.pout_ptr[i + 1]; k++) so = so + dmax(sum[n.pout_idx[k]], 0.0) * DT;
-        for (int k = n.pinf_ptr[i]; k < n.pinf_ptr[i + 1]; k++) so = so + dmax(-sum[n.pinf_idx[k]], 0.0) * DT;
+        for (int k = __ldg(&n.pout_ptr[i]); k < __ldg(&n.pout_ptr[i + 1]); k++) so = so + dmax(sum[__ldg(&n.pout_idx[k])], 0.0) * DT;
+        for (int k = __ldg(&n.pinf_ptr[i]); k < __ldg(&n.pinf_ptr[i + 1]); k++) so = so + dmax(-sum[__ldg(&n.pinf_idx[k])], 0.0) * DT;
     }
     const double dout = dmax(so, 1.E-10);
     const double dsto = w.rivsto(gi) + w.fldsto(gi);
@@ -894,8 +947,8 @@ __global__ void k_rate(Net n, State s, int advance, cudaGraphConditionalHandle h
 // ------------------------------------------------------------------------------------------
 __device__ __forceinline__ double scaled_pathsum(const Net &n, const double *sum_raw, const double *rate_m, int p) {
     const double v = sum_raw[p];
-    if (n.pth_skip[p] & 1) return v;
-    return v >= 0.0 ? v * rate_m[n.pth_up[p]] : v * rate_m[n.pth_dn[p]];
+    if (__ldg(&n.pth_skip[p]) & 1) return v;
+    return v >= 0.0 ? v * rate_m[__ldg(&n.pth_up[p])] : v * rate_m[__ldg(&n.pth_dn[p])];
 }
 
 // bifurcation paths in phase C: LSPAMAT path rescale (:494-517), CALC_VARS_PRE copy, diagnostics
@@ -905,8 +958,8 @@ __device__ __forceinline__ void path_rescale(const Net &n, const State &s, int m
     const size_t base = (size_t)m * n.N;
     const size_t pb = (size_t)m * Lp * P;
     const double *rate_m = s.rate + base;
-    const bool sk = n.pth_skip[p] & 1;
-    const int u = n.pth_up[p], d = n.pth_dn[p];
+    const bool sk = __ldg(&n.pth_skip[p]) & 1;
+    const int u = __ldg(&n.pth_up[p]), d = __ldg(&n.pth_dn[p]);
     double asum = 0.0;
     for (int l = 0; l < Lp; l++) {
         const size_t o = pb + (size_t)l * P + p;
@@ -934,8 +987,14 @@ __device__ __forceinline__ void cell_store(const Net &n, const State &s, const O
     const size_t base = (size_t)m * n.N;
     const size_t gi = base + i;
     const double *rate_m = s.rate + base;
+    // the cell's own state is read up front, before anything is stored: in the compiler's view a
+    // store may alias any later load of another state array and would hold that load back
     const double rate_i = w.rate(gi);
     double rout = w.rivout_raw(gi), fout = w.fldout_raw(gi);
+    const double runoff = w.runoff(gi);
+    const double rivsto0 = w.rivsto(gi), fldsto0 = w.fldsto(gi), rivdph0 = w.rivdph(gi);
+    const double frc = w.fldfrc(gi);
+    const double levsto = n.llevee ? w.levsto(gi) : 0.0;
     // own outflow after the LSPAMAT rescale (:456-473)
     if (i < n.R) {
         const double r = (rout > 0.0) ? rate_i : rate_m[w.next(i)];
@@ -949,7 +1008,7 @@ __device__ __forceinline__ void cell_store(const Net &n, const State &s, const O
     double rinf = 0.0, finf = 0.0;
     const int u1 = w.up_hi(i);
     for (int k = w.up_lo(i); k < u1; k++) {
-        const int j = n.up_idx[k];
+        const int j = __ldg(&n.up_idx[k]);
         const double rj = s.rivout_raw[base + j], fj = s.fldout_raw[base + j];
         const double r = (rj > 0.0) ? rate_m[j] : rate_i;
         rinf = rinf + rj * r;
@@ -959,32 +1018,22 @@ __device__ __forceinline__ void cell_store(const Net &n, const State &s, const O
     bool has_path = false;
     if (n.lpthout) {
         const double *sum = s.pthsum_raw + (size_t)m * n.P;
-        const int o0 = n.pout_ptr[i], o1 = n.pout_ptr[i + 1], f0 = n.pinf_ptr[i], f1 = n.pinf_ptr[i + 1];
+        const int o0 = __ldg(&n.pout_ptr[i]), o1 = __ldg(&n.pout_ptr[i + 1]), f0 = __ldg(&n.pinf_ptr[i]), f1 = __ldg(&n.pinf_ptr[i + 1]);
         has_path = (o1 > o0) || (f1 > f0);
-        for (int k = o0; k < o1; k++) pout = pout + scaled_pathsum(n, sum, rate_m, n.pout_idx[k]);
-        for (int k = f0; k < f1; k++) pout = pout - scaled_pathsum(n, sum, rate_m, n.pinf_idx[k]);
+        for (int k = o0; k < o1; k++) pout = pout + scaled_pathsum(n, sum, rate_m, __ldg(&n.pout_idx[k]));
+        for (int k = f0; k < f1; k++) pout = pout - scaled_pathsum(n, sum, rate_m, __ldg(&n.pinf_idx[k]));
     }
-    const double runoff = w.runoff(gi);
-    // CMF_DAMOUT_WATBAL, src/cmf_ctrl_damout_mod.F90:516-535
-    double dmiss = 0.0;
-    if (n.ldamout) {
-        const int d = n.dam_id[i];
-        if (d >= 0) {
-            const double inflow = (rinf + finf) + runoff;
-            const double outflw = rout + fout;
-            const double s0 = s.damsto[gi];
-            const double s1 = (s0 + inflow * DT) - outflw * DT;
-            s.damsto[gi] = s1;
-            dmiss = ((s0 - s1) + inflow * DT) - outflw * DT;
-        }
+    // CMF_DAMOUT_WATBAL, src/cmf_ctrl_damout_mod.F90:516-535 (the new dam storage is stored below)
+    double dmiss = 0.0, damsto1 = 0.0;
+    const int dam = n.ldamout ? __ldg(&n.dam_id[i]) : -1;
+    if (dam >= 0) {
+        const double inflow = (rinf + finf) + runoff;
+        const double outflw = rout + fout;
+        const double s0 = s.damsto[gi];
+        damsto1 = (s0 + inflow * DT) - outflw * DT;
+        dmiss = ((s0 - damsto1) + inflow * DT) - outflw * DT;
     }
     bput(11, dmiss);
-    // CALC_VARS_PRE, src/cmf_ctrl_physics_mod.F90:254-277
-    const double rivsto0 = w.rivsto(gi), fldsto0 = w.fldsto(gi);
-    s.rivout_pre[gi] = rout;
-    s.fldout_pre[gi] = fout;
-    s.rivdph_pre[gi] = w.rivdph(gi);
-    s.fldsto_pre[gi] = fldsto0;
     // CMF_CALC_STONXT, src/cmf_calc_stonxt_mod.F90:53-100
     bput(0, rivsto0 + fldsto0);
     bput(3, rinf * DT + finf * DT);
@@ -996,13 +1045,17 @@ __device__ __forceinline__ void cell_store(const Net &n, const State &s, const O
     if (fs < 0.0) { rs = dmax(rs + fs, 0.0); fs = 0.0; }
     bput(1, rs + fs);
     const double outflw = rout + fout;
-    const double frc = w.fldfrc(gi);
     rs = rs + (runoff * (1.0 - frc)) * DT;       // D2GDWRTN is zero without groundwater delay
     fs = fs + (runoff * frc) * DT;
-    const double levsto = n.llevee ? w.levsto(gi) : 0.0;
     bput(2, n.llevee ? (rs + fs) + levsto : rs + fs);
     // stage scheme, :125
     const StageOut o = n.llevee ? stage_levee(n, w, i, rs, fs, levsto) : stage_def(n, w, i, rs, fs);
+    // CALC_VARS_PRE, src/cmf_ctrl_physics_mod.F90:254-277, and the dam storage
+    s.rivout_pre[gi] = rout;
+    s.fldout_pre[gi] = fout;
+    s.rivdph_pre[gi] = rivdph0;
+    s.fldsto_pre[gi] = fldsto0;
+    if (dam >= 0) s.damsto[gi] = damsto1;
     // CMF_CheckNanB-style probe (src/cmf_utils_mod.F90:807-815) on the new storage: a NaN or
     // infinite runoff or state surfaces as a positive status instead of a silent NaN state
     if (!isfinite((o.rivsto + o.fldsto) + o.levsto)) s.ctl[m].err = kErrNonFinite;
@@ -1019,31 +1072,34 @@ __device__ __forceinline__ void cell_store(const Net &n, const State &s, const O
         s.pthout[gi] = pout;
         s.outflw[gi] = outflw;
     }
-    // CMF_DIAG_AVEMAX_ADPSTP / GETAVE_ADPSTP, src/cmf_calc_diag_mod.F90:104-221
-    if (n.ldiag) {
+    // CMF_DIAG_AVEMAX_ADPSTP / GETAVE_ADPSTP, src/cmf_calc_diag_mod.F90:104-221.  The sub-steps
+    // before the last one are accumulated by the next sub-step's phase A (diag_carry_store), except
+    // D2PTHOUT_aAVG: D2PTHINF is never written by the reference (always 0), and a cell without
+    // bifurcation channels adds +0 every sub-step, so its average (and output average) stays at the
+    // +0 the arrays were created with; cells with channels accumulate it here every sub-step.
+    if (n.ldiag && (last || has_path)) {
         const double na = nadd + DT;
         // CMF_DIAG_AVEMAX_OUTPUT (src/cmf_calc_diag_mod.F90:272-318) on the last sub-step: the
         // output interval accumulates the finished sub-step average times DT_DEF
         const bool out = last && n.ldiag_out;
         const double ddef = c.dt_def;
-        // a store is skipped when the sub-step leaves the accumulator's bits unchanged (a zero
-        // discharge added to a running sum, a maximum that did not move): the array holds the same
-        // bits either way
-        auto same = [](double a, double b) { return __double_as_longlong(a) == __double_as_longlong(b); };
         auto acc = [&](double prev, double *a, double *oa, double v) {
             double x = first ? v * DT : prev + v * DT;
             if (last) x = x / na;
-            if (first || last || !same(x, prev)) a[gi] = x;
+            if (first || last || !same_bits(x, prev)) a[gi] = x;
             if (out) oa[gi] = oa[gi] + x * ddef;
         };
-        acc(first ? 0.0 : w.a_rivout(gi), s.a_rivout, s.o_rivout, rout);
-        acc(first ? 0.0 : w.a_fldout(gi), s.a_fldout, s.o_fldout, fout);
-        acc(first ? 0.0 : w.a_outflw(gi), s.a_outflw, s.o_outflw, outflw);
-        // D2PTHOUT_aAVG: D2PTHINF is never written by the reference (always 0), and a cell without
-        // bifurcation channels adds +0 every sub-step, so its average (and output average) stays at
-        // the +0 the arrays were created with: nothing to read or write
         if (has_path) acc(first ? 0.0 : w.a_pthout(gi), s.a_pthout, s.o_pthout, pout);
         if (last) {
+            // every previous accumulator is read before the first of them is stored
+            const double pro = first ? 0.0 : w.a_rivout(gi), pfo = first ? 0.0 : w.a_fldout(gi);
+            const double pof = first ? 0.0 : w.a_outflw(gi);
+            const double pmo = first ? 0.0 : w.m_outflw(gi), pmd = first ? 0.0 : w.m_rivdph(gi);
+            const double pms = first ? 0.0 : w.m_storge(gi);
+            const double dinf = n.ldamout ? s.daminf[gi] : 0.0, pdi = (first || !n.ldamout) ? 0.0 : s.a_daminf[gi];
+            acc(pro, s.a_rivout, s.o_rivout, rout);
+            acc(pfo, s.a_fldout, s.o_fldout, fout);
+            acc(pof, s.a_outflw, s.o_outflw, outflw);
             // runoff and DT are constant over the outer step: the same running sum of
             // runoff*DT the accumulator would hold, rebuilt in registers on the last sub-step
             const double rdt = runoff * DT;
@@ -1052,21 +1108,19 @@ __device__ __forceinline__ void cell_store(const Net &n, const State &s, const O
             a = a / na;
             s.a_runoff[gi] = a;
             if (out) s.o_runoff[gi] = s.o_runoff[gi] + a * ddef;
-        }
-        if (n.ldamout) acc(first ? 0.0 : s.a_daminf[gi], s.a_daminf, s.o_daminf, s.daminf[gi]);
-        const double stg = n.llevee ? (o.rivsto + o.fldsto) + o.levsto : o.rivsto + o.fldsto;
-        const double pmo = first ? 0.0 : w.m_outflw(gi), pmd = first ? 0.0 : w.m_rivdph(gi);
-        const double pms = first ? 0.0 : w.m_storge(gi);
-        const double mo = dmax(pmo, fabs(outflw));
-        const double md = dmax(pmd, o.rivdph);
-        const double ms = dmax(pms, stg);
-        if (first || !same(mo, pmo)) s.m_outflw[gi] = mo;
-        if (first || !same(md, pmd)) s.m_rivdph[gi] = md;
-        if (first || !same(ms, pms)) s.m_storge[gi] = ms;
-        if (out) {
-            s.om_outflw[gi] = dmax(s.om_outflw[gi], fabs(mo));
-            s.om_rivdph[gi] = dmax(s.om_rivdph[gi], md);
-            s.om_storge[gi] = dmax(s.om_storge[gi], ms);
+            if (n.ldamout) acc(pdi, s.a_daminf, s.o_daminf, dinf);
+            const double stg = n.llevee ? (o.rivsto + o.fldsto) + o.levsto : o.rivsto + o.fldsto;
+            const double mo = dmax(pmo, fabs(outflw));
+            const double md = dmax(pmd, o.rivdph);
+            const double ms = dmax(pms, stg);
+            s.m_outflw[gi] = mo;
+            s.m_rivdph[gi] = md;
+            s.m_storge[gi] = ms;
+            if (out) {
+                s.om_outflw[gi] = dmax(s.om_outflw[gi], fabs(mo));
+                s.om_rivdph[gi] = dmax(s.om_rivdph[gi], md);
+                s.om_storge[gi] = dmax(s.om_storge[gi], ms);
+            }
         }
     }
 }
@@ -1189,31 +1243,31 @@ __global__ void k_outpre(Net n, State s, int ncell_blocks) {
         if (i >= n.N) return;
         const size_t gi = base + i;
         const double rivdph = s.rivdph[gi];
-        const double sfc = n.rivelv[i] + rivdph;
+        const double sfc = __ldg(&n.rivelv[i]) + rivdph;
         s.sfcelv[gi] = sfc;
         s.rivdph_pre[gi] = rivdph;
         double dslope, dsfcmax, dflw;
         if (i < n.R) {
-            const int j = n.next[i];
-            const double sfcj = n.rivelv[j] + s.rivdph[base + j];
+            const int j = __ldg(&n.next[i]);
+            const double sfcj = __ldg(&n.rivelv[j]) + s.rivdph[base + j];
             dsfcmax = dmax(sfc, sfcj);
-            dslope = (sfc - sfcj) * (1.0 / n.nxtdst[i]);
-            dflw = dsfcmax - n.rivelv[i];
+            dslope = (sfc - sfcj) * (1.0 / __ldg(&n.nxtdst[i]));
+            dflw = dsfcmax - __ldg(&n.rivelv[i]);
         } else {
             dsfcmax = sfc;
-            dslope = (sfc - n.dwnelv[i]) * (1.0 / n.pdstmth);
+            dslope = (sfc - __ldg(&n.dwnelv[i])) * (1.0 / n.pdstmth);
             dflw = rivdph;
         }
         const double dslope_f = dmax(-0.005, dmin(0.005, dslope));
-        const double darea = n.rivwth[i] * dflw;
+        const double darea = __ldg(&n.rivwth[i]) * dflw;
         double rout = 0.0;
         if (darea > CMF_F(1.E-5)) {
-            rout = darea * (((1.0 / n.rivman[i]) * pow(dflw, p23)) * sqrt(fabs(dslope)));
+            rout = darea * (((1.0 / __ldg(&n.rivman[i])) * pow(dflw, p23)) * sqrt(fabs(dslope)));
             if (dslope < 0.0) rout = -rout;
         }
-        const double dflw_f = dmax(dsfcmax - n.elevtn[i], 0.0);
-        double dare_f = s.fldsto[gi] * (1.0 / n.rivlen[i]);
-        dare_f = dmax(dare_f - s.flddph[gi] * n.rivwth[i], 0.0);
+        const double dflw_f = dmax(dsfcmax - __ldg(&n.elevtn[i]), 0.0);
+        double dare_f = s.fldsto[gi] * (1.0 / __ldg(&n.rivlen[i]));
+        dare_f = dmax(dare_f - s.flddph[gi] * __ldg(&n.rivwth[i]), 0.0);
         double fout = 0.0;
         if (dare_f > CMF_F(1.E-5)) {
             fout = dare_f * (((1.0 / n.pmanfld) * pow(dflw_f, p23)) * sqrt(fabs(dslope_f)));
@@ -1224,17 +1278,17 @@ __global__ void k_outpre(Net n, State s, int ncell_blocks) {
     } else {
         const int p = (blockIdx.x - ncell_blocks) * blockDim.x + threadIdx.x;
         if (p >= n.P) return;
-        const int u = n.pth_up[p], d = n.pth_dn[p];
+        const int u = __ldg(&n.pth_up[p]), d = __ldg(&n.pth_dn[p]);
         if (u < 0 || d < 0) return;                    // path leaves the domain
         const size_t pb = (size_t)m * n.Lp * n.P;
-        const double su = n.rivelv[u] + s.rivdph[base + u], sd = n.rivelv[d] + s.rivdph[base + d];
-        const double dslope = (su - sd) * (1.0 / n.pth_dst[p]);
+        const double su = __ldg(&n.rivelv[u]) + s.rivdph[base + u], sd = __ldg(&n.rivelv[d]) + s.rivdph[base + d];
+        const double dslope = (su - sd) * (1.0 / __ldg(&n.pth_dst[p]));
         for (int l = 0; l < n.Lp; l++) {
             const size_t o = (size_t)l * n.P + p;
-            const double dflw = dmax(dmax(su, sd) - n.pth_elv[o], 0.0);
+            const double dflw = dmax(dmax(su, sd) - __ldg(&n.pth_elv[o]), 0.0);
             double f = 0.0;
             if (dflw > CMF_F(1.E-5)) {
-                f = (n.pth_wth[o] * dflw) * (((1.0 / n.pth_man[l]) * pow(dflw, p23)) * sqrt(fabs(dslope)));
+                f = (__ldg(&n.pth_wth[o]) * dflw) * (((1.0 / __ldg(&n.pth_man[l])) * pow(dflw, p23)) * sqrt(fabs(dslope)));
                 if (dslope < 0.0) f = -f;
             }
             s.pthflw_pre[pb + o] = f;
@@ -1283,7 +1337,7 @@ __global__ void k_runoff_map(Net n, State s, RunoffMap r, const double *__restri
         }
     } else {
         const double v = val(r.inpx[i], r.inpy[i]);
-        if (v != rmis) out = dmax((v * n.grarea[i]) / r.drofunit, 0.0);
+        if (v != rmis) out = dmax((v * __ldg(&n.grarea[i])) / r.drofunit, 0.0);
     }
     s.runoff[(size_t)m * n.N + i] = out;
 }

@@ -442,7 +442,7 @@ __global__ void __launch_bounds__(kTile, 2) k_persist(Net n, State s, PersistArg
             const StageOut o = n.llevee ? stage_levee(n, w, i, s.rivsto[gi], s.fldsto[gi], s.levsto[gi])
                                         : stage_def(n, w, i, s.rivsto[gi], s.fldsto[gi]);
             store_stage(n, s, gi, i, o);
-            if (n.ladpstp && n.i2mask[i] == 0) key = cfl_key(n.pcadp, (i < n.R) ? n.nxtdst[i] : n.pdstmth, n.pgrv, o.rivdph);
+            if (n.ladpstp && __ldg(&n.i2mask[i]) == 0) key = cfl_key(n.pcadp, (i < n.R) ? __ldg(&n.nxtdst[i]) : n.pdstmth, n.pgrv, o.rivdph);
         }
         if (n.ladpstp) {
             for (int o = 16; o > 0; o >>= 1) key = dmin(key, __shfl_down_sync(0xffffffffu, key, o));
