@@ -201,19 +201,21 @@ def phase_bytes(N: int, E: int, L_bar: float, P: int, Lp: int, nlev: int, ndam: 
     D2OUTFLW, D2FLDARE, D2SFCELV and the runoff average -- are not counted).
       k_flux : static 7x8 (RIVELV ELEVTN NXTDST RIVWTH RIVHGT RIVLEN RIVMAN) + I1NEXT 4 + state reads
                8x8 (RIVDPH RIVDPH_PRE RIVOUT_PRE FLDOUT_PRE FLDSTO FLDDPH FLDSTO_PRE STORGE)
-               + writes 2x8 (RIVOUT FLDOUT) + velocity average r/w 16 (diagnostics) = 140 (+16) B/cell
+               + writes 2x8 (RIVOUT FLDOUT) = 140 B/cell, + diagnostics: velocity average r/w 16 and
+               the previous sub-step's 7 accumulators r/w 112 (rivout fldout outflw daminf averages,
+               outflw rivdph storge maxima)                                 = 140 (+128) B/cell
                + per path: endpoints 8, DST 8, skip 4, ELV/WTH/FLW_PRE/FLW 32 x Lp, FLWSUM 8
       k_rate : RIVOUT FLDOUT 16 + CSR 4 + 4/edge + RIVSTO FLDSTO 16 + RATE 8        = 48 B/cell
                + path CSR 8 and FLWSUM 8 per path end
       k_store: RIVOUT FLDOUT RATE 24 + CSR 8 + I1NEXT 4 + RIVSTO FLDSTO RIVDPH FLDFRC RUNOFF 40
                + RIVSTOMAX RIVLEN RIVWTH GRAREA 32 + layers 16 L_bar + writes 10x8 80 (_PRE x4,
-               RIVSTO FLDSTO RIVDPH FLDDPH FLDFRC STORGE) + diagnostics 7 accumulators r/w 112
-                                                                             = 188+16 L_bar (+112)
+               RIVSTO FLDSTO RIVDPH FLDDPH FLDFRC STORGE)                   = 188+16 L_bar
+               (the last sub-step's own accumulators, once per outer step, are not counted)
                + levee: index 4/cell + 7 params + LEVSTO r/w + LEVDPH w per levee cell
                + dams: 112 B per dam, paths: FLW r/w 16 x Lp + FLWSUM 16 per path"""
-    flux = N * (140 + (16 if ldiag else 0)) + P * (8 + 8 + 4 + 32 * Lp + 8) + ndam * 112
+    flux = N * (140 + (128 if ldiag else 0)) + P * (8 + 8 + 4 + 32 * Lp + 8) + ndam * 112
     rate = N * 48 + (E - N) * 4 + P * 2 * (8 + 8)
-    store = N * (188 + 16 * L_bar + (112 if ldiag else 0)) + N * 4 + nlev * (7 * 8 + 16 + 8) + ndam * 112 + P * (16 * Lp + 16)
+    store = N * (188 + 16 * L_bar) + N * 4 + nlev * (7 * 8 + 16 + 8) + ndam * 112 + P * (16 * Lp + 16)
     return {"k_flux": flux, "k_rate": rate, "k_store": store}
 
 
