@@ -578,7 +578,9 @@ __device__ __forceinline__ double rate_min1(double a, double b) { return (a >= b
 struct DiagPrev {
     double rivout, fldout, outflw, daminf, dinf, mout, mdph, msto;
 };
-__device__ __forceinline__ DiagPrev diag_carry_load(const Net &n, const State &s, size_t gi, bool first) {
+// `daminf` is the previous sub-step's D2DAMINF (phase A captures it before replacing it)
+__device__ __forceinline__ DiagPrev diag_carry_load(const Net &n, const State &s, size_t gi, bool first,
+                                                    double daminf) {
     DiagPrev p;
     p.rivout = first ? 0.0 : s.a_rivout[gi];
     p.fldout = first ? 0.0 : s.a_fldout[gi];
@@ -586,7 +588,7 @@ __device__ __forceinline__ DiagPrev diag_carry_load(const Net &n, const State &s
     p.mout = first ? 0.0 : s.m_outflw[gi];
     p.mdph = first ? 0.0 : s.m_rivdph[gi];
     p.msto = first ? 0.0 : s.m_storge[gi];
-    p.dinf = n.ldamout ? s.daminf[gi] : 0.0;
+    p.dinf = daminf;
     p.daminf = (first || !n.ldamout) ? 0.0 : s.a_daminf[gi];
     return p;
 }
@@ -631,6 +633,8 @@ __device__ __forceinline__ void cell_outflow(const Net &n, const State &s, const
     const double rivout_old = split ? s.rivout_cur[gi] : rivout_pre;
     const double fldout_pre = w.fldout_pre(gi), storge = w.storge(gi);
     const bool carry = n.ldiag && k > 0;   // diagnostics of sub-step k-1 (diag_carry_store)
+    bool dinf_taken = false;                 // D2DAMINF of sub-step k-1 read before the dam code replaced it
+    double dinf_prev = 0.0;
     double rout, fout = 0.0, rvel;
     if (i < n.R) {
         const int j = w.next(i);
@@ -738,6 +742,10 @@ __device__ __forceinline__ void cell_outflow(const Net &n, const State &s, const
                     }
                 }
             }
+            if (carry) {
+                dinf_prev = s.daminf[gi];
+                dinf_taken = true;
+            }
             s.daminf[gi] = dinf;
             if (code == 10 && i < n.R) {
                 // UPDATE_INFLOW 1c: kinematic outflow upstream of a dam
@@ -791,7 +799,11 @@ __device__ __forceinline__ void cell_outflow(const Net &n, const State &s, const
     }
     s.rivout_raw[gi] = rout;
     s.fldout_raw[gi] = fout;
-    if (carry) diag_carry_store(n, s, gi, DT, k == 1, diag_carry_load(n, s, gi, k == 1), rivout_pre, fldout_pre, rivdph, storge);
+    if (carry) {
+        const double dinf = dinf_taken ? dinf_prev : (n.ldamout ? s.daminf[gi] : 0.0);
+        diag_carry_store(n, s, gi, DT, k == 1, diag_carry_load(n, s, gi, k == 1, dinf), rivout_pre, fldout_pre,
+                         rivdph, storge);
+    }
     // D2RIVVEL is observed after the last sub-step; its sub-step average is accumulated here
     // (CMF_DIAG_AVEMAX_ADPSTP, src/cmf_calc_diag_mod.F90:104-161) instead of in phase C
     const bool first = (k == 0), last = (k == c.nt - 1);

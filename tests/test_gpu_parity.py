@@ -28,6 +28,11 @@ def _models(case_dir, **kw):
     return h, g, o
 
 
+# every sub-step average and maximum of CMF_DIAG_AVEMAX_ADPSTP / GETAVE_ADPSTP
+SUBSTEP_DIAG = ["rivout_aavg", "fldout_aavg", "outflw_aavg", "rivvel_aavg", "pthout_aavg", "runoff_aavg",
+                "daminf_aavg", "storge_amax", "outflw_amax", "rivdph_amax"]
+
+
 def _compare_state(g, o, tag, member=0, extra=()):
     st = g.get_state()
     dg = g.get_diag()
@@ -38,9 +43,7 @@ def _compare_state(g, o, tag, member=0, extra=()):
         ("fldout", st["fldout"][member], o.d("fldout")),
         ("rivdph", dg["rivdph"][member], o.d("rivdph")),
         ("flddph", dg["flddph"][member], o.d("flddph")),
-        ("rivout_aavg", dg["rivout_aavg"][member], o.d("rivout_aavg")),
-        ("storge_amax", dg["storge_amax"][member], o.d("storge_amax")),
-    ] + list(extra)
+    ] + [(n, dg[n][member], o.d(n)) for n in SUBSTEP_DIAG] + list(extra)
     msgs = []
     for name, a, b in fields:
         ok, worst, bad = rel_close(a, b, RTOL)
