@@ -110,6 +110,10 @@ class ClockSampler:
         while self.proc and not self.lines and time.perf_counter() - t0 < timeout:
             time.sleep(0.01)
 
+    def mark_load(self):
+        """Start of the loaded span (the replay of the timed steps that precedes the timed region)."""
+        self.load = time.perf_counter()
+
     def mark_start(self):
         self.window = [time.perf_counter(), None]
 
@@ -125,14 +129,18 @@ class ClockSampler:
             except subprocess.TimeoutExpired:
                 self.proc.kill()
 
-    def summary(self) -> dict:
+    def summary(self, loaded: bool = False) -> dict:
+        """Median SM clock, maximum and throttle reasons over the timed window, or (loaded=True) over
+        the whole loaded span from mark_load() to the window's end."""
         sm, mx, reasons = [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         lines = self.lines
         if self.window and self.window[1]:
-            # samples that arrived during the marked window (plus one interval of reporting lag)
+            # samples that arrived during the marked span (plus one interval of reporting lag)
             lag = self.interval_ms / 1e3
-            sel = [x for x in lines if self.window[0] <= x[0] <= self.window[1] + lag]
+            t0 = getattr(self, "load", None) if loaded else None
+            t0 = self.window[0] if t0 is None else t0
+            sel = [x for x in lines if t0 <= x[0] <= self.window[1] + lag]
             lines = sel if sel else lines
         for _, ln in lines:
             p = [x.strip() for x in ln.split(",")]
@@ -326,6 +334,7 @@ def gpu_arm(args) -> int:
     # record holds samples under this load even though the timed region itself is short.
     clk = ClockSampler(local).__enter__()
     clk.wait_first()
+    clk.mark_load()
     t_rep = time.perf_counter()
     while not args.no_replay and time.perf_counter() - t_rep < 0.5:
         g.set_state(snapshot)
@@ -431,7 +440,11 @@ def gpu_arm(args) -> int:
                              f"of the OpenMP oracle, {csecs:.1f} s on {threads} host threads",
                    "single_thread": {"value": cells1 / csecs1, "unit": UNIT, "cores": 1,
                                      "sample": f"{done1} coupling steps of the same window, serial oracle, {csecs1:.1f} s"}}
-        clocks = clk.summary()
+        # the loaded span: the untimed replay of the same coupling steps right before the timed
+        # region plus the timed region itself (which alone lasts only tens of milliseconds)
+        clocks = clk.summary(loaded=True)
+        clocks["span"] = "replay of the timed steps (0.5 s) + timed region"
+        clocks["timed_region"] = clk.summary()
         nthist = {str(k): int(v) for k, v in enumerate(hist) if v}
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": K, "warmup": W,

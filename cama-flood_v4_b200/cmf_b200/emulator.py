@@ -48,6 +48,9 @@ def _emu_lib():
         vp, i, f, d = C.c_void_p, C.c_int, C.c_float, C.c_double
         lib.cmf_emu_gemm.argtypes = [i, i, i, vp, i, i, vp, i, i, vp, i, vp, i, vp, i, i, i, vp]
         lib.cmf_emu_gemm_mma.argtypes = [i, i, i, vp, i, i, vp, i, i, vp, i, vp, i, vp, i, i, i, vp]
+        lib.cmf_emu_gemm_splitk_ws_floats.restype = C.c_size_t
+        lib.cmf_emu_gemm_splitk_ws_floats.argtypes = [i, i, i, i]
+        lib.cmf_emu_gemm_splitk.argtypes = [i, i, i, vp, i, i, vp, i, i, vp, i, i, vp, C.c_size_t, vp]
         lib.cmf_emu_relu_bwd.argtypes = [i, vp, vp, vp, vp, vp]
         lib.cmf_emu_colsum.argtypes = [i, i, vp, vp, vp]
         lib.cmf_emu_mse_grad.argtypes = [i, i, i, vp, vp, vp, vp, vp, vp]
@@ -216,7 +219,13 @@ class MLP:
             a = acts[li]
             K_in = a.shape[1]
             n_out = self.W[li].shape[1]
-            self._gemm(K_in, n_out, R, a, K_in, 1, dZb, n_out, 0, C=self.gW[li], acc=1, ksplit=ks)      # a^T dZ
+            # a^T dZ, split over the rows with the slices summed in a fixed order (deterministic)
+            need = int(self.lib.cmf_emu_gemm_splitk_ws_floats(K_in, n_out, R, ks))
+            if getattr(self, "_ws", None) is None or self._ws.numel() < need:
+                self._ws = torch.empty(need, dtype=torch.float32, device=self.dev)
+            echeck(self.lib.cmf_emu_gemm_splitk(K_in, n_out, R, a.data_ptr(), K_in, 1, dZb.data_ptr(), n_out, 0,
+                                                self.gW[li].data_ptr(), n_out, ks, self._ws.data_ptr(),
+                                                self._ws.numel(), self.stream), "gemm_splitk")
             echeck(self.lib.cmf_emu_colsum(R, n_out, dZf.data_ptr(), self.gb[li].data_ptr(), self.stream), "colsum")
             if li == 0:
                 break

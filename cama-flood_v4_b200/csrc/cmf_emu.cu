@@ -776,6 +776,9 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_mlp_tc(const __nv_bfloat16 *_
 // the chunk's MMAs (M=128, N=NT, K=16, bf16 x bf16 -> fp32) into a tensor-memory accumulator and
 // commits them to the buffer's mbarrier, which completes (bounded wait) before the buffer is refilled.
 // Epilogue: thread t owns row t (TMEM lane t) and reads its NT accumulator columns 32 at a time.
+// With `zstride` > 0 every K slice stores its own partial product at C + blockIdx.z * zstride
+// (plain stores, no bias or ReLU); k_splitk_reduce then adds the slices to the output in slice
+// order, so a split-K product is the same bits on every run.
 // ------------------------------------------------------------------------------------------
 constexpr int kGThreads = 128;                          // = rows of the tile = TMEM lanes
 constexpr int kGK = 64;                                 // K per staged chunk
@@ -814,8 +817,9 @@ __global__ void __launch_bounds__(kGThreads) k_gemm_tc(int M, int N, int K, cons
                                                        int transA, const __nv_bfloat16 *__restrict__ B, int ldb, int transB,
                                                        float *C, int ldc, __nv_bfloat16 *Cb, int ldcb,
                                                        const float *__restrict__ bias, int relu, int accumulate,
-                                                       int k_per_split, int wait_limit) {
+                                                       int k_per_split, int wait_limit, size_t zstride) {
     extern __shared__ __align__(1024) unsigned char sm[];
+    if (zstride) C += blockIdx.z * zstride;
     uint64_t *mbar = reinterpret_cast<uint64_t *>(sm + 2 * kGBuf);
     uint32_t *tslot = reinterpret_cast<uint32_t *>(sm + 2 * kGBuf + 16);
     const int tid = threadIdx.x, warp = tid >> 5;
@@ -924,6 +928,17 @@ __global__ void __launch_bounds__(kGThreads) k_gemm_tc(int M, int N, int K, cons
     if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(tmem), "r"(NT) : "memory");
 }
 
+// C[r][c] = ((C[r][c] + P_0[r][c]) + P_1[r][c]) + ...: the split-K slices in slice order
+__global__ void k_splitk_reduce(int M, int N, int splits, const float *__restrict__ ws, float *C, int ldc) {
+    const size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const size_t MN = (size_t)M * N;
+    if (e >= MN) return;
+    const int r = (int)(e / N), c = (int)(e - (size_t)r * N);
+    float x = C[(size_t)r * ldc + c];
+    for (int z = 0; z < splits; z++) x += ws[z * MN + e];
+    C[(size_t)r * ldc + c] = x;
+}
+
 }  // namespace
 
 extern "C" {
@@ -950,14 +965,58 @@ int cmf_emu_gemm(int M, int N, int K, const void *A, int lda, int transA, const 
         dim3 grid((M + 127) / 128, N / 128, splits);
         k_gemm_tc<128><<<grid, kGThreads, kGSmem, st>>>(M, N, K, (const __nv_bfloat16 *)A, lda, transA, (const __nv_bfloat16 *)B,
                                                        ldb, transB, C, ldc, (__nv_bfloat16 *)Cb, ldcb, bias, relu, accumulate,
-                                                       kps, g_tc_wait_limit);
+                                                       kps, g_tc_wait_limit, (size_t)0);
     } else {
         EMU_TRY(cudaFuncSetAttribute(k_gemm_tc<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, kGSmem));
         dim3 grid((M + 127) / 128, N / 64, splits);
         k_gemm_tc<64><<<grid, kGThreads, kGSmem, st>>>(M, N, K, (const __nv_bfloat16 *)A, lda, transA, (const __nv_bfloat16 *)B,
                                                       ldb, transB, C, ldc, (__nv_bfloat16 *)Cb, ldcb, bias, relu, accumulate,
-                                                      kps, g_tc_wait_limit);
+                                                      kps, g_tc_wait_limit, (size_t)0);
     }
+    EMU_TRY(cudaGetLastError());
+    return CMF_OK;
+}
+
+size_t cmf_emu_gemm_splitk_ws_floats(int M, int N, int K, int ksplit) {
+    if (M <= 0 || N <= 0 || K <= 0) return 0;
+    if (ksplit < 1) ksplit = 1;
+    const int kps = ((K / ksplit + kGK - 1) / kGK) * kGK;
+    return (size_t)((K + kps - 1) / kps) * (size_t)M * (size_t)N;
+}
+
+int cmf_emu_gemm_splitk(int M, int N, int K, const void *A, int lda, int transA, const void *B, int ldb, int transB,
+                        float *C, int ldc, int ksplit, float *workspace, size_t workspace_floats, void *stream) {
+    if (M % TM || N % TN || K % TK || M <= 0 || N <= 0 || K <= 0)
+        return emu_err(CMF_E_ARG, "cmf_emu_gemm_splitk: M,N must be multiples of 64 and K of 32");
+    if ((lda % 8) || (ldb % 8) || ((uintptr_t)A & 15) || ((uintptr_t)B & 15))
+        return emu_err(CMF_E_ARG, "cmf_emu_gemm_splitk: lda, ldb must be multiples of 8 and A, B 16-byte aligned");
+    if (!C || !workspace) return emu_err(CMF_E_ARG, "cmf_emu_gemm_splitk: C and workspace are required");
+    int dev = 0, major = 0;
+    EMU_TRY(cudaGetDevice(&dev));
+    EMU_TRY(cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev));
+    if (major != 10) return emu_err(CMF_E_NO_DEVICE, "cmf_emu_gemm_splitk: needs an sm_100 device");
+    if (ksplit < 1) ksplit = 1;
+    const int kps = ((K / ksplit + kGK - 1) / kGK) * kGK;
+    const int splits = (K + kps - 1) / kps;
+    const size_t MN = (size_t)M * N;
+    if (workspace_floats < (size_t)splits * MN)
+        return emu_err(CMF_E_ARG, "cmf_emu_gemm_splitk: workspace smaller than cmf_emu_gemm_splitk_ws_floats()");
+    cudaStream_t st = (cudaStream_t)stream;
+    if (N % 128 == 0) {
+        EMU_TRY(cudaFuncSetAttribute(k_gemm_tc<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, kGSmem));
+        dim3 grid((M + 127) / 128, N / 128, splits);
+        k_gemm_tc<128><<<grid, kGThreads, kGSmem, st>>>(M, N, K, (const __nv_bfloat16 *)A, lda, transA, (const __nv_bfloat16 *)B,
+                                                       ldb, transB, workspace, N, nullptr, 0, nullptr, 0, 0, kps,
+                                                       g_tc_wait_limit, MN);
+    } else {
+        EMU_TRY(cudaFuncSetAttribute(k_gemm_tc<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, kGSmem));
+        dim3 grid((M + 127) / 128, N / 64, splits);
+        k_gemm_tc<64><<<grid, kGThreads, kGSmem, st>>>(M, N, K, (const __nv_bfloat16 *)A, lda, transA, (const __nv_bfloat16 *)B,
+                                                      ldb, transB, workspace, N, nullptr, 0, nullptr, 0, 0, kps,
+                                                      g_tc_wait_limit, MN);
+    }
+    EMU_TRY(cudaGetLastError());
+    k_splitk_reduce<<<(unsigned)((MN + 255) / 256), 256, 0, st>>>(M, N, splits, workspace, C, ldc);
     EMU_TRY(cudaGetLastError());
     return CMF_OK;
 }

@@ -352,6 +352,13 @@ int cmf_gpu_ctx_copy_member(cmf_gpu_ctx *dst, int32_t dst_member, cmf_gpu_ctx *s
 int cmf_emu_gemm(int M, int N, int K, const void *A, int lda, int transA, const void *B, int ldb, int transB,
                  float *C, int ldc, void *Cb, int ldcb, const float *bias, int relu, int accumulate, int ksplit,
                  void *stream);
+/* Deterministic split-K on the same tensor cores: C[M,N] += op(A) op(B) with K split into
+ * `ksplit` slices whose partial products go to `workspace` (at least
+ * cmf_emu_gemm_splitk_ws_floats(M, N, K, ksplit) floats, 16-byte aligned) and are added to C in
+ * slice order, so the result is the same bits on every run (the training's weight gradients). */
+size_t cmf_emu_gemm_splitk_ws_floats(int M, int N, int K, int ksplit);
+int cmf_emu_gemm_splitk(int M, int N, int K, const void *A, int lda, int transA, const void *B, int ldb, int transB,
+                        float *C, int ldc, int ksplit, float *workspace, size_t workspace_floats, void *stream);
 /* The same contract on the legacy mma.sync tiles (kept as the cross-check of cmf_emu_gemm). */
 int cmf_emu_gemm_mma(int M, int N, int K, const void *A, int lda, int transA, const void *B, int ldb, int transB,
                      float *C, int ldc, void *Cb, int ldcb, const float *bias, int relu, int accumulate, int ksplit,

@@ -99,6 +99,69 @@ def test_gemm_kernel_matches_numpy(ta, tb, ks, M, N, K):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("ta,tb,ks,M,N,K", [(1, 0, 4, 128, 128, 16384), (1, 0, 3, 64, 64, 1024), (0, 1, 2, 128, 64, 256)])
+def test_splitk_gemm_is_deterministic(ta, tb, ks, M, N, K):
+    """Split-K on the tensor cores with the slices summed in slice order: C += op(A) op(B) within
+    fp32 accumulation tolerance of float64 numpy, and the same bits on every call."""
+    import torch
+
+    from cmf_b200.emulator import _emu_lib, echeck
+    from emu_ref import to_bf16
+
+    lib = _emu_lib()
+    rng = np.random.default_rng(ks + M + N + K)
+    A = to_bf16(rng.standard_normal((K, M) if ta else (M, K)))
+    B = to_bf16(rng.standard_normal((N, K) if tb else (K, N)))
+    C0 = rng.standard_normal((M, N)).astype(np.float32)
+    dev = torch.device("cuda", 0)
+    tA = torch.tensor(A, device=dev).to(torch.bfloat16)
+    tB = torch.tensor(B, device=dev).to(torch.bfloat16)
+    need = int(lib.cmf_emu_gemm_splitk_ws_floats(M, N, K, ks))
+    assert need >= M * N * min(ks, K // 64)
+    ws = torch.empty(need, dtype=torch.float32, device=dev)
+    outs = []
+    for _ in range(3):
+        C = torch.tensor(C0, device=dev)
+        echeck(lib.cmf_emu_gemm_splitk(M, N, K, tA.data_ptr(), A.shape[1], ta, tB.data_ptr(), B.shape[1], tb,
+                                       C.data_ptr(), N, ks, ws.data_ptr(), need, None), "gemm_splitk")
+        outs.append(C.cpu().numpy())
+    torch.cuda.synchronize()
+    assert lib.cmf_emu_mlp_tc_status() == 0
+    ref = C0.astype(np.float64) + (A.T if ta else A).astype(np.float64) @ (B.T if tb else B).astype(np.float64)
+    assert np.allclose(outs[0], ref, rtol=1e-5, atol=1e-3 * np.sqrt(K / 256))
+    for o in outs[1:]:
+        assert np.array_equal(o.view(np.uint32), outs[0].view(np.uint32))
+    # a workspace below the required size is refused, not overrun
+    assert lib.cmf_emu_gemm_splitk(M, N, K, tA.data_ptr(), A.shape[1], ta, tB.data_ptr(), B.shape[1], tb,
+                                   torch.zeros(M, N, device=dev).data_ptr(), N, ks, ws.data_ptr(), need - 1, None) != 0
+
+
+@pytest.mark.gpu
+def test_training_is_deterministic():
+    """Two trainings from the same seed on the same rows end with the same weights, bit for bit
+    (row sampling is seeded and every reduction, split-K included, runs in a fixed order)."""
+    import torch
+
+    from cmf_b200 import emulator as E
+
+    dev = torch.device("cuda", 0)
+    rng = np.random.default_rng(7)
+    Xh = rng.standard_normal((40000, E.NFEAT)).astype(np.float32)
+    th = (0.3 * Xh[:, 0] - 0.2 * Xh[:, 5] + 0.1 * Xh[:, 9] * Xh[:, 2]).astype(np.float32)
+    X = torch.zeros(Xh.shape[0], E.IN, dtype=torch.bfloat16, device=dev)
+    X[:, :E.NFEAT] = torch.tensor(Xh, device=dev).to(torch.bfloat16)
+    t = torch.tensor(th, device=dev)
+    Ws = []
+    for _ in range(2):
+        mlp = E.MLP(dev, seed=0, lr=2e-3)
+        E.train(mlp, X, t, iters=12, batch=16384, seed=0)
+        torch.cuda.synchronize()
+        Ws.append([w.detach().cpu().numpy().copy() for w in mlp.W] + [v.detach().cpu().numpy().copy() for v in mlp.b])
+    for a, b in zip(*Ws):
+        assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
+
+
+@pytest.mark.gpu
 def test_training_kernels_gradients_match_cpu_reference():
     import torch
 
