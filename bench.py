@@ -535,12 +535,13 @@ def members_line(h, dev, M, base_fields, base, K, roof_args) -> dict:
     fused = fused_minimum_bytes(Nn, Lbar, P, Lp, nlev, ndam)
     gbs = fused * sub / secs / 1e9
     peak = measured_peaks()["hbm_gbs"]
+    sched = {k: v for k, v in g.schedule().items() if k != "kernels"}
     g.close()
     del fields
     torch.cuda.empty_cache()
     return {"members": M, "cell_substeps_per_s": N * sub / secs, "ms_per_step": secs / K * 1e3,
             "nt_mean": sub / (K * M), "step_achieved_gbs": gbs, "step_frac": gbs / peak,
-            "l2": "working set far above L2 (no flush needed)", "steps": K}
+            "l2": "working set far above L2 (no flush needed)", "steps": K, "schedule": sched}
 
 
 # ------------------------------------------------------------------------- batched config 2

@@ -376,8 +376,8 @@ class PhysicsGPU:
         q = _abi.Schedule()
         check(self.lib.cmf_gpu_ctx_get_schedule(self.h, C.byref(q)), "get_schedule")
         d = {f: getattr(q, f) for f, _ in _abi.Schedule._fields_}
-        d["kernels"] = ("one persistent cooperative kernel per coupling step (grid barriers between phases, tiles "
-                        "of 256 cells streamed by bulk asynchronous copies)" if q.mode == 2 else
+        d["kernels"] = ("one persistent cooperative kernel per coupling step (grid barriers between phases, "
+                        "tiles of 256 cells interleaved over the CTAs)" if q.mode == 2 else
                         "graph: stage, NT/DT, {flux, rate, store} x NT, budget")
         return d
 

@@ -102,14 +102,12 @@ struct cmf_gpu_ctx {
     void *rgrid = nullptr;
     size_t rgrid_bytes = 0;
 
-    // every device array gets 16 bytes of zeroed slack after its end: the persistent kernel's bulk
-    // copies fetch 16-byte aligned ranges, which may end up to 16 bytes past the last element
     template <class T>
     int alloc(T **p, size_t n) {
         void *q = nullptr;
         if (n == 0) n = 1;
-        CUDA_TRY(cudaMalloc(&q, n * sizeof(T) + 16));
-        CUDA_TRY(cudaMemsetAsync(q, 0, n * sizeof(T) + 16, stream));
+        CUDA_TRY(cudaMalloc(&q, n * sizeof(T)));
+        CUDA_TRY(cudaMemsetAsync(q, 0, n * sizeof(T), stream));
         allocs.push_back(q);
         *p = static_cast<T *>(q);
         return CMF_OK;
@@ -668,8 +666,7 @@ int finish_outer(cmf_gpu_ctx *c, int32_t *nt_out, double *dt_out, cmf_budget *b)
         if (berr) {
             CUDA_TRY(cudaMemsetAsync(&c->st.loop->bar_err, 0, sizeof(int), c->stream));
             CUDA_TRY(cudaStreamSynchronize(c->stream));
-            return set_err(CMF_E_BARRIER, berr == 2 ? "persistent kernel: a bulk copy did not complete within its bound"
-                                                    : "persistent kernel: a grid barrier did not complete within its bound");
+            return set_err(CMF_E_BARRIER, "persistent kernel: a grid barrier did not complete within its bound");
         }
     }
     int err = 0;

@@ -143,11 +143,11 @@ struct State {
 __device__ __forceinline__ double dmax(double a, double b) { return (a > b) ? a : b; }
 __device__ __forceinline__ double dmin(double a, double b) { return (a < b) ? a : b; }
 
-// Own-cell reads of the per-cell code go through an accessor.  OwnG reads the arrays in global
-// memory (the phase kernels); the persistent kernel's accessors read the same values from the
-// shared-memory tiles its bulk copies filled.  The arithmetic is shared, so both produce the same
-// bits.  Static maps are indexed by the cell i, member state by g = m*N + i; reads of another
-// cell (downstream, upstream, path ends) always go to global memory through Net/State.
+// Own-cell reads of the per-cell code go through an accessor (OwnG: the arrays in global memory,
+// static maps through the read-only path), so that a kernel could stage a cell's own values
+// elsewhere without touching the arithmetic.  Static maps are indexed by the cell i, member state
+// by g = m*N + i; reads of another cell (downstream, upstream, path ends) go to global memory
+// through Net/State.
 #define CMF_OWN_STATIC(name) \
     __device__ __forceinline__ double name(int i) const { return __ldg(&n.name[i]); }
 #define CMF_OWN_STATE(name) \

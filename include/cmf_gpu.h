@@ -43,7 +43,7 @@ extern "C" {
 #define CMF_E_NT_CAP          2  /* adaptive sub-step count above the cap (non-finite DT_MIN)     */
 #define CMF_E_NO_DEVICE       3  /* no CUDA device or the sm_100a kernels cannot run on it       */
 #define CMF_E_NONFINITE       4  /* a sub-step produced a NaN/infinite storage (NaN runoff...)   */
-#define CMF_E_BARRIER         5  /* a bounded device-side wait (grid barrier, bulk copy) ran out */
+#define CMF_E_BARRIER         5  /* a bounded device-side wait (persistent grid barrier) ran out */
 
 /* ---- dimensions (src/yos_cmf_map.F90, src/yos_cmf_input.F90) ----------------------------- */
 typedef struct cmf_dims {
@@ -81,7 +81,7 @@ typedef struct cmf_opts {
     int32_t launch_mode; /* 0: one CUDA graph per coupling step with a device-side sub-step loop;
                             1: host-driven launches (reads NT back before the sub-steps);
                             2: one persistent cooperative kernel per coupling step (grid barriers
-                               between the phases, tiles streamed by bulk asynchronous copies)    */
+                               between the phases, cell tiles interleaved over the CTAs)          */
     int32_t device;      /* CUDA device ordinal                                                   */
     int32_t block_size;  /* 0: the online autotuner picks the schedule (launch_mode 0); else
                             threads per block of the phase kernels (64..256)                     */

@@ -1,5 +1,5 @@
 """The persistent schedule (launch_mode 2): one cooperative kernel per coupling step with grid
-barriers between the phases and the tiles streamed into shared memory by bulk asynchronous copies.
+barriers between the phases and the cell tiles interleaved over the CTAs.
 
 It runs the same per-cell arithmetic as the graph of phase kernels, so states, NT/DT and budgets
 must equal that path bit for bit (the budgets with the same 256-cell partial blocks), and the oracle
