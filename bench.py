@@ -380,7 +380,8 @@ def gpu_arm(args) -> int:
 
     # ---- e2e through the public API with host buffers, the same window from the same state
     g.set_state(snapshot)
-    dsum = {"outflw_aavg": np.zeros(M * N)}
+    # the step's averaged discharge is read back into pinned host memory, like the runoff comes from it
+    dsum = {"outflw_aavg": torch.zeros(M * N, dtype=torch.float64).pin_memory().numpy()}
     e2e_sub = 0
     budgets = []
     if ws > 1:
@@ -459,7 +460,8 @@ def gpu_arm(args) -> int:
                                    else "host-driven kernel launches")},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": M * N * 8,
                     "d2h_bytes_per_step": M * N * 8 + M * 160,
-                    "window": "the same coupling steps as `value`, restarted from the saved state"},
+                    "window": "the same coupling steps as `value`, restarted from the saved state",
+                    "host_buffers": "pinned (runoff in, averaged discharge out)"},
             "mass_balance": closure(budgets),
             "gpu_launches": int(launches),
             "roofline": roof,

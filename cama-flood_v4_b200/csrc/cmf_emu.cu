@@ -517,34 +517,39 @@ __global__ void k_emu_update(EmuNet n, const int *active, double dt, const doubl
 // ------------------------------------------------------------------------------------------
 // Fused inference on the 5th-generation tensor cores (tcgen05, sm_100a).
 //
-// A CTA of 512 threads owns 128-row tiles of a persistent grid.  All four layers' weights sit in
-// shared memory as the MMA's B operands and the tile's activations as its A operand, both in the
-// K-major no-swizzle canonical layout: 16-byte rows of 8 bf16 grouped in 8-row core matrices,
-// byte offset (k/8)*(R*16) + (r/8)*128 + (r%8)*16 for an R-row operand (stride between the
-// 8-row groups 128 B, between the 8-wide k chunks R*16 B).  One thread issues the tcgen05.mma of
-// a layer (M=128, N=128 or 16, K=16 per instruction, fp32 accumulator in 128 TMEM columns) and a
-// tcgen05.commit onto an mbarrier; every thread waits on it (bounded), reads its row's accumulator
-// with tcgen05.ld (warp w reads TMEM lanes 32*(w%4).., columns 32*(w/4)..), adds the bias, applies
-// ReLU and the bf16 rounding in one cvt and stores the next layer's A operand.  The next tile's X
-// rows are fetched into registers while the current tile's layers run.  The last layer (N=16, column 0
-// real) adds b3 and writes y.  The rounding points equal the layer-by-layer chain (bf16 inputs,
-// fp32 accumulation, bf16 activations); the order of the fp32 additions inside an MMA is the
-// hardware's, so results agree with the mma.sync path to fp32 rounding, not bit for bit.
+// One CTA per SM (a persistent grid) holds all four layers' weights in shared memory once, as
+// the MMAs' B operands, and runs four 128-row tiles at a time: warpgroup s (warps 4s..4s+3) owns
+// tile slot s -- its activation buffer (the next MMA's A operand) and 128 of the SM's 512
+// tensor-memory columns -- and a seventeenth warp issues the MMAs.  Both operands use the K-major
+// no-swizzle canonical layout: 16-byte rows of 8 bf16 grouped in 8-row core matrices, byte offset
+// (k/8)*(R*16) + (r/8)*128 + (r%8)*16 for an R-row operand.  Per layer of a slot: the warpgroup
+// writes the A operand, arrives on the slot's `ready` mbarrier; the MMA warp, polling all four
+// slots, issues that layer's tcgen05.mma chain (M=128, N=128 or 16, K=16 per instruction, fp32
+// accumulator in the slot's columns) and commits it to the slot's `done` mbarrier; the warpgroup
+// waits on it, reads its rows with tcgen05.ld (warp 4s+q owns TMEM lanes 32q..32q+31), adds the
+// bias, applies ReLU and the bf16 rounding in one cvt and writes the next A operand.  While one
+// slot runs its epilogue the tensor pipe serves the others.  The last layer (N=16, column 0 real)
+// adds b3 and writes y.  Every wait is bounded: a wait that runs out raises the CTA's abort flag,
+// every warpgroup leaves at its next vote, and the MMA warp drains the MMAs it issued (one more
+// commit, waited for with the full bound) before the tensor memory is released.  The rounding
+// points equal the layer-by-layer chain (bf16 inputs, fp32 accumulation, bf16 activations) and the
+// K=16 steps run in the same order, so the outputs equal that chain bit for bit.
 // ------------------------------------------------------------------------------------------
-#ifndef CMF_TC_THREADS
-#define CMF_TC_THREADS 512
-#endif
-constexpr int kTcRows = 128, kTcThreads = CMF_TC_THREADS, kTcCols = 128;
-constexpr int kTcColsPerThread = kTcRows * kTcCols / kTcThreads;   // accumulator columns one thread reads
+constexpr int kTcRows = 128;
+constexpr int kTcSlots = 4;                           // tiles in flight per CTA
+constexpr int kTcEpi = 128 * kTcSlots;                // epilogue threads (4 warpgroups)
+constexpr int kTcThreads = kTcEpi + 32;               // + the MMA warp
 constexpr int kTcW0 = 0;                              // byte offsets inside the packed image
 constexpr int kTcW1 = kTcW0 + 128 * 32 * 2;           // layer 0: N=128, K=32
 constexpr int kTcW2 = kTcW1 + 128 * 128 * 2;          // layers 1, 2: N=128, K=128
 constexpr int kTcW3 = kTcW2 + 128 * 128 * 2;          // layer 3: N=16, K=128
 constexpr int kTcWBytes = kTcW3 + 16 * 128 * 2;
-constexpr int kTcA = kTcWBytes;                       // activations: 128 rows x 128 k
-constexpr int kTcBias = kTcA + kTcRows * 128 * 2;     // b0 b1 b2 (3 x 128 floats), b3[0]
-constexpr int kTcMisc = kTcBias + (3 * 128 + 4) * 4;  // mbarrier (8 B), TMEM address (4 B)
-constexpr int kTcSmem = kTcMisc + 16;
+constexpr int kTcABytes = kTcRows * 128 * 2;          // one slot's activations: 128 rows x 128 k
+constexpr int kTcA = kTcWBytes;
+constexpr int kTcBias = kTcA + kTcSlots * kTcABytes;  // b0 b1 b2 (3 x 128 floats), b3[0]
+constexpr int kTcMisc = kTcBias + (3 * 128 + 4) * 4;  // ready[4], done[4], drain mbarriers; TMEM address; abort
+constexpr int kTcSmem = kTcMisc + (2 * kTcSlots + 1) * 8 + 16;
+constexpr int kTcCols = 128 * kTcSlots;               // tensor-memory columns of the CTA
 #ifndef CMF_TC_WAIT_LIMIT
 #define CMF_TC_WAIT_LIMIT (1 << 20)
 #endif
@@ -640,47 +645,83 @@ __device__ __forceinline__ uint32_t relu_bf16x2(float lo, float hi) {
     return d;
 }
 
-// layer epilogue: bias + ReLU + bf16 of this thread's columns of row r into the next layer's A operand
-__device__ __forceinline__ void tc_epilogue_hidden(uint32_t tmem_row, int col0, const float *bias, unsigned char *sA, int r) {
+// layer epilogue: bias + ReLU + bf16 of the 128 accumulator columns of row r into the next
+// layer's A operand (two 32-column loads in flight)
+__device__ __forceinline__ void tc_epilogue_hidden(uint32_t tmem_row, const float *bias, unsigned char *sA, int r) {
 #pragma unroll
-    for (int h = 0; h < kTcColsPerThread / 32; h++) {
-        uint32_t v[32];
-        tmem_ld32(tmem_row + col0 + 32 * h, v);
+    for (int h = 0; h < 4; h += 2) {
+        uint32_t v[2][32];
+        tmem_ld32(tmem_row + 32 * h, v[0]);
+        tmem_ld32(tmem_row + 32 * (h + 1), v[1]);
         tmem_wait_ld();
 #pragma unroll
-        for (int q = 0; q < 4; q++) {
-            const int c = col0 + 32 * h + 8 * q;      // first of 8 columns = k chunk c/8 of the next layer
-            uint4 u;
-            uint32_t *w = reinterpret_cast<uint32_t *>(&u);
+        for (int g = 0; g < 2; g++) {
 #pragma unroll
-            for (int j = 0; j < 4; j++)
-                w[j] = relu_bf16x2(__uint_as_float(v[8 * q + 2 * j]) + bias[c + 2 * j],
-                                   __uint_as_float(v[8 * q + 2 * j + 1]) + bias[c + 2 * j + 1]);
-            *reinterpret_cast<uint4 *>(sA + canon_off(r, c, kTcRows)) = u;
+            for (int q = 0; q < 4; q++) {
+                const int c = 32 * (h + g) + 8 * q;       // first of 8 columns = k chunk c/8 of the next layer
+                uint4 u;
+                uint32_t *w = reinterpret_cast<uint32_t *>(&u);
+#pragma unroll
+                for (int j = 0; j < 4; j++)
+                    w[j] = relu_bf16x2(__uint_as_float(v[g][8 * q + 2 * j]) + bias[c + 2 * j],
+                                       __uint_as_float(v[g][8 * q + 2 * j + 1]) + bias[c + 2 * j + 1]);
+                *reinterpret_cast<uint4 *>(sA + canon_off(r, c, kTcRows)) = u;
+            }
         }
     }
 }
 
-__global__ void __launch_bounds__(kTcThreads, 2) k_mlp_tc(const __nv_bfloat16 *__restrict__ X, int ldx, int rows,
+__device__ __forceinline__ void named_bar(int id, int nthreads) {
+    asm volatile("bar.sync %0, %1;" :: "r"(id), "r"(nthreads) : "memory");
+}
+// named barrier with an OR over the participants' flags: every participant gets the same answer
+__device__ __forceinline__ bool named_bar_or(int id, int nthreads, bool v) {
+    uint32_t r;
+    asm volatile(
+        "{\n\t.reg .pred p, q;\n\t"
+        "setp.ne.u32 q, %1, 0;\n\t"
+        "bar.red.or.pred p, %2, %3, q;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(r) : "r"((uint32_t)v), "r"(id), "r"(nthreads) : "memory");
+    return r != 0;
+}
+__device__ __forceinline__ void mbar_arrive(uint32_t mbar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" :: "r"(mbar) : "memory");
+}
+__device__ __forceinline__ bool mbar_try(uint32_t mbar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(ok) : "r"(mbar), "r"(parity) : "memory");
+    return ok != 0;
+}
+
+__global__ void __launch_bounds__(kTcThreads, 1) k_mlp_tc(const __nv_bfloat16 *__restrict__ X, int ldx, int rows,
                                                         const uint4 *__restrict__ wimg, const float *__restrict__ b0,
                                                         const float *__restrict__ b1, const float *__restrict__ b2,
                                                         const float *__restrict__ b3, float *__restrict__ y,
                                                         int wait_limit) {
     extern __shared__ __align__(1024) unsigned char sm[];
-    unsigned char *sA = sm + kTcA;
     float *sb = reinterpret_cast<float *>(sm + kTcBias);
-    uint64_t *mbar = reinterpret_cast<uint64_t *>(sm + kTcMisc);
-    uint32_t *tslot = reinterpret_cast<uint32_t *>(sm + kTcMisc + 8);
+    uint64_t *ready = reinterpret_cast<uint64_t *>(sm + kTcMisc);
+    uint64_t *done = ready + kTcSlots;
+    uint64_t *drain = done + kTcSlots;
+    uint32_t *tslot = reinterpret_cast<uint32_t *>(drain + 1);
+    volatile int *abort_flag = reinterpret_cast<volatile int *>(tslot + 1);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     // weights and biases into shared memory
     for (int e = tid; e < kTcWBytes / 16; e += kTcThreads) reinterpret_cast<uint4 *>(sm)[e] = wimg[e];
     for (int e = tid; e < 128; e += kTcThreads) { sb[e] = b0[e]; sb[128 + e] = b1[e]; sb[256 + e] = b2[e]; }
     if (tid == 0) {
         sb[384] = b3[0];
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_u32(mbar)) : "memory");
+        for (int q = 0; q < 2 * kTcSlots + 1; q++)
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_u32(ready + q)) : "memory");
+        *abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    if (warp == 0) {   // one warp allocates the accumulator columns and releases the allocation permit
+    if (warp == 0) {   // one warp allocates the CTA's accumulator columns and releases the allocation permit
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
                      :: "r"(smem_u32(tslot)), "r"(kTcCols) : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
@@ -690,79 +731,132 @@ __global__ void __launch_bounds__(kTcThreads, 2) k_mlp_tc(const __nv_bfloat16 *_
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = *tslot;
-    const uint32_t mb = smem_u32(mbar);
-    const uint32_t sw = smem_u32(sm), sa = smem_u32(sA);
-    const uint32_t id128 = umma_idesc_bf16_f32(128, 128), id16 = umma_idesc_bf16_f32(128, 16);
-    const int r = 32 * (warp & 3) + lane;                    // this thread's row (TMEM lane)
-    const uint32_t tmem_row = tmem + ((uint32_t)(32 * (warp & 3)) << 16);
-    const int col0 = kTcColsPerThread * (warp >> 2);         // this thread's accumulator columns
-    uint32_t phase = 0;
-    bool failed = false;
     const int ntiles = (rows + kTcRows - 1) / kTcRows;
-    uint4 xnext = make_uint4(0u, 0u, 0u, 0u);                // this thread's X chunk of the first tile
-    {
-        const int row = blockIdx.x * kTcRows + (tid >> 2);
-        if (row < rows) xnext = *reinterpret_cast<const uint4 *>(X + (size_t)row * ldx + (tid & 3) * 8);
-    }
-    for (int tile = blockIdx.x; tile < ntiles && !failed; tile += gridDim.x) {
-        const int row0 = tile * kTcRows;
-        // X tile -> A operand (k 0..31): 128 rows x 4 chunks of 16 bytes, one chunk per thread,
-        // fetched during the previous tile (xnext); then fetch the next tile's chunk
-        static_assert(kTcRows * 4 == kTcThreads, "one X chunk per thread");
-        {
-            const int rr = tid >> 2, kc = tid & 3;
-            *reinterpret_cast<uint4 *>(sA + canon_off(rr, kc * 8, kTcRows)) = xnext;
-            const int nrow = row0 + gridDim.x * kTcRows + rr;
-            xnext = make_uint4(0u, 0u, 0u, 0u);
-            if (nrow < rows) xnext = *reinterpret_cast<const uint4 *>(X + (size_t)nrow * ldx + kc * 8);
-        }
-        fence_async_smem();
-        tc_fence_before();
-        __syncthreads();
+    const int stride = kTcSlots * (int)gridDim.x;             // tiles of slot s: first + j * stride
+    if (warp < kTcSlots * 4) {
+        // ---- epilogue warpgroup of slot s
+        const int sl = warp >> 2, q = warp & 3;
+        const int r = 32 * q + lane;                          // this thread's row == TMEM lane
+        unsigned char *sA = sm + kTcA + sl * kTcABytes;
+        const uint32_t trow = tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(128 * sl);
+        const uint32_t rd = smem_u32(ready + sl), dn = smem_u32(done + sl);
+        const int bar = 1 + sl;                               // named barrier of the warpgroup
+        uint32_t dphase = 0;
+        bool go = true;
+        int t = blockIdx.x * kTcSlots + sl;
+        uint4 xn[4];                                          // this row's X (32 bf16) of tile t
+#pragma unroll
+        for (int kc = 0; kc < 4; kc++) xn[kc] = make_uint4(0u, 0u, 0u, 0u);
+        if (t < ntiles && t * kTcRows + r < rows)
+#pragma unroll
+            for (int kc = 0; kc < 4; kc++) xn[kc] = *reinterpret_cast<const uint4 *>(X + (size_t)(t * kTcRows + r) * ldx + kc * 8);
+        for (; t < ntiles && go; t += stride) {
+            const int row = t * kTcRows + r;
+#pragma unroll
+            for (int kc = 0; kc < 4; kc++) *reinterpret_cast<uint4 *>(sA + canon_off(r, kc * 8, kTcRows)) = xn[kc];
+            // the next tile's row of X, fetched while this tile's layers run
+            const int tn = t + stride;
+#pragma unroll
+            for (int kc = 0; kc < 4; kc++) xn[kc] = make_uint4(0u, 0u, 0u, 0u);
+            if (tn < ntiles && tn * kTcRows + r < rows)
+#pragma unroll
+                for (int kc = 0; kc < 4; kc++) xn[kc] = *reinterpret_cast<const uint4 *>(X + (size_t)(tn * kTcRows + r) * ldx + kc * 8);
+            fence_async_smem();
+            tc_fence_before();
+            named_bar(bar, 128);
+            if (r == 0) mbar_arrive(rd);
 #pragma unroll 1
-        for (int layer = 0; layer < 4; layer++) {
-            if (tid == 0) {
+            for (int layer = 0; layer < 4; layer++) {
+                // bounded wait for this layer's MMAs, then a warpgroup-uniform vote on the outcome
+                // (an OR over the warpgroup's flags, so no thread goes on to a barrier the others left)
+                bool fail = false;
+                int spins = 0;
+                while (!mbar_try(dn, dphase)) {
+                    if (*abort_flag) { fail = true; break; }
+                    if (++spins > wait_limit) { *abort_flag = 1; fail = true; break; }
+                }
+                if (named_bar_or(bar, 128, fail)) { go = false; break; }
+                dphase ^= 1u;
                 tc_fence_after();
-                const int ksteps = layer == 0 ? 2 : 8;
-                const uint32_t wb = sw + (layer == 0 ? kTcW0 : layer == 1 ? kTcW1 : layer == 2 ? kTcW2 : kTcW3);
-                const uint32_t blbo = layer == 3 ? 16 * 16 : 128 * 16;
-                for (int s = 0; s < ksteps; s++) {
-                    const uint64_t ad = umma_smem_desc(sa + 2 * s * (128 * 16), 128 * 16, 128);
-                    const uint64_t bd = umma_smem_desc(wb + 2 * s * blbo, blbo, 128);
-                    umma_bf16(tmem, ad, bd, layer == 3 ? id16 : id128, s > 0 ? 1u : 0u);
-                }
-                umma_commit(mb);
-            }
-            const bool ok = mbar_wait(mb, phase, wait_limit);
-            if (__syncthreads_or(ok ? 0 : 1)) { failed = true; break; }   // block-uniform exit
-            phase ^= 1u;
-            tc_fence_after();
-            if (layer < 3) {
-                tc_epilogue_hidden(tmem_row, col0, sb + 128 * layer, sA, r);
-                fence_async_smem();
-                tc_fence_before();
-                __syncthreads();
-            } else {
-                if (warp < 4) {
+                if (layer < 3) {
+                    tc_epilogue_hidden(trow, sb + 128 * layer, sA, r);
+                    fence_async_smem();
+                    tc_fence_before();
+                    named_bar(bar, 128);
+                    if (r == 0) mbar_arrive(rd);
+                } else {
                     uint32_t v;
-                    tmem_ld1(tmem_row, v);
+                    tmem_ld1(trow, v);
                     tmem_wait_ld();
-                    if (row0 + r < rows) y[row0 + r] = __uint_as_float(v) + sb[384];
+                    if (row < rows) y[row] = __uint_as_float(v) + sb[384];
+                    tc_fence_before();
+                    named_bar(bar, 128);   // the slot's columns and A buffer are free for the next tile
                 }
-                tc_fence_before();
-                __syncthreads();
             }
         }
+    } else {
+      if (lane == 0) {
+        // ---- MMA warp: issues every layer of every slot as its A operand becomes ready
+        const uint32_t sw = smem_u32(sm);
+        const uint32_t id128 = umma_idesc_bf16_f32(128, 128), id16 = umma_idesc_bf16_f32(128, 16);
+        int left[kTcSlots], layer[kTcSlots];
+        uint32_t rphase[kTcSlots];
+        int remaining = 0;
+#pragma unroll
+        for (int sl = 0; sl < kTcSlots; sl++) {
+            const int t0 = blockIdx.x * kTcSlots + sl;
+            left[sl] = t0 < ntiles ? 4 * ((ntiles - 1 - t0) / stride + 1) : 0;
+            layer[sl] = 0;
+            rphase[sl] = 0u;
+            remaining += left[sl];
+        }
+        bool issued_any = false;
+        int spins = 0;
+        while (remaining > 0) {
+            bool progressed = false;
+#pragma unroll
+            for (int sl = 0; sl < kTcSlots; sl++) {
+                if (left[sl] == 0 || !mbar_try(smem_u32(ready + sl), rphase[sl])) continue;
+                rphase[sl] ^= 1u;
+                tc_fence_after();
+                const int L = layer[sl];
+                const int ksteps = L == 0 ? 2 : 8;
+                const uint32_t wb = sw + (L == 0 ? kTcW0 : L == 1 ? kTcW1 : L == 2 ? kTcW2 : kTcW3);
+                const uint32_t blbo = L == 3 ? 16 * 16 : 128 * 16;
+                const uint32_t sa = sw + kTcA + sl * kTcABytes;
+                for (int st = 0; st < ksteps; st++) {
+                    const uint64_t ad = umma_smem_desc(sa + 2 * st * (128 * 16), 128 * 16, 128);
+                    const uint64_t bd = umma_smem_desc(wb + 2 * st * blbo, blbo, 128);
+                    umma_bf16(tmem + 128 * sl, ad, bd, L == 3 ? id16 : id128, st > 0 ? 1u : 0u);
+                }
+                umma_commit(smem_u32(done + sl));
+                issued_any = true;
+                layer[sl] = (L + 1) & 3;
+                left[sl]--;
+                remaining--;
+                progressed = true;
+            }
+            if (progressed) {
+                spins = 0;
+            } else {
+                if (*abort_flag) break;
+                if (++spins > wait_limit) { *abort_flag = 1; break; }
+            }
+        }
+        if (issued_any) {
+            // every MMA this thread issued completes before the columns are released, also those
+            // whose completion no warpgroup waited for after an abort: one more commit tracks all
+            // of them, waited for with the full bound
+            umma_commit(smem_u32(drain));
+            mbar_wait(smem_u32(drain), 0u, kTcWaitLimit);
+        }
+      }
+      __syncwarp();
     }
-    if (failed) {
-        if (tid == 0) atomicExch(&g_mlp_tc_status, 1);
-        // the MMA of this phase may still be in flight: wait for it (full bound, whatever the
-        // launch's bound was) before the accumulator columns are released
-        mbar_wait(mb, phase, kTcWaitLimit);
-        tc_fence_before();
-        __syncthreads();
-        tc_fence_after();
-    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (*abort_flag && tid == 0) atomicExch(&g_mlp_tc_status, 1);
     if (warp == 0)
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(tmem), "r"(kTcCols) : "memory");
 }
@@ -1119,7 +1213,8 @@ int cmf_emu_mlp_tc(const void *X, int ldx, int rows, const void *pack, const flo
     EMU_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     EMU_TRY(cudaFuncSetAttribute(k_mlp_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem));
     const int ntiles = (rows + kTcRows - 1) / kTcRows;
-    const int grid = ntiles < 2 * sms ? ntiles : 2 * sms;
+    const int want = (ntiles + kTcSlots - 1) / kTcSlots;
+    const int grid = want < sms ? want : sms;
     k_mlp_tc<<<grid, kTcThreads, kTcSmem, (cudaStream_t)stream>>>((const __nv_bfloat16 *)X, ldx, rows, (const uint4 *)pack,
                                                                   b0, b1, b2, b3, y, g_tc_wait_limit);
     EMU_TRY(cudaGetLastError());
