@@ -153,7 +153,7 @@ def measure(host, device, members: int = 256, days: int = 2, judge_slots: int = 
     table.sort(key=lambda r: -r["speedup_vs_plain"])
     nse_hourly = E.nse(est.reshape(H, -1), truth.reshape(H, -1))
     cells = N * members * H
-    flops = 2.0 * rows * (32 * 128 + 128 * 128 * 2 + 128 * 16)
+    flops = 2.0 * rows * (32 * 128 + 128 * 128 * 2 + 128 * 8)   # 75.8 kFLOP per row, as time_inference counts
     return {
         "members": members, "days": days, "gauges": len(G), "judge_slots": judge_slots,
         "plain_cell_coupling_steps_per_s": cells / plain_s,
