@@ -82,6 +82,7 @@ struct cmf_gpu_ctx {
     std::vector<void *> allocs;
     Sched sched;                // the launch schedule of the outer step
     int persist_grid = 0;       // co-resident CTAs of the persistent kernel (0: it cannot run here)
+    bool l2_window = false;     // the hot maps sit under a persisting L2 access-policy window
     bool persist = false;       // outer steps run as one persistent cooperative launch
     Tuner tune;                 // online autotuner state
     int nlev = 0, ndam_placed = 0;
@@ -339,6 +340,79 @@ int build_net(cmf_gpu_ctx *c, const cmf_map_ptrs *mp) {
             (rc = c->upload(&n.adjvol, adj)) || (rc = c->upload(&n.r_volupa, rvu)))
             return rc;
     }
+    return CMF_OK;
+}
+
+// ---- hot maps in L2 ----------------------------------------------------------------------------
+// The maps every sub-step reads (about 120 B per cell) are moved into one allocation, and the
+// context's stream gets a persisting L2 access-policy window over it (kernels launched or
+// captured on that stream carry it), so the member state streaming through L2 does not evict
+// them.  Only when the whole allocation fits one window (config 1: 36 MB).  The persisting
+// carve-out is a process-wide limit of the CUDA context: raised to the largest window any live
+// library context needs, and put back when the last of them is destroyed.  Same bits: the kernels
+// read identical copies.
+std::mutex g_l2_mu;
+int g_l2_users = 0;
+size_t g_l2_saved = 0, g_l2_limit = 0;
+
+int hot_maps_window(cmf_gpu_ctx *c) {
+    cmf::Net &n = c->net;
+    const size_t N = (size_t)c->dims.nseqall;
+    struct Item { const void **field; size_t bytes; };
+    const Item items[] = {
+        {(const void **)&n.rivelv, N * 8}, {(const void **)&n.elevtn, N * 8}, {(const void **)&n.rivwth, N * 8},
+        {(const void **)&n.rivhgt, N * 8}, {(const void **)&n.rivlen, N * 8}, {(const void **)&n.rivman, N * 8},
+        {(const void **)&n.grarea, N * 8}, {(const void **)&n.rivstomax, N * 8}, {(const void **)&n.inv_nxtdst, N * 8},
+        {(const void **)&n.inv_rivwth, N * 8}, {(const void **)&n.inv_rivlen, N * 8},
+        {(const void **)&n.next, N * 4}, {(const void **)&n.up_ptr, (N + 1) * 4}, {(const void **)&n.up_idx, c->E * 4},
+        {(const void **)&n.i1dam, N * 4}, {(const void **)&n.dam_id, N * 4}, {(const void **)&n.lev_id, N * 4},
+        {(const void **)&n.pout_ptr, (N + 1) * 4}, {(const void **)&n.pinf_ptr, (N + 1) * 4}};
+    size_t total = 0;
+    for (const Item &it : items) total += (it.bytes + 255) & ~(size_t)255;
+    int max_persist = 0, max_win = 0;
+    CUDA_TRY(cudaDeviceGetAttribute(&max_persist, cudaDevAttrMaxPersistingL2CacheSize, c->device));
+    CUDA_TRY(cudaDeviceGetAttribute(&max_win, cudaDevAttrMaxAccessPolicyWindowSize, c->device));
+    if (max_persist <= 0 || max_win <= 0 || total > (size_t)max_win) return CMF_OK;
+    char *arena = nullptr;
+    CUDA_TRY(cudaMalloc(&arena, total));
+    c->allocs.push_back(arena);
+    std::vector<const void *> old;
+    size_t off = 0;
+    for (const Item &it : items) {
+        if (it.bytes) CUDA_TRY(cudaMemcpyAsync(arena + off, *it.field, it.bytes, cudaMemcpyDeviceToDevice, c->stream));
+        old.push_back(*it.field);
+        *it.field = arena + off;
+        off += (it.bytes + 255) & ~(size_t)255;
+    }
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    for (const void *p : old) {   // the separate allocations the maps came from
+        auto at = std::find(c->allocs.begin(), c->allocs.end(), p);
+        if (at != c->allocs.end()) {
+            cudaFree(*at);
+            c->allocs.erase(at);
+        }
+    }
+    const size_t persist = std::min(total, (size_t)max_persist);
+    {
+        std::lock_guard<std::mutex> lk(g_l2_mu);
+        if (g_l2_users == 0) {
+            CUDA_TRY(cudaDeviceGetLimit(&g_l2_saved, cudaLimitPersistingL2CacheSize));
+            g_l2_limit = g_l2_saved;
+        }
+        if (persist > g_l2_limit) {
+            CUDA_TRY(cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, persist));
+            g_l2_limit = persist;
+        }
+        g_l2_users++;
+    }
+    c->l2_window = true;
+    cudaStreamAttrValue v{};
+    v.accessPolicyWindow.base_ptr = arena;
+    v.accessPolicyWindow.num_bytes = total;
+    v.accessPolicyWindow.hitRatio = (float)std::min(1.0, (double)persist / (double)total);
+    v.accessPolicyWindow.hitProp = cudaAccessPropertyPersisting;
+    v.accessPolicyWindow.missProp = cudaAccessPropertyStreaming;
+    CUDA_TRY(cudaStreamSetAttribute(c->stream, cudaStreamAttributeAccessPolicyWindow, &v));
     return CMF_OK;
 }
 
@@ -805,6 +879,7 @@ int cmf_gpu_create(const cmf_dims *dims, const cmf_params *params, const cmf_map
     if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess)
         return fail(set_err(CMF_E_CUDA, "cudaStreamCreate failed"));
     if ((rc = build_net(c, maps))) return fail(rc);
+    if ((rc = hot_maps_window(c))) return fail(rc);
     if ((rc = alloc_state(c))) return fail(rc);
     if ((rc = persist_setup(c))) return fail(rc);
     if (opts->launch_mode < 0 || opts->launch_mode > 2) return fail(set_err(CMF_E_ARG, "launch_mode must be 0, 1 or 2"));
@@ -871,6 +946,14 @@ int cmf_gpu_destroy(cmf_gpu_ctx *c) {
     for (void *p : c->allocs) cudaFree(p);
     if (c->rgrid) cudaFree(c->rgrid);
     if (c->stream) cudaStreamDestroy(c->stream);
+    if (c->l2_window) {
+        std::lock_guard<std::mutex> lk(g_l2_mu);
+        if (--g_l2_users == 0) {
+            cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, g_l2_saved);
+            cudaCtxResetPersistingL2Cache();
+            g_l2_limit = g_l2_saved;
+        }
+    }
     delete c;
     return CMF_OK;
 }
