@@ -746,9 +746,11 @@ def cfg4_arm(args) -> int:
         from cmf_b200 import surrogate
 
         try:
+            # the headline controller setting only: a 16-member judge context of this domain alone
+            # would need about 29 GB next to the two 57 GB ensemble contexts
             sur = surrogate.measure(h, dev, members=Mmax, days=args.sur_days, forcing_distinct=2,
                                     snapshot_weighting=args.sur_snapshots,
-                                    trajectory_forcing=args.sur_traj_forcing or None)
+                                    trajectory_forcing=args.sur_traj_forcing or None, pareto=())
         except Exception as e:       # reported, never silently replaced by another number
             sur = {"error": f"{type(e).__name__}: {e}"}
     line = {
