@@ -561,7 +561,7 @@ class SurrogateEnsemble:
     def __init__(self, host, mlp: MLP, members: int, judge_slots: int, gauges: np.ndarray, tol_rel: float = 0.05,
                  resync_hours: int = 24, schedule: dict | None = None):
         """schedule: launch schedule for the judging plain solver (PhysicsGPU.set_schedule keys), e.g. the
-        one the plain ensemble tuned; without it the judge runs phase kernels at 128 threads."""
+        one the plain ensemble tuned; without it the judging solver runs phase kernels at 128 threads."""
         import torch
 
         from .model import PhysicsGPU
