@@ -380,20 +380,29 @@ def gpu_arm(args) -> int:
 
     # ---- e2e through the public API with host buffers, the same window from the same state
     g.set_state(snapshot)
-    # the step's averaged discharge is read back into pinned host memory, like the runoff comes from it
-    dsum = {"outflw_aavg": torch.zeros(M * N, dtype=torch.float64).pin_memory().numpy()}
+    # pipelined public API: the next step's runoff uploads from pinned host memory while a step
+    # runs, and every finished step's averaged discharge reads back into pinned host memory while
+    # the next one runs (two buffers, so a read-back never lands in the one the host reads)
+    outs = [{"outflw_aavg": torch.zeros(M * N, dtype=torch.float64).pin_memory().numpy()} for _ in range(2)]
+    rin = [runoff_host[base + k].numpy() for k in range(K)]
     e2e_sub = 0
     budgets = []
     if ws > 1:
         dist.barrier()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
+    g.put_runoff_async(rin[0])
     for k in range(K):
-        g.put_runoff(runoff_host[base + k].numpy())
-        nt, _, bud = g.advance()
+        g.advance_async()
+        if k + 1 < K:
+            g.put_runoff_async(rin[k + 1])
+        if k > 0:
+            g.io_wait()              # step k-1's discharge is in the host buffer
+        nt, _, bud = g.wait()
         e2e_sub += int(nt.sum())
         budgets.append(bud[0])
-        g.get_diag_fields(dsum)
+        g.get_diag_fields_async(outs[k % 2])
+    g.io_wait()
     e2e_secs = time.perf_counter() - t0
     if ws > 1:
         t = torch.tensor([e2e_secs], device=dev, dtype=torch.float64)
@@ -461,7 +470,10 @@ def gpu_arm(args) -> int:
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": M * N * 8,
                     "d2h_bytes_per_step": M * N * 8 + M * 160,
                     "window": "the same coupling steps as `value`, restarted from the saved state",
-                    "host_buffers": "pinned (runoff in, averaged discharge out)"},
+                    "host_buffers": "pinned (runoff in, averaged discharge out)",
+                    "io": "pipelined: the next step's runoff uploads and the finished step's discharge "
+                          "reads back while a step runs (put_runoff_async / advance_async / wait / "
+                          "get_diag_async / io_wait)"},
             "mass_balance": closure(budgets),
             "gpu_launches": int(launches),
             "roofline": roof,

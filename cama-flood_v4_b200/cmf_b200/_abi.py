@@ -110,7 +110,8 @@ EXPORTS = [
     "cmf_host_load", "cmf_host_free", "cmf_host_describe", "cmf_host_state", "cmf_host_conv_resol", "cmf_host_grid",
     "cmf_gpu_stage_noalloc", "cmf_gpu_ctx_nt_stats", "cmf_gpu_ctx_diag_output", "cmf_gpu_ctx_get_diag_output",
     "cmf_gpu_diag_output", "cmf_gpu_get_diag_output", "cmf_gpu_ctx_persist_selftest", "cmf_gpu_ctx_launch_mode",
-    "cmf_gpu_ctx_get_schedule", "cmf_gpu_ctx_set_schedule",
+    "cmf_gpu_ctx_get_schedule", "cmf_gpu_ctx_set_schedule", "cmf_gpu_ctx_put_runoff_async",
+    "cmf_gpu_ctx_advance_async", "cmf_gpu_ctx_wait", "cmf_gpu_ctx_get_diag_async", "cmf_gpu_ctx_io_wait",
 ]
 
 _lib = None
@@ -139,6 +140,11 @@ def load(build_if_missing: bool = True):
     lib.cmf_gpu_ctx_put_runoff.argtypes = [vp, f64p, f64p]
     lib.cmf_gpu_ctx_physics_advance.argtypes = [vp, C.c_double, i32p, f64p, C.POINTER(Budget)]
     lib.cmf_gpu_ctx_get_diag.argtypes = [vp, C.POINTER(DiagPtrs)]
+    lib.cmf_gpu_ctx_put_runoff_async.argtypes = [vp, f64p]
+    lib.cmf_gpu_ctx_advance_async.argtypes = [vp, C.c_double]
+    lib.cmf_gpu_ctx_wait.argtypes = [vp, i32p, f64p, C.POINTER(Budget)]
+    lib.cmf_gpu_ctx_get_diag_async.argtypes = [vp, C.POINTER(DiagPtrs)]
+    lib.cmf_gpu_ctx_io_wait.argtypes = [vp]
     lib.cmf_gpu_ctx_advance_device.argtypes = [vp, C.c_double, C.c_int32, vp, C.c_int64]
     lib.cmf_gpu_ctx_synchronize.argtypes = [vp]
     lib.cmf_gpu_ctx_last_nt.argtypes = [vp, i32p, f64p]

@@ -432,6 +432,40 @@ class PhysicsGPU:
         check(self.lib.cmf_gpu_ctx_get_diag_output(self.h, C.byref(dp)), "get_diag_output")
         return {k: v.reshape(self.M, -1) for k, v in out.items()}
 
+    # ---- pipelined host I/O: the next step's runoff uploads while a step runs, and a finished
+    # step's diagnostics read back while the next one runs (host arrays should be pinned)
+    def put_runoff_async(self, runoff: np.ndarray) -> None:
+        """Stages D2RUNOFF of the next outer step (float64, nmembers * NSEQALL, C-contiguous; the
+        array must stay alive and unchanged until the next advance has been launched)."""
+        if runoff.dtype != np.float64 or not runoff.flags.c_contiguous or runoff.size != self.M * self.N:
+            raise ValueError("runoff must be a C-contiguous float64 array of nmembers * NSEQALL values")
+        check(self.lib.cmf_gpu_ctx_put_runoff_async(self.h, runoff.ctypes.data_as(_abi.f64p)), "put_runoff_async")
+
+    def advance_async(self, dt_def: float | None = None) -> None:
+        dt_def = self.host.dt if dt_def is None else dt_def
+        check(self.lib.cmf_gpu_ctx_advance_async(self.h, dt_def), "advance_async")
+
+    def wait(self):
+        """Finishes the step advance_async launched: (nt, dt, budgets) like advance()."""
+        nt = np.zeros(self.M, dtype=np.int32)
+        dt = np.zeros(self.M)
+        b = (_abi.Budget * self.M)()
+        check(self.lib.cmf_gpu_ctx_wait(self.h, nt.ctypes.data_as(_abi.i32p), dt.ctypes.data_as(_abi.f64p), b), "wait")
+        return nt, dt, [{f: getattr(b[m], f) for f in _abi.BUDGET_FIELDS} for m in range(self.M)]
+
+    def get_diag_fields_async(self, out: dict) -> None:
+        """Starts the read-back of the named diagnostics into the caller's float64 arrays (they
+        land by io_wait(); the arrays must stay alive until then)."""
+        dp = _abi.DiagPtrs()
+        for n, a in out.items():
+            if n not in _abi.DIAG_FIELDS or a.dtype != np.float64 or not a.flags.c_contiguous:
+                raise ValueError(n)
+            setattr(dp, n, a.ctypes.data_as(_abi.f64p))
+        check(self.lib.cmf_gpu_ctx_get_diag_async(self.h, C.byref(dp)), "get_diag_async")
+
+    def io_wait(self) -> None:
+        check(self.lib.cmf_gpu_ctx_io_wait(self.h), "io_wait")
+
     def get_diag_fields(self, out: dict) -> dict:
         """Copies only the named diagnostics into the caller's float64 arrays (others skipped)."""
         dp = _abi.DiagPtrs()

@@ -92,6 +92,14 @@ struct cmf_gpu_ctx {
     cudaGraphExec_t exec = nullptr;
     cudaGraphConditionalHandle cond{};
     double dt_def_dev = -1.0;
+    // pipelined host I/O (created on first use): a copy stream, the runoff staging buffer, the
+    // staging of diagnostics read back while the next step runs, and their events
+    cudaStream_t io = nullptr;
+    cudaEvent_t ev_in = nullptr, ev_stage_free = nullptr, ev_out_staged = nullptr, ev_out_done = nullptr;
+    double *rstage = nullptr;
+    bool in_pending = false;    // a runoff field waits in rstage for the next advance
+    bool launched = false;      // an outer step was launched by advance_async and not yet waited for
+    std::vector<double *> ostage;   // per diagnostic field (DIAG order), allocated on first request
     int64_t launches = 0;
     // host staging for the per-member control block
     std::vector<cmf::MemberCtl> hctl;
@@ -780,6 +788,56 @@ constexpr int kTuneWarm = 4;   // outer steps before the autotuner's first candi
 
 }  // namespace
 
+// ---- pipelined host I/O ------------------------------------------------------------------------
+int io_setup(cmf_gpu_ctx *c) {
+    if (c->io) return CMF_OK;
+    CUDA_TRY(cudaStreamCreateWithFlags(&c->io, cudaStreamNonBlocking));
+    for (cudaEvent_t *e : {&c->ev_in, &c->ev_stage_free, &c->ev_out_staged, &c->ev_out_done})
+        CUDA_TRY(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+    int rc;
+    if ((rc = c->alloc(&c->rstage, (size_t)c->dims.nmembers * c->dims.nseqall))) return rc;
+    return CMF_OK;
+}
+
+// the runoff field staged by put_runoff_async becomes D2RUNOFF ahead of the next outer step
+int apply_staged_runoff(cmf_gpu_ctx *c) {
+    if (!c->in_pending) return CMF_OK;
+    const size_t MN = (size_t)c->dims.nmembers * c->dims.nseqall;
+    CUDA_TRY(cudaStreamWaitEvent(c->stream, c->ev_in, 0));
+    CUDA_TRY(cudaMemcpyAsync(c->st.runoff, c->rstage, MN * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+    CUDA_TRY(cudaEventRecord(c->ev_stage_free, c->stream));
+    c->in_pending = false;
+    return CMF_OK;
+}
+
+// the device arrays behind the named host buffers of a cmf_diag_ptrs (fields without a device
+// array in this configuration are skipped); `slot` numbers the fields for the async staging
+struct DiagField { double *dst; const double *src; size_t n; int slot; };
+std::vector<DiagField> diag_fields(const cmf_gpu_ctx *c, const cmf_diag_ptrs *p) {
+    const size_t MN = (size_t)c->dims.nmembers * c->dims.nseqall;
+    const size_t MP = (size_t)c->dims.nmembers * c->net.P;
+    const size_t MPL = MP * c->net.Lp;
+    const cmf::State &s = c->st;
+    const bool dg = c->opts.ldiag != 0;
+    const DiagField t[] = {
+        {p->rivdph, s.rivdph, MN, 0}, {p->flddph, s.flddph, MN, 1}, {p->fldfrc, s.fldfrc, MN, 2}, {p->fldare, s.fldare, MN, 3},
+        {p->sfcelv, s.sfcelv, MN, 4}, {p->storge, s.storge, MN, 5}, {p->rivvel, s.rivvel, MN, 6}, {p->rivinf, s.rivinf, MN, 7},
+        {p->fldinf, s.fldinf, MN, 8}, {p->pthout, s.pthout, MN, 9}, {p->outflw, s.outflw, MN, 10},
+        {p->pthflwsum, s.pthsum, MP, 11}, {p->levdph, c->opts.llevee ? s.levdph : nullptr, MN, 12},
+        {p->rivout_aavg, dg ? s.a_rivout : nullptr, MN, 13}, {p->fldout_aavg, dg ? s.a_fldout : nullptr, MN, 14},
+        {p->outflw_aavg, dg ? s.a_outflw : nullptr, MN, 15}, {p->rivvel_aavg, dg ? s.a_rivvel : nullptr, MN, 16},
+        {p->pthout_aavg, dg ? s.a_pthout : nullptr, MN, 17}, {p->runoff_aavg, dg ? s.a_runoff : nullptr, MN, 18},
+        {p->daminf_aavg, dg && c->opts.ldamout ? s.a_daminf : nullptr, MN, 19},
+        {p->storge_amax, dg ? s.m_storge : nullptr, MN, 20}, {p->outflw_amax, dg ? s.m_outflw : nullptr, MN, 21},
+        {p->rivdph_amax, dg ? s.m_rivdph : nullptr, MN, 22}, {p->pthflw_aavg, dg ? s.a_pthflw : nullptr, MPL, 23},
+        {p->pthflwsum_aavg, dg ? s.a_pthsum : nullptr, MP, 24}};
+    std::vector<DiagField> out;
+    for (const DiagField &x : t)
+        if (x.dst && x.src && x.n) out.push_back(x);
+    return out;
+}
+constexpr int kDiagSlots = 25;
+
 extern "C" {
 
 int cmf_gpu_abi_version(void) { return CMF_GPU_ABI_VERSION; }
@@ -945,6 +1003,10 @@ int cmf_gpu_destroy(cmf_gpu_ctx *c) {
     if (c->tune.e1) cudaEventDestroy(c->tune.e1);
     for (void *p : c->allocs) cudaFree(p);
     if (c->rgrid) cudaFree(c->rgrid);
+    if (c->io) cudaStreamSynchronize(c->io);
+    for (cudaEvent_t e : {c->ev_in, c->ev_stage_free, c->ev_out_staged, c->ev_out_done})
+        if (e) cudaEventDestroy(e);
+    if (c->io) cudaStreamDestroy(c->io);
     if (c->stream) cudaStreamDestroy(c->stream);
     if (c->l2_window) {
         std::lock_guard<std::mutex> lk(g_l2_mu);
@@ -1195,6 +1257,7 @@ int cmf_gpu_ctx_put_runoff(cmf_gpu_ctx *c, const double *runoff, const double *r
     CUDA_TRY(cudaSetDevice(c->device));
     const size_t MN = (size_t)c->dims.nmembers * c->dims.nseqall;
     CUDA_TRY(cudaMemcpyAsync(c->st.runoff, runoff, MN * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    c->in_pending = false;   // the newest field wins over one staged by put_runoff_async
     return CMF_OK;
 }
 
@@ -1203,10 +1266,48 @@ int cmf_gpu_ctx_physics_advance(cmf_gpu_ctx *c, double dt_def, int32_t *nt_out, 
     CUDA_TRY(cudaSetDevice(c->device));
     int rc;
     if ((rc = sync_dt_def(c, dt_def))) return rc;
+    if ((rc = apply_staged_runoff(c))) return rc;
     if ((rc = launch_outer(c))) return rc;
     CUDA_TRY(cudaGetLastError());
+    c->launched = false;
     return finish_outer(c, nt_out, dt_out, b);
 }
+
+int cmf_gpu_ctx_put_runoff_async(cmf_gpu_ctx *c, const double *runoff) {
+    if (!c || !runoff) return set_err(CMF_E_ARG, "null argument");
+    CUDA_TRY(cudaSetDevice(c->device));
+    int rc;
+    if ((rc = io_setup(c))) return rc;
+    const size_t MN = (size_t)c->dims.nmembers * c->dims.nseqall;
+    // the staging buffer is free once the previous staged field was copied into D2RUNOFF
+    CUDA_TRY(cudaStreamWaitEvent(c->io, c->ev_stage_free, 0));
+    CUDA_TRY(cudaMemcpyAsync(c->rstage, runoff, MN * sizeof(double), cudaMemcpyHostToDevice, c->io));
+    CUDA_TRY(cudaEventRecord(c->ev_in, c->io));
+    c->in_pending = true;
+    return CMF_OK;
+}
+
+int cmf_gpu_ctx_advance_async(cmf_gpu_ctx *c, double dt_def) {
+    if (!c) return set_err(CMF_E_STATE, "no context");
+    if (c->launched) return set_err(CMF_E_STATE, "advance_async: the previous step was not waited for");
+    CUDA_TRY(cudaSetDevice(c->device));
+    int rc;
+    if ((rc = sync_dt_def(c, dt_def))) return rc;
+    if ((rc = apply_staged_runoff(c))) return rc;
+    if ((rc = launch_outer(c))) return rc;
+    CUDA_TRY(cudaGetLastError());
+    c->launched = true;
+    return CMF_OK;
+}
+
+int cmf_gpu_ctx_wait(cmf_gpu_ctx *c, int32_t *nt_out, double *dt_out, cmf_budget *b) {
+    if (!c) return set_err(CMF_E_STATE, "no context");
+    if (!c->launched) return set_err(CMF_E_STATE, "wait: no outer step was launched by advance_async");
+    CUDA_TRY(cudaSetDevice(c->device));
+    c->launched = false;
+    return finish_outer(c, nt_out, dt_out, b);
+}
+
 
 int cmf_gpu_ctx_advance_device(cmf_gpu_ctx *c, double dt_def, int32_t ksteps, const double *runoff_dev, int64_t stride) {
     if (!c || ksteps < 0) return set_err(CMF_E_ARG, "bad argument");
@@ -1578,35 +1679,47 @@ int cmf_gpu_ctx_get_diag(cmf_gpu_ctx *c, const cmf_diag_ptrs *p) {
     if (!c || !p) return set_err(CMF_E_ARG, "null argument");
     CUDA_TRY(cudaSetDevice(c->device));
     const size_t MN = (size_t)c->dims.nmembers * c->dims.nseqall;
-    const size_t MP = (size_t)c->dims.nmembers * c->net.P;
-    const size_t MPL = MP * c->net.Lp;
-    cmf::State &s = c->st;
     int rc;
-    struct { double *dst; const double *src; size_t n; } t[] = {
-        {p->rivdph, s.rivdph, MN}, {p->flddph, s.flddph, MN}, {p->fldfrc, s.fldfrc, MN}, {p->fldare, s.fldare, MN},
-        {p->sfcelv, s.sfcelv, MN}, {p->storge, s.storge, MN}, {p->rivvel, s.rivvel, MN}, {p->rivinf, s.rivinf, MN},
-        {p->fldinf, s.fldinf, MN}, {p->pthout, s.pthout, MN}, {p->outflw, s.outflw, MN},
-        {p->pthflwsum, s.pthsum, MP}, {p->levdph, c->opts.llevee ? s.levdph : nullptr, MN}};
-    for (auto &x : t) {
-        if (!x.dst || !x.src || !x.n) continue;
+    for (const DiagField &x : diag_fields(c, p))
         if ((rc = d2h(c, x.dst, x.src, x.n))) return rc;
-    }
-    if (c->opts.ldiag) {
-        struct { double *dst; const double *src; size_t n; } a[] = {
-            {p->rivout_aavg, s.a_rivout, MN}, {p->fldout_aavg, s.a_fldout, MN}, {p->outflw_aavg, s.a_outflw, MN},
-            {p->rivvel_aavg, s.a_rivvel, MN}, {p->pthout_aavg, s.a_pthout, MN}, {p->runoff_aavg, s.a_runoff, MN},
-            {p->daminf_aavg, c->opts.ldamout ? s.a_daminf : nullptr, MN}, {p->storge_amax, s.m_storge, MN},
-            {p->outflw_amax, s.m_outflw, MN}, {p->rivdph_amax, s.m_rivdph, MN}, {p->pthflw_aavg, s.a_pthflw, MPL},
-            {p->pthflwsum_aavg, s.a_pthsum, MP}};
-        for (auto &x : a) {
-            if (!x.dst || !x.src || !x.n) continue;
-            if ((rc = d2h(c, x.dst, x.src, x.n))) return rc;
-        }
-    }
     // GDWRTN/ROFSUB are zero without groundwater delay or LROSPLIT (both refused)
     if (p->gdwrtn_aavg) std::memset(p->gdwrtn_aavg, 0, MN * sizeof(double));
     if (p->rofsub_aavg) std::memset(p->rofsub_aavg, 0, MN * sizeof(double));
     CUDA_TRY(cudaStreamSynchronize(c->stream));
+    return CMF_OK;
+}
+
+// The named diagnostics as they stand after the steps enqueued so far are copied on the device
+// into staging buffers (ordered before any later step), then to the host buffers on the copy
+// stream, overlapping the next step; cmf_gpu_ctx_io_wait blocks until they landed.
+int cmf_gpu_ctx_get_diag_async(cmf_gpu_ctx *c, const cmf_diag_ptrs *p) {
+    if (!c || !p) return set_err(CMF_E_ARG, "null argument");
+    if (p->gdwrtn_aavg || p->rofsub_aavg) return set_err(CMF_E_ARG, "get_diag_async: GDWRTN/ROFSUB are not staged");
+    CUDA_TRY(cudaSetDevice(c->device));
+    int rc;
+    if ((rc = io_setup(c))) return rc;
+    if (c->ostage.empty()) c->ostage.assign(kDiagSlots, nullptr);
+    const std::vector<DiagField> fs = diag_fields(c, p);
+    // the staging buffers are free once the previous read-back landed
+    CUDA_TRY(cudaStreamWaitEvent(c->stream, c->ev_out_done, 0));
+    for (const DiagField &x : fs) {
+        double *&st = c->ostage[x.slot];
+        if (!st && (rc = c->alloc(&st, x.n))) return rc;
+        CUDA_TRY(cudaMemcpyAsync(st, x.src, x.n * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+    }
+    CUDA_TRY(cudaEventRecord(c->ev_out_staged, c->stream));
+    CUDA_TRY(cudaStreamWaitEvent(c->io, c->ev_out_staged, 0));
+    for (const DiagField &x : fs)
+        CUDA_TRY(cudaMemcpyAsync(x.dst, c->ostage[x.slot], x.n * sizeof(double), cudaMemcpyDeviceToHost, c->io));
+    CUDA_TRY(cudaEventRecord(c->ev_out_done, c->io));
+    return CMF_OK;
+}
+
+int cmf_gpu_ctx_io_wait(cmf_gpu_ctx *c) {
+    if (!c) return set_err(CMF_E_STATE, "no context");
+    if (!c->io) return CMF_OK;
+    CUDA_TRY(cudaSetDevice(c->device));
+    CUDA_TRY(cudaStreamSynchronize(c->io));
     return CMF_OK;
 }
 

@@ -183,6 +183,23 @@ int cmf_gpu_ctx_physics_advance(cmf_gpu_ctx *ctx, double dt_def, int32_t *nt_out
                                 cmf_budget *budget_out);
 int cmf_gpu_ctx_get_diag(cmf_gpu_ctx *ctx, const cmf_diag_ptrs *dg);
 
+/* Pipelined host I/O for C, C++ and Python hosts (the Fortran shim keeps the calls above): the
+ * next step's runoff is uploaded while the current step runs, and a finished step's diagnostics
+ * are read back while the next one runs.  Host buffers should be pinned for the copies to overlap.
+ *   put_runoff_async  copies D2RUNOFF of the next outer step into a device staging buffer on a
+ *                     copy stream; the next advance (async or not) makes it D2RUNOFF;
+ *   advance_async     launches one outer step and returns; one step at a time;
+ *   wait              finishes the launched step (NT, DT, budgets, statuses as physics_advance);
+ *   get_diag_async    stages the named diagnostics as they stand after the steps enqueued so far
+ *                     (device copies ordered before any later step), then copies them to the host
+ *                     buffers on the copy stream (GDWRTN/ROFSUB not accepted);
+ *   io_wait           blocks until every staged read-back has landed in the host buffers. */
+int cmf_gpu_ctx_put_runoff_async(cmf_gpu_ctx *ctx, const double *runoff);
+int cmf_gpu_ctx_advance_async(cmf_gpu_ctx *ctx, double dt_def);
+int cmf_gpu_ctx_wait(cmf_gpu_ctx *ctx, int32_t *nt_out, double *dt_out, cmf_budget *budget_out);
+int cmf_gpu_ctx_get_diag_async(cmf_gpu_ctx *ctx, const cmf_diag_ptrs *dg);
+int cmf_gpu_ctx_io_wait(cmf_gpu_ctx *ctx);
+
 /* Device-resident pipeline (no host round trip): runoff already in device memory, ksteps outer
  * steps enqueued on the context's stream; runoff_dev holds ksteps consecutive [nmembers][NSEQMAX]
  * fields (or one field reused when runoff_stride is 0). */
