@@ -466,6 +466,11 @@ class PhysicsGPU:
     def io_wait(self) -> None:
         check(self.lib.cmf_gpu_ctx_io_wait(self.h), "io_wait")
 
+    def pipeline(self, outs: list) -> "Pipeline":
+        """The pipelined calls of a step loop with their ctypes arguments built once: `outs` are
+        dicts of float64 host arrays (named diagnostics), one dict per read-back buffer."""
+        return Pipeline(self, outs)
+
     def get_diag_fields(self, out: dict) -> dict:
         """Copies only the named diagnostics into the caller's float64 arrays (others skipped)."""
         dp = _abi.DiagPtrs()
@@ -538,3 +543,41 @@ class PhysicsBatch:
         except Exception:
             pass
 
+
+class Pipeline:
+    """Per-step calls of a pipelined loop (advance_async / wait / get_diag_async / io_wait) with
+    their argument structs prebuilt, so that the host's part of the gap between two steps is a few
+    C calls."""
+
+    def __init__(self, g: PhysicsGPU, outs: list):
+        self.g, self.lib, self.h, self.dt = g, g.lib, g.h, g.host.dt
+        self.nt = np.zeros(g.M, dtype=np.int32)
+        self.dtv = np.zeros(g.M)
+        self.b = (_abi.Budget * g.M)()
+        self._nt_p, self._dt_p = self.nt.ctypes.data_as(_abi.i32p), self.dtv.ctypes.data_as(_abi.f64p)
+        self.outs = outs
+        self.dps = []
+        for out in outs:
+            dp = _abi.DiagPtrs()
+            for n, a in out.items():
+                if n not in _abi.DIAG_FIELDS or a.dtype != np.float64 or not a.flags.c_contiguous:
+                    raise ValueError(n)
+                setattr(dp, n, a.ctypes.data_as(_abi.f64p))
+            self.dps.append(dp)
+
+    def advance(self) -> None:
+        check(self.lib.cmf_gpu_ctx_advance_async(self.h, self.dt), "advance_async")
+
+    def wait(self) -> np.ndarray:
+        """Finishes the launched step; returns NT per member (DT in .dtv, budgets via budget())."""
+        check(self.lib.cmf_gpu_ctx_wait(self.h, self._nt_p, self._dt_p, self.b), "wait")
+        return self.nt
+
+    def budget(self, m: int) -> dict:
+        return {f: getattr(self.b[m], f) for f in _abi.BUDGET_FIELDS}
+
+    def read_back(self, slot: int) -> None:
+        check(self.lib.cmf_gpu_ctx_get_diag_async(self.h, C.byref(self.dps[slot])), "get_diag_async")
+
+    def io_wait(self) -> None:
+        check(self.lib.cmf_gpu_ctx_io_wait(self.h), "io_wait")

@@ -98,11 +98,16 @@ struct cmf_gpu_ctx {
     cudaEvent_t ev_in = nullptr, ev_stage_free = nullptr, ev_out_staged = nullptr, ev_out_done = nullptr;
     double *rstage = nullptr;
     bool in_pending = false;    // a runoff field waits in rstage for the next advance
-    bool launched = false;      // an outer step was launched by advance_async and not yet waited for
+    // outer steps launched by advance_async and not yet waited for (at most two): each launch
+    // copies the control blocks after its step into its own pinned ring slot
+    int inflight = 0, head = 0;
+    cmf::MemberCtl *ring[2] = {nullptr, nullptr};
+    cudaEvent_t ev_ctl[2] = {nullptr, nullptr};
     std::vector<double *> ostage;   // per diagnostic field (DIAG order), allocated on first request
     int64_t launches = 0;
     // host staging for the per-member control block
     std::vector<cmf::MemberCtl> hctl;
+    cmf::MemberCtl *hctl_pin = nullptr;   // pinned landing buffer of the per-step read-back
     // sea-level boundary inputs (allocated on first use)
     double *bnd_sealev = nullptr, *bnd_meansl = nullptr;
     // runoff interpolation (input matrix or nearest cell) and the staging of runoff fields
@@ -700,9 +705,14 @@ int launch_outer(cmf_gpu_ctx *c) {
     return tune_end(c, trial);
 }
 
+// the per-member control blocks after a step, read through a pinned buffer (a direct DMA, no
+// staging through pageable memory: this read sits between one outer step and the next launch)
 int read_ctl(cmf_gpu_ctx *c) {
-    CUDA_TRY(cudaMemcpyAsync(c->hctl.data(), c->st.ctl, c->hctl.size() * sizeof(cmf::MemberCtl), cudaMemcpyDeviceToHost, c->stream));
+    const size_t bytes = c->hctl.size() * sizeof(cmf::MemberCtl);
+    if (!c->hctl_pin) CUDA_TRY(cudaMallocHost(&c->hctl_pin, bytes));
+    CUDA_TRY(cudaMemcpyAsync(c->hctl_pin, c->st.ctl, bytes, cudaMemcpyDeviceToHost, c->stream));
     CUDA_TRY(cudaStreamSynchronize(c->stream));
+    std::memcpy(c->hctl.data(), c->hctl_pin, bytes);
     return CMF_OK;
 }
 
@@ -738,9 +748,8 @@ int d2h(cmf_gpu_ctx *c, T *dst, const T *src, size_t n) {
 }
 
 // state arrays of the boundary are [M][NSEQMAX]; the device keeps [M][NSEQALL] (== NSEQMAX here)
-int finish_outer(cmf_gpu_ctx *c, int32_t *nt_out, double *dt_out, cmf_budget *b) {
-    int rc = read_ctl(c);
-    if (rc) return rc;
+// NT, DT, budgets and statuses of the step whose control blocks are in c->hctl
+int process_ctl(cmf_gpu_ctx *c, int32_t *nt_out, double *dt_out, cmf_budget *b) {
     if (c->persist) {
         int berr = 0;
         CUDA_TRY(cudaMemcpyAsync(&berr, &c->st.loop->bar_err, sizeof berr, cudaMemcpyDeviceToHost, c->stream));
@@ -771,6 +780,10 @@ int finish_outer(cmf_gpu_ctx *c, int32_t *nt_out, double *dt_out, cmf_budget *b)
         int bad = -1;
         for (size_t m = 0; m < c->hctl.size(); m++)
             if (c->hctl[m].err && bad < 0) bad = (int)m;
+        // clear the error words on the device: after every step already launched (drained first),
+        // from the control blocks as they stand then
+        int rc = read_ctl(c);
+        if (rc) return rc;
         for (auto &x : c->hctl) x.err = 0;
         CUDA_TRY(cudaMemcpyAsync(c->st.ctl, c->hctl.data(), c->hctl.size() * sizeof(cmf::MemberCtl), cudaMemcpyHostToDevice, c->stream));
         CUDA_TRY(cudaStreamSynchronize(c->stream));
@@ -783,6 +796,12 @@ int finish_outer(cmf_gpu_ctx *c, int32_t *nt_out, double *dt_out, cmf_budget *b)
     return CMF_OK;
 }
 
+int finish_outer(cmf_gpu_ctx *c, int32_t *nt_out, double *dt_out, cmf_budget *b) {
+    int rc = read_ctl(c);
+    if (rc) return rc;
+    return process_ctl(c, nt_out, dt_out, b);
+}
+
 cmf_gpu_ctx *g_default = nullptr;
 constexpr int kTuneWarm = 4;   // outer steps before the autotuner's first candidate
 
@@ -792,8 +811,9 @@ constexpr int kTuneWarm = 4;   // outer steps before the autotuner's first candi
 int io_setup(cmf_gpu_ctx *c) {
     if (c->io) return CMF_OK;
     CUDA_TRY(cudaStreamCreateWithFlags(&c->io, cudaStreamNonBlocking));
-    for (cudaEvent_t *e : {&c->ev_in, &c->ev_stage_free, &c->ev_out_staged, &c->ev_out_done})
+    for (cudaEvent_t *e : {&c->ev_in, &c->ev_stage_free, &c->ev_out_staged, &c->ev_out_done, &c->ev_ctl[0], &c->ev_ctl[1]})
         CUDA_TRY(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+    for (auto &r : c->ring) CUDA_TRY(cudaMallocHost(&r, c->hctl.size() * sizeof(cmf::MemberCtl)));
     int rc;
     if ((rc = c->alloc(&c->rstage, (size_t)c->dims.nmembers * c->dims.nseqall))) return rc;
     return CMF_OK;
@@ -1004,8 +1024,11 @@ int cmf_gpu_destroy(cmf_gpu_ctx *c) {
     for (void *p : c->allocs) cudaFree(p);
     if (c->rgrid) cudaFree(c->rgrid);
     if (c->io) cudaStreamSynchronize(c->io);
-    for (cudaEvent_t e : {c->ev_in, c->ev_stage_free, c->ev_out_staged, c->ev_out_done})
+    if (c->hctl_pin) cudaFreeHost(c->hctl_pin);
+    for (cudaEvent_t e : {c->ev_in, c->ev_stage_free, c->ev_out_staged, c->ev_out_done, c->ev_ctl[0], c->ev_ctl[1]})
         if (e) cudaEventDestroy(e);
+    for (auto *r : c->ring)
+        if (r) cudaFreeHost(r);
     if (c->io) cudaStreamDestroy(c->io);
     if (c->stream) cudaStreamDestroy(c->stream);
     if (c->l2_window) {
@@ -1265,11 +1288,11 @@ int cmf_gpu_ctx_physics_advance(cmf_gpu_ctx *c, double dt_def, int32_t *nt_out, 
     if (!c) return set_err(CMF_E_STATE, "no context");
     CUDA_TRY(cudaSetDevice(c->device));
     int rc;
+    if (c->inflight) return set_err(CMF_E_STATE, "physics_advance: steps launched by advance_async are not waited for");
     if ((rc = sync_dt_def(c, dt_def))) return rc;
     if ((rc = apply_staged_runoff(c))) return rc;
     if ((rc = launch_outer(c))) return rc;
     CUDA_TRY(cudaGetLastError());
-    c->launched = false;
     return finish_outer(c, nt_out, dt_out, b);
 }
 
@@ -1289,23 +1312,32 @@ int cmf_gpu_ctx_put_runoff_async(cmf_gpu_ctx *c, const double *runoff) {
 
 int cmf_gpu_ctx_advance_async(cmf_gpu_ctx *c, double dt_def) {
     if (!c) return set_err(CMF_E_STATE, "no context");
-    if (c->launched) return set_err(CMF_E_STATE, "advance_async: the previous step was not waited for");
+    if (c->inflight >= 2) return set_err(CMF_E_STATE, "advance_async: two steps are in flight; wait for the oldest first");
     CUDA_TRY(cudaSetDevice(c->device));
     int rc;
+    if ((rc = io_setup(c))) return rc;
     if ((rc = sync_dt_def(c, dt_def))) return rc;
     if ((rc = apply_staged_runoff(c))) return rc;
     if ((rc = launch_outer(c))) return rc;
     CUDA_TRY(cudaGetLastError());
-    c->launched = true;
+    const int slot = (c->head + c->inflight) % 2;
+    CUDA_TRY(cudaMemcpyAsync(c->ring[slot], c->st.ctl, c->hctl.size() * sizeof(cmf::MemberCtl), cudaMemcpyDeviceToHost,
+                             c->stream));
+    CUDA_TRY(cudaEventRecord(c->ev_ctl[slot], c->stream));
+    c->inflight++;
     return CMF_OK;
 }
 
 int cmf_gpu_ctx_wait(cmf_gpu_ctx *c, int32_t *nt_out, double *dt_out, cmf_budget *b) {
     if (!c) return set_err(CMF_E_STATE, "no context");
-    if (!c->launched) return set_err(CMF_E_STATE, "wait: no outer step was launched by advance_async");
+    if (!c->inflight) return set_err(CMF_E_STATE, "wait: no outer step was launched by advance_async");
     CUDA_TRY(cudaSetDevice(c->device));
-    c->launched = false;
-    return finish_outer(c, nt_out, dt_out, b);
+    const int slot = c->head;
+    c->head = (c->head + 1) % 2;
+    c->inflight--;
+    CUDA_TRY(cudaEventSynchronize(c->ev_ctl[slot]));
+    std::memcpy(c->hctl.data(), c->ring[slot], c->hctl.size() * sizeof(cmf::MemberCtl));
+    return process_ctl(c, nt_out, dt_out, b);
 }
 
 

@@ -188,8 +188,11 @@ int cmf_gpu_ctx_get_diag(cmf_gpu_ctx *ctx, const cmf_diag_ptrs *dg);
  * are read back while the next one runs.  Host buffers should be pinned for the copies to overlap.
  *   put_runoff_async  copies D2RUNOFF of the next outer step into a device staging buffer on a
  *                     copy stream; the next advance (async or not) makes it D2RUNOFF;
- *   advance_async     launches one outer step and returns; one step at a time;
- *   wait              finishes the launched step (NT, DT, budgets, statuses as physics_advance);
+ *   advance_async     launches one outer step and returns; at most two steps in flight, so the
+ *                     next step is queued while the host handles the previous one;
+ *   wait              finishes the oldest launched step (NT, DT, budgets, statuses as
+ *                     physics_advance; after a failed step the device is drained before its error
+ *                     word is cleared); physics_advance refuses while steps are in flight;
  *   get_diag_async    stages the named diagnostics as they stand after the steps enqueued so far
  *                     (device copies ordered before any later step), then copies them to the host
  *                     buffers on the copy stream (GDWRTN/ROFSUB not accepted);

@@ -39,24 +39,48 @@ def test_pipelined_io_equals_synchronous(case_dirs):
         got.append(pipe.wait())
         pipe.get_diag_fields_async(outs[k])
     pipe.io_wait()
+    # two steps in flight: step k+1 is queued before the host waits for step k
+    two = PhysicsGPU(h)
+    outs2 = [{f: torch.zeros(h.dims.nseqall, dtype=torch.float64).pin_memory().numpy() for f in FIELDS} for _ in range(K)]
+    got2 = []
+    two.put_runoff_async(series[0])
+    two.advance_async()
+    two.get_diag_fields_async(outs2[0])
+    two.put_runoff_async(series[1])
+    two.advance_async()
+    for k in range(K):
+        got2.append(two.wait())
+        two.io_wait()                                  # step k's read-back (step k+1's is not queued yet)
+        if k + 1 < K:
+            two.get_diag_fields_async(outs2[k + 1])    # after step k+1's launch, before step k+2's
+        if k + 2 < K:
+            two.put_runoff_async(series[k + 2])
+            two.advance_async()
+    two.io_wait()
     for k in range(K):
         nt, dt, bud, out = ref[k]
+        for nt2, dt2, bud2 in (got[k], got2[k]):
+            assert np.array_equal(nt, nt2) and np.array_equal(dt, dt2), k
+            assert bud == bud2, k
+        for f in FIELDS:
+            assert np.array_equal(out[f].view(np.uint64), outs2[k][f].view(np.uint64)), (k, f)
         nt2, dt2, bud2 = got[k]
         assert np.array_equal(nt, nt2) and np.array_equal(dt, dt2), k
         assert bud == bud2, k
         for f in FIELDS:
             assert np.array_equal(out[f].view(np.uint64), outs[k][f].view(np.uint64)), (k, f)
-    s1, s2 = sync.get_state(), pipe.get_state()
+    s1, s2, s3 = sync.get_state(), pipe.get_state(), two.get_state()
     for key in ("rivsto", "fldsto", "rivout", "fldout"):
-        assert np.array_equal(s1[key], s2[key]), key
+        assert np.array_equal(s1[key], s2[key]) and np.array_equal(s1[key], s3[key]), key
     sync.close()
     pipe.close()
+    two.close()
 
 
 @pytest.mark.gpu
 def test_pipelined_io_call_order(case_dirs):
-    """One launched step at a time; wait needs a launched step; a synchronous put_runoff replaces
-    a staged field."""
+    """At most two launched steps; wait needs a launched step; the synchronous advance refuses
+    while steps are in flight; a synchronous put_runoff replaces a staged field."""
     from cmf_b200 import HostModel, PhysicsGPU
 
     h = HostModel(case_dirs["cfg1s"])
@@ -66,15 +90,20 @@ def test_pipelined_io_call_order(case_dirs):
         g.wait()
     g.put_runoff(r)
     g.advance_async()
+    g.advance_async()
     with pytest.raises(RuntimeError):
         g.advance_async()
+    with pytest.raises(RuntimeError):
+        g.advance()
     g.wait()
+    g.wait()
+    ref.put_runoff(r)
+    ref.advance()
+    ref.advance()
     # a staged field, then a synchronous one: the synchronous field is the one the step uses
     g.put_runoff_async(np.zeros_like(r))
     g.put_runoff(r)
     g.advance()
-    ref.put_runoff(r)
-    ref.advance()
     ref.put_runoff(r)
     ref.advance()
     assert np.array_equal(g.get_state()["rivsto"], ref.get_state()["rivsto"])
