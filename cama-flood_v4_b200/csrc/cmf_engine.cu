@@ -92,9 +92,11 @@ struct cmf_gpu_ctx {
     cudaGraphExec_t exec = nullptr;
     cudaGraphConditionalHandle cond{};
     double dt_def_dev = -1.0;
-    // pipelined host I/O (created on first use): a copy stream, the runoff staging buffer, the
-    // staging of diagnostics read back while the next step runs, and their events
-    cudaStream_t io = nullptr;
+    // pipelined host I/O (created on first use): copy streams for uploads (io) and read-backs
+    // (io_out; separate, so that an upload never queues behind a read-back that waits for a step),
+    // the runoff staging buffer, the staging of diagnostics read back while the next step runs,
+    // and their events
+    cudaStream_t io = nullptr, io_out = nullptr;
     cudaEvent_t ev_in = nullptr, ev_stage_free = nullptr, ev_out_staged = nullptr, ev_out_done = nullptr;
     double *rstage = nullptr;
     bool in_pending = false;    // a runoff field waits in rstage for the next advance
@@ -811,6 +813,7 @@ constexpr int kTuneWarm = 4;   // outer steps before the autotuner's first candi
 int io_setup(cmf_gpu_ctx *c) {
     if (c->io) return CMF_OK;
     CUDA_TRY(cudaStreamCreateWithFlags(&c->io, cudaStreamNonBlocking));
+    CUDA_TRY(cudaStreamCreateWithFlags(&c->io_out, cudaStreamNonBlocking));
     for (cudaEvent_t *e : {&c->ev_in, &c->ev_stage_free, &c->ev_out_staged, &c->ev_out_done, &c->ev_ctl[0], &c->ev_ctl[1]})
         CUDA_TRY(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
     for (auto &r : c->ring) CUDA_TRY(cudaMallocHost(&r, c->hctl.size() * sizeof(cmf::MemberCtl)));
@@ -1024,12 +1027,14 @@ int cmf_gpu_destroy(cmf_gpu_ctx *c) {
     for (void *p : c->allocs) cudaFree(p);
     if (c->rgrid) cudaFree(c->rgrid);
     if (c->io) cudaStreamSynchronize(c->io);
+    if (c->io_out) cudaStreamSynchronize(c->io_out);
     if (c->hctl_pin) cudaFreeHost(c->hctl_pin);
     for (cudaEvent_t e : {c->ev_in, c->ev_stage_free, c->ev_out_staged, c->ev_out_done, c->ev_ctl[0], c->ev_ctl[1]})
         if (e) cudaEventDestroy(e);
     for (auto *r : c->ring)
         if (r) cudaFreeHost(r);
     if (c->io) cudaStreamDestroy(c->io);
+    if (c->io_out) cudaStreamDestroy(c->io_out);
     if (c->stream) cudaStreamDestroy(c->stream);
     if (c->l2_window) {
         std::lock_guard<std::mutex> lk(g_l2_mu);
@@ -1740,10 +1745,10 @@ int cmf_gpu_ctx_get_diag_async(cmf_gpu_ctx *c, const cmf_diag_ptrs *p) {
         CUDA_TRY(cudaMemcpyAsync(st, x.src, x.n * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
     }
     CUDA_TRY(cudaEventRecord(c->ev_out_staged, c->stream));
-    CUDA_TRY(cudaStreamWaitEvent(c->io, c->ev_out_staged, 0));
+    CUDA_TRY(cudaStreamWaitEvent(c->io_out, c->ev_out_staged, 0));
     for (const DiagField &x : fs)
-        CUDA_TRY(cudaMemcpyAsync(x.dst, c->ostage[x.slot], x.n * sizeof(double), cudaMemcpyDeviceToHost, c->io));
-    CUDA_TRY(cudaEventRecord(c->ev_out_done, c->io));
+        CUDA_TRY(cudaMemcpyAsync(x.dst, c->ostage[x.slot], x.n * sizeof(double), cudaMemcpyDeviceToHost, c->io_out));
+    CUDA_TRY(cudaEventRecord(c->ev_out_done, c->io_out));
     return CMF_OK;
 }
 
@@ -1751,7 +1756,7 @@ int cmf_gpu_ctx_io_wait(cmf_gpu_ctx *c) {
     if (!c) return set_err(CMF_E_STATE, "no context");
     if (!c->io) return CMF_OK;
     CUDA_TRY(cudaSetDevice(c->device));
-    CUDA_TRY(cudaStreamSynchronize(c->io));
+    CUDA_TRY(cudaStreamSynchronize(c->io_out));
     return CMF_OK;
 }
 
