@@ -386,6 +386,15 @@ def gpu_arm(args) -> int:
     outs = [{"outflw_aavg": torch.zeros(M * N, dtype=torch.float64).pin_memory().numpy()} for _ in range(2)]
     rin = [runoff_host[base + k].numpy() for k in range(K)]
     io = g.pipeline(outs)            # the per-step calls with their ctypes arguments built once
+    # untimed: two pipelined steps create the copy streams, pinned rings and staging buffers (a
+    # one-time setup, like the context itself); then the saved state again
+    for w in range(2):
+        g.put_runoff_async(rin[w % K])
+        io.advance()
+        io.wait()
+        io.read_back(w % 2)
+        io.io_wait()
+    g.set_state(snapshot)
     e2e_sub = 0
     budgets = []
     if ws > 1:
