@@ -20,7 +20,7 @@ PARETO = ((2, 0.05), (16, 0.05), (64, 0.05), (256, 0.05), (256, 0.02))
 
 
 def measure(host, device, members: int = 256, days: int = 2, judge_slots: int = 2, train_members: int = 8,
-            train_hours: int = 96, train_iters: int = 6000, train_batch: int = 16384, train_noise: float = 0.02,
+            train_hours: int = 192, train_iters: int = 6000, train_batch: int = 16384, train_noise: float = 0.02,
             cells_per_snapshot: int | None = 65536, seed: int = 100, gauges: int = 100, tol_rel: float = 0.05,
             spinup: int = 24, forcing_distinct: int = 8, snapshot_weighting: str = "uniform",
             trajectory_forcing: int | None = None, pareto=PARETO) -> dict:
