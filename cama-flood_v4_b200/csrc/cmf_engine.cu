@@ -1351,6 +1351,9 @@ int cmf_gpu_ctx_advance_device(cmf_gpu_ctx *c, double dt_def, int32_t ksteps, co
     CUDA_TRY(cudaSetDevice(c->device));
     int rc;
     if ((rc = sync_dt_def(c, dt_def))) return rc;
+    // a field staged by put_runoff_async: the first step's runoff unless device fields are given
+    if (runoff_dev) c->in_pending = false;
+    else if (ksteps > 0 && (rc = apply_staged_runoff(c))) return rc;
     const size_t MN = (size_t)c->dims.nmembers * c->dims.nseqall;
     for (int k = 0; k < ksteps; k++) {
         if (runoff_dev)
