@@ -99,6 +99,8 @@ typedef struct {
     double dam_miss;
     int last_nt;
     double last_dt, last_dtmin;
+    void (*substep_hook)(void *ctx, int it);   /* tests only: sees each sub-step's fields */
+    void *substep_ctx;
     char err[256];
 } orc_model;
 
@@ -1338,6 +1340,7 @@ int orc_substeps(orc_model *m, double dt_min, int *nt_out, double *dt_out) {
         if (m->lpthout) memcpy(m->pthflw_pre, m->pthflw, sizeof(double) * (size_t)m->npthout * m->npthlev);
         calc_stonxt(m, DT);
         physics_fldstg(m);
+        if (m->substep_hook) m->substep_hook(m->substep_ctx, it);
         diag_avemax_adpstp(m, DT);
     }
     diag_getave_adpstp(m);
@@ -1345,6 +1348,13 @@ int orc_substeps(orc_model *m, double dt_min, int *nt_out, double *dt_out) {
     if (nt_out) *nt_out = NT;
     if (dt_out) *dt_out = DT;
     return 0;
+}
+
+/* A test hook called after each sub-step's stage update, before CMF_DIAG_AVEMAX_ADPSTP reads the
+ * sub-step's fields (NULL removes it). */
+void orc_set_substep_hook(orc_model *m, void (*fn)(void *, int), void *ctx) {
+    m->substep_hook = fn;
+    m->substep_ctx = ctx;
 }
 
 int orc_physics_advance(orc_model *m, int *nt_out, double *dt_out) {
@@ -1681,6 +1691,7 @@ double *orc_darray(orc_model *m, const char *name, int *len) {
         {"pthflw_pre", m->pthflw_pre, PL}, {"damsto", m->damsto, N}, {"daminf", m->daminf, N}, {"levsto", m->levsto, N},
         {"rivinf", m->rivinf, N}, {"rivdph", m->rivdph, N}, {"rivvel", m->rivvel, N}, {"fldinf", m->fldinf, N},
         {"flddph", m->flddph, N}, {"fldfrc", m->fldfrc, N}, {"fldare", m->fldare, N}, {"pthout", m->pthout, N},
+        {"pthinf", m->pthinf, N},
         {"sfcelv", m->sfcelv, N}, {"outflw", m->outflw, N}, {"storge", m->storge, N}, {"levdph", m->levdph, N},
         {"pthflwsum", m->pthflwsum, P}, {"rate", m->rate, N}, {"stoout", m->stoout, N},
         {"rivout_aavg", m->rivout_a, N}, {"fldout_aavg", m->fldout_a, N}, {"outflw_aavg", m->outflw_a, N},

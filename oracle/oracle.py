@@ -57,8 +57,12 @@ def _lib(omp: bool = False):
     lib.orc_diag_output.argtypes = [C.c_void_p, C.c_int]
     lib.orc_nadd_out.argtypes = [C.c_void_p]
     lib.orc_nadd_out.restype = C.c_double
+    lib.orc_set_substep_hook.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
     _LIBS[key] = lib
     return lib
+
+
+_HOOK = C.CFUNCTYPE(None, C.c_void_p, C.c_int)
 
 
 class Oracle:
@@ -152,6 +156,16 @@ class Oracle:
         """CMF_DIAG_RESET_OUTPUT / CMF_DIAG_AVEMAX_OUTPUT / CMF_DIAG_GETAVE_OUTPUT
         (src/cmf_calc_diag_mod.F90:222-356): op = "reset", "avemax" or "getave"."""
         self.lib.orc_diag_output(self.h, {"reset": 0, "avemax": 1, "getave": 2}[op])
+
+    def on_substep(self, fn) -> None:
+        """Calls fn(it) after each sub-step's stage update, before the sub-step averages read its
+        fields (it = 1..NT); None removes the hook."""
+        if fn is None:
+            self._hook = None
+            self.lib.orc_set_substep_hook(self.h, None, None)
+            return
+        self._hook = _HOOK(lambda ctx, it: fn(it))
+        self.lib.orc_set_substep_hook(self.h, C.cast(self._hook, C.c_void_p), None)
 
     def nadd_out(self) -> float:
         return float(self.lib.orc_nadd_out(self.h))

@@ -906,6 +906,66 @@ def test_inflow_storage_update_and_stage_every_cell(case_dirs, tmp_path):
     assert np.count_nonzero(got["fldsto"]) > 0.5 * N
 
 
+def test_substep_diagnostics_known_answer(case_dirs):
+    """CMF_DIAG_RESET/AVEMAX/GETAVE_ADPSTP (src/cmf_calc_diag_mod.F90:50-221) in the oracle: each
+    sub-step's discharges, velocity, runoff, dam inflow and path flows are captured after its stage
+    update (the point CMF_PHYSICS_ADVANCE calls the diagnostics, src/cmf_ctrl_physics_mod.F90:139),
+    and the outer step's sums, maxima and averages are restated here in the reference's operation
+    order, bit for bit, over spun-up outer steps of the stress case (several sub-steps each)."""
+    from oracle import Oracle
+
+    o = Oracle(case_dirs["stress"])
+    series = list(runoff_series(o.d("grarea"), "stress", 10, hourly=True))
+    avg = ["rivout", "fldout", "rivvel", "outflw", "runoff"] + (["daminf"] if o.ndam else [])
+    mx = ["storge", "rivdph"]
+    cap = avg + mx + ["pthout", "pthinf", "pthflw"]
+    sub = []
+    o.on_substep(lambda it: sub.append({f: o.d(f) for f in cap}))
+    P, Lp = o.npthout, o.npthlev
+    nts = []
+    for r in series:
+        sub.clear()
+        o.put_runoff(r)
+        nt, DT = o.advance()
+        assert len(sub) == nt
+        nts.append(nt)
+        nadd = 0.0
+        for _ in range(nt):
+            nadd = nadd + DT
+        assert o.budget()["nadd"] == nadd
+        z = np.zeros(o.nseqmax)
+        for f in avg:
+            acc = z
+            for v in sub:
+                acc = acc + v[f] * DT
+            assert np.array_equal(o.d(f + "_aavg").view(np.int64), (acc / nadd).view(np.int64)), f
+        acc = z
+        for v in sub:
+            acc = (acc + v["pthout"] * DT) - v["pthinf"] * DT
+        assert np.array_equal(o.d("pthout_aavg").view(np.int64), (acc / nadd).view(np.int64))
+        for f in mx + ["outflw"]:
+            m = z
+            for v in sub:
+                x = np.abs(v[f]) if f == "outflw" else v[f]
+                m = np.where(m >= x, m, x)               # MAX(accumulator, value)
+            assert np.array_equal(o.d(f + "_amax").view(np.int64), m.view(np.int64)), f
+        acc = np.zeros(P * Lp)
+        for v in sub:
+            acc = acc + v["pthflw"] * DT
+        pavg = acc / nadd
+        assert np.array_equal(o.d("pthflw_aavg").view(np.int64), pavg.view(np.int64))
+        psum = np.zeros(P)
+        for lv in range(Lp):
+            psum = psum + pavg[lv * P:(lv + 1) * P]
+        assert np.array_equal(o.d("pthflwsum_aavg").view(np.int64), psum.view(np.int64))
+    o.on_substep(None)
+    # the case exercises what the averages cover: several sub-steps, floodplain flow, paths, dams
+    assert max(nts) > 1
+    assert np.count_nonzero(sub[-1]["fldout"]) > 0 and np.count_nonzero(sub[-1]["pthout"]) > 0
+    assert not o.ndam or np.count_nonzero(sub[-1]["daminf"]) > 0
+    assert np.any(sub[0]["rivdph"] > sub[-1]["rivdph"]) and np.any(sub[0]["rivdph"] < sub[-1]["rivdph"])
+
+
 def test_output_interval_diagnostics_known_answer(case_dirs):
     """CMF_DIAG_AVEMAX/GETAVE/RESET_OUTPUT (src/cmf_calc_diag_mod.F90:222-356) in the oracle: after
     each outer step the output sums gain aAVG*DT (DT = DT_DEF again, src/cmf_ctrl_physics_mod.F90:145)
