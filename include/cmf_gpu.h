@@ -205,7 +205,9 @@ int cmf_gpu_ctx_io_wait(cmf_gpu_ctx *ctx);
 
 /* Device-resident pipeline (no host round trip): runoff already in device memory, ksteps outer
  * steps enqueued on the context's stream; runoff_dev holds ksteps consecutive [nmembers][NSEQMAX]
- * fields (or one field reused when runoff_stride is 0). */
+ * fields (or one field reused when runoff_stride is 0).  With runoff_dev NULL the steps use the
+ * context's D2RUNOFF, after applying a field staged by put_runoff_async; with runoff_dev given, a
+ * staged field is discarded. */
 int cmf_gpu_ctx_advance_device(cmf_gpu_ctx *ctx, double dt_def, int32_t ksteps,
                                const double *runoff_dev, int64_t runoff_stride);
 int cmf_gpu_ctx_synchronize(cmf_gpu_ctx *ctx);
