@@ -1019,15 +1019,16 @@ int cmf_gpu_create(const cmf_dims *dims, const cmf_params *params, const cmf_map
 int cmf_gpu_destroy(cmf_gpu_ctx *c) {
     if (!c) return CMF_OK;
     cudaSetDevice(c->device);
+    // every stream drained (steps, staged uploads, read-backs) before anything they use is freed
     if (c->stream) cudaStreamSynchronize(c->stream);
+    if (c->io) cudaStreamSynchronize(c->io);
+    if (c->io_out) cudaStreamSynchronize(c->io_out);
     if (c->exec) cudaGraphExecDestroy(c->exec);
     if (c->graph) cudaGraphDestroy(c->graph);
     if (c->tune.e0) cudaEventDestroy(c->tune.e0);
     if (c->tune.e1) cudaEventDestroy(c->tune.e1);
     for (void *p : c->allocs) cudaFree(p);
     if (c->rgrid) cudaFree(c->rgrid);
-    if (c->io) cudaStreamSynchronize(c->io);
-    if (c->io_out) cudaStreamSynchronize(c->io_out);
     if (c->hctl_pin) cudaFreeHost(c->hctl_pin);
     for (cudaEvent_t e : {c->ev_in, c->ev_stage_free, c->ev_out_staged, c->ev_out_done, c->ev_ctl[0], c->ev_ctl[1]})
         if (e) cudaEventDestroy(e);
