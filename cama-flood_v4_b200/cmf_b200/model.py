@@ -398,18 +398,31 @@ class PhysicsGPU:
         """Status of the persistent kernel's bounded-wait check (CMF_E_BARRIER = 5 when it works)."""
         return int(self.lib.cmf_gpu_ctx_persist_selftest(self.h, int(wait_ns)))
 
+    def diag_len(self, name: str) -> int:
+        """Elements of the named diagnostic over all members (the host array's size)."""
+        MP = self.M * max(self.P, 1)
+        if name in ("pthflwsum", "pthflwsum_aavg"):
+            return MP
+        if name == "pthflw_aavg":
+            return MP * max(self.Lp, 1)
+        return self.M * self.N
+
+    def _diag_ptrs(self, out: dict) -> "_abi.DiagPtrs":
+        """Pointer struct for named float64 host arrays, each checked for name, type and size."""
+        dp = _abi.DiagPtrs()
+        for n, a in out.items():
+            if n not in _abi.DIAG_FIELDS or a.dtype != np.float64 or not a.flags.c_contiguous:
+                raise ValueError(n)
+            if a.size < self.diag_len(n):
+                raise ValueError(f"{n}: {a.size} elements, {self.diag_len(n)} needed")
+            setattr(dp, n, a.ctypes.data_as(_abi.f64p))
+        return dp
+
     def get_diag(self) -> dict:
         dp = _abi.DiagPtrs()
         out = {}
-        MP = self.M * max(self.P, 1)
         for n in _abi.DIAG_FIELDS:
-            if n == "pthflwsum" or n == "pthflwsum_aavg":
-                ln = MP
-            elif n == "pthflw_aavg":
-                ln = MP * max(self.Lp, 1)
-            else:
-                ln = self.M * self.N
-            a = np.zeros(ln)
+            a = np.zeros(self.diag_len(n))
             out[n] = a
             setattr(dp, n, a.ctypes.data_as(_abi.f64p))
         check(self.lib.cmf_gpu_ctx_get_diag(self.h, C.byref(dp)), "get_diag")
@@ -456,11 +469,7 @@ class PhysicsGPU:
     def get_diag_fields_async(self, out: dict) -> None:
         """Starts the read-back of the named diagnostics into the caller's float64 arrays (they
         land by io_wait(); the arrays must stay alive until then)."""
-        dp = _abi.DiagPtrs()
-        for n, a in out.items():
-            if n not in _abi.DIAG_FIELDS or a.dtype != np.float64 or not a.flags.c_contiguous:
-                raise ValueError(n)
-            setattr(dp, n, a.ctypes.data_as(_abi.f64p))
+        dp = self._diag_ptrs(out)
         check(self.lib.cmf_gpu_ctx_get_diag_async(self.h, C.byref(dp)), "get_diag_async")
 
     def io_wait(self) -> None:
@@ -473,11 +482,7 @@ class PhysicsGPU:
 
     def get_diag_fields(self, out: dict) -> dict:
         """Copies only the named diagnostics into the caller's float64 arrays (others skipped)."""
-        dp = _abi.DiagPtrs()
-        for n, a in out.items():
-            if n not in _abi.DIAG_FIELDS or a.dtype != np.float64 or not a.flags.c_contiguous:
-                raise ValueError(n)
-            setattr(dp, n, a.ctypes.data_as(_abi.f64p))
+        dp = self._diag_ptrs(out)
         check(self.lib.cmf_gpu_ctx_get_diag(self.h, C.byref(dp)), "get_diag")
         return out
 
@@ -556,14 +561,7 @@ class Pipeline:
         self.b = (_abi.Budget * g.M)()
         self._nt_p, self._dt_p = self.nt.ctypes.data_as(_abi.i32p), self.dtv.ctypes.data_as(_abi.f64p)
         self.outs = outs
-        self.dps = []
-        for out in outs:
-            dp = _abi.DiagPtrs()
-            for n, a in out.items():
-                if n not in _abi.DIAG_FIELDS or a.dtype != np.float64 or not a.flags.c_contiguous:
-                    raise ValueError(n)
-                setattr(dp, n, a.ctypes.data_as(_abi.f64p))
-            self.dps.append(dp)
+        self.dps = [g._diag_ptrs(out) for out in outs]
 
     def advance(self) -> None:
         check(self.lib.cmf_gpu_ctx_advance_async(self.h, self.dt), "advance_async")

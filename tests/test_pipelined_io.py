@@ -109,3 +109,18 @@ def test_pipelined_io_call_order(case_dirs):
     assert np.array_equal(g.get_state()["rivsto"], ref.get_state()["rivsto"])
     g.close()
     ref.close()
+
+
+def test_diag_buffers_checked_on_host():
+    """The Python API checks each named host buffer's name, type and size before the library
+    copies into it (a short buffer would be overrun by the read-back)."""
+    from cmf_b200 import PhysicsGPU
+
+    g = object.__new__(PhysicsGPU)          # host logic only: no device context
+    g.M, g.N, g.P, g.Lp, g.h = 2, 10, 3, 4, None
+    assert (g.diag_len("rivdph"), g.diag_len("pthflwsum_aavg"), g.diag_len("pthflw_aavg")) == (20, 6, 24)
+    g._diag_ptrs({"rivdph": np.zeros(20), "pthflw_aavg": np.zeros(24)})
+    for bad in ({"rivdph": np.zeros(19)}, {"rivdph": np.zeros(20, np.float32)}, {"nosuch": np.zeros(20)},
+                {"pthflw_aavg": np.zeros(23)}, {"outflw_aavg": np.zeros(40)[::2]}):
+        with pytest.raises(ValueError):
+            g._diag_ptrs(bad)
