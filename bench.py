@@ -579,101 +579,153 @@ def cfg2_arm(args) -> int:
     (50k to 2M cells, config-1 laws), every coupling step one graph launch for all domains and
     members, each member with its own adaptive DT.  Forcing: the config-1 AR(1) field of each
     domain times a per-member lognormal(0, 0.3) factor field, spatially smoothed (bilinear
-    upsampling of a 16x coarser Gaussian field), resident in HBM."""
+    upsampling of a 16x coarser Gaussian field), resident in HBM.  Under torchrun the domain x
+    member units are bin-packed over the ranks by cells x expected NT (regions.pack_units); the
+    total work is fixed (strong scaling) and each rank advances its units with one graph launch."""
+    import datetime
+
     import torch
 
-    from cmf_b200 import HostModel, PhysicsBatch, PhysicsGPU, synth
+    from cmf_b200 import HostModel, PhysicsBatch, PhysicsGPU, regions, synth
     from cmf_b200 import emulator as E
 
     ws, rank, local = dist_env()
-    if ws > 1 and rank != 0:
-        return 0
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
+    if ws > 1:
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     M, W, K = args.members, args.warmup, args.steps
-    hosts, ctxs, views, facs, gens = [], [], [], [], []
     t_gen = time.perf_counter()
-    for sp in synth.spec_config2():
-        d = os.path.join(CASE_CACHE, sp.name)
-        if not os.path.exists(os.path.join(d, "input_cmf.nam")):
-            synth.write_case(synth.make_case(sp), d + ".tmp")
-            os.rename(d + ".tmp", d)
-        hosts.append(HostModel(d))
+    specs = synth.spec_config2()
+    if rank == 0:
+        for sp in specs:
+            d = os.path.join(CASE_CACHE, sp.name)
+            if not os.path.exists(os.path.join(d, "input_cmf.nam")):
+                synth.write_case(synth.make_case(sp), d + ".tmp")
+                os.rename(d + ".tmp", d)
+    if ws > 1:
+        dist.barrier()
+    hosts = [HostModel(os.path.join(CASE_CACHE, sp.name)) for sp in specs]
     t_gen = time.perf_counter() - t_gen
+    nt_exp = [regions.expected_nt(h.map("nxtdst"), h.map("rivhgt"), h.dims.nseqriv, h.dt) for h in hosts]
+    owned = regions.pack_units([h.dims.nseqall * n for h, n in zip(hosts, nt_exp)], M, ws)[rank]
+    used, ctxs, views, facs, gens = [], [], [], [], []
     g = torch.Generator(device=dev).manual_seed(7)
     for k, h in enumerate(hosts):
-        p = PhysicsGPU(h, nmembers=M, device=local)
-        ctxs.append(p)
-        views.append(E.Features(p, np.ones(p.N)).runoff_view())
+        # every rank draws all M members' factor fields, so member m's forcing does not depend on
+        # the rank count; a rank keeps the rows of the members it owns
         z = torch.randn(M, 1, h.ny // 16 + 2, h.nx // 16 + 2, generator=g, device=dev, dtype=torch.float64)
+        if not owned[k]:
+            continue
         z = torch.nn.functional.interpolate(z, size=(h.ny, h.nx), mode="bilinear", align_corners=False)[:, 0]
         z = z[:, torch.as_tensor(h.i1seqy - 1, device=dev), torch.as_tensor(h.i1seqx - 1, device=dev)]
         z = z / z.std(dim=1, keepdim=True)
-        facs.append(torch.exp(0.3 * z - 0.045))
+        p = PhysicsGPU(h, nmembers=len(owned[k]), device=local)
+        used.append(k)
+        ctxs.append(p)
+        views.append(E.Features(p, np.ones(p.N)).runoff_view())
+        facs.append(torch.exp(0.3 * z[torch.as_tensor(owned[k], device=dev)] - 0.045))
         gens.append(synth.AR1GammaRunoff(p.N, 100 + k))
-    batch = PhysicsBatch(ctxs)
-    stream = torch.cuda.ExternalStream(batch.stream, device=dev)
+        del z
+    batch = PhysicsBatch(ctxs) if ctxs else None
+    stream = torch.cuda.ExternalStream(batch.stream, device=dev) if batch else torch.cuda.current_stream(dev)
     cur = torch.cuda.current_stream(dev)
 
-    def put(k):
-        for h, v, f, gen in zip(hosts, views, facs, gens):
-            base = np.maximum((gen.next().astype(np.float64) * h.map("grarea")) / 86400000.0, 0.0)
+    def put():
+        for k, v, f, gen in zip(used, views, facs, gens):
+            base = np.maximum((gen.next().astype(np.float64) * hosts[k].map("grarea")) / 86400000.0, 0.0)
             torch.mul(torch.from_numpy(base).to(dev)[None, :], f, out=v)
         cur.synchronize()
 
-    for k in range(SPINUP_STEPS + W):
-        put(k)
-        batch.launch()
-        batch.synchronize()
+    for _ in range(SPINUP_STEPS + W):
+        put()
+        if batch:
+            batch.launch()
+            batch.synchronize()
     c0 = [c.counters() for c in ctxs]
     ms = 0.0
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    if ws > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
     with ClockSampler(local) as clk:
-        for k in range(K):
-            put(k)
+        for _ in range(K):
+            put()
             ev[0].record(stream)
-            batch.launch()
+            if batch:
+                batch.launch()
             ev[1].record(stream)
             ev[1].synchronize()
             ms += ev[0].elapsed_time(ev[1])
+    torch.cuda.synchronize()
+    if ws > 1:
+        dist.barrier()
     c1 = [c.counters() for c in ctxs]
     secs = ms / 1e3
     cells = 0
     abytes = 0.0
-    nts = []
-    for h, p, a, b in zip(hosts, ctxs, c0, c1):
+    nts = [0.0] * len(hosts)
+    for k, p, a, b in zip(used, ctxs, c0, c1):
+        h = hosts[k]
         sub = b["member_substeps"] - a["member_substeps"]
         cells += h.dims.nseqall * sub
-        nts.append(sub / (K * M))
+        nts[k] = sub / (K * p.M)
         nlev = int(np.sum(h.map("levbassto") < 1e17)) if h.opts.llevee else 0
         pb = phase_bytes(h.dims.nseqall, int(h.map("i1upn").sum()), 0.0, p.P, p.Lp, nlev, h.dims.ndam, True)
         abytes += sum(pb.values()) * sub
+    if ws > 1:
+        t = torch.tensor([secs], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        secs = float(t.item())
+        tot = torch.tensor([float(cells), abytes], device=dev, dtype=torch.float64)
+        dist.all_reduce(tot, op=dist.ReduceOp.SUM)
+        cells, abytes = float(tot[0].item()), float(tot[1].item())
+        # member-weighted mean NT per domain over the ranks holding it
+        w = torch.tensor([nts[k] * len(owned[k]) for k in range(len(hosts))] + [len(ms_) for ms_ in owned],
+                         device=dev, dtype=torch.float64)
+        dist.all_reduce(w, op=dist.ReduceOp.SUM)
+        nd = len(hosts)
+        nts = [float(w[k].item() / w[nd + k].item()) if w[nd + k].item() else 0.0 for k in range(nd)]
+    bsizes = [c.block_size for c in ctxs]
+    if batch:
+        batch.close()
+    for c in ctxs:
+        c.close()
+    if rank != 0:
+        if ws > 1:
+            dist.destroy_process_group()
+        return 0
     peaks = measured_peaks()
     value = cells / secs
     achieved = abytes / secs / 1e9
     line = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": K, "warmup": W,
-        "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": K, "warmup": W,
+        "ms_per_step": secs * 1e3 / K, "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+        "dtype": "f64",
         "data": "synthetic (seeded config-2 domains in the reference's map formats)",
         "config": {"workload": "config2: 8 regional domains (config-1 laws), " +
                                ", ".join(str(h.dims.nseqall) for h in hosts) + " cells, "
-                               f"{M} members each, one graph launch per coupling step",
+                               f"{M} members each, one graph launch per coupling step per GPU",
                    "members": M, "cells_total": int(sum(h.dims.nseqall for h in hosts)),
                    "nt_mean_per_domain": [round(x, 2) for x in nts],
-                   "block_sizes": [c.block_size for c in ctxs], "case_generation_s": round(t_gen, 1),
+                   "nt_expected_per_domain": nt_exp,
+                   "partition": "domain x member units bin-packed over the GPUs by cells x expected NT",
+                   "units_per_gpu_rank0": [len(x) for x in owned],
+                   "block_sizes_rank0": bsizes, "case_generation_s": round(t_gen, 1),
                    "l2": "working set far above L2 (no flush needed)"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                     "frac": achieved / peaks["hbm_gbs"], "traffic": None, "kernel": "sub-step kernels (all)",
-                     "peak_source": peaks["source"] + " (hbm_gbs, burst copy)",
+                     "frac": achieved / peaks["hbm_gbs"] / ws, "traffic": None, "kernel": "sub-step kernels (all)",
+                     "peak_source": peaks["source"] + " (hbm_gbs, burst copy, per GPU)",
                      "note": "algorithmic bytes of k_flux+k_rate+k_store per member sub-step (L_bar taken as 0), "
-                             "stage/CFL and control kernels not counted"},
+                             "stage/CFL and control kernels not counted; achieved over all GPUs"},
         "clocks": clk.summary(),
         "gpu_launches": None,
     }
     print(json.dumps(line))
-    batch.close()
-    for c in ctxs:
-        c.close()
+    if ws > 1:
+        dist.destroy_process_group()
     return 0
 
 

@@ -119,3 +119,37 @@ def members_for_rank(nmembers: int, world: int, rank: int) -> list:
     base, extra = divmod(nmembers, world)
     start = rank * base + min(rank, extra)
     return list(range(start, start + base + (1 if rank < extra else 0)))
+
+
+def expected_nt(nxtdst: np.ndarray, rivhgt: np.ndarray, nseqriv: int, dt: float = 3600.0,
+                fill: float = 0.5, pcadp: float = 0.7, pdstmth: float = 10000.0, pgrv: float = 9.8) -> int:
+    """Sub-steps per outer step that CALC_ADPSTP (src/cmf_ctrl_physics_mod.F90:161-206) gives when
+    every channel holds `fill` of its bank height: DT_MIN over the cells' CFL keys
+    PCADP*DDST*(PGRV*DDPH)**(-0.5) (mouths use PDSTMTH), then NT = INT(DT/DT_MIN - 0.01) + 1.  An
+    estimate of a member's work per outer step before the run has a state of its own."""
+    n = nxtdst.size
+    ddst = np.where(np.arange(n) < nseqriv, nxtdst, pdstmth)
+    ddph = np.maximum(rivhgt * fill, 0.01)
+    dt_min = min(dt, float(np.min((pcadp * ddst) * (pgrv * ddph) ** -0.5))) if n else dt
+    return int(dt * (1.0 / dt_min) - float(np.float32(0.01))) + 1
+
+
+def pack_units(loads, nmembers: int, world: int) -> list:
+    """Members x domains over `world` ranks: unit (d, m) is member m of domain d, with weight
+    loads[d] (cells x expected NT of one member).  Greedy bin-packing, largest unit first (ties:
+    lower domain, then lower member), each unit to the rank with the least load so far (ties: lower
+    rank).  Returns, per rank, a list over domains of the member ids it owns (ascending); every unit
+    is owned once, and no rank's load exceeds the mean by more than the largest unit."""
+    loads = [float(x) for x in loads]
+    order = sorted(((d, m) for d in range(len(loads)) for m in range(nmembers)),
+                   key=lambda u: (-loads[u[0]], u[0], u[1]))
+    acc = [0.0] * world
+    owned = [[[] for _ in loads] for _ in range(world)]
+    for d, m in order:
+        r = min(range(world), key=lambda k: (acc[k], k))
+        acc[r] += loads[d]
+        owned[r][d].append(m)
+    for per in owned:
+        for ms in per:
+            ms.sort()
+    return owned

@@ -6,6 +6,7 @@ regional run must equal the whole-domain run bit for bit."""
 from __future__ import annotations
 
 import datetime
+import math
 import os
 import socket
 
@@ -129,6 +130,67 @@ def test_gloo_member_sharding_covers_every_member_once(tmp_path, nmembers):
                        start_method="spawn")
     for r in (0, 1):
         assert np.all(np.load(os.path.join(str(tmp_path), f"members{r}.npy")) == 1)
+
+
+def _units_worker(rank, world, port, loads, nmembers, out_dir):
+    import torch
+    import torch.distributed as dist
+    import sys
+
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    sys.path[:0] = [os.path.join(root, "cama-flood_v4_b200")]
+    from cmf_b200.regions import pack_units
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    mine = torch.zeros(len(loads), nmembers, dtype=torch.int64)
+    load = torch.zeros(world, dtype=torch.float64)
+    for d, ms in enumerate(pack_units(loads, nmembers, world)[rank]):     # each rank packs on its own
+        for m in ms:
+            mine[d, m] += 1
+            load[rank] += loads[d]
+    dist.all_reduce(mine)
+    dist.all_reduce(load)
+    np.save(os.path.join(out_dir, f"units{rank}.npy"), mine.numpy())
+    np.save(os.path.join(out_dir, f"loads{rank}.npy"), load.numpy())
+    dist.destroy_process_group()
+
+
+def test_gloo_domain_member_packing_covers_every_unit_once(tmp_path):
+    """Members x domains of uneven size over two gloo ranks (the config-2 partition): each rank
+    packs independently, every (domain, member) unit is owned exactly once, and the ranks' loads
+    (cells x expected NT) differ by at most the largest unit."""
+    import torch.multiprocessing as mp
+
+    loads = [49424 * 24, 84124 * 25, 142834 * 25, 241678 * 26, 410196 * 30, 695486 * 30, 1177949 * 33, 1997245 * 45]
+    mp.start_processes(_units_worker, args=(2, _free_port(), loads, 7, str(tmp_path)), nprocs=2, join=True,
+                       start_method="spawn")
+    for r in (0, 1):
+        assert np.all(np.load(os.path.join(str(tmp_path), f"units{r}.npy")) == 1)
+        ld = np.load(os.path.join(str(tmp_path), f"loads{r}.npy"))
+        assert ld.sum() == 7 * sum(loads) and ld.max() - ld.min() <= max(loads)
+
+
+def test_pack_units_and_expected_nt():
+    from cmf_b200.regions import expected_nt, pack_units
+
+    loads = [5.0, 3.0, 3.0, 1.0]
+    for world in (1, 2, 3, 5, 40):
+        owned = pack_units(loads, 6, world)
+        seen = sorted((d, m) for per in owned for d, ms in enumerate(per) for m in ms)
+        assert seen == [(d, m) for d in range(4) for m in range(6)]
+        acc = [sum(len(ms) * loads[d] for d, ms in enumerate(per)) for per in owned]
+        assert max(acc) <= sum(loads) * 6 / world + max(loads)
+        assert all(ms == sorted(ms) for per in owned for ms in per)
+    assert pack_units(loads, 6, 2) == pack_units(list(loads), 6, 2)            # deterministic
+    # CALC_ADPSTP on a half-full channel: the key of the shortest, deepest reach decides NT
+    dst = np.array([12000.0, 3000.0, 8000.0, 50000.0])
+    hgt = np.array([4.0, 9.0, 2.0, 6.0])
+    keys = [(0.7 * d) * math.pow(9.8 * max(h * 0.5, 0.01), -0.5) for d, h in zip(dst[:3], hgt[:3])]
+    keys.append((0.7 * 10000.0) * math.pow(9.8 * 3.0, -0.5))                 # the mouth: PDSTMTH
+    dt_min = min([3600.0] + keys)
+    assert expected_nt(dst, hgt, 3) == int(3600.0 * (1.0 / dt_min) - float(np.float32(0.01))) + 1 == 12
 
 
 @pytest.mark.gpu
