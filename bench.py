@@ -667,8 +667,10 @@ def cfg2_arm(args) -> int:
     cells = 0
     abytes = 0.0
     nts = [0.0] * len(hosts)
+    launches = 0
     for k, p, a, b in zip(used, ctxs, c0, c1):
         h = hosts[k]
+        launches += p.launches_per_step() * K + p.launches_per_substep() * (b["loop_iters"] - a["loop_iters"])
         sub = b["member_substeps"] - a["member_substeps"]
         cells += h.dims.nseqall * sub
         nts[k] = sub / (K * p.M)
@@ -721,7 +723,8 @@ def cfg2_arm(args) -> int:
                      "note": "algorithmic bytes of k_flux+k_rate+k_store per member sub-step (L_bar taken as 0), "
                              "stage/CFL and control kernels not counted; achieved over all GPUs"},
         "clocks": clk.summary(),
-        "gpu_launches": None,
+        "gpu_launches": launches,
+        "gpu_launches_scope": "rank 0",
     }
     print(json.dumps(line))
     if ws > 1:
