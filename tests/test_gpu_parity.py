@@ -499,3 +499,47 @@ def test_output_diagnostics_vs_oracle(case_dirs):
             g.diag_output("reset")
             outputs += 1
     assert outputs == 5
+
+
+# edge sizes: a lone mouth (one cell, no river cell), 33 cells with every option (a partial warp,
+# paths, levees, dams, low banks), and a 37-cell single channel
+EDGE_CASES = {
+    "one": dict(nx=1, ny=1, n_mouths=1, seed=5),
+    "ragged": dict(nx=11, ny=3, n_mouths=2, seed=6, lpthout=True, npthout=4, llevee=True, ldamout=True, ndam=2,
+                   rivhgt_scale=0.3),
+    "row": dict(nx=37, ny=1, n_mouths=1, seed=8),
+}
+
+
+@pytest.mark.parametrize("name", list(EDGE_CASES))
+def test_edge_size_networks_vs_oracle(tmp_path, name):
+    """Networks smaller than a warp or a block, and ragged against both: NT/DT bit-exact every step
+    and every field within 1e-9 over 12 flooded hours (the context tunes its schedule meanwhile)."""
+    from cmf_b200 import synth
+
+    d = synth.write_case(synth.make_case(synth.CaseSpec(name=name, land_frac=1.0, **EDGE_CASES[name])),
+                         str(tmp_path / name))
+    h, g, o = _models(d)
+    for r in runoff_series(o.d("grarea"), "stress", 12, hourly=True):
+        g.put_runoff(r)
+        o.put_runoff(r)
+        nt, dt, _ = g.advance()
+        assert (int(nt[0]), float(dt[0])) == o.advance()
+    _compare_state(g, o, name)
+    g.close()
+
+
+def test_fixed_dt_chain_vs_oracle(tmp_path):
+    """LADPSTP off (one sub-step of DT_DEF) on the 3-cell chain of the oracle's known-answer test."""
+    from test_oracle import _chain_case
+
+    d, _ = _chain_case(tmp_path, 600.0)
+    h, g, o = _models(d)
+    for k in range(6):
+        r = np.array([3.0, 4.0, 0.0]) * (1 + k)
+        g.put_runoff(r)
+        o.put_runoff(r)
+        nt, dt, _ = g.advance()
+        assert (int(nt[0]), float(dt[0])) == o.advance() == (1, 600.0)
+    _compare_state(g, o, "chain")
+    g.close()
