@@ -220,7 +220,9 @@ def phase_bytes(N: int, E: int, L_bar: float, P: int, Lp: int, nlev: int, ndam: 
                RIVSTO FLDSTO RIVDPH FLDDPH FLDFRC STORGE)                   = 188+16 L_bar
                (the last sub-step's own accumulators, once per outer step, are not counted)
                + levee: index 4/cell + 7 params + LEVSTO r/w + LEVDPH w per levee cell
-               + dams: 112 B per dam, paths: FLW r/w 16 x Lp + FLWSUM 16 per path"""
+               + dams: 112 B per dam, paths: FLW r/w 16 x Lp + FLWSUM 16 per path
+    k_store walks the upstream lists through a 4-slot table (16 B per cell, one dependent load
+    fewer); the count keeps the CSR's compulsory bytes, so the fraction it gives is conservative."""
     flux = N * (140 + (128 if ldiag else 0)) + P * (8 + 8 + 4 + 32 * Lp + 8) + ndam * 112
     rate = N * 48 + (E - N) * 4 + P * 2 * (8 + 8)
     store = N * (188 + 16 * L_bar) + N * 4 + nlev * (7 * 8 + 16 + 8) + ndam * 112 + P * (16 * Lp + 16)

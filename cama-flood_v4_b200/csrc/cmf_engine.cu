@@ -215,8 +215,16 @@ int build_net(cmf_gpu_ctx *c, const cmf_map_ptrs *mp) {
         up_ptr[i + 1] = (int)up_idx.size();
     }
     c->E = up_idx.size();
+    constexpr int S = cmf::kUpSlots;
+    std::vector<int> up_ell((size_t)S * N, -1);
+    for (int i = 0; i < N; i++) {
+        const int k0 = up_ptr[i], nu = up_ptr[i + 1] - k0;
+        for (int k = 0; k < std::min(nu, S); k++) up_ell[(size_t)k * N + i] = up_idx[k0 + k];
+        if (nu > S) up_ell[(size_t)(S - 1) * N + i] = -2 - (k0 + S - 1);
+    }
     int rc;
-    if ((rc = c->upload(&n.next, next)) || (rc = c->upload(&n.up_ptr, up_ptr)) || (rc = c->upload(&n.up_idx, up_idx)))
+    if ((rc = c->upload(&n.next, next)) || (rc = c->upload(&n.up_ptr, up_ptr)) || (rc = c->upload(&n.up_idx, up_idx)) ||
+        (rc = c->upload(&n.up_ell, up_ell)))
         return rc;
     std::vector<int> i2mask(mp->i2mask, mp->i2mask + N);
     if ((rc = c->upload(&n.i2mask, i2mask))) return rc;
@@ -380,6 +388,7 @@ int hot_maps_window(cmf_gpu_ctx *c) {
         {(const void **)&n.grarea, N * 8}, {(const void **)&n.rivstomax, N * 8}, {(const void **)&n.inv_nxtdst, N * 8},
         {(const void **)&n.inv_rivwth, N * 8}, {(const void **)&n.inv_rivlen, N * 8},
         {(const void **)&n.next, N * 4}, {(const void **)&n.up_ptr, (N + 1) * 4}, {(const void **)&n.up_idx, c->E * 4},
+        {(const void **)&n.up_ell, N * 4 * cmf::kUpSlots},
         {(const void **)&n.i1dam, N * 4}, {(const void **)&n.dam_id, N * 4}, {(const void **)&n.lev_id, N * 4},
         {(const void **)&n.pout_ptr, (N + 1) * 4}, {(const void **)&n.pinf_ptr, (N + 1) * 4}};
     size_t total = 0;

@@ -44,6 +44,7 @@ constexpr size_t kSmallCellMembers = size_t(1) << 19;   // untuned start: `small
 #define CMF_STAGE_MINB 6
 #endif
 constexpr int kCellThreads = 256;
+constexpr int kUpSlots = 4;        // upstream cells per cell held in Net::up_ell
 
 constexpr int kBudgets = 12;       // stopre stonxt stonew rivinf rivout stopre2 stonew2 rivsto fldsto fldare levsto dammiss
 // dynamic shared memory of k_store: the last sub-step's budget terms, kBudgets per thread
@@ -90,6 +91,11 @@ struct Net {
     const int *__restrict__ next;       // [N] 0-based downstream (river cells)
     const int *__restrict__ up_ptr;     // [N+1] upstream CSR, ascending sequence (I1UPST order)
     const int *__restrict__ up_idx;
+    // [kUpSlots][N] the first upstream cells of each cell in I1UPST order, -1 past the last; with
+    // more than kUpSlots of them the last slot holds -2 - (CSR position of the kUpSlots-th), and the
+    // walk goes on in up_idx.  All slots of a cell are read at once, so the upstream values are
+    // gathered one dependent load after the cell's own reads instead of two (pointer, index, value).
+    const int *__restrict__ up_ell;
     const int *__restrict__ i2mask;     // [N]
     const double *__restrict__ rivelv, *__restrict__ elevtn, *__restrict__ nxtdst, *__restrict__ rivwth;
     const double *__restrict__ rivhgt, *__restrict__ rivlen, *__restrict__ rivman, *__restrict__ grarea;
@@ -161,6 +167,7 @@ struct OwnG {
     __device__ __forceinline__ int next(int i) const { return __ldg(&n.next[i]); }
     __device__ __forceinline__ int up_lo(int i) const { return __ldg(&n.up_ptr[i]); }
     __device__ __forceinline__ int up_hi(int i) const { return __ldg(&n.up_ptr[i + 1]); }
+    __device__ __forceinline__ int up_slot(int k, int i) const { return __ldg(&n.up_ell[(size_t)k * n.N + i]); }
     __device__ __forceinline__ int i1dam(int i) const { return __ldg(&n.i1dam[i]); }
     CMF_OWN_STATE(rivsto) CMF_OWN_STATE(fldsto) CMF_OWN_STATE(levsto) CMF_OWN_STATE(rivdph)
     CMF_OWN_STATE(rivdph_pre) CMF_OWN_STATE(rivout_pre) CMF_OWN_STATE(fldout_pre) CMF_OWN_STATE(fldsto_pre)
@@ -171,6 +178,26 @@ struct OwnG {
 };
 #undef CMF_OWN_STATIC
 #undef CMF_OWN_STATE
+
+// f(j) for every upstream cell j of cell i, in I1UPST order (the order of every upstream sum)
+template <class Own, class F>
+__device__ __forceinline__ void for_each_upstream(const Net &n, const Own &w, int i, F f) {
+    int slot[kUpSlots];
+#pragma unroll
+    for (int k = 0; k < kUpSlots; k++) slot[k] = w.up_slot(k, i);
+#pragma unroll
+    for (int k = 0; k < kUpSlots - 1; k++) {
+        if (slot[k] < 0) return;
+        f(slot[k]);
+    }
+    const int last = slot[kUpSlots - 1];
+    if (last >= 0) {
+        f(last);
+    } else if (last < -1) {                       // more than kUpSlots upstream cells
+        const int k1 = __ldg(&n.up_ptr[i + 1]);
+        for (int k = -2 - last; k < k1; k++) f(__ldg(&n.up_idx[k]));
+    }
+}
 
 
 // x**(-7._JPRB/3._JPRB) and x**(-4._JPRB/3._JPRB) of the local-inertial flux formulas
@@ -920,6 +947,7 @@ template <class Own>
 __device__ __forceinline__ void cell_rate(const Net &n, const State &s, const Own &w, int m, int i, double DT) {
     const size_t base = (size_t)m * n.N, gi = base + i;
     double so = dmax(w.rivout_raw(gi), 0.0) + dmax(w.fldout_raw(gi), 0.0);
+    // the CSR walk: at full occupancy the slot table's 16 B per cell cost more than its saved round
     const int u1 = w.up_hi(i);
     for (int k = w.up_lo(i); k < u1; k++) {
         const int j = __ldg(&n.up_idx[k]);
@@ -1018,14 +1046,12 @@ __device__ __forceinline__ void cell_store(const Net &n, const State &s, const O
     }
     // inflow from the upstream cells, rescaled on the fly (:481-489); next(j) == i
     double rinf = 0.0, finf = 0.0;
-    const int u1 = w.up_hi(i);
-    for (int k = w.up_lo(i); k < u1; k++) {
-        const int j = __ldg(&n.up_idx[k]);
+    for_each_upstream(n, w, i, [&](int j) {
         const double rj = s.rivout_raw[base + j], fj = s.fldout_raw[base + j];
         const double r = (rj > 0.0) ? rate_m[j] : rate_i;
         rinf = rinf + rj * r;
         finf = finf + fj * r;
-    }
+    });
     double pout = 0.0;
     bool has_path = false;
     if (n.lpthout) {
