@@ -373,12 +373,19 @@ int build_net(cmf_gpu_ctx *c, const cmf_map_ptrs *mp) {
 // them.  Only when the whole allocation fits one window (config 1: 36 MB).  The persisting
 // carve-out is a process-wide limit of the CUDA context: raised to the largest window any live
 // library context needs, and put back when the last of them is destroyed.  Same bits: the kernels
-// read identical copies.
+// read identical copies.  One context at a time holds a window: several windows (the domains of a
+// batch) would each claim the carve-out, thrash one another inside it and leave the rest of the
+// L2 too small for the neighbour gathers of the member state; a context created while another
+// holds the window keeps its maps where they are, as a domain too large for one window does.
 std::mutex g_l2_mu;
 int g_l2_users = 0;
 size_t g_l2_saved = 0, g_l2_limit = 0;
 
 int hot_maps_window(cmf_gpu_ctx *c) {
+    {
+        std::lock_guard<std::mutex> lk(g_l2_mu);
+        if (g_l2_users > 0) return CMF_OK;
+    }
     cmf::Net &n = c->net;
     const size_t N = (size_t)c->dims.nseqall;
     struct Item { const void **field; size_t bytes; };
