@@ -514,7 +514,8 @@ def gpu_arm(args) -> int:
 
 def roofline(g, N, E, Lbar, P, Lp, nlev, ndam, M, loop_iters, K, secs) -> dict:
     """Dominant kernel's achieved bandwidth on algorithmic bytes (live CUDA-event timing on the
-    library's stream) and the whole step's, on the survey's fused-minimum bytes."""
+    library's stream) and the whole step's, on the fused minimum per cell-sub-step (316 + 16 L_bar
+    B, plus 32 + 40 Lp per path, 80 per levee cell and 112 per dam)."""
     phases = g.time_phases(reps=10)
     pb = phase_bytes(N, E, Lbar, P, Lp, nlev, ndam, True)
     per_sub_ms = {k: phases[k] for k in ("k_flux", "k_rate", "k_store")}
