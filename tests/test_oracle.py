@@ -1008,3 +1008,28 @@ def test_output_interval_diagnostics_known_answer(case_dirs):
             nadd = 0.0
     assert o.nadd_out() == 3 * 3600.0
     assert np.array_equal(o.d("outflw_oavg"), sums["outflw"])     # not yet averaged
+
+
+@pytest.mark.parametrize("shape", [dict(nx=1, ny=1, n_mouths=1, seed=5),
+                                   dict(nx=11, ny=3, n_mouths=2, seed=6, lpthout=True, npthout=4, llevee=True,
+                                        ldamout=True, ndam=2, rivhgt_scale=0.3),
+                                   dict(nx=37, ny=1, n_mouths=1, seed=8)])
+def test_budget_identity_on_edge_shapes(tmp_path, shape):
+    """CALC_WATBAL's flux and stage budgets (src/cmf_ctrl_physics_mod.F90:216-248) close at round-off
+    on the edge-size networks the GPU parity tests use (a lone mouth, a partial warp with every
+    option, a single channel) under flooding runoff, and no storage goes negative."""
+    from cmf_b200 import synth
+    from oracle import Oracle
+
+    d = synth.write_case(synth.make_case(synth.CaseSpec(name="edge", land_frac=1.0, **shape)), str(tmp_path / "edge"))
+    o = Oracle(d)
+    for r in runoff_series(o.d("grarea"), "stress", 12, hourly=True):
+        o.put_runoff(r)
+        o.advance()
+        b = o.budget()
+        scale = max(abs(b["stonxt"]), 1.0)
+        assert abs(-(b["stopre"] - b["stonxt"] + b["rivinf"] - b["rivout"])) <= 1e-12 * scale
+        assert abs(-(b["stopre2"] - b["stonew2"])) <= 1e-12 * scale
+        assert abs(b["dam_miss"]) <= 1e-12 * scale
+        assert np.all(o.d("rivsto") >= 0.0) and np.all(o.d("fldsto") >= 0.0)
+    assert o.d("fldsto").max() > 0.0                     # the runoff floods the floodplain
